@@ -1,0 +1,202 @@
+"""Python host interface of the join operators, mirroring the reference's
+operator API for this path:
+
+* ``Context.amhj(query_type, relations, ooc, ws, dro, fib)`` is
+  ``exec-AMHJ <NORMAL|TRI|FOUR> <path> <ooc> <ws> <dro> <fib>``
+  (MHJ-GPU/exec_AMHJ.cu:218-246) / ``OOC<..>::execute`` (MHJ-GPU/ooc.cuh:77-82);
+* ``Context.lftj(relations, algo, ooc, ws)`` is
+  ``exec-LFTJ <path> <0=BFS|1=DFS> <ooc> <ws>`` (LFTJ-GPU/exec_LFTJ.cu:261-268) /
+  ``OOCWrapper::execute_with_{BFS,DFS}`` (LFTJ-GPU/ooc_wrapper.cuh:404-427).
+
+Every call goes through libamj.so; nothing here computes a join.  Errors
+raise ``AmjError`` carrying the C status instead of exiting the process as
+the reference does (common-utils/cuda/cuda_base.cuh:43-57).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+_QUERY = {"NORMAL": L.AMJ_QUERY_NORMAL, "TRI": L.AMJ_QUERY_TRI, "FOUR": L.AMJ_QUERY_FOUR}
+_ALGO = {"BFS": L.AMJ_LFTJ_BFS, "DFS": L.AMJ_LFTJ_DFS, 0: L.AMJ_LFTJ_BFS, 1: L.AMJ_LFTJ_DFS}
+_LAYOUT = {"bucket": L.AMJ_LAYOUT_BUCKET, "oa": L.AMJ_LAYOUT_OPEN_ADDR, "open_addr": L.AMJ_LAYOUT_OPEN_ADDR,
+           "cuckoo": L.AMJ_LAYOUT_CUCKOO}
+STAT_NAMES = ["tasks_pushed", "tasks_popped", "residual_units", "rows_written_main", "rows_written_residual",
+              "estimate", "fallbacks", "slices"]
+
+
+@dataclass
+class Result:
+    count: int
+    checksum: int
+    num_attrs: int
+    build_ms: float
+    probe_ms: float
+    total_ms: float
+    stats: dict
+    columns: Optional[list] = None  # k numpy int32 arrays (attribute order) when materialised
+
+    def tuples(self) -> np.ndarray:
+        """Materialised tuples as an (rows, k) array."""
+        if self.columns is None:
+            raise ValueError("result was not materialised")
+        return np.stack(self.columns, axis=1) if self.columns else np.zeros((0, 0), np.int32)
+
+
+class Relation:
+    """A relation registered with a context.
+
+    ``cols`` are int32 columns: numpy arrays (copied to the device, or kept on
+    the host for out-of-core probing with ``streamed=True``) or CUDA tensors
+    (borrowed, must stay alive; the Relation keeps a reference)."""
+
+    def __init__(self, ctx: "Context", cols: Sequence, attrs: Sequence[int], streamed: bool = False):
+        lib = L.load()
+        self.ctx = ctx
+        self._keep = []
+        ncols = len(cols)
+        if ncols == 0 or ncols != len(attrs):
+            raise ValueError("need one attribute per column")
+        ptrs = (C.POINTER(C.c_int32) * ncols)()
+        n = None
+        where = L.AMJ_MEM_HOST
+        for i, col in enumerate(cols):
+            if hasattr(col, "data_ptr") and hasattr(col, "is_cuda") and col.is_cuda:
+                import torch
+                if col.dtype != torch.int32 or not col.is_contiguous():
+                    raise ValueError("device columns must be contiguous torch.int32")
+                ptrs[i] = C.cast(C.c_void_p(col.data_ptr()), C.POINTER(C.c_int32))
+                where = L.AMJ_MEM_DEVICE
+                length = col.numel()
+            else:
+                arr = np.ascontiguousarray(np.asarray(col), dtype=np.int32)
+                ptrs[i] = arr.ctypes.data_as(C.POINTER(C.c_int32))
+                length = arr.shape[0]
+                col = arr
+                if streamed:
+                    where = L.AMJ_MEM_HOST_STREAMED
+            self._keep.append(col)
+            if n is None:
+                n = length
+            elif n != length:
+                raise ValueError("columns differ in length")
+        attr_arr = (C.c_uint32 * ncols)(*[int(a) for a in attrs])
+        handle = C.c_void_p()
+        L.check(lib.amj_rel_create(ctx.handle, n, ncols, attr_arr, ptrs, where, C.byref(handle)), "rel_create")
+        if where == L.AMJ_MEM_HOST:
+            self._keep = []  # copied to the device
+        self.handle = handle
+        self.n = int(n)
+        self.attrs = [int(a) for a in attrs]
+        self.where = where
+
+    def release(self):
+        if getattr(self, "handle", None):
+            L.load().amj_rel_release(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class Context:
+    """One CUDA device and stream (amj_ctx)."""
+
+    def __init__(self, device: int = 0, layout: str = "bucket", load_factor: float = 0.5, task_chunk: int = 1024,
+                 spin_limit_ms: int = 5000, task_capacity: int = 1 << 20, ooc_slice_rows: int = 0,
+                 mem_budget: int = 0):
+        lib = L.load()
+        o = L.amj_opts()
+        o.block_size = 256
+        o.layout = _LAYOUT[layout]
+        o.load_factor = load_factor
+        o.task_chunk = task_chunk
+        o.spin_limit_ms = spin_limit_ms
+        o.task_capacity = task_capacity
+        o.ooc_slice_rows = ooc_slice_rows
+        o.mem_budget = mem_budget
+        h = C.c_void_p()
+        L.check(lib.amj_ctx_create(device, C.byref(o), C.byref(h)), "ctx_create")
+        self.handle = h
+
+    def relation(self, cols, attrs, streamed: bool = False) -> Relation:
+        return Relation(self, cols, attrs, streamed=streamed)
+
+    def _result(self, res: L.amj_result, materialize: bool) -> Result:
+        cols = None
+        if materialize:
+            k = res.num_attrs
+            rows = int(res.rows)
+            cols = []
+            for a in range(k):
+                if rows:
+                    cols.append(np.ctypeslib.as_array(res.cols[a], shape=(rows,)).copy())
+                else:
+                    cols.append(np.zeros(0, np.int32))
+        out = Result(count=int(res.count), checksum=int(res.checksum), num_attrs=int(res.num_attrs),
+                     build_ms=float(res.build_ms), probe_ms=float(res.probe_ms), total_ms=float(res.total_ms),
+                     stats={STAT_NAMES[i]: int(res.stats[i]) for i in range(8)}, columns=cols)
+        L.load().amj_result_release(C.byref(res))
+        return out
+
+    def amhj(self, query_type, relations: Sequence[Relation], ooc: int = 0, ws: int = 0, dro: int = 0,
+             fib: int = 0, materialize: bool = False, reorder: bool = True) -> Result:
+        lib = L.load()
+        qt = _QUERY[query_type] if isinstance(query_type, str) else int(query_type)
+        arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
+        flags = (L.AMJ_F_MATERIALIZE | L.AMJ_F_HOST_RESULT) if materialize else 0
+        if not reorder:
+            flags |= L.AMJ_F_NO_REORDER
+        res = L.amj_result()
+        L.check(lib.amj_amhj_execute(self.handle, qt, arr, len(relations), int(ooc), int(ws), int(dro), int(fib),
+                                     flags, C.byref(res)), "amhj_execute")
+        return self._result(res, materialize)
+
+    def lftj(self, relations: Sequence[Relation], algo="DFS", ooc: int = 0, ws: int = 1,
+             materialize: bool = False) -> Result:
+        lib = L.load()
+        arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
+        flags = (L.AMJ_F_MATERIALIZE | L.AMJ_F_HOST_RESULT) if materialize else 0
+        res = L.amj_result()
+        L.check(lib.amj_lftj_execute(self.handle, arr, len(relations), _ALGO[algo], int(ooc), int(ws), flags,
+                                     C.byref(res)), "lftj_execute")
+        return self._result(res, materialize)
+
+    def sync(self):
+        L.check(L.load().amj_ctx_sync(self.handle), "ctx_sync")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().amj_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cuda_device_available() -> bool:
+    """True when libamj can create a context on device 0."""
+    lib = L.load()
+    h = C.c_void_p()
+    st = lib.amj_ctx_create(0, None, C.byref(h))
+    if st == L.AMJ_OK:
+        lib.amj_ctx_destroy(h)
+        return True
+    return False

@@ -1,0 +1,657 @@
+// AMHJ operator host side: query compilation, index builds, and the count /
+// write / direct-output / work-sharing / out-of-core passes.
+//
+// Reference entry: test_general + OOC::execute (MHJ-GPU/exec_AMHJ.cu:10-213,
+// MHJ-GPU/ooc.cuh:77-307) dispatching AMHJ / AMHJ_WS / AMHJ_DRO / AMHJ_WS_DRO /
+// AMHJ_FIB (exec_AMHJ.cu:163-198).
+//
+// Query compilation follows exec_AMHJ.cu:70-89 (NORMAL) and the hard-coded
+// TRI / FOUR attribute patterns (exec_AMHJ.cu:32-69, 126-138): an attribute
+// already bound by an earlier relation is compared, a new one is bound.  All
+// bound attributes are compared (the reference's single_join_key=false
+// semantics, common_kernels.cuh:41-53).  Two choices differ from the
+// reference and leave the result bag unchanged:
+//  - a build relation whose columns are all bound (a pure filter, e.g. C(0,2)
+//    of the triangle) is indexed on the pair of its columns, so its lookup is
+//    one bucket instead of a scan of every row sharing the first value;
+//  - such filters move to the earliest level at which their attributes are
+//    bound (AMJ_F_NO_REORDER keeps the query order).
+#include "amhj_kernel.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+
+namespace amj {
+
+struct LevelSpec {
+    const amj_rel *rel;
+    int ncols;
+    int src_col[4];    // relation column feeding index column c (index column 0 is the key)
+    int attr[4];       // attribute of index column c
+    int key_mode;
+    uint8_t cmp_mask, bind_mask;
+};
+
+struct HostPlan {
+    const amj_rel *probe = nullptr;
+    int probe_attr[AMJ_MAX_COLS] = {};
+    int L = 0, k = 0;
+    LevelSpec lv[AMJ_MAX_BUILD_TABLES];
+    int last_src[AMJ_MAX_ATTRS] = {};
+};
+
+struct RelAttrs {
+    const amj_rel *rel;
+    int ncols;
+    int attr[AMJ_MAX_COLS];
+};
+
+static int compile_plan(int query_type, amj_rel *const *rels, int nrels, int flags, HostPlan *hp) {
+    std::vector<RelAttrs> tabs;
+    if (query_type == AMJ_QUERY_NORMAL) {
+        if (nrels < 1) return fail(AMJ_EINVAL, "AMHJ: no relations");
+        if (nrels - 1 > AMJ_MAX_BUILD_TABLES) return fail(AMJ_EUNSUPPORTED, "AMHJ: more than 6 build relations");
+        for (int i = 0; i < nrels; i++) {
+            RelAttrs t{rels[i], rels[i]->ncols, {}};
+            for (int c = 0; c < t.ncols; c++) t.attr[c] = (int)rels[i]->attrs[c];
+            tabs.push_back(t);
+        }
+    } else if (query_type == AMJ_QUERY_TRI || query_type == AMJ_QUERY_FOUR) {
+        if (nrels != 1 || rels[0]->ncols != 2)
+            return fail(AMJ_EINVAL, "AMHJ TRI/FOUR: expected one 2-column edge relation");
+        // A(0,1),B(1,2),C(0,2)  /  A(0,1),B(1,2),C(2,3),D(0,3),E(0,2),F(1,3)
+        static const int tri[3][2] = {{0, 1}, {1, 2}, {0, 2}};
+        static const int four[6][2] = {{0, 1}, {1, 2}, {2, 3}, {0, 3}, {0, 2}, {1, 3}};
+        const int nt = query_type == AMJ_QUERY_TRI ? 3 : 6;
+        for (int i = 0; i < nt; i++) {
+            RelAttrs t{rels[0], 2, {}};
+            t.attr[0] = query_type == AMJ_QUERY_TRI ? tri[i][0] : four[i][0];
+            t.attr[1] = query_type == AMJ_QUERY_TRI ? tri[i][1] : four[i][1];
+            tabs.push_back(t);
+        }
+    } else {
+        return fail(AMJ_EINVAL, "AMHJ: unknown query type");
+    }
+    // attributes must be exactly 0..k-1
+    uint32_t seen = 0;
+    for (auto &t : tabs)
+        for (int c = 0; c < t.ncols; c++) seen |= 1u << t.attr[c];
+    int k = 0;
+    while (k < 32 && ((seen >> k) & 1)) k++;
+    if (seen != ((1u << k) - 1) || k > AMJ_MAX_ATTRS)
+        return fail(AMJ_EINVAL, "AMHJ: the relations' attributes must be exactly 0..k-1 with k <= 8");
+    hp->k = k;
+    hp->probe = tabs[0].rel;
+    for (int c = 0; c < tabs[0].ncols; c++) hp->probe_attr[c] = tabs[0].attr[c];
+    uint32_t bound = 0;
+    for (int c = 0; c < tabs[0].ncols; c++) bound |= 1u << tabs[0].attr[c];
+    std::vector<RelAttrs> rem(tabs.begin() + 1, tabs.end());
+    int L = 0;
+    while (!rem.empty()) {
+        size_t pick = 0;
+        if (!(flags & AMJ_F_NO_REORDER)) {
+            for (size_t i = 0; i < rem.size(); i++) {
+                bool all = true;
+                for (int c = 0; c < rem[i].ncols; c++) all &= ((bound >> rem[i].attr[c]) & 1) != 0;
+                if (all) {
+                    pick = i;
+                    break;
+                }
+            }
+        }
+        RelAttrs t = rem[pick];
+        rem.erase(rem.begin() + pick);
+        if (t.ncols > 4) return fail(AMJ_EUNSUPPORTED, "AMHJ: build relations have at most 4 columns");
+        int kc = -1;   // key column: the first column whose attribute is bound
+        for (int c = 0; c < t.ncols && kc < 0; c++)
+            if ((bound >> t.attr[c]) & 1) kc = c;
+        if (kc < 0) return fail(AMJ_EUNSUPPORTED, "AMHJ: a build relation shares no attribute with the relations before it");
+        LevelSpec &ls = hp->lv[L];
+        ls.rel = t.rel;
+        ls.ncols = t.ncols;
+        int w = 0;
+        ls.src_col[w] = kc;
+        ls.attr[w++] = t.attr[kc];
+        for (int c = 0; c < t.ncols; c++)
+            if (c != kc) {
+                ls.src_col[w] = c;
+                ls.attr[w++] = t.attr[c];
+            }
+        ls.cmp_mask = ls.bind_mask = 0;
+        for (int c = 0; c < t.ncols; c++) {
+            if ((bound >> ls.attr[c]) & 1) ls.cmp_mask |= 1u << c;
+            else ls.bind_mask |= 1u << c;
+        }
+        ls.key_mode = (t.ncols == 2 && ls.cmp_mask == 3u) ? KEY_PAIR : KEY_SINGLE;
+        for (int c = 0; c < t.ncols; c++) bound |= 1u << ls.attr[c];
+        L++;
+    }
+    hp->L = L;
+    for (int a = 0; a < AMJ_MAX_ATTRS; a++) hp->last_src[a] = -1;
+    if (L > 0) {
+        const LevelSpec &last = hp->lv[L - 1];
+        for (int c = 0; c < last.ncols; c++)
+            if ((last.bind_mask >> c) & 1) hp->last_src[last.attr[c]] = c;
+    }
+    return AMJ_OK;
+}
+
+struct IndexKey {
+    const amj_rel *rel;
+    int src[4];
+    int ncols, key_mode, layout;
+    bool operator<(const IndexKey &o) const {
+        return std::tie(rel, src[0], src[1], src[2], src[3], ncols, key_mode, layout) <
+               std::tie(o.rel, o.src[0], o.src[1], o.src[2], o.src[3], o.ncols, o.key_mode, o.layout);
+    }
+};
+
+struct ExecScratch {
+    std::map<IndexKey, HashIndex> indexes;
+    DBuf<ProbeState> st;
+    DBuf<Task> tasks;
+    DBuf<unsigned int> ready;
+    DBuf<Breakpoint> units;
+};
+
+double event_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0.0;
+    }
+    return (double)ms;
+}
+
+template <int MODE, bool WS>
+static int launch_probe_t(amj_ctx *ctx, const ProbeLaunch &PL, size_t smem) {
+    auto kern = amhj_probe_kernel<MODE, WS>;
+    AMJ_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PROBE_THREADS, smem));
+    if (per_sm < 1) return fail(AMJ_EUNSUPPORTED, "AMHJ: probe frontier does not fit in shared memory");
+    uint64_t grid = (uint64_t)ctx->num_sms * per_sm;
+    const uint64_t need = (PL.batch_count + PROBE_WARPS - 1) / PROBE_WARPS;
+    if (!WS && MODE != PM_RESIDUAL && need < grid) grid = need ? need : 1;
+    if (MODE == PM_RESIDUAL) {
+        const uint64_t rneed = (PL.batch_count + PROBE_WARPS - 1) / PROBE_WARPS;
+        if (rneed < grid) grid = rneed ? rneed : 1;
+    }
+    if (WS) {
+        // every warp starts counted as busy
+        const unsigned int warps = (unsigned int)(grid * PROBE_WARPS);
+        AMJ_CUDA_TRY(cudaMemcpyAsync(&PL.st->busy, &warps, sizeof(warps), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    kern<<<(unsigned)grid, PROBE_THREADS, smem, ctx->stream>>>(PL);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    return AMJ_OK;
+}
+
+static int launch_probe(amj_ctx *ctx, const ProbeLaunch &PL, int mode, bool ws) {
+    const size_t smem = (size_t)PROBE_WARPS * PL.P.warp_bytes;
+    if (mode == PM_COUNT) return ws ? launch_probe_t<PM_COUNT, true>(ctx, PL, smem) : launch_probe_t<PM_COUNT, false>(ctx, PL, smem);
+    if (mode == PM_WRITE) return ws ? launch_probe_t<PM_WRITE, true>(ctx, PL, smem) : launch_probe_t<PM_WRITE, false>(ctx, PL, smem);
+    return ws ? launch_probe_t<PM_RESIDUAL, true>(ctx, PL, smem) : launch_probe_t<PM_RESIDUAL, false>(ctx, PL, smem);
+}
+
+static int reset_state(amj_ctx *ctx, ProbeState *st, unsigned int *ready, uint32_t task_cap) {
+    AMJ_CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(ProbeState), ctx->stream));
+    if (ready) AMJ_CUDA_TRY(cudaMemsetAsync(ready, 0, (size_t)task_cap * sizeof(unsigned int), ctx->stream));
+    return AMJ_OK;
+}
+
+static int read_state(amj_ctx *ctx, const ProbeState *d, ProbeState *h, const char *what) {
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(ProbeState), cudaMemcpyDeviceToHost, ctx->stream));
+    return status_check(ctx, what);
+}
+
+static int alloc_cols(amj_ctx *ctx, int k, uint64_t rows, int32_t **cols) {
+    for (int a = 0; a < k; a++) {
+        int rc = dev_alloc(ctx, (void **)&cols[a], (rows ? rows : 1) * sizeof(int32_t));
+        if (rc != AMJ_OK) {
+            for (int b = 0; b < a; b++) dev_free(ctx, cols[b]);
+            return rc;
+        }
+    }
+    return AMJ_OK;
+}
+
+int finish_result_columns(amj_ctx *ctx, amj_result *res, int flags) {
+    if (!(flags & AMJ_F_HOST_RESULT) || res->on_host) return AMJ_OK;
+    int32_t *host[AMJ_MAX_ATTRS] = {};
+    for (int a = 0; a < res->num_attrs; a++) {
+        if (!res->cols[a]) continue;
+        if (cudaMallocHost((void **)&host[a], (res->rows ? res->rows : 1) * sizeof(int32_t)) != cudaSuccess) {
+            (void)cudaGetLastError();
+            for (int b = 0; b < a; b++) cudaFreeHost(host[b]);
+            return fail(AMJ_ENOMEM, "result: pinned host allocation failed");
+        }
+        if (res->rows)
+            AMJ_CUDA_TRY(cudaMemcpyAsync(host[a], res->cols[a], res->rows * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+    }
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int a = 0; a < res->num_attrs; a++) {
+        if (!res->cols[a]) continue;
+        dev_free(ctx, res->cols[a]);
+        res->cols[a] = host[a];
+    }
+    res->on_host = 1;
+    return AMJ_OK;
+}
+
+// Everything of one execute call except the index builds: the passes over
+// probe rows [row_lo, row_hi).  Accumulates into *res (count, checksum,
+// stats); with materialise, appends rows to `out` (device columns with
+// `out_cap` rows from `out_base`) and reports rows written.
+struct PassResult {
+    uint64_t count = 0, checksum = 0, rows = 0;
+    int32_t *cols[AMJ_MAX_ATTRS] = {};
+};
+
+static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bool dro, bool materialize,
+                      uint64_t row_lo, uint64_t row_hi, PassResult *pr, amj_result *res) {
+    ProbePlan &P = PL.P;
+    P.row_lo = row_lo;
+    P.row_hi = row_hi;
+    const uint64_t rows = row_hi - row_lo;
+    const uint64_t nbatches = (rows + 31) / 32;
+    const uint32_t task_cap = ws ? P.task_cap : 0u;
+    ProbeState h{};
+    PL.batch_stride = 1;
+    PL.batch_count = nbatches;
+    const int k = P.k;
+
+    if (!materialize) {
+        P.dro = 0;
+        AMJ_TRY(reset_state(ctx, PL.st, ws ? PL.task_ready : nullptr, task_cap));
+        AMJ_TRY(launch_probe(ctx, PL, PM_COUNT, ws));
+        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ count"));
+        pr->count = h.count;
+        pr->checksum = h.checksum;
+        res->stats[0] += h.tasks_pushed;
+        res->stats[1] += h.tasks_popped;
+        return AMJ_OK;
+    }
+    if (!dro) {
+        // two passes: count, exact allocation, write (reference AMHJ_evaluate, AMHJ.cuh:314-377)
+        P.dro = 0;
+        AMJ_TRY(reset_state(ctx, PL.st, ws ? PL.task_ready : nullptr, task_cap));
+        AMJ_TRY(launch_probe(ctx, PL, PM_COUNT, ws));
+        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ count"));
+        const uint64_t total = h.count;
+        res->stats[0] += h.tasks_pushed;
+        res->stats[1] += h.tasks_popped;
+        AMJ_TRY(alloc_cols(ctx, k, total, pr->cols));
+        for (int a = 0; a < k; a++) P.out[a] = pr->cols[a];
+        P.out_cap = total;
+        AMJ_TRY(reset_state(ctx, PL.st, ws ? PL.task_ready : nullptr, task_cap));
+        AMJ_TRY(launch_probe(ctx, PL, PM_WRITE, ws));
+        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ write"));
+        if (h.count != total || h.out_cursor != total)
+            return fail(AMJ_ECUDA, "AMHJ: write pass disagrees with count pass");
+        pr->count = total;
+        pr->checksum = h.checksum;
+        pr->rows = total;
+        res->stats[3] += total;
+        return AMJ_OK;
+    }
+    // ---- direct result output (reference AMHJ_DRO, MHJ-GPU/Joins/AMHJ_DRO.cuh:506-707)
+    // 1. estimate |OUT| by counting a strided sample of probe batches
+    uint64_t estimate = 0;
+    {
+        const uint64_t want = 4096;   // batches sampled
+        const uint64_t stride = nbatches > want ? nbatches / want : 1;
+        P.dro = 0;
+        AMJ_TRY(reset_state(ctx, PL.st, nullptr, 0));
+        PL.batch_stride = stride;
+        PL.batch_count = (nbatches + stride - 1) / stride;
+        AMJ_TRY(launch_probe(ctx, PL, PM_COUNT, false));
+        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ DRO sampling"));
+        const double sampled_rows = std::min<double>((double)PL.batch_count * 32.0, (double)rows);
+        const double est = sampled_rows > 0 ? (double)h.count * (double)rows / sampled_rows : 0.0;
+        estimate = (uint64_t)(est * 1.05) + 1024;
+        PL.batch_stride = 1;
+        PL.batch_count = nbatches;
+    }
+    res->stats[5] += estimate;
+    // 2. one write pass into the estimated buffer, recording breakpoints
+    int32_t *main_cols[AMJ_MAX_ATTRS] = {};
+    AMJ_TRY(alloc_cols(ctx, k, estimate, main_cols));
+    for (int a = 0; a < k; a++) P.out[a] = main_cols[a];
+    P.out_cap = estimate;
+    P.dro = 1;
+    const uint64_t unit_cap = nbatches + task_cap + 64;
+    if (X.units.n < unit_cap) AMJ_TRY(X.units.alloc(ctx, unit_cap));
+    PL.units = X.units.p;
+    P.unit_cap = (uint32_t)std::min<uint64_t>(unit_cap, 0xffffffffull);
+    AMJ_TRY(reset_state(ctx, PL.st, ws ? PL.task_ready : nullptr, task_cap));
+    int rc = launch_probe(ctx, PL, PM_WRITE, ws);
+    if (rc == AMJ_OK) rc = read_state(ctx, PL.st, &h, "AMHJ DRO main write");
+    if (rc != AMJ_OK) {
+        for (int a = 0; a < k; a++) dev_free(ctx, main_cols[a]);
+        return rc;
+    }
+    const uint64_t total = h.count;
+    const uint64_t written = std::min<uint64_t>(total, estimate);
+    res->stats[0] += h.tasks_pushed;
+    res->stats[1] += h.tasks_popped;
+    res->stats[3] += written;
+    pr->count = total;
+    pr->checksum = h.checksum;
+    pr->rows = total;
+    if (total <= estimate) {
+        for (int a = 0; a < k; a++) pr->cols[a] = main_cols[a];
+        return AMJ_OK;
+    }
+    // 3. residual: resume the overflowed units after the rows they wrote
+    const uint32_t n_units = h.n_units;
+    res->stats[2] += n_units;
+    rc = alloc_cols(ctx, k, total, pr->cols);
+    if (rc != AMJ_OK) {
+        for (int a = 0; a < k; a++) dev_free(ctx, main_cols[a]);
+        return rc;
+    }
+    for (int a = 0; a < k; a++) {
+        if (written)
+            AMJ_CUDA_TRY(cudaMemcpyAsync(pr->cols[a], main_cols[a], written * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+        dev_free(ctx, main_cols[a]);
+        P.out[a] = pr->cols[a] + written;
+    }
+    P.out_cap = total - written;
+    P.dro = 0;
+    // keep the task queue contents: the residual replays tasks by slot
+    AMJ_CUDA_TRY(cudaMemsetAsync(PL.st, 0, sizeof(ProbeState), ctx->stream));
+    PL.batch_count = n_units;
+    AMJ_TRY(launch_probe(ctx, PL, PM_RESIDUAL, ws));
+    AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ DRO residual write"));
+    if (h.out_cursor != total - written)
+        return fail(AMJ_ECUDA, "AMHJ DRO: residual pass wrote " + std::to_string(h.out_cursor) + " rows, expected " +
+                                   std::to_string(total - written));
+    res->stats[4] += h.out_cursor;
+    return AMJ_OK;
+}
+
+static int fill_level(const LevelSpec &ls, const HashIndex &ix, LevelDesc *d) {
+    std::memset(d, 0, sizeof(*d));
+    d->buc_ptrs = ix.buc_ptrs.p;
+    for (int c = 0; c < 4; c++) d->col[c] = ix.cols[c].p;
+    d->slots = ix.slots.p;
+    d->mask = ix.mask;
+    d->layout = (int8_t)ix.layout;
+    d->key_mode = (int8_t)ix.key_mode;
+    d->ncols = (int8_t)ls.ncols;
+    d->key_attr[0] = (int8_t)ls.attr[0];
+    d->key_attr[1] = (int8_t)(ls.ncols > 1 ? ls.attr[1] : 0);
+    d->cmp_mask = ls.cmp_mask;
+    d->bind_mask = ls.bind_mask;
+    for (int c = 0; c < 4; c++) d->attr[c] = (int8_t)(c < ls.ncols ? ls.attr[c] : 0);
+    return AMJ_OK;
+}
+
+// ---- out-of-core (reference OOC::execute ooc=1, MHJ-GPU/ooc.cuh:166-306) ----
+// The probe relation is processed in slices.  When it lives in host memory
+// (AMJ_MEM_HOST_STREAMED) each slice is copied into one of two device staging
+// buffers on a side stream while the previous slice is joined, and the
+// materialised rows of every slice go back to host memory, so neither the
+// input nor the output has to fit on the device.  Build relations stay
+// resident, as in the reference.
+int amhj_ooc_execute(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch *X, const amj_rel *probe, bool ws, bool dro,
+                     bool materialize, int flags, amj_result *out) {
+    (void)flags;
+    const int nc = probe->ncols;
+    const uint64_t n = probe->n;
+    const bool host = probe->where == AMJ_MEM_HOST_STREAMED;
+    uint64_t slice = ctx->opts.ooc_slice_rows;
+    if (!slice) {
+        size_t fr = 0, tot = 0;
+        AMJ_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+        const uint64_t budget = ctx->opts.mem_budget ? ctx->opts.mem_budget : fr / 2;
+        slice = budget / 8 / ((uint64_t)nc * 4);
+    }
+    slice = std::max<uint64_t>(1024, (slice + 31) / 32 * 32);
+    const uint64_t nslices = n ? (n + slice - 1) / slice : 0;
+    const int k = PL.P.k;
+
+    DBuf<int32_t> stage[2][AMJ_MAX_COLS];
+    cudaEvent_t ready[2] = {nullptr, nullptr};
+    bool registered[AMJ_MAX_COLS] = {};
+    auto cleanup = [&]() {
+        for (int b = 0; b < 2; b++)
+            if (ready[b]) cudaEventDestroy(ready[b]);
+        for (int c = 0; c < nc; c++)
+            if (registered[c]) cudaHostUnregister((void *)probe->h_cols[c]);
+        (void)cudaGetLastError();
+    };
+    if (host) {
+        for (int b = 0; b < 2; b++) {
+            for (int c = 0; c < nc; c++) {
+                int rc = stage[b][c].alloc(ctx, std::min<uint64_t>(slice, n ? n : 1));
+                if (rc != AMJ_OK) { cleanup(); return rc; }
+            }
+            if (cudaEventCreateWithFlags(&ready[b], cudaEventDisableTiming) != cudaSuccess) {
+                cleanup();
+                return fail(AMJ_ECUDA, "ooc: event creation failed");
+            }
+        }
+        // page-lock the caller's columns so the staging copies run asynchronously
+        for (int c = 0; c < nc; c++)
+            registered[c] = cudaHostRegister((void *)probe->h_cols[c], n * sizeof(int32_t),
+                                             cudaHostRegisterReadOnly) == cudaSuccess;
+        (void)cudaGetLastError();
+    }
+    auto stage_copy = [&](uint64_t s) -> int {
+        const int b = (int)(s & 1);
+        const uint64_t lo = s * slice, hi = std::min(n, lo + slice);
+        for (int c = 0; c < nc; c++)
+            AMJ_CUDA_TRY(cudaMemcpyAsync(stage[b][c].p, probe->h_cols[c] + lo, (hi - lo) * sizeof(int32_t),
+                                         cudaMemcpyHostToDevice, ctx->side_stream[0]));
+        AMJ_CUDA_TRY(cudaEventRecord(ready[b], ctx->side_stream[0]));
+        return AMJ_OK;
+    };
+    std::vector<std::vector<int32_t>> hcols(materialize ? k : 0);
+    uint64_t count = 0, checksum = 0;
+    int rc = AMJ_OK;
+    if (host && nslices) rc = stage_copy(0);
+    for (uint64_t s = 0; rc == AMJ_OK && s < nslices; s++) {
+        const uint64_t lo = s * slice, hi = std::min(n, lo + slice);
+        uint64_t rlo = lo, rhi = hi;
+        if (host) {
+            const int b = (int)(s & 1);
+            rc = cudaStreamWaitEvent(ctx->stream, ready[b], 0) == cudaSuccess ? AMJ_OK : AMJ_ECUDA;
+            if (rc != AMJ_OK) break;
+            for (int c = 0; c < nc; c++) PL.P.probe_col[c] = stage[b][c].p;
+            rlo = 0;
+            rhi = hi - lo;
+            // the other buffer was last read by slice s-1, which has completed
+            if (s + 1 < nslices) rc = stage_copy(s + 1);
+            if (rc != AMJ_OK) break;
+        }
+        PassResult pr;
+        rc = run_passes(ctx, PL, *X, ws, dro, materialize, rlo, rhi, &pr, out);
+        if (rc != AMJ_OK) break;
+        count += pr.count;
+        checksum += pr.checksum;
+        if (materialize) {
+            for (int a = 0; a < k && rc == AMJ_OK; a++) {
+                const size_t old = hcols[a].size();
+                hcols[a].resize(old + pr.rows);
+                if (pr.rows && cudaMemcpyAsync(hcols[a].data() + old, pr.cols[a], pr.rows * sizeof(int32_t),
+                                               cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
+                    rc = fail(AMJ_ECUDA, "ooc: result copy failed");
+            }
+            if (rc == AMJ_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = fail(AMJ_ECUDA, "ooc: sync failed");
+            for (int a = 0; a < k; a++) dev_free(ctx, pr.cols[a]);
+        }
+    }
+    if (rc == AMJ_OK) (void)cudaStreamSynchronize(ctx->side_stream[0]);
+    cleanup();
+    if (rc != AMJ_OK) return rc;
+    out->count = count;
+    out->checksum = checksum;
+    out->stats[7] = nslices;
+    if (materialize) {
+        auto *o = new ResultOwner();
+        o->ctx = ctx;
+        out->priv = o;
+        out->on_host = 1;
+        out->rows = count;
+        for (int a = 0; a < k; a++) {
+            if (cudaMallocHost((void **)&out->cols[a], (count ? count : 1) * sizeof(int32_t)) != cudaSuccess) {
+                (void)cudaGetLastError();
+                return fail(AMJ_ENOMEM, "ooc: pinned result allocation failed");
+            }
+            if (count) std::memcpy(out->cols[a], hcols[a].data(), count * sizeof(int32_t));
+        }
+    }
+    return AMJ_OK;
+}
+
+}  // namespace amj
+
+using namespace amj;
+
+extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *rels, int nrels, int ooc, int ws,
+                                int dro, int fib, int flags, amj_result *out) {
+    if (!ctx || !out || !rels || nrels <= 0) return fail(AMJ_EINVAL, "amhj_execute: bad arguments");
+    for (int i = 0; i < nrels; i++)
+        if (!rels[i]) return fail(AMJ_EINVAL, "amhj_execute: null relation");
+    AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
+    HostPlan hp;
+    AMJ_TRY(compile_plan(query_type, rels, nrels, flags, &hp));
+    result_init(out, hp.k);
+    const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
+    // frequent-item buffering runs on the work-sharing kernel (reference
+    // AMHJ_WS_FIB, exec_AMHJ.cu:171-176)
+    const bool use_ws = ws != 0 || fib != 0;
+    const int layout = ctx->opts.layout;
+
+    cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
+    AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
+
+    for (int i = 0; i < nrels; i++)
+        if (rels[i]->where == AMJ_MEM_HOST_STREAMED && !(i == 0 && ooc))
+            return fail(AMJ_EINVAL, "amhj_execute: only the probe relation of an ooc=1 query may stay on the host");
+
+    ExecScratch X;
+    // ---- build phase
+    std::vector<const HashIndex *> lvix(hp.L);
+    for (int l = 0; l < hp.L; l++) {
+        const LevelSpec &ls = hp.lv[l];
+        IndexKey key{ls.rel, {-1, -1, -1, -1}, ls.ncols, ls.key_mode, layout};
+        for (int c = 0; c < ls.ncols; c++) key.src[c] = ls.src_col[c];
+        auto it = X.indexes.find(key);
+        if (it == X.indexes.end()) {
+            HashIndex ix;
+            const int32_t *cols[4];
+            for (int c = 0; c < ls.ncols; c++) cols[c] = ls.rel->d_cols[ls.src_col[c]];
+            int rc = build_hash_index(ctx, cols, ls.ncols, ls.rel->n, layout, ls.key_mode, ctx->opts.load_factor, &ix);
+            if (rc != AMJ_OK && layout == AMJ_LAYOUT_CUCKOO && rc == AMJ_EOVERFLOW) {
+                // more copies of a key than two cuckoo buckets hold: bucket layout for this table
+                ix = HashIndex();
+                rc = build_hash_index(ctx, cols, ls.ncols, ls.rel->n, AMJ_LAYOUT_BUCKET, ls.key_mode,
+                                      ctx->opts.load_factor, &ix);
+                out->stats[6]++;
+            }
+            if (rc != AMJ_OK) return rc;
+            it = X.indexes.emplace(key, std::move(ix)).first;
+        }
+        lvix[l] = &it->second;
+    }
+    AMJ_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
+
+    // ---- probe plan
+    ProbeLaunch PL;
+    std::memset(&PL, 0, sizeof(PL));
+    ProbePlan &P = PL.P;
+    P.L = (int8_t)hp.L;
+    P.k = (int8_t)hp.k;
+    P.probe_ncols = (int8_t)hp.probe->ncols;
+    for (int c = 0; c < hp.probe->ncols && c < AMJ_MAX_COLS; c++) {
+        P.probe_col[c] = hp.probe->d_cols[c];
+        P.probe_attr[c] = (int8_t)hp.probe_attr[c];
+    }
+    for (int a = 0; a < AMJ_MAX_ATTRS; a++) P.last_src[a] = (int8_t)hp.last_src[a];
+    for (int l = 0; l < hp.L; l++) fill_level(hp.lv[l], *lvix[l], &P.lv[l]);
+    P.task_chunk = (uint32_t)ctx->opts.task_chunk;
+    P.task_cap = (uint32_t)std::min<uint64_t>(ctx->opts.task_capacity, 0x7fffffffull);
+    P.spin_limit_ns = (uint64_t)ctx->opts.spin_limit_ms * 1000000ull;
+    P.depth_bytes = frontier_bytes(hp.k);
+    P.warp_bytes = (uint32_t)hp.L * P.depth_bytes;
+    AMJ_TRY(X.st.alloc(ctx, 1));
+    PL.st = X.st.p;
+    PL.status = ctx->d_status;
+    if (use_ws) {
+        AMJ_TRY(X.tasks.alloc(ctx, P.task_cap));
+        AMJ_TRY(X.ready.alloc(ctx, P.task_cap));
+        PL.tasks = X.tasks.p;
+        PL.task_ready = X.ready.p;
+    }
+    AMJ_TRY(status_reset(ctx));
+
+    int rc = AMJ_OK;
+    if (hp.L == 0) {
+        // a single relation: the result is the relation itself
+        const amj_rel *r = hp.probe;
+        if (r->where == AMJ_MEM_HOST_STREAMED) return fail(AMJ_EUNSUPPORTED, "amhj_execute: single host relation");
+        std::vector<int32_t> tmp;
+        out->count = r->n;
+        std::vector<std::vector<int32_t>> hcols(hp.k, std::vector<int32_t>(r->n));
+        for (int c = 0; c < r->ncols; c++)
+            AMJ_CUDA_TRY(cudaMemcpyAsync(hcols[hp.probe_attr[c]].data(), r->d_cols[c], r->n * 4, cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        std::vector<const int32_t *> cp(hp.k);
+        for (int a = 0; a < hp.k; a++) cp[a] = hcols[a].data();
+        AMJ_TRY(amj_checksum_host(cp.data(), hp.k, r->n, &out->checksum));
+        if (materialize) {
+            int32_t *cols[AMJ_MAX_ATTRS] = {};
+            AMJ_TRY(alloc_cols(ctx, hp.k, r->n, cols));
+            for (int c = 0; c < r->ncols; c++)
+                AMJ_CUDA_TRY(cudaMemcpyAsync(cols[hp.probe_attr[c]], r->d_cols[c], r->n * 4, cudaMemcpyDeviceToDevice,
+                                             ctx->stream));
+            auto *o = new ResultOwner();
+            o->ctx = ctx;
+            out->priv = o;
+            for (int a = 0; a < hp.k; a++) out->cols[a] = cols[a];
+            out->rows = r->n;
+        }
+    } else if (ooc || hp.probe->where == AMJ_MEM_HOST_STREAMED) {
+        rc = amhj_ooc_execute(ctx, PL, &X, hp.probe, use_ws, dro != 0, materialize, flags, out);
+    } else {
+        PassResult pr;
+        rc = run_passes(ctx, PL, X, use_ws, dro != 0, materialize, 0, hp.probe->n, &pr, out);
+        if (rc == AMJ_OK) {
+            out->count = pr.count;
+            out->checksum = pr.checksum;
+            if (materialize) {
+                auto *o = new ResultOwner();
+                o->ctx = ctx;
+                out->priv = o;
+                for (int a = 0; a < hp.k; a++) out->cols[a] = pr.cols[a];
+                out->rows = pr.rows;
+            }
+        }
+    }
+    if (rc != AMJ_OK) {
+        amj_result_release(out);
+        return rc;
+    }
+    AMJ_CUDA_TRY(cudaEventRecord(e2, ctx->stream));
+    AMJ_CUDA_TRY(cudaEventSynchronize(e2));
+    out->build_ms = event_ms(e0, e1);
+    out->probe_ms = event_ms(e1, e2);
+    out->total_ms = event_ms(e0, e2);
+    if (materialize) {
+        rc = finish_result_columns(ctx, out, flags);
+        if (rc != AMJ_OK) {
+            amj_result_release(out);
+            return rc;
+        }
+    }
+    return AMJ_OK;
+}

@@ -1,0 +1,394 @@
+// The AMHJ probe kernel.  MODE 0 counts (with the checksum), MODE 1 writes
+// (two-pass write or the DRO main pass), MODE 2 is the DRO residual pass.
+#pragma once
+#include "amhj_probe.cuh"
+
+namespace amj {
+
+enum ProbeMode : int { PM_COUNT = 0, PM_WRITE = 1, PM_RESIDUAL = 2 };
+
+struct ProbeLaunch {
+    ProbePlan P;
+    ProbeState *st;
+    Task *tasks;
+    unsigned int *task_ready;
+    Breakpoint *units;
+    DevStatus *status;
+    uint64_t batch_stride;   // batch b covers rows row_lo + b*batch_stride*32 ...
+    uint64_t batch_count;    // number of batches
+};
+
+__device__ __forceinline__ bool ws_push(const ProbeLaunch &L, const int32_t *vals, int k, uint32_t s, uint32_t sz,
+                                        uint8_t depth) {
+    ProbeState *st = L.st;
+    if (ld_volatile_u32(&st->q_tail) >= L.P.task_cap) return false;
+    const uint32_t slot = atomicAdd(&st->q_tail, 1u);
+    if (slot >= L.P.task_cap) return false;
+    Task *t = &L.tasks[slot];
+    for (int a = 0; a < k; a++) t->vals[a] = vals[a * 32];
+    t->s = s;
+    t->aux = 0;
+    t->sz = sz;
+    t->depth = depth;
+    t->m8 = 0;
+    __threadfence();
+    atomicExch(&L.task_ready[slot], 1u);
+    atomicAdd(&st->tasks_pushed, 1ull);
+    return true;
+}
+
+// Split rule shared by every mode so a DRO residual replay truncates exactly
+// where the main pass did: a contiguous range longer than twice the task
+// size keeps one task's worth; the rest becomes two tasks (pushed only when
+// `push` is set).  `vals` points at the entry's column in the frontier.
+template <int MODE, bool WS>
+__device__ __forceinline__ uint32_t maybe_split(const ProbeLaunch &L, const LevelDesc &lv, const int32_t *vals,
+                                                uint32_t s, uint32_t sz, int depth) {
+    if (!WS || lv.layout == AMJ_LAYOUT_CUCKOO) return sz;
+    const uint32_t chunk = L.P.task_chunk;
+    if (sz <= 2 * chunk) return sz;
+    const uint32_t rem = sz - chunk, half = rem / 2;
+    if (MODE == PM_RESIDUAL) return chunk;
+    // push the tail first so a failure leaves a contiguous kept range
+    if (!ws_push(L, vals, L.P.k, s + chunk + half, rem - half, (uint8_t)depth)) {
+        if (L.P.dro) report_error(L.status, (unsigned)-AMJ_EOVERFLOW, SITE_WS_QUEUE, sz);
+        return sz;
+    }
+    if (!ws_push(L, vals, L.P.k, s + chunk, half, (uint8_t)depth)) {
+        if (L.P.dro) report_error(L.status, (unsigned)-AMJ_EOVERFLOW, SITE_WS_QUEUE, sz);
+        return chunk + half;
+    }
+    return chunk;
+}
+
+// Idle protocol of work sharing, run by lane 0.  Returns 1 with a task slot,
+// 0 when all work is done (or on error / timeout).
+__device__ int ws_acquire(const ProbeLaunch &L, uint32_t &slot_out) {
+    ProbeState *st = L.st;
+    const uint32_t cap = L.P.task_cap;
+    bool busy = true;
+    unsigned long long t0 = globaltimer_ns();
+    while (true) {
+        uint32_t h = ld_volatile_u32(&st->q_head);
+        uint32_t t = ld_volatile_u32(&st->q_tail);
+        if (t > cap) t = cap;
+        if (h < t) {
+            if (!busy) {
+                atomicAdd(&st->busy, 1u);
+                busy = true;
+                __threadfence();
+            }
+            if (atomicCAS(&st->q_head, h, h + 1) == h) {
+                // wait for the pusher to publish the task
+                unsigned long long w0 = globaltimer_ns();
+                while (ld_volatile_u32(&L.task_ready[h]) == 0u) {
+                    if (globaltimer_ns() - w0 > L.P.spin_limit_ns) {
+                        report_error(L.status, (unsigned)-AMJ_ETIMEOUT, SITE_WS_SLOT, h);
+                        return 0;
+                    }
+                    __nanosleep(64);
+                }
+                __threadfence();
+                atomicAdd(&st->tasks_popped, 1ull);
+                slot_out = h;
+                return 1;
+            }
+            continue;
+        }
+        if (busy) {
+            __threadfence();
+            atomicSub(&st->busy, 1u);
+            busy = false;
+            t0 = globaltimer_ns();
+        }
+        if (ld_volatile_u32(&st->busy) == 0u) {
+            __threadfence();
+            h = ld_volatile_u32(&st->q_head);
+            t = ld_volatile_u32(&st->q_tail);
+            if (t > cap) t = cap;
+            if (h >= t) return 0;
+        }
+        if (ld_volatile_u32(&L.status->code) != 0u) return 0;
+        if (globaltimer_ns() - t0 > L.P.spin_limit_ns) {
+            report_error(L.status, (unsigned)-AMJ_ETIMEOUT, SITE_WS_IDLE, 0);
+            return 0;
+        }
+        __nanosleep(256);
+    }
+}
+
+template <int MODE, bool WS>
+__global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_constant__ ProbeLaunch L) {
+    extern __shared__ __align__(16) char smem[];
+    const ProbePlan &P = L.P;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    char *wbase = smem + (threadIdx.x >> 5) * P.warp_bytes;
+    unsigned long long cnt = 0, chk = 0;
+    int depth = -1;
+
+    // unit bookkeeping for direct result output
+    uint32_t u_kind = 0, u_id = 0;
+    unsigned long long u_emitted = 0, u_written = 0, u_skip = 0;
+    bool u_over = false, u_live = false;
+    unsigned long long res_next = 0;   // residual: next breakpoint index
+
+    while (true) {
+        if (depth < 0) {
+            // ---- unit finished: record a breakpoint if its output overflowed
+            if (MODE == PM_WRITE && P.dro && u_live && u_over && lane == 0) {
+                const unsigned idx = atomicAdd(&L.st->n_units, 1u);
+                if (idx < P.unit_cap) {
+                    L.units[idx].kind = u_kind;
+                    L.units[idx].id = u_id;
+                    L.units[idx].written = u_written;
+                } else {
+                    report_error(L.status, (unsigned)-AMJ_EOVERFLOW, SITE_OUT_OVERFLOW, idx);
+                }
+            }
+            u_live = false;
+            u_over = false;
+            u_emitted = u_written = 0;
+
+            // ---- acquire the next unit
+            int have = 0;          // 1 probe batch, 2 task
+            uint64_t row0 = 0;
+            uint32_t tslot = 0;
+            if (MODE == PM_RESIDUAL) {
+                if (lane == 0) res_next = atomicAdd(&L.st->next_batch, 1ull);
+                res_next = __shfl_sync(AMJ_FULL_MASK, res_next, 0);
+                if (res_next >= L.batch_count) break;
+                const Breakpoint bp = L.units[res_next];
+                u_skip = bp.written;
+                if (bp.kind == 0) {
+                    have = 1;
+                    row0 = P.row_lo + (uint64_t)bp.id * 32;
+                } else {
+                    have = 2;
+                    tslot = bp.id;
+                }
+            } else {
+                unsigned long long b = 0;
+                if (lane == 0) b = atomicAdd(&L.st->next_batch, 1ull);
+                b = __shfl_sync(AMJ_FULL_MASK, b, 0);
+                if (b < L.batch_count) {
+                    row0 = P.row_lo + b * L.batch_stride * 32;
+                    if (row0 < P.row_hi) {
+                        have = 1;
+                        u_kind = 0;
+                        u_id = (uint32_t)(b * L.batch_stride);
+                    }
+                }
+                if (!have) {
+                    if (!WS) break;
+                    int got = 0;
+                    if (lane == 0) got = ws_acquire(L, tslot);
+                    got = __shfl_sync(AMJ_FULL_MASK, got, 0);
+                    tslot = __shfl_sync(AMJ_FULL_MASK, tslot, 0);
+                    if (!got) break;
+                    have = 2;
+                    u_kind = 1;
+                    u_id = tslot;
+                }
+            }
+            u_live = true;
+
+            if (have == 1) {
+                // ---- depth 0: 32 probe tuples, coalesced column loads
+                Frontier F = frontier_at(wbase, P, 0);
+                const uint64_t row = row0 + lane;
+                const bool valid = row < P.row_hi;
+                for (int c = 0; c < P.probe_ncols; c++)
+                    F.vals[P.probe_attr[c] * 32 + lane] = valid ? P.probe_col[c][row] : 0;
+                __syncwarp();
+                uint32_t s = 0, aux = 0, sz = 0;
+                uint8_t m8 = 0;
+                if (valid) {
+                    sz = level_lookup(P.lv[0], [&](int a) { return F.vals[a * 32 + lane]; }, s, aux, m8);
+                    sz = maybe_split<MODE, WS>(L, P.lv[0], F.vals + lane, s, sz, 0);
+                }
+                F.s[lane] = s;
+                F.aux[lane] = aux;
+                F.m8[lane] = m8;
+                const unsigned long long ps = warp_inclusive_scan((unsigned long long)sz, lane);
+                F.psum[lane] = ps;
+                if (lane == 31) {
+                    F.meta[0] = 0;
+                    F.meta[1] = ps;
+                    F.meta[2] = 32;
+                }
+                __syncwarp();
+                depth = 0;
+            } else {
+                // ---- a work-sharing task: one entry at its depth
+                const Task t = L.tasks[tslot];
+                const int td = t.depth;
+                for (int d = 0; d < td; d++) {
+                    Frontier E = frontier_at(wbase, P, d);
+                    if (lane == 0) {
+                        E.meta[0] = 0;
+                        E.meta[1] = 0;
+                        E.meta[2] = 0;
+                    }
+                }
+                Frontier F = frontier_at(wbase, P, td);
+                if (lane < P.k) F.vals[lane * 32] = t.vals[lane];
+                __syncwarp();
+                if (lane == 0) {
+                    const uint32_t sz = maybe_split<MODE, WS>(L, P.lv[td], F.vals, t.s, t.sz, td);
+                    F.s[0] = t.s;
+                    F.aux[0] = t.aux;
+                    F.m8[0] = t.m8;
+                    F.psum[0] = sz;
+                    F.meta[0] = 0;
+                    F.meta[1] = sz;
+                    F.meta[2] = 1;
+                }
+                __syncwarp();
+                depth = td;
+            }
+            continue;
+        }
+
+        // ---- expand one 32-candidate chunk of the frontier at `depth`
+        Frontier F = frontier_at(wbase, P, depth);
+        const unsigned long long cursor = F.meta[0], total = F.meta[1];
+        const int n = (int)F.meta[2];
+        __syncwarp();
+        if (cursor >= total) {
+            depth--;
+            continue;
+        }
+        if (lane == 0) F.meta[0] = cursor + 32;
+        const LevelDesc &lv = P.lv[depth];
+        const unsigned long long j = cursor + lane;
+        bool matched = false;
+        int o = 0;
+        int32_t cv[4] = {0, 0, 0, 0};
+        if (j < total) {
+            int lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (F.psum[mid] > j) hi = mid;
+                else lo = mid + 1;
+            }
+            o = lo;
+            const unsigned long long start = o ? F.psum[o - 1] : 0ull;
+            const uint32_t slot = candidate_slot(lv, F.s[o], F.aux[o], F.m8[o], (uint32_t)(j - start));
+            load_candidate(lv, slot, lv.cmp_mask | lv.bind_mask, cv);
+            matched = true;
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                if (c < lv.ncols && ((lv.cmp_mask >> c) & 1)) matched &= (cv[c] == F.vals[lv.attr[c] * 32 + o]);
+        }
+        const unsigned mm = __ballot_sync(AMJ_FULL_MASK, matched);
+        const int idx = __popc(mm & lt);
+
+        if (depth == P.L - 1) {
+            // ---- emit
+            int32_t tv[AMJ_MAX_ATTRS];
+            uint64_t h = AMJ_CHECKSUM_SEED;
+            if (matched) {
+#pragma unroll
+                for (int a = 0; a < AMJ_MAX_ATTRS; a++) {
+                    if (a < P.k) {
+                        const int src = P.last_src[a];
+                        const int32_t v = src < 0 ? F.vals[a * 32 + o]
+                                                  : (src == 0 ? cv[0] : src == 1 ? cv[1] : src == 2 ? cv[2] : cv[3]);
+                        tv[a] = v;
+                        h = amj_hash_step(h, v);
+                    }
+                }
+            }
+            if (MODE == PM_COUNT) {
+                if (matched) {
+                    cnt++;
+                    chk += h;
+                }
+            } else if (mm) {
+                const int tot = __popc(mm);
+                if (MODE == PM_WRITE) {
+                    unsigned long long base = 0;
+                    if (lane == 0) base = atomicAdd(&L.st->out_cursor, (unsigned long long)tot);
+                    base = __shfl_sync(AMJ_FULL_MASK, base, 0);
+                    const unsigned long long pos = base + idx;
+                    if (matched) {
+                        cnt++;
+                        chk += h;
+                        if (pos < P.out_cap) {
+#pragma unroll
+                            for (int a = 0; a < AMJ_MAX_ATTRS; a++)
+                                if (a < P.k) P.out[a][pos] = tv[a];
+                        }
+                    }
+                    if (!u_over) {
+                        if (base + tot <= P.out_cap) u_written += tot;
+                        else {
+                            u_written += base < P.out_cap ? P.out_cap - base : 0ull;
+                            u_over = true;
+                        }
+                    }
+                    u_emitted += tot;
+                } else {
+                    // residual: skip what the main pass wrote
+                    const bool keep = matched && (u_emitted + idx >= u_skip);
+                    const unsigned km = __ballot_sync(AMJ_FULL_MASK, keep);
+                    if (km) {
+                        unsigned long long base = 0;
+                        if (lane == 0) base = atomicAdd(&L.st->out_cursor, (unsigned long long)__popc(km));
+                        base = __shfl_sync(AMJ_FULL_MASK, base, 0);
+                        const unsigned long long pos = base + __popc(km & lt);
+                        if (keep) {
+                            cnt++;
+                            chk += h;
+                            if (pos < P.out_cap) {
+#pragma unroll
+                                for (int a = 0; a < AMJ_MAX_ATTRS; a++)
+                                    if (a < P.k) P.out[a][pos] = tv[a];
+                            }
+                        }
+                    }
+                    u_emitted += tot;
+                }
+            }
+            continue;
+        }
+        if (!mm) continue;
+
+        // ---- matches become the next frontier
+        Frontier C = frontier_at(wbase, P, depth + 1);
+        const LevelDesc &nl = P.lv[depth + 1];
+        uint32_t s = 0, aux = 0, sz = 0;
+        uint8_t m8 = 0;
+        if (matched) {
+            for (int a = 0; a < P.k; a++) C.vals[a * 32 + idx] = F.vals[a * 32 + o];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                if (c < lv.ncols && ((lv.bind_mask >> c) & 1)) C.vals[lv.attr[c] * 32 + idx] = cv[c];
+            sz = level_lookup(nl, [&](int a) { return C.vals[a * 32 + idx]; }, s, aux, m8);
+            sz = maybe_split<MODE, WS>(L, nl, C.vals + idx, s, sz, depth + 1);
+            C.s[idx] = s;
+            C.aux[idx] = aux;
+            C.m8[idx] = m8;
+        }
+        const unsigned long long ps = warp_inclusive_scan((unsigned long long)(matched ? sz : 0u), lane);
+        if (matched) C.psum[idx] = ps;
+        const unsigned long long ctot = __shfl_sync(AMJ_FULL_MASK, ps, 31);
+        if (lane == 0) {
+            C.meta[0] = 0;
+            C.meta[1] = ctot;
+            C.meta[2] = (unsigned long long)__popc(mm);
+        }
+        __syncwarp();
+        if (ctot) depth++;
+    }
+
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if (lane == 0 && (cnt || chk)) {
+        atomicAdd(&L.st->count, cnt);
+        atomicAdd(&L.st->checksum, chk);
+    }
+}
+
+}  // namespace amj

@@ -1,0 +1,186 @@
+// AMHJ multi-way probe: device-side plan, frontier layout and the probe
+// kernel template.  Included by amhj.cu only.
+//
+// Reference: AMHJ_count / AMHJ_write (MHJ-GPU/Joins/AMHJ.cuh:20-280) run one
+// warp per probe tuple and a depth-first search with backtracking over the
+// build tables; at each level the warp scans a bucket 32 slots at a time and
+// keeps up to 32 matches (common_kernels.cuh:27-67).
+//
+// Here a warp runs the depth-first search over *frontiers* of up to 32
+// partial tuples: depth 0 holds 32 probe tuples, depth d+1 the matches of one
+// 32-candidate chunk of depth d.  The candidates of a frontier are the
+// concatenation of its entries' bucket ranges; every lane takes one candidate
+// (owner found by a 5-step binary search over the entries' prefix sums in
+// shared memory), so all 32 lanes work even when buckets hold 1-4 rows, and
+// the rows of a bucket are read by consecutive lanes (coalesced).  Matches are
+// compacted with a ballot into the next frontier, whose bucket ranges the
+// matching lanes look up in parallel.  At the last depth matches are counted
+// (with the tuple checksum) or written with one output reservation per warp
+// per chunk.  Work sharing splits candidate ranges longer than twice the task
+// size: the entry keeps one task's worth and the rest goes to a device task
+// queue as two halves; idle warps pop tasks.  Every wait in the kernel is
+// bounded by %globaltimer and reports into the status block.
+#pragma once
+#include "amj_ops.cuh"
+
+namespace amj {
+
+constexpr int PROBE_THREADS = 256;
+constexpr int PROBE_WARPS = PROBE_THREADS / 32;
+
+struct LevelDesc {
+    const uint32_t *buc_ptrs;
+    const int32_t *col[4];
+    const int2 *slots;
+    uint32_t mask;
+    int8_t layout, key_mode, ncols, npad;
+    int8_t key_attr[2];
+    uint8_t cmp_mask, bind_mask;
+    int8_t attr[4];
+};
+
+struct ProbePlan {
+    uint64_t row_lo, row_hi;            // probe rows handled by this launch
+    const int32_t *probe_col[AMJ_MAX_COLS];
+    int8_t probe_attr[AMJ_MAX_COLS];
+    int8_t probe_ncols, L, k, pad0;
+    int8_t last_src[AMJ_MAX_ATTRS];     // output attr a: -1 from the tuple, c >= 0 from last level column c
+    LevelDesc lv[AMJ_MAX_BUILD_TABLES];
+    int32_t *out[AMJ_MAX_ATTRS];
+    uint64_t out_cap;
+    uint32_t task_chunk;
+    uint32_t task_cap;
+    uint64_t spin_limit_ns;
+    uint32_t depth_bytes;               // shared memory per frontier
+    uint32_t warp_bytes;                // shared memory per warp
+    // DRO: units that overflowed the output are recorded for the residual pass
+    uint32_t dro;                       // 1: main pass of direct result output
+    uint32_t unit_cap;
+};
+
+struct ProbeState {
+    unsigned long long next_batch;
+    unsigned long long count;
+    unsigned long long checksum;
+    unsigned long long out_cursor;
+    unsigned long long overflow_rows;
+    unsigned int q_head, q_tail;
+    unsigned int busy;
+    unsigned int n_units;
+    unsigned long long tasks_pushed, tasks_popped;
+};
+
+struct Task {
+    int32_t vals[AMJ_MAX_ATTRS];
+    uint32_t s, aux, sz;
+    uint8_t depth, m8, pad[2];
+};
+
+// DRO breakpoint: a unit (probe batch or task) whose output did not fit; the
+// residual pass re-enumerates it, skipping the `written` rows it already wrote.
+struct Breakpoint {
+    uint32_t kind;      // 0 probe batch, 1 task
+    uint32_t id;        // batch number or task slot
+    unsigned long long written;
+};
+
+// ---- shared-memory frontier of one depth ----
+// vals[k][32] int32 | s[32] u32 | aux[32] u32 | psum[32] u64 | m8[32] u8 | meta
+struct Frontier {
+    int32_t *vals;
+    uint32_t *s;
+    uint32_t *aux;
+    unsigned long long *psum;
+    uint8_t *m8;
+    unsigned long long *meta;   // [0] cursor, [1] total, [2] n
+};
+
+__device__ __forceinline__ Frontier frontier_at(char *wbase, const ProbePlan &P, int d) {
+    char *p = wbase + (uint32_t)d * P.depth_bytes;
+    Frontier f;
+    f.vals = (int32_t *)p;
+    p += 128 * P.k;
+    f.s = (uint32_t *)p;
+    p += 128;
+    f.aux = (uint32_t *)p;
+    p += 128;
+    f.psum = (unsigned long long *)p;
+    p += 256;
+    f.meta = (unsigned long long *)p;
+    p += 32;
+    f.m8 = (uint8_t *)p;
+    return f;
+}
+
+__host__ __device__ inline uint32_t frontier_bytes(int k) { return 128u * k + 128 + 128 + 256 + 32 + 32; }
+
+// Look up the candidate range of table `lv` for a tuple whose values are
+// given by get(attr).  Returns the range size.
+template <class Get>
+__device__ __forceinline__ uint32_t level_lookup(const LevelDesc &lv, Get &&get, uint32_t &s, uint32_t &aux,
+                                                 uint8_t &m8) {
+    const int32_t k0 = get(lv.key_attr[0]);
+    const int32_t k1 = lv.key_mode == KEY_PAIR ? get(lv.key_attr[1]) : 0;
+    aux = 0;
+    m8 = 0;
+    if (lv.layout == AMJ_LAYOUT_BUCKET) {
+        const uint32_t h = (lv.key_mode == KEY_PAIR ? hash_pair(k0, k1) : (uint32_t)k0) & lv.mask;
+        s = lv.buc_ptrs[h];
+        return lv.buc_ptrs[h + 1] - s;
+    }
+    const uint32_t hh = lv.key_mode == KEY_PAIR ? hash_pair(k0, k1) : hash_key(k0);
+    if (lv.layout == AMJ_LAYOUT_OPEN_ADDR) {
+        // run of occupied slots starting at the home slot
+        uint32_t p = hh & lv.mask, len = 0;
+        s = p;
+        while (len <= lv.mask) {
+            const int2 v = lv.slots[p];
+            if (v.x == OA_EMPTY_KEY) break;
+            len++;
+            p = (p + 1) & lv.mask;
+        }
+        return len;
+    }
+    // cuckoo: both buckets, keep a bitmask of the slots whose key matches
+    const uint32_t b1 = hh & lv.mask;
+    const uint32_t b2 = (hash_key((int32_t)(hh ^ 0x5bd1e995u)) ^ 0x9e3779b9u) & lv.mask;
+    uint32_t m = 0;
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+        const uint32_t slot = t < 4 ? b1 * CUCKOO_SLOTS + t : b2 * CUCKOO_SLOTS + (t - 4);
+        if (t >= 4 && b2 == b1) break;
+        const int2 v = lv.slots[slot];
+        const bool eq = v.x == k0 && (lv.key_mode != KEY_PAIR || v.y == k1);
+        if (eq) m |= 1u << t;
+    }
+    s = b1;
+    aux = b2;
+    m8 = (uint8_t)m;
+    return __popc(m);
+}
+
+// column c of candidate number `local` of an entry
+__device__ __forceinline__ uint32_t candidate_slot(const LevelDesc &lv, uint32_t s, uint32_t aux, uint8_t m8,
+                                                   uint32_t local) {
+    if (lv.layout == AMJ_LAYOUT_BUCKET) return s + local;
+    if (lv.layout == AMJ_LAYOUT_OPEN_ADDR) return (s + local) & lv.mask;
+    // cuckoo: local-th set bit of m8
+    uint32_t m = m8;
+    for (uint32_t t = 0; t < local; t++) m &= m - 1;
+    const uint32_t t = __ffs(m) - 1;
+    return t < 4 ? s * CUCKOO_SLOTS + t : aux * CUCKOO_SLOTS + (t - 4);
+}
+
+__device__ __forceinline__ void load_candidate(const LevelDesc &lv, uint32_t slot, uint8_t need, int32_t *v) {
+    if (lv.layout == AMJ_LAYOUT_BUCKET) {
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < lv.ncols && ((need >> c) & 1)) v[c] = lv.col[c][slot];
+    } else {
+        const int2 p = lv.slots[slot];
+        v[0] = p.x;
+        v[1] = p.y;
+    }
+}
+
+}  // namespace amj

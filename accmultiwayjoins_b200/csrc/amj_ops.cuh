@@ -1,0 +1,69 @@
+// Index structures and operator entry points shared between the translation
+// units of libamj.
+#pragma once
+#include "amj_cuda.cuh"
+
+struct ResultOwner {
+    amj_ctx *ctx = nullptr;
+};
+
+namespace amj {
+
+void result_init(amj_result *res, int k);
+
+// Key of a hash index: the build relation's first column, or the pair of
+// its first two columns (used when every column of the build relation is
+// already bound at its level, i.e. the table only filters).
+enum KeyMode : int { KEY_SINGLE = 0, KEY_PAIR = 1 };
+
+constexpr int32_t OA_EMPTY_KEY = INT32_MIN;   // open addressing / cuckoo empty slot marker
+constexpr int CUCKOO_SLOTS = 4;                // slots per cuckoo bucket (one 32-byte sector)
+
+// A hash index over a build relation with at most 4 columns.  For the bucket
+// layout the relation's columns are stored in bucket order next to each other
+// (structure of arrays) so a probe reads the key and the bound payload from
+// the same position: no row-id indirection into the original relation, unlike
+// the reference's hash_keys / idx_in_origin / data[] triple
+// (MHJ-GPU/Relation.cuh:50-63).  Open addressing and cuckoo store (c0, c1)
+// pairs in 8-byte slots, four to a 32-byte sector.
+struct HashIndex {
+    int layout = AMJ_LAYOUT_BUCKET;
+    int key_mode = KEY_SINGLE;
+    uint64_t n = 0;
+    int ncols = 0;
+    uint32_t mask = 0;             // buckets-1, capacity-1, or cuckoo buckets-1
+    DBuf<uint32_t> buc_ptrs;       // bucket layout: buckets+1 offsets
+    DBuf<int32_t> cols[4];         // bucket layout: columns in bucket order
+    DBuf<int2> slots;              // open addressing / cuckoo
+};
+
+int build_hash_index(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, uint64_t n, int layout,
+                     int key_mode, float load_factor, HashIndex *out);
+
+// 2-level trie (CSR): level 0 distinct first-column values, offsets into
+// level 1, level 1 second-column values sorted within each group.
+struct Trie2 {
+    uint64_t len0 = 0, len1 = 0;
+    DBuf<int32_t> data0;
+    DBuf<uint64_t> off0;
+    DBuf<int32_t> data1;
+    DBuf<int32_t> src1;        // level-0 value of every level-1 entry (sorted first column)
+    DBuf<uint64_t> rowptr;     // dense child offsets for values rp_min .. rp_min+rp_count-1 (+1 end entry)
+    int32_t rp_min = 0;
+    uint64_t rp_count = 0;     // 0 when no dense array was built
+};
+
+int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out);
+
+// time between two events recorded on the context stream (ms)
+double event_ms(cudaEvent_t a, cudaEvent_t b);
+
+// copy materialised device result columns to pinned host memory (when asked)
+int finish_result_columns(amj_ctx *ctx, amj_result *res, int flags);
+
+}  // namespace amj
+
+struct amj_trie {
+    amj_ctx *ctx = nullptr;
+    amj::Trie2 t;
+};

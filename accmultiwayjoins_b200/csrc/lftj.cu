@@ -1,0 +1,477 @@
+// ALFTJ: leapfrog triejoin over 2-level tries, DFS and BFS.
+//
+// Query shape: the triangle R(a,b) S(b,c) T(a,c) with attribute order a,b,c,
+// as a self-join over one edge relation (LFTJ-GPU/exec_LFTJ.cu:96-102,
+// 218-222) or over three relations whose attributes form that pattern.
+//
+// DFS (reference ALFTJ_count / ALFTJ_write, LFTJ-GPU/ALFTJ.cuh:213-1043):
+// level a is the level-0 array of R (= T's), level b the children of a in R
+// (the level-1 entries of R, walked edge by edge), level c the intersection
+// of S's children of b with T's children of a.  Persistent warps claim 32
+// level-1 entries of R at a time.  Per entry the two child ranges are found
+// with one dense row-pointer load each (or a binary search of level 0).
+// Short pairs are intersected by the owning lane with a sequential merge;
+// long pairs by the whole warp: 32 needles of the shorter list against a
+// 32-wide window of the longer one, membership by a shuffle binary search,
+// and ballot-driven galloping (exponential then 32-ary search) over runs that
+// cannot match.  Counting and the tuple checksum happen in registers; in
+// write mode each warp reserves output rows with one atomic per round.
+//
+// BFS (reference LFTJ_BFS np_join_np / p_join_np / p_join_p,
+// LFTJ-GPU/LFTJ_BFS.cuh:143-500): level-synchronous.  One kernel counts the
+// candidates of every (a,b) entry (the shorter of its two child lists), a
+// scan turns the counts into candidate offsets, and a load-balanced kernel
+// gives every thread one candidate c: the owning entry is found by a
+// shared-memory binary search over the tile's offsets, then c is looked up in
+// the other child list.  Everything runs on the device, including the load
+// balancing the reference does on the CPU (LFTJ_BFS.cuh:396-397), and the
+// count it computes is returned (the reference returns 0, :496).
+#include "amj_ops.cuh"
+
+#include <algorithm>
+
+namespace amj {
+
+struct TrieRef {
+    const int32_t *data0;
+    const uint64_t *off0;
+    const int32_t *data1;
+    const uint64_t *rowptr;
+    uint64_t len0;
+    uint64_t rp_count;
+    int32_t rp_min;
+};
+
+struct TriArgs {
+    const int32_t *r_src;   // level-0 value of every level-1 entry of R (a)
+    const int32_t *r_dst;   // level-1 values of R (b)
+    uint64_t r_n;
+    TrieRef S, T;
+    unsigned long long *cursor;
+    unsigned long long *count;
+    unsigned long long *checksum;
+    unsigned long long *out_cursor;
+    int32_t *out[3];
+    uint64_t out_cap;
+    int small_sum;   // merge by one lane when |X|+|Y| <= small_sum
+};
+
+__device__ __forceinline__ void child_range(const TrieRef &t, int32_t v, uint64_t &s, uint64_t &e) {
+    if (t.rp_count) {
+        const int64_t idx = (int64_t)v - (int64_t)t.rp_min;
+        if (idx >= 0 && (uint64_t)idx < t.rp_count) {
+            s = t.rowptr[idx];
+            e = t.rowptr[idx + 1];
+        } else {
+            s = e = 0;
+        }
+        return;
+    }
+    uint64_t lo = 0, hi = t.len0;
+    while (lo < hi) {
+        uint64_t mid = (lo + hi) >> 1;
+        if (t.data0[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo < t.len0 && t.data0[lo] == v) {
+        s = t.off0[lo];
+        e = t.off0[lo + 1];
+    } else {
+        s = e = 0;
+    }
+}
+
+// first index in [lo, hi) whose value is >= target (hi if none); warp-uniform
+// arguments, all lanes must call.  Exponential probe then 32-ary narrowing.
+__device__ __forceinline__ uint64_t warp_lower_bound(const int32_t *A, uint64_t lo, uint64_t hi, int32_t target,
+                                                     int lane) {
+    if (lo >= hi) return hi;
+    // exponential: lane l probes lo + 2^(l+5) - 1
+    {
+        const uint64_t off = lane < 27 ? ((uint64_t)32 << lane) - 1 : ~0ull;
+        const uint64_t p = lo + off;
+        const bool inr = off != ~0ull && p < hi;
+        const bool less = inr && A[p] < target;
+        const unsigned m = __ballot_sync(AMJ_FULL_MASK, less);
+        const int c = __popc(m);   // probes 0..c-1 are below target
+        const uint64_t nlo = c ? lo + ((uint64_t)32 << (c - 1)) : lo;
+        const uint64_t q = lo + ((uint64_t)32 << c) - 1;   // first probe not below (or past the end)
+        hi = (c < 27 && q < hi) ? q : hi;
+        lo = nlo;
+    }
+    while (hi - lo > 32) {
+        const uint64_t step = (hi - lo + 31) >> 5;
+        const uint64_t p = lo + step * (uint64_t)(lane + 1) - 1;
+        const bool inr = p < hi;
+        const bool less = inr && A[p] < target;
+        const int c = __popc(__ballot_sync(AMJ_FULL_MASK, less));
+        const uint64_t q = lo + step * (uint64_t)(c + 1) - 1;
+        lo = lo + step * (uint64_t)c;
+        if (q < hi) hi = q;
+    }
+    const uint64_t p = lo + lane;
+    const bool less = p < hi && A[p] < target;
+    return lo + (uint64_t)__popc(__ballot_sync(AMJ_FULL_MASK, less));
+}
+
+// Warp-cooperative intersection of two strictly increasing arrays.  Calls
+// emit(value) on the lanes that hold a common value.  Warp-uniform arguments.
+template <class Emit>
+__device__ __forceinline__ void warp_intersect(const int32_t *X, uint64_t nx, const int32_t *Y, uint64_t ny, int lane,
+                                               Emit &&emit) {
+    const int32_t *B = X, *A = Y;
+    uint64_t nb = nx, na = ny;
+    if (nb > na) {
+        B = Y; A = X;
+        nb = ny; na = nx;
+    }
+    uint64_t i = 0, j = 0;
+    while (i < nb && j < na) {
+        const uint64_t bi = i + lane;
+        const bool bval = bi < nb;
+        const int32_t bv = bval ? B[bi] : 0;
+        const uint32_t nvb = (nb - i) < 32 ? (uint32_t)(nb - i) : 32u;
+        const int32_t bfirst = __shfl_sync(AMJ_FULL_MASK, bv, 0);
+        const int32_t blast = __shfl_sync(AMJ_FULL_MASK, bv, nvb - 1);
+        // gallop the haystack past values below the first needle
+        {
+            const uint64_t k = (j + 31 < na) ? j + 31 : na - 1;
+            const int32_t a31 = A[k];
+            if (a31 < bfirst) {
+                if (k == na - 1) break;
+                j = warp_lower_bound(A, j + 32, na, bfirst, lane);
+                if (j >= na) break;
+            }
+        }
+        const uint64_t aj = j + lane;
+        const bool aval = aj < na;
+        const int32_t av = aval ? A[aj] : 0;
+        const uint32_t nva = (na - j) < 32 ? (uint32_t)(na - j) : 32u;
+        const int32_t afirst = __shfl_sync(AMJ_FULL_MASK, av, 0);
+        const int32_t alast = __shfl_sync(AMJ_FULL_MASK, av, nva - 1);
+        // gallop the needles past values below the window
+        if (blast < afirst) {
+            i = warp_lower_bound(B, i + nvb, nb, afirst, lane);
+            continue;
+        }
+        int pos = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int cand = pos + step;
+            const int32_t v = __shfl_sync(AMJ_FULL_MASK, av, cand & 31);
+            if ((uint32_t)cand < nva && v <= bv) pos = cand;
+        }
+        const int32_t at = __shfl_sync(AMJ_FULL_MASK, av, pos);
+        const bool decided = bval && bv <= alast;
+        if (decided && at == bv) emit(bv);
+        if (alast < blast) {
+            i += __popc(__ballot_sync(AMJ_FULL_MASK, decided));
+            j += nva;
+        } else {
+            i += nvb;
+            j += __popc(__ballot_sync(AMJ_FULL_MASK, aval && av <= blast));
+        }
+    }
+}
+
+template <bool WRITE>
+__global__ __launch_bounds__(256) void lftj_tri_dfs_kernel(const __grid_constant__ TriArgs A) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long cnt = 0, chk = 0;
+    while (true) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(A.cursor, 32ull);
+        base = __shfl_sync(AMJ_FULL_MASK, base, 0);
+        if (base >= A.r_n) break;
+        const uint64_t j = base + lane;
+        const bool valid = j < A.r_n;
+        int32_t a = 0, b = 0;
+        uint64_t sb = 0, eb = 0, ta = 0, ea = 0;
+        if (valid) {
+            a = A.r_src[j];
+            b = A.r_dst[j];
+            child_range(A.S, b, sb, eb);
+            if (eb > sb) child_range(A.T, a, ta, ea);
+        }
+        const uint64_t lb = eb - sb, la = ea - ta;
+        const bool active = valid && lb && la;
+        const bool small = active && (lb + la <= (uint64_t)A.small_sum);
+        const uint64_t hab = amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a), b);
+        // lane-local merge of short pairs
+        if (!WRITE) {
+            if (small) {
+                uint64_t p = sb, q = ta;
+                while (p < eb && q < ea) {
+                    const int32_t x = A.S.data1[p], y = A.T.data1[q];
+                    if (x == y) {
+                        cnt++;
+                        chk += amj_hash_step(hab, x);
+                        p++;
+                        q++;
+                    } else if (x < y) p++;
+                    else q++;
+                }
+            }
+        } else {
+            // count, reserve once per warp, then write
+            uint32_t mine = 0;
+            if (small) {
+                uint64_t p = sb, q = ta;
+                while (p < eb && q < ea) {
+                    const int32_t x = A.S.data1[p], y = A.T.data1[q];
+                    if (x == y) { mine++; p++; q++; }
+                    else if (x < y) p++;
+                    else q++;
+                }
+            }
+            const uint32_t incl = warp_inclusive_scan(mine, lane);
+            const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, incl, 31);
+            unsigned long long wbase = 0;
+            if (lane == 0 && tot) wbase = atomicAdd(A.out_cursor, (unsigned long long)tot);
+            wbase = __shfl_sync(AMJ_FULL_MASK, wbase, 0);
+            unsigned long long pos = wbase + incl - mine;
+            if (small && mine) {
+                uint64_t p = sb, q = ta;
+                while (p < eb && q < ea) {
+                    const int32_t x = A.S.data1[p], y = A.T.data1[q];
+                    if (x == y) {
+                        if (pos < A.out_cap) {
+                            A.out[0][pos] = a; A.out[1][pos] = b; A.out[2][pos] = x;
+                        }
+                        pos++;
+                        cnt++;
+                        chk += amj_hash_step(hab, x);
+                        p++; q++;
+                    } else if (x < y) p++;
+                    else q++;
+                }
+            }
+        }
+        // warp-cooperative intersection of long pairs
+        unsigned big = __ballot_sync(AMJ_FULL_MASK, active && !small);
+        while (big) {
+            const int l = __ffs(big) - 1;
+            big &= big - 1;
+            const int32_t wa = __shfl_sync(AMJ_FULL_MASK, a, l);
+            const int32_t wb = __shfl_sync(AMJ_FULL_MASK, b, l);
+            const uint64_t wsb = __shfl_sync(AMJ_FULL_MASK, sb, l), web = __shfl_sync(AMJ_FULL_MASK, eb, l);
+            const uint64_t wta = __shfl_sync(AMJ_FULL_MASK, ta, l), wea = __shfl_sync(AMJ_FULL_MASK, ea, l);
+            const uint64_t whab = __shfl_sync(AMJ_FULL_MASK, hab, l);
+            if (!WRITE) {
+                warp_intersect(A.S.data1 + wsb, web - wsb, A.T.data1 + wta, wea - wta, lane, [&](int32_t c) {
+                    cnt++;
+                    chk += amj_hash_step(whab, c);
+                });
+            } else {
+                // one reservation per round: count this round's matches with a ballot inside emit
+                warp_intersect(A.S.data1 + wsb, web - wsb, A.T.data1 + wta, wea - wta, lane, [&](int32_t c) {
+                    cnt++;
+                    chk += amj_hash_step(whab, c);
+                    const unsigned long long p = atomicAdd(A.out_cursor, 1ull);
+                    if (p < A.out_cap) {
+                        A.out[0][p] = wa; A.out[1][p] = wb; A.out[2][p] = c;
+                    }
+                });
+            }
+        }
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if (lane == 0 && cnt) {
+        atomicAdd(A.count, cnt);
+        atomicAdd(A.checksum, chk);
+    }
+}
+
+// ---- BFS ----
+
+// candidates of entry j: the shorter child list of (S(b), T(a)); 0 when either is empty
+__global__ void lftj_tri_bfs_count_kernel(const __grid_constant__ TriArgs A, unsigned long long *cand) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < A.r_n; j += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t sb, eb, ta = 0, ea = 0;
+        child_range(A.S, A.r_dst[j], sb, eb);
+        if (eb > sb) child_range(A.T, A.r_src[j], ta, ea);
+        const uint64_t lb = eb - sb, la = ea - ta;
+        cand[j] = (lb && la) ? (lb < la ? lb : la) : 0ull;
+    }
+}
+
+constexpr int BFS_TILE = 2048;
+constexpr int BFS_THREADS = 256;
+constexpr int BFS_SMEM_ENTRIES = 2048;
+
+__device__ __forceinline__ uint64_t upper_bound_u64(const unsigned long long *a, uint64_t lo, uint64_t hi,
+                                                    unsigned long long v) {
+    while (lo < hi) {
+        uint64_t mid = (lo + hi) >> 1;
+        if (a[mid] <= v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <bool WRITE>
+__global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const __grid_constant__ TriArgs A,
+                                                                          const unsigned long long *__restrict__ offs,
+                                                                          unsigned long long total) {
+    __shared__ unsigned long long s_off[BFS_SMEM_ENTRIES + 1];
+    __shared__ uint64_t s_e0, s_e1;
+    unsigned long long cnt = 0, chk = 0;
+    const int lane = threadIdx.x & 31;
+    for (unsigned long long tile = blockIdx.x * (unsigned long long)BFS_TILE; tile < total;
+         tile += (unsigned long long)gridDim.x * BFS_TILE) {
+        const unsigned long long tend = (tile + BFS_TILE < total) ? tile + BFS_TILE : total;
+        if (threadIdx.x == 0) {
+            // entries owning candidates tile .. tend-1: offs[e] <= t < offs[e+1]
+            s_e0 = upper_bound_u64(offs, 0, A.r_n, tile) - 1;
+            s_e1 = upper_bound_u64(offs, 0, A.r_n, tend - 1) - 1;
+        }
+        __syncthreads();
+        const uint64_t e0 = s_e0, e1 = s_e1;
+        const uint64_t ne = e1 - e0 + 1;
+        const bool in_smem = ne <= BFS_SMEM_ENTRIES;
+        if (in_smem)
+            for (uint64_t k = threadIdx.x; k < ne; k += BFS_THREADS) s_off[k] = offs[e0 + k];
+        __syncthreads();
+        for (unsigned long long t = tile + threadIdx.x; t < tend; t += BFS_THREADS) {
+            uint64_t e;
+            if (in_smem) {
+                uint64_t lo = 0, hi = ne;
+                while (lo < hi) {
+                    uint64_t mid = (lo + hi) >> 1;
+                    if (s_off[mid] <= t) lo = mid + 1;
+                    else hi = mid;
+                }
+                e = e0 + lo - 1;
+            } else {
+                e = upper_bound_u64(offs, e0, e1 + 1, t) - 1;
+            }
+            const unsigned long long k = t - offs[e];
+            const int32_t a = A.r_src[e], b = A.r_dst[e];
+            uint64_t sb, eb, ta, ea;
+            child_range(A.S, b, sb, eb);
+            child_range(A.T, a, ta, ea);
+            // expand the shorter list, search the longer
+            const bool s_short = (eb - sb) <= (ea - ta);
+            const int32_t c = s_short ? A.S.data1[sb + k] : A.T.data1[ta + k];
+            const int32_t *hay = s_short ? A.T.data1 : A.S.data1;
+            uint64_t lo = s_short ? ta : sb, hi = s_short ? ea : eb;
+            while (lo < hi) {
+                uint64_t mid = (lo + hi) >> 1;
+                if (hay[mid] < c) lo = mid + 1;
+                else hi = mid;
+            }
+            const bool found = lo < (s_short ? ea : eb) && hay[lo] == c;
+            if (found) {
+                cnt++;
+                chk += amj_hash_step(amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a), b), c);
+                if (WRITE) {
+                    const unsigned long long p = atomicAdd(A.out_cursor, 1ull);
+                    if (p < A.out_cap) {
+                        A.out[0][p] = a; A.out[1][p] = b; A.out[2][p] = c;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if (lane == 0 && cnt) {
+        atomicAdd(A.count, cnt);
+        atomicAdd(A.checksum, chk);
+    }
+}
+
+// ---- host side ----
+
+struct LftjCounters {
+    unsigned long long cursor, count, checksum, out_cursor;
+};
+
+static TrieRef trie_ref(const Trie2 &t) {
+    TrieRef r;
+    r.data0 = t.data0.p;
+    r.off0 = t.off0.p;
+    r.data1 = t.data1.p;
+    r.rowptr = t.rowptr.p;
+    r.len0 = t.len0;
+    r.rp_count = t.rp_count;
+    r.rp_min = t.rp_min;
+    return r;
+}
+
+// Run the triangle join over tries R, S, T (R's level-1 entries are the
+// (a,b) pairs).  Count + checksum always; with `out` non-null the tuples are
+// written too (out_cap rows available).
+int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
+                  uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
+                  uint64_t r_lo, uint64_t r_hi) {
+    TriArgs A{};
+    if (r_hi > R.len1) r_hi = R.len1;
+    if (r_lo > r_hi) r_lo = r_hi;
+    A.r_src = R.src1.p + r_lo;
+    A.r_dst = R.data1.p + r_lo;
+    A.r_n = r_hi - r_lo;
+    A.S = trie_ref(S);
+    A.T = trie_ref(T);
+    A.small_sum = small_sum;
+    DBuf<LftjCounters> ctr;
+    AMJ_TRY(ctr.alloc(ctx, 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(ctr.p, 0, sizeof(LftjCounters), ctx->stream));
+    A.cursor = &ctr.p->cursor;
+    A.count = &ctr.p->count;
+    A.checksum = &ctr.p->checksum;
+    A.out_cursor = &ctr.p->out_cursor;
+    const bool write = out != nullptr;
+    if (write) {
+        for (int i = 0; i < 3; i++) A.out[i] = out[i];
+        A.out_cap = out_cap;
+    }
+    if (A.r_n) {
+        if (algo == AMJ_LFTJ_DFS) {
+            int per_sm = 0;
+            AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, write ? lftj_tri_dfs_kernel<true> : lftj_tri_dfs_kernel<false>, 256, 0));
+            if (per_sm < 1) per_sm = 1;
+            const unsigned grid = (unsigned)(ctx->num_sms * per_sm);
+            if (write) lftj_tri_dfs_kernel<true><<<grid, 256, 0, ctx->stream>>>(A);
+            else lftj_tri_dfs_kernel<false><<<grid, 256, 0, ctx->stream>>>(A);
+            AMJ_CUDA_TRY(cudaGetLastError());
+        } else {
+            DBuf<unsigned long long> cand;
+            AMJ_TRY(cand.alloc(ctx, A.r_n + 1));
+            const unsigned g1 = (unsigned)std::min<uint64_t>((A.r_n + 255) / 256, (uint64_t)ctx->num_sms * 16);
+            lftj_tri_bfs_count_kernel<<<g1, 256, 0, ctx->stream>>>(A, cand.p);
+            AMJ_CUDA_TRY(cudaGetLastError());
+            AMJ_TRY(scan_exclusive_u64(ctx, (const uint64_t *)cand.p, (uint64_t *)cand.p, A.r_n,
+                                       (uint64_t *)cand.p + A.r_n));
+            unsigned long long total = 0;
+            AMJ_CUDA_TRY(cudaMemcpyAsync(&total, cand.p + A.r_n, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
+            AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            if (total) {
+                int per_sm = 0;
+                AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &per_sm, write ? lftj_tri_bfs_expand_kernel<true> : lftj_tri_bfs_expand_kernel<false>,
+                    BFS_THREADS, 0));
+                if (per_sm < 1) per_sm = 1;
+                const uint64_t tiles = (total + BFS_TILE - 1) / BFS_TILE;
+                const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)ctx->num_sms * per_sm);
+                if (write)
+                    lftj_tri_bfs_expand_kernel<true><<<grid, BFS_THREADS, 0, ctx->stream>>>(A, cand.p, total);
+                else
+                    lftj_tri_bfs_expand_kernel<false><<<grid, BFS_THREADS, 0, ctx->stream>>>(A, cand.p, total);
+                AMJ_CUDA_TRY(cudaGetLastError());
+            }
+        }
+    }
+    LftjCounters h{};
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&h, ctr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    *count = h.count;
+    *checksum = h.checksum;
+    if (written) *written = write ? (h.out_cursor < out_cap ? h.out_cursor : out_cap) : 0;
+    return AMJ_OK;
+}
+
+}  // namespace amj

@@ -1,0 +1,149 @@
+// ALFTJ operator host side: query discovery, trie builds, and the count /
+// write / out-of-core passes of amj_lftj_execute.
+//
+// Reference: query_processing + LFTJ_exec (LFTJ-GPU/exec_LFTJ.cu:31-254),
+// OOCWrapper::execute_with_{BFS,DFS} (LFTJ-GPU/ooc_wrapper.cuh:174-427).
+// One relation is the triangle self-join (three tries share one CSR,
+// exec_LFTJ.cu:96-102, 198-222); two relations are rejected
+// (exec_LFTJ.cu:92-95); three relations must carry the attribute pairs
+// (0,1), (1,2), (0,2).  Each trie is built with its columns in attribute
+// order, as the reference orders them through a std::map (exec_LFTJ.cu:148-156).
+#include "amj_ops.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace amj {
+int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
+                  uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
+                  uint64_t r_lo, uint64_t r_hi);
+}
+
+using namespace amj;
+
+static int build_rel_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t) {
+    if (r->ncols != 2) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must have two columns");
+    if (r->where == AMJ_MEM_HOST_STREAMED) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must be on the device");
+    const bool swap = r->attrs[0] > r->attrs[1];
+    return build_trie2(ctx, r->d_cols[swap ? 1 : 0], r->d_cols[swap ? 0 : 1], r->n, t);
+}
+
+extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int ws, int flags,
+                                amj_result *out) {
+    if (!ctx || !out || !rels || nrels <= 0) return fail(AMJ_EINVAL, "lftj_execute: bad arguments");
+    if (algo != AMJ_LFTJ_BFS && algo != AMJ_LFTJ_DFS) return fail(AMJ_EINVAL, "lftj_execute: algo must be 0 (BFS) or 1 (DFS)");
+    if (nrels == 2) return fail(AMJ_EINVAL, "lftj_execute: wrong number of datasets: 2");
+    for (int i = 0; i < nrels; i++)
+        if (!rels[i]) return fail(AMJ_EINVAL, "lftj_execute: null relation");
+    if (nrels > 3) return fail(AMJ_EUNSUPPORTED, "lftj_execute: at most 3 relations (MAX_NUM_TABLES)");
+    AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
+    result_init(out, 3);
+    cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
+    AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
+
+    Trie2 tries[3];
+    const Trie2 *R = nullptr, *S = nullptr, *T = nullptr;
+    if (nrels == 1) {
+        AMJ_TRY(build_rel_trie(ctx, rels[0], &tries[0]));
+        R = S = T = &tries[0];
+    } else {
+        for (int i = 0; i < 3; i++) {
+            if (rels[i]->ncols != 2) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must have two columns");
+            const uint32_t lo = std::min(rels[i]->attrs[0], rels[i]->attrs[1]);
+            const uint32_t hi = std::max(rels[i]->attrs[0], rels[i]->attrs[1]);
+            const Trie2 **slot = (lo == 0 && hi == 1) ? &R : (lo == 1 && hi == 2) ? &S : (lo == 0 && hi == 2) ? &T : nullptr;
+            if (!slot || *slot)
+                return fail(AMJ_EUNSUPPORTED, "LFTJ: three relations must carry attributes (0,1), (1,2) and (0,2)");
+            AMJ_TRY(build_rel_trie(ctx, rels[i], &tries[i]));
+            *slot = &tries[i];
+        }
+    }
+    AMJ_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
+
+    // ws=0: every (a,b) pair intersected by its own lane; ws=1: long pairs
+    // shared by the whole warp
+    const int small_sum = ws ? 48 : 0x7fffffff;
+    const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
+    const uint64_t nr = R->len1;
+    uint64_t slice = nr;
+    if (ooc) {
+        slice = ctx->opts.ooc_slice_rows ? ctx->opts.ooc_slice_rows : std::max<uint64_t>(1, nr / 8);
+        slice = std::max<uint64_t>(32, slice);
+    }
+    uint64_t count = 0, checksum = 0;
+    std::vector<std::vector<int32_t>> hcols(ooc && materialize ? 3 : 0);
+    int32_t *dcols[3] = {nullptr, nullptr, nullptr};
+    int rc = AMJ_OK;
+    for (uint64_t lo = 0; rc == AMJ_OK && (lo < nr || (lo == 0 && nr == 0)); lo += slice) {
+        const uint64_t hi = std::min(nr, lo + slice);
+        uint64_t c = 0, h = 0, w = 0;
+        rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, lo, hi);
+        if (rc != AMJ_OK) break;
+        if (materialize) {
+            int32_t *cols[3] = {nullptr, nullptr, nullptr};
+            for (int a = 0; a < 3 && rc == AMJ_OK; a++) rc = dev_alloc(ctx, (void **)&cols[a], (c ? c : 1) * 4);
+            uint64_t c2 = 0, h2 = 0;
+            if (rc == AMJ_OK)
+                rc = lftj_triangle(ctx, *R, *S, *T, algo, cols, c, &c2, &h2, &w, small_sum, lo, hi);
+            if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
+                rc = fail(AMJ_ECUDA, "LFTJ: write pass disagrees with count pass");
+            if (rc == AMJ_OK && ooc) {
+                for (int a = 0; a < 3; a++) {
+                    const size_t old = hcols[a].size();
+                    hcols[a].resize(old + c);
+                    if (c && cudaMemcpyAsync(hcols[a].data() + old, cols[a], c * 4, cudaMemcpyDeviceToHost,
+                                             ctx->stream) != cudaSuccess)
+                        rc = fail(AMJ_ECUDA, "LFTJ ooc: result copy failed");
+                }
+                if (rc == AMJ_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+                    rc = fail(AMJ_ECUDA, "LFTJ ooc: sync failed");
+                for (int a = 0; a < 3; a++) dev_free(ctx, cols[a]);
+            } else {
+                for (int a = 0; a < 3; a++) dcols[a] = cols[a];
+            }
+        }
+        count += c;
+        checksum += h;
+        out->stats[7]++;
+        if (nr == 0) break;
+    }
+    if (rc != AMJ_OK) {
+        for (int a = 0; a < 3; a++) dev_free(ctx, dcols[a]);
+        return rc;
+    }
+    out->count = count;
+    out->checksum = checksum;
+    if (materialize) {
+        auto *o = new ResultOwner();
+        o->ctx = ctx;
+        out->priv = o;
+        out->rows = count;
+        if (ooc) {
+            out->on_host = 1;
+            for (int a = 0; a < 3; a++) {
+                if (cudaMallocHost((void **)&out->cols[a], (count ? count : 1) * 4) != cudaSuccess) {
+                    (void)cudaGetLastError();
+                    amj_result_release(out);
+                    return fail(AMJ_ENOMEM, "LFTJ: pinned result allocation failed");
+                }
+                if (count) std::memcpy(out->cols[a], hcols[a].data(), count * 4);
+            }
+        } else {
+            for (int a = 0; a < 3; a++) out->cols[a] = dcols[a];
+        }
+    }
+    AMJ_CUDA_TRY(cudaEventRecord(e2, ctx->stream));
+    AMJ_CUDA_TRY(cudaEventSynchronize(e2));
+    out->build_ms = event_ms(e0, e1);
+    out->probe_ms = event_ms(e1, e2);
+    out->total_ms = event_ms(e0, e2);
+    if (materialize) {
+        rc = finish_result_columns(ctx, out, flags);
+        if (rc != AMJ_OK) {
+            amj_result_release(out);
+            return rc;
+        }
+    }
+    return AMJ_OK;
+}

@@ -1,0 +1,267 @@
+// IndexedTrie construction and .tr (de)serialisation for 2-column relations.
+//
+// Reference: constructSortedTrie (LFTJ-GPU/multi_partitioning.cuh:129-293)
+// sorts the tuples with CUB / Thrust, marks value changes (extractMasks,
+// :104), and compacts the distinct values and their child offsets with
+// segmented selects and scans.  Here: one min/max reduction sizes a compact
+// sort key (c0 - min0) << bits1 | (c1 - min1) so the LSD radix sort runs only
+// over the bits that vary (40 bits -> 5 passes for 2^20 vertices), then one
+// kernel unpacks level 1 and flags group heads, a scan numbers the heads and
+// a scatter writes level 0 and its offsets.  A dense row-pointer array over
+// the level-0 value range is added when that range is small, so a probe can
+// find a value's children with one load instead of a binary search.
+#include "amj_ops.cuh"
+
+#include <cstdio>
+#include <cstring>
+
+namespace amj {
+
+__global__ void minmax_pairs_kernel(const int32_t *__restrict__ c0, const int32_t *__restrict__ c1, uint64_t n,
+                                    uint32_t *mm /* min0,max0,min1,max1 in sign-flipped order */) {
+    uint32_t mn0 = 0xffffffffu, mx0 = 0, mn1 = 0xffffffffu, mx1 = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t a = (uint32_t)c0[i] ^ 0x80000000u, b = (uint32_t)c1[i] ^ 0x80000000u;
+        mn0 = min(mn0, a); mx0 = max(mx0, a);
+        mn1 = min(mn1, b); mx1 = max(mx1, b);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        mn0 = min(mn0, __shfl_xor_sync(AMJ_FULL_MASK, mn0, d));
+        mx0 = max(mx0, __shfl_xor_sync(AMJ_FULL_MASK, mx0, d));
+        mn1 = min(mn1, __shfl_xor_sync(AMJ_FULL_MASK, mn1, d));
+        mx1 = max(mx1, __shfl_xor_sync(AMJ_FULL_MASK, mx1, d));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&mm[0], mn0); atomicMax(&mm[1], mx0);
+        atomicMin(&mm[2], mn1); atomicMax(&mm[3], mx1);
+    }
+}
+
+__global__ void pack_trie_keys_kernel(const int32_t *__restrict__ c0, const int32_t *__restrict__ c1, uint64_t n,
+                                      uint32_t min0, uint32_t min1, int bits1, uint64_t *__restrict__ items) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t a = ((uint32_t)c0[i] ^ 0x80000000u) - min0;
+        uint64_t b = ((uint32_t)c1[i] ^ 0x80000000u) - min1;
+        items[i] = (a << bits1) | b;
+    }
+}
+
+__device__ __forceinline__ int32_t unflip(uint64_t v, uint32_t mn) {
+    return (int32_t)(((uint32_t)v + mn) ^ 0x80000000u);
+}
+
+__global__ void unpack_trie_kernel(const uint64_t *__restrict__ items, uint64_t n, uint32_t min0, uint32_t min1,
+                                   int bits1, int32_t *__restrict__ data1, int32_t *__restrict__ src1,
+                                   uint32_t *__restrict__ head) {
+    const uint64_t m1 = bits1 >= 64 ? ~0ull : ((1ull << bits1) - 1);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = items[i];
+        data1[i] = unflip(v & m1, min1);
+        src1[i] = unflip(v >> bits1, min0);
+        head[i] = (i == 0 || (items[i - 1] >> bits1) != (v >> bits1)) ? 1u : 0u;
+    }
+}
+
+__global__ void scatter_level0_kernel(const uint64_t *__restrict__ items, const uint32_t *__restrict__ head,
+                                      const uint32_t *__restrict__ pos, uint64_t n, uint32_t min0, int bits1,
+                                      int32_t *__restrict__ data0, uint64_t *__restrict__ off0, uint64_t len0) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        // head[] was scanned in place into pos[]; recompute the head flag
+        const bool h = (i == 0) || ((items[i - 1] >> bits1) != (items[i] >> bits1));
+        if (h) {
+            const uint32_t p = pos[i];
+            data0[p] = unflip(items[i] >> bits1, min0);
+            off0[p] = i;
+        }
+        if (i == 0) off0[len0] = n;
+    }
+    (void)head;
+}
+
+// child counts of every level-0 value, indexed densely by value - min
+__global__ void dense_counts_kernel(const int32_t *__restrict__ data0, const uint64_t *__restrict__ off0,
+                                    uint64_t len0, int32_t vmin, uint64_t *__restrict__ counts) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len0; i += (uint64_t)gridDim.x * blockDim.x)
+        counts[(uint64_t)((int64_t)data0[i] - (int64_t)vmin)] = off0[i + 1] - off0[i];
+}
+
+static unsigned grid_for(amj_ctx *ctx, uint64_t n) {
+    uint64_t g = (n + 255) / 256, cap = (uint64_t)ctx->num_sms * 16;
+    return (unsigned)(g == 0 ? 1 : (g > cap ? cap : g));
+}
+
+static int bits_for(uint32_t range) {
+    int b = 0;
+    while (b < 32 && (range >> b) != 0) b++;
+    return b;
+}
+
+int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out) {
+    if (n >= (1ull << 32) - 4096) return fail(AMJ_EUNSUPPORTED, "trie build: 2^32 or more rows");
+    out->len1 = n;
+    if (n == 0) {
+        out->len0 = 0;
+        AMJ_TRY(out->off0.alloc(ctx, 1));
+        AMJ_CUDA_TRY(cudaMemsetAsync(out->off0.p, 0, sizeof(uint64_t), ctx->stream));
+        AMJ_TRY(out->data0.alloc(ctx, 1));
+        AMJ_TRY(out->data1.alloc(ctx, 1));
+        return AMJ_OK;
+    }
+    DBuf<uint32_t> mm;
+    AMJ_TRY(mm.alloc(ctx, 8));
+    const uint32_t init[4] = {0xffffffffu, 0u, 0xffffffffu, 0u};
+    AMJ_CUDA_TRY(cudaMemcpyAsync(mm.p, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    minmax_pairs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_c0, d_c1, n, mm.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    uint32_t h_mm[4];
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h_mm, mm.p, sizeof(h_mm), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    const uint32_t min0 = h_mm[0], min1 = h_mm[2];
+    const int bits0 = bits_for(h_mm[1] - min0), bits1 = bits_for(h_mm[3] - min1);
+
+    DBuf<uint64_t> a, b;
+    AMJ_TRY(a.alloc(ctx, n));
+    AMJ_TRY(b.alloc(ctx, n));
+    pack_trie_keys_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_c0, d_c1, n, min0, min1, bits1, a.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    uint64_t *sorted = nullptr;
+    AMJ_TRY(radix_sort_u64(ctx, a.p, b.p, n, SK_IDENT, 0, bits0 + bits1, &sorted));
+
+    AMJ_TRY(out->data1.alloc(ctx, n));
+    AMJ_TRY(out->src1.alloc(ctx, n));
+    DBuf<uint32_t> head;
+    AMJ_TRY(head.alloc(ctx, n + 1));
+    unpack_trie_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, min0, min1, bits1, out->data1.p,
+                                                                   out->src1.p, head.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_TRY(scan_exclusive_u32(ctx, head.p, head.p, n, head.p + n));
+    uint32_t len0 = 0;
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&len0, head.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    out->len0 = len0;
+    AMJ_TRY(out->data0.alloc(ctx, len0));
+    AMJ_TRY(out->off0.alloc(ctx, (uint64_t)len0 + 1));
+    scatter_level0_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, head.p, head.p, n, min0, bits1,
+                                                                      out->data0.p, out->off0.p, len0);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    // dense row pointers when the level-0 value range is small against the trie
+    const uint64_t range = (uint64_t)(h_mm[1] - min0) + 1;
+    if (range <= 4 * (uint64_t)len0 + 4096 && range < (1ull << 31)) {
+        out->rp_min = (int32_t)(min0 ^ 0x80000000u);
+        out->rp_count = range;
+        AMJ_TRY(out->rowptr.alloc(ctx, range + 1));
+        AMJ_CUDA_TRY(cudaMemsetAsync(out->rowptr.p, 0, (range + 1) * sizeof(uint64_t), ctx->stream));
+        dense_counts_kernel<<<grid_for(ctx, len0), 256, 0, ctx->stream>>>(out->data0.p, out->off0.p, len0,
+                                                                          out->rp_min, out->rowptr.p);
+        AMJ_CUDA_TRY(cudaGetLastError());
+        AMJ_TRY(scan_exclusive_u64(ctx, out->rowptr.p, out->rowptr.p, range + 1, nullptr));
+    }
+    return AMJ_OK;
+}
+
+}  // namespace amj
+
+using namespace amj;
+
+extern "C" int amj_trie_build(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, amj_trie **out) {
+    if (!ctx || !out || (n && (!d_c0 || !d_c1))) return fail(AMJ_EINVAL, "trie_build: null argument");
+    *out = nullptr;
+    auto *t = new amj_trie();
+    t->ctx = ctx;
+    int rc = build_trie2(ctx, d_c0, d_c1, n, &t->t);
+    if (rc == AMJ_OK) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "trie_build");
+    }
+    if (rc != AMJ_OK) {
+        delete t;
+        return rc;
+    }
+    *out = t;
+    return AMJ_OK;
+}
+
+extern "C" int amj_trie_view(const amj_trie *t, uint64_t *len0, uint64_t *len1, const int32_t **d_data0,
+                             const uint64_t **d_offsets0, const int32_t **d_data1) {
+    if (!t) return fail(AMJ_EINVAL, "trie_view: null trie");
+    if (len0) *len0 = t->t.len0;
+    if (len1) *len1 = t->t.len1;
+    if (d_data0) *d_data0 = t->t.data0.p;
+    if (d_offsets0) *d_offsets0 = t->t.off0.p;
+    if (d_data1) *d_data1 = t->t.data1.p;
+    return AMJ_OK;
+}
+
+extern "C" void amj_trie_release(amj_trie *t) {
+    if (!t) return;
+    if (t->ctx) (void)cudaSetDevice(t->ctx->device);
+    delete t;
+}
+
+// .tr layout (LFTJ-GPU/IndexedTrie.cuh:122-156): uint32 num_attrs, uint64
+// data_len[num_attrs], uint32 attr_list[num_attrs], the int32 data of each
+// level, then the uint64 offsets of every level but the last
+// (data_len[l]+1 entries each).
+extern "C" int amj_trie_save(const amj_trie *t, const char *path, uint32_t a0, uint32_t a1) {
+    if (!t || !path) return fail(AMJ_EINVAL, "trie_save: null argument");
+    amj_ctx *ctx = t->ctx;
+    const uint64_t l0 = t->t.len0, l1 = t->t.len1;
+    std::vector<int32_t> d0(l0), d1(l1);
+    std::vector<uint64_t> o0(l0 + 1);
+    if (l0) AMJ_CUDA_TRY(cudaMemcpyAsync(d0.data(), t->t.data0.p, l0 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (l1) AMJ_CUDA_TRY(cudaMemcpyAsync(d1.data(), t->t.data1.p, l1 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(o0.data(), t->t.off0.p, (l0 + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(AMJ_EIO, std::string("trie_save: cannot open ") + path);
+    const uint32_t na = 2;
+    const uint64_t lens[2] = {l0, l1};
+    const uint32_t attrs[2] = {a0, a1};
+    bool ok = std::fwrite(&na, 4, 1, f) == 1 && std::fwrite(lens, 8, 2, f) == 2 && std::fwrite(attrs, 4, 2, f) == 2 &&
+              (l0 == 0 || std::fwrite(d0.data(), 4, l0, f) == l0) && (l1 == 0 || std::fwrite(d1.data(), 4, l1, f) == l1) &&
+              std::fwrite(o0.data(), 8, l0 + 1, f) == l0 + 1;
+    if (std::fclose(f) != 0) ok = false;
+    return ok ? AMJ_OK : fail(AMJ_EIO, std::string("trie_save: write failed for ") + path);
+}
+
+extern "C" int amj_trie_load(amj_ctx *ctx, const char *path, amj_trie **out, uint32_t *a0, uint32_t *a1) {
+    if (!ctx || !path || !out) return fail(AMJ_EINVAL, "trie_load: null argument");
+    *out = nullptr;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(AMJ_EIO, std::string("trie_load: cannot open ") + path);
+    uint32_t na = 0;
+    uint64_t lens[2] = {0, 0};
+    uint32_t attrs[2] = {0, 0};
+    if (std::fread(&na, 4, 1, f) != 1 || na != 2 || std::fread(lens, 8, 2, f) != 2 || std::fread(attrs, 4, 2, f) != 2) {
+        std::fclose(f);
+        return fail(AMJ_EIO, "trie_load: bad header (only 2-level tries are supported)");
+    }
+    const uint64_t l0 = lens[0], l1 = lens[1];
+    std::vector<int32_t> d0(l0), d1(l1);
+    std::vector<uint64_t> o0(l0 + 1);
+    bool ok = (l0 == 0 || std::fread(d0.data(), 4, l0, f) == l0) && (l1 == 0 || std::fread(d1.data(), 4, l1, f) == l1) &&
+              std::fread(o0.data(), 8, l0 + 1, f) == l0 + 1;
+    std::fclose(f);
+    if (!ok || o0[l0] != l1) return fail(AMJ_EIO, "trie_load: truncated or inconsistent file");
+    auto *t = new amj_trie();
+    t->ctx = ctx;
+    t->t.len0 = l0;
+    t->t.len1 = l1;
+    int rc = t->t.data0.alloc(ctx, l0 ? l0 : 1);
+    if (rc == AMJ_OK) rc = t->t.data1.alloc(ctx, l1 ? l1 : 1);
+    if (rc == AMJ_OK) rc = t->t.off0.alloc(ctx, l0 + 1);
+    if (rc == AMJ_OK && l0 && cudaMemcpyAsync(t->t.data0.p, d0.data(), l0 * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) rc = AMJ_ECUDA;
+    if (rc == AMJ_OK && l1 && cudaMemcpyAsync(t->t.data1.p, d1.data(), l1 * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) rc = AMJ_ECUDA;
+    if (rc == AMJ_OK && cudaMemcpyAsync(t->t.off0.p, o0.data(), (l0 + 1) * 8, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) rc = AMJ_ECUDA;
+    if (rc == AMJ_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = AMJ_ECUDA;
+    if (rc != AMJ_OK) {
+        (void)cudaGetLastError();
+        delete t;
+        return rc == AMJ_ECUDA ? fail(rc, "trie_load: device copy failed") : rc;
+    }
+    if (a0) *a0 = attrs[0];
+    if (a1) *a1 = attrs[1];
+    *out = t;
+    return AMJ_OK;
+}

@@ -1,0 +1,190 @@
+/*
+ * amj.h - C ABI of the B200-native multi-way join operators (AMHJ multi-way
+ * hash join, ALFTJ leapfrog triejoin).
+ *
+ * Conventions
+ *  - Every entry point returns an int status: AMJ_OK (0) or a negative
+ *    AMJ_E* code.  amj_last_error() gives a message for the calling thread.
+ *    The reference instead logs and calls exit(1) (common-utils/cuda/cuda_base.cuh:43-57).
+ *  - No torch types and no CUDA types appear here: streams are `void*`
+ *    (a cudaStream_t), device buffers are plain pointers.
+ *  - A context (amj_ctx) binds one CUDA device and one stream.  Use one
+ *    context per host thread.
+ *  - Relations and results are owned by the library until released.
+ *  - Attribute values are int32, counts are uint64.  The checksum is defined
+ *    in amj_checksum.h.
+ *
+ * Reference seams replaced (file:line within RapidsAtHKUST/AccMultiwayJoins):
+ *  - exec-AMHJ CLI            MHJ-GPU/exec_AMHJ.cu:218-246     -> amj_amhj_execute
+ *  - OOC<...>::execute        MHJ-GPU/ooc.cuh:77-82            -> amj_amhj_execute
+ *  - exec-LFTJ CLI            LFTJ-GPU/exec_LFTJ.cu:261-268    -> amj_lftj_execute
+ *  - OOCWrapper::execute_with_{BFS,DFS}
+ *                             LFTJ-GPU/ooc_wrapper.cuh:404-427 -> amj_lftj_execute
+ *  - RadixPartitioner::splitKI MHJ-GPU/Indexing/radix_partitioning.cuh:576
+ *                                                              -> amj_bucket_build
+ *  - constructSortedTrie      LFTJ-GPU/multi_partitioning.cuh:129 -> amj_trie_build
+ *  - read_rel_cols_mmap / write_rel_cols_mmap
+ *                             common-utils/file_io.h:44-121    -> amj_db_read / amj_db_write
+ */
+#ifndef AMJ_H
+#define AMJ_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- limits (reference: MHJ-GPU/conf.h:22-24, LFTJ-GPU/config.h:16-17) ---- */
+#define AMJ_MAX_ATTRS        8   /* attributes in a result tuple             */
+#define AMJ_MAX_BUILD_TABLES 6   /* build (hash) tables of one AMHJ query    */
+#define AMJ_MAX_COLS         8   /* columns of one relation                  */
+
+/* ---- status codes ---- */
+#define AMJ_OK            0
+#define AMJ_EINVAL       -1   /* bad argument                                */
+#define AMJ_ENOMEM       -2   /* device or host allocation failed            */
+#define AMJ_EOVERFLOW    -3   /* a bounded device structure overflowed       */
+#define AMJ_ETIMEOUT     -4   /* a bounded device wait ran out               */
+#define AMJ_ECUDA        -5   /* a CUDA runtime call failed                  */
+#define AMJ_EUNSUPPORTED -6   /* query shape not supported by this operator  */
+#define AMJ_EIO          -7   /* file I/O error                              */
+#define AMJ_EREJECT      -8   /* admission control rejected the request      */
+
+/* ---- exec-AMHJ query types (MHJ-GPU/exec_AMHJ.cu:5-7) ---- */
+#define AMJ_QUERY_NORMAL 0    /* relations given in query order              */
+#define AMJ_QUERY_TRI    1    /* triangle over one edge relation             */
+#define AMJ_QUERY_FOUR   2    /* 4-clique over one edge relation             */
+
+/* ---- exec-LFTJ algorithm types (LFTJ-GPU/exec_LFTJ.cu:36-39) ---- */
+#define AMJ_LFTJ_BFS 0
+#define AMJ_LFTJ_DFS 1
+
+/* ---- hash-table layouts for AMHJ build tables ---- */
+#define AMJ_LAYOUT_BUCKET    0  /* radix-partitioned bucket CSR (reference default) */
+#define AMJ_LAYOUT_OPEN_ADDR 1  /* linear probing, 32-byte-sector slots            */
+#define AMJ_LAYOUT_CUCKOO    2  /* bucketised cuckoo, unique keys only             */
+
+/* ---- execute flags ---- */
+#define AMJ_F_MATERIALIZE  0x1  /* write the result tuples (else count+checksum) */
+#define AMJ_F_HOST_RESULT  0x2  /* copy materialised columns to host memory      */
+#define AMJ_F_NO_REORDER   0x4  /* keep fully-bound tables at their query position */
+
+/* ---- relation residency ---- */
+#define AMJ_MEM_DEVICE 0   /* columns are device pointers, borrowed            */
+#define AMJ_MEM_HOST   1   /* columns are host pointers, copied to the device  */
+#define AMJ_MEM_HOST_STREAMED 2 /* host columns kept on host (pinned) for ooc  */
+
+typedef struct amj_ctx  amj_ctx;
+typedef struct amj_rel  amj_rel;
+typedef struct amj_trie amj_trie;
+
+typedef struct amj_opts {
+    int      block_size;       /* threads per block of the probe kernels (0: 256) */
+    int      layout;           /* AMJ_LAYOUT_* for AMHJ build tables              */
+    float    load_factor;      /* open addressing load factor (0: 0.5)            */
+    int      task_chunk;       /* work-sharing task size in candidates (0: 1024)  */
+    uint32_t spin_limit_ms;    /* bound on every device-side wait (0: 5000)       */
+    uint64_t task_capacity;    /* work-sharing queue capacity in tasks (0: 1<<20) */
+    uint64_t ooc_slice_rows;   /* ooc probe slice rows (0: derived from budget)   */
+    uint64_t mem_budget;       /* device bytes the ooc planner may use (0: free/2) */
+} amj_opts;
+
+typedef struct amj_result {
+    uint64_t count;                   /* bag cardinality                       */
+    uint64_t checksum;                /* sum of tuple hashes mod 2^64          */
+    int32_t  num_attrs;               /* k, attributes per tuple               */
+    int32_t  on_host;                 /* cols[] are host pointers              */
+    int32_t *cols[AMJ_MAX_ATTRS];     /* column-major tuples, attribute order  */
+    uint64_t rows;                    /* rows present in cols[]                */
+    double   build_ms;                /* index build, device time              */
+    double   probe_ms;                /* join, device time                     */
+    double   total_ms;                /* whole call, device time               */
+    uint64_t stats[8];                /* operator counters, see amj_stat_name  */
+    void    *priv;                    /* library-owned                          */
+} amj_result;
+
+/* ---- library / context ---- */
+const char *amj_last_error(void);
+const char *amj_version(void);
+int  amj_ctx_create(int device, const amj_opts *opts, amj_ctx **out);
+void amj_ctx_destroy(amj_ctx *ctx);
+int  amj_ctx_set_stream(amj_ctx *ctx, void *cuda_stream);
+int  amj_ctx_sync(amj_ctx *ctx);
+const char *amj_stat_name(int i);
+
+/* ---- relations (MHJ-GPU/Relation.cuh:9-38) ---- */
+int  amj_rel_create(amj_ctx *ctx, uint64_t n, int ncols, const uint32_t *attrs,
+                    const int32_t *const *cols, int where, amj_rel **out);
+void amj_rel_release(amj_rel *rel);
+int  amj_rel_info(const amj_rel *rel, uint64_t *n, int *ncols, uint32_t *attrs);
+
+/* ---- AMHJ: exec-AMHJ <NORMAL|TRI|FOUR> <path> <ooc> <ws> <dro> <fib> ----
+ * NORMAL: rels[0] is the probe relation, rels[1..] the build relations in
+ * query order; each build relation is hashed on its first column.  TRI and
+ * FOUR take one 2-column edge relation (nrels == 1).  Results follow the
+ * multi-attribute compare semantics (every attribute already bound is
+ * compared, MHJ-GPU/common_kernels.cuh:41-53). */
+int  amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *rels, int nrels,
+                      int ooc, int ws, int dro, int fib, int flags, amj_result *out);
+
+/* ---- ALFTJ: exec-LFTJ <path> <0=BFS|1=DFS> <ooc> <ws> ----
+ * nrels == 1: triangle self-join R(a,b) S(b,c) T(a,c) over one edge relation.
+ * nrels >= 3: multi-way join of 2-column relations (attributes from rels).
+ * nrels == 2 is rejected, as in the reference (LFTJ-GPU/exec_LFTJ.cu:92-95). */
+int  amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels,
+                      int algo, int ooc, int ws, int flags, amj_result *out);
+
+void amj_result_release(amj_result *res);
+
+/* ---- building blocks on device pointers, enqueued on the context stream ----
+ * amj_bucket_build: bucket-CSR index of n keys with `buckets` (a power of two)
+ * buckets, bucket = key & (buckets-1).  Writes hash_keys[n], idx_in_origin[n]
+ * (row ids) and buc_ptrs[buckets+1].  Rows inside a bucket are in ascending
+ * row order.  (MHJ-GPU/Indexing/radix_partitioning.cuh:576) */
+int  amj_bucket_build(amj_ctx *ctx, const int32_t *d_keys, uint64_t n, uint64_t buckets,
+                      int32_t *d_hash_keys, uint32_t *d_idx_in_origin, uint32_t *d_buc_ptrs);
+
+/* amj_trie_build: 2-level IndexedTrie of the pairs (c0[i], c1[i]): the
+ * distinct c0 values ascending (level 0), their child offsets, and the c1
+ * values sorted inside each c0 group (level 1, duplicates kept).
+ * (LFTJ-GPU/multi_partitioning.cuh:129-293, LFTJ-GPU/IndexedTrie.cuh:21-31) */
+int  amj_trie_build(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n,
+                    amj_trie **out);
+/* device views of a trie: level-0 values, level-0 offsets (len0+1 entries),
+ * level-1 values */
+int  amj_trie_view(const amj_trie *t, uint64_t *len0, uint64_t *len1,
+                   const int32_t **d_data0, const uint64_t **d_offsets0,
+                   const int32_t **d_data1);
+/* .tr serialisation, byte layout of IndexedTrie::serialization
+ * (LFTJ-GPU/IndexedTrie.cuh:122-156) with attrs {a0,a1} */
+int  amj_trie_save(const amj_trie *t, const char *path, uint32_t a0, uint32_t a1);
+int  amj_trie_load(amj_ctx *ctx, const char *path, amj_trie **out, uint32_t *a0, uint32_t *a1);
+void amj_trie_release(amj_trie *t);
+
+/* ---- seeded synthetic data (host, deterministic, OpenMP) ---- */
+int  amj_gen_uniform_i32(int32_t *out, uint64_t n, int64_t lo, int64_t hi_excl,
+                         uint64_t seed, uint64_t stream);
+int  amj_gen_permutation_i32(int32_t *out, uint64_t n, uint64_t seed, uint64_t stream);
+/* Zipf(theta) ranks over [0, domain); rank r maps to rank_to_key[r] when given */
+int  amj_gen_zipf_i32(int32_t *out, uint64_t n, uint64_t domain, double theta,
+                      const int32_t *rank_to_key, uint64_t seed, uint64_t stream);
+/* R-MAT graph: nedges draws with quadrant probabilities (a,b,c,1-a-b-c) over
+ * 2^scale vertices; self-loops dropped, edges oriented u<v, duplicates
+ * removed, then shuffled.  src/dst need room for nedges; *n_out = E'. */
+int  amj_gen_rmat(int scale, uint64_t nedges, double a, double b, double c, uint64_t seed,
+                  int32_t *src, int32_t *dst, uint64_t *n_out);
+
+/* ---- .db files: column-major int32, name "<rows>_<attr0>_<attr1>...db" ---- */
+int  amj_db_write(const char *path, uint64_t n, int ncols, const int32_t *const *cols);
+int  amj_db_read(const char *path, uint64_t n, int ncols, int32_t *const *cols);
+int  amj_db_parse_name(const char *path, uint64_t *n, int *ncols, uint32_t *attrs);
+
+/* ---- host checksum of column-major tuples (same definition as the GPU) ---- */
+int  amj_checksum_host(const int32_t *const *cols, int k, uint64_t n, uint64_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMJ_H */
