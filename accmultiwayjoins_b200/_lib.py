@@ -50,6 +50,8 @@ class amj_opts(C.Structure):
         ("task_capacity", C.c_uint64),
         ("ooc_slice_rows", C.c_uint64),
         ("mem_budget", C.c_uint64),
+        ("lftj_heavy_degree", C.c_uint32),
+        ("dro_headroom", C.c_float),
     ]
 
 
@@ -91,6 +93,7 @@ SIGNATURES = {
     "amj_ctx_set_stream": (C.c_int, [_P, _P]),
     "amj_ctx_sync": (C.c_int, [_P]),
     "amj_stat_name": (C.c_char_p, [C.c_int]),
+    "amj_ctx_launch_count": (C.c_int, [_P, _U64P]),
     "amj_rel_create": (C.c_int, [_P, C.c_uint64, C.c_int, _U32P, C.POINTER(_I32P), C.c_int, C.POINTER(_P)]),
     "amj_rel_release": (None, [_P]),
     "amj_rel_info": (C.c_int, [_P, _U64P, C.POINTER(C.c_int), _U32P]),
@@ -102,9 +105,11 @@ SIGNATURES = {
     "amj_bucket_build": (C.c_int, [_P, _P, C.c_uint64, C.c_uint64, _P, _P, _P]),
     "amj_trie_build": (C.c_int, [_P, _P, _P, C.c_uint64, C.POINTER(_P)]),
     "amj_trie_view": (C.c_int, [_P, _U64P, _U64P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+    "amj_trie_download": (C.c_int, [_P, _I32P, _U64P, _I32P]),
     "amj_trie_save": (C.c_int, [_P, C.c_char_p, C.c_uint32, C.c_uint32]),
     "amj_trie_load": (C.c_int, [_P, C.c_char_p, C.POINTER(_P), _U32P, _U32P]),
     "amj_trie_release": (None, [_P]),
+    "amj_selftest_bounded_wait": (C.c_int, [_P, C.c_uint32]),
     "amj_gen_uniform_i32": (C.c_int, [_I32P, C.c_uint64, C.c_int64, C.c_int64, C.c_uint64, C.c_uint64]),
     "amj_gen_permutation_i32": (C.c_int, [_I32P, C.c_uint64, C.c_uint64, C.c_uint64]),
     "amj_gen_zipf_i32": (C.c_int, [_I32P, C.c_uint64, C.c_uint64, C.c_double, _I32P, C.c_uint64, C.c_uint64]),

@@ -15,7 +15,8 @@ the reference does (common-utils/cuda/cuda_base.cuh:43-57).
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, field
+import weakref
+from dataclasses import dataclass
 from typing import Optional, Sequence
 
 import numpy as np
@@ -91,13 +92,17 @@ class Relation:
         if where == L.AMJ_MEM_HOST:
             self._keep = []  # copied to the device
         self.handle = handle
+        ctx._relations.add(self)
         self.n = int(n)
         self.attrs = [int(a) for a in attrs]
         self.where = where
 
     def release(self):
+        """Free the relation; a relation must be released before its context
+        (Context.close releases the ones still alive)."""
         if getattr(self, "handle", None):
-            L.load().amj_rel_release(self.handle)
+            if getattr(self.ctx, "handle", None):
+                L.load().amj_rel_release(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -112,7 +117,7 @@ class Context:
 
     def __init__(self, device: int = 0, layout: str = "bucket", load_factor: float = 0.5, task_chunk: int = 1024,
                  spin_limit_ms: int = 5000, task_capacity: int = 1 << 20, ooc_slice_rows: int = 0,
-                 mem_budget: int = 0):
+                 mem_budget: int = 0, lftj_heavy_degree: int = 0, dro_headroom: float = 0.0):
         lib = L.load()
         o = L.amj_opts()
         o.block_size = 256
@@ -123,7 +128,11 @@ class Context:
         o.task_capacity = task_capacity
         o.ooc_slice_rows = ooc_slice_rows
         o.mem_budget = mem_budget
+        o.lftj_heavy_degree = lftj_heavy_degree
+        o.dro_headroom = dro_headroom
         h = C.c_void_p()
+        self.handle = None
+        self._relations = weakref.WeakSet()
         L.check(lib.amj_ctx_create(device, C.byref(o), C.byref(h)), "ctx_create")
         self.handle = h
 
@@ -175,6 +184,8 @@ class Context:
 
     def close(self):
         if getattr(self, "handle", None):
+            for r in list(self._relations):
+                r.release()
             L.load().amj_ctx_destroy(self.handle)
             self.handle = None
 

@@ -185,6 +185,7 @@ static int launch_probe_t(amj_ctx *ctx, const ProbeLaunch &PL, size_t smem) {
         const unsigned int warps = (unsigned int)(grid * PROBE_WARPS);
         AMJ_CUDA_TRY(cudaMemcpyAsync(&PL.st->busy, &warps, sizeof(warps), cudaMemcpyHostToDevice, ctx->stream));
     }
+    note_launch(ctx);
     kern<<<(unsigned)grid, PROBE_THREADS, smem, ctx->stream>>>(PL);
     AMJ_CUDA_TRY(cudaGetLastError());
     return AMJ_OK;
@@ -264,6 +265,27 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
     PL.batch_stride = 1;
     PL.batch_count = nbatches;
     const int k = P.k;
+    // work sharing: balance level 0 by candidates instead of probe rows
+    DBuf<unsigned long long> l0;
+    P.lbs = 0;
+    P.l0_start = nullptr;
+    uint64_t nchunks = 0;
+    if (ws && rows) {
+        AMJ_TRY(l0.alloc(ctx, rows + 1));
+        P.l0_start = l0.p;
+        const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 16);
+        note_launch(ctx);
+        amhj_l0_sizes_kernel<<<g, 256, 0, ctx->stream>>>(P, l0.p);
+        AMJ_CUDA_TRY(cudaGetLastError());
+        AMJ_TRY(scan_exclusive_u64(ctx, (const uint64_t *)l0.p, (uint64_t *)l0.p, rows, (uint64_t *)l0.p + rows));
+        unsigned long long total = 0;
+        AMJ_CUDA_TRY(cudaMemcpyAsync(&total, l0.p + rows, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        nchunks = (total + 31) / 32;
+        if (nchunks > 0xffffffffull) return fail(AMJ_EUNSUPPORTED, "AMHJ: more than 2^37 level-0 candidates in one slice");
+        P.lbs = 1;
+        PL.batch_count = nchunks;
+    }
 
     if (!materialize) {
         P.dro = 0;
@@ -306,16 +328,19 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
         const uint64_t want = 4096;   // batches sampled
         const uint64_t stride = nbatches > want ? nbatches / want : 1;
         P.dro = 0;
+        const uint32_t lbs = P.lbs;
+        P.lbs = 0;
         AMJ_TRY(reset_state(ctx, PL.st, nullptr, 0));
         PL.batch_stride = stride;
         PL.batch_count = (nbatches + stride - 1) / stride;
         AMJ_TRY(launch_probe(ctx, PL, PM_COUNT, false));
         AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ DRO sampling"));
+        P.lbs = lbs;
         const double sampled_rows = std::min<double>((double)PL.batch_count * 32.0, (double)rows);
         const double est = sampled_rows > 0 ? (double)h.count * (double)rows / sampled_rows : 0.0;
-        estimate = (uint64_t)(est * 1.05) + 1024;
+        estimate = (uint64_t)(est * (ctx->opts.dro_headroom > 0.f ? ctx->opts.dro_headroom : 1.05f)) + 1024;
         PL.batch_stride = 1;
-        PL.batch_count = nbatches;
+        PL.batch_count = P.lbs ? nchunks : nbatches;
     }
     res->stats[5] += estimate;
     // 2. one write pass into the estimated buffer, recording breakpoints
@@ -324,7 +349,7 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
     for (int a = 0; a < k; a++) P.out[a] = main_cols[a];
     P.out_cap = estimate;
     P.dro = 1;
-    const uint64_t unit_cap = nbatches + task_cap + 64;
+    const uint64_t unit_cap = (P.lbs ? nchunks : nbatches) + task_cap + 64;
     if (X.units.n < unit_cap) AMJ_TRY(X.units.alloc(ctx, unit_cap));
     PL.units = X.units.p;
     P.unit_cap = (uint32_t)std::min<uint64_t>(unit_cap, 0xffffffffull);
@@ -333,6 +358,14 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
     if (rc == AMJ_OK) rc = read_state(ctx, PL.st, &h, "AMHJ DRO main write");
     if (rc != AMJ_OK) {
         for (int a = 0; a < k; a++) dev_free(ctx, main_cols[a]);
+        if (rc == AMJ_EOVERFLOW && ws) {
+            // The residual replay needs every split of the main pass to have
+            // reached the task queue; when the queue filled up, redo the
+            // direct output without work sharing.
+            AMJ_TRY(status_reset(ctx));
+            res->stats[6]++;
+            return run_passes(ctx, PL, X, false, dro, materialize, row_lo, row_hi, pr, res);
+        }
         return rc;
     }
     const uint64_t total = h.count;

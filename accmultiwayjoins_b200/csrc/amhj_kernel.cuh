@@ -117,6 +117,114 @@ __device__ int ws_acquire(const ProbeLaunch &L, uint32_t &slot_out) {
     }
 }
 
+
+// last index r in [0, n) with E[r] <= g (E non-decreasing, E[0] <= g); warp-uniform call
+__device__ __forceinline__ uint64_t warp_row_of(const unsigned long long *E, uint64_t n, unsigned long long g, int lane) {
+    uint64_t lo = 0, hi = n;   // answer in [lo, hi)
+    while (hi - lo > 32) {
+        const uint64_t step = (hi - lo + 31) >> 5;
+        const uint64_t p = lo + step * (uint64_t)lane;
+        const bool le = p < hi && E[p] <= g;
+        const int c = __popc(__ballot_sync(AMJ_FULL_MASK, le));   // probes 0..c-1 are <= g, c >= 1
+        lo = lo + step * (uint64_t)(c - 1);
+        const uint64_t nh = lo + step;
+        if (nh < hi) hi = nh;
+    }
+    const uint64_t p = lo + lane;
+    const bool le = p < hi && E[p] <= g;
+    return lo + (uint64_t)__popc(__ballot_sync(AMJ_FULL_MASK, le)) - 1;
+}
+
+// Depth-0 frontier of level-0 chunk `c`: lane j takes candidate 32c + j of the
+// concatenated level-0 ranges; its entry is that single candidate of its row.
+template <int MODE, bool WS>
+__device__ __forceinline__ bool load_l0_chunk(const ProbeLaunch &L, char *wbase, unsigned long long c, int lane) {
+    const ProbePlan &P = L.P;
+    const uint64_t rows = P.row_hi - P.row_lo;
+    const unsigned long long total = P.l0_start[rows];
+    const unsigned long long g0 = c * 32ull;
+    if (g0 >= total) return false;
+    const unsigned long long g = g0 + lane;
+    const bool valid = g < total;
+    // row of the chunk's first candidate, then each lane's row from a window of 32 row starts
+    const uint64_t r0 = warp_row_of(P.l0_start, rows, g0, lane);
+    const uint64_t wr = r0 + lane;
+    const unsigned long long ws = wr < rows ? P.l0_start[wr] : ~0ull;
+    int pos = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const int cand = pos + step;
+        const unsigned long long v = __shfl_sync(AMJ_FULL_MASK, ws, cand & 31);
+        if (v <= g) pos = cand;
+    }
+    uint64_t row = r0 + pos;
+    if (valid && pos == 31 && row + 1 < rows && P.l0_start[row + 1] <= g) {
+        // more than 32 rows lie inside this chunk: plain binary search
+        uint64_t lo = row + 1, hi = rows;
+        while (hi - lo > 1) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (P.l0_start[mid] <= g) lo = mid;
+            else hi = mid;
+        }
+        row = lo;
+    }
+    Frontier F = frontier_at(wbase, P, 0);
+    const uint64_t prow = P.row_lo + row;
+    for (int cc = 0; cc < P.probe_ncols; cc++)
+        F.vals[P.probe_attr[cc] * 32 + lane] = valid ? P.probe_col[cc][prow] : 0;
+    __syncwarp();
+    uint32_t s = 0, aux = 0, sz = 0;
+    uint8_t m8 = 0;
+    if (valid) {
+        const uint32_t k = (uint32_t)(g - P.l0_start[row]);
+        level_lookup(P.lv[0], [&](int a) { return F.vals[a * 32 + lane]; }, s, aux, m8);
+        if (P.lv[0].layout == AMJ_LAYOUT_CUCKOO) {
+            uint32_t m = m8;
+            for (uint32_t t = 0; t < k; t++) m &= m - 1;
+            m8 = (uint8_t)(m & (~m + 1u));   // keep the k-th matching slot only
+        } else {
+            s += k;
+        }
+        sz = 1;
+    }
+    F.s[lane] = s;
+    F.aux[lane] = aux;
+    F.m8[lane] = m8;
+    const unsigned long long ps = warp_inclusive_scan((unsigned long long)sz, lane);
+    F.psum[lane] = ps;
+    if (lane == 31) {
+        F.meta[0] = 0;
+        F.meta[1] = ps;
+        F.meta[2] = 32;
+    }
+    __syncwarp();
+    return true;
+}
+
+// level-0 candidate counts of probe rows row_lo..row_hi-1
+__global__ void amhj_l0_sizes_kernel(const __grid_constant__ ProbePlan P, unsigned long long *sizes) {
+    const uint64_t rows = P.row_hi - P.row_lo;
+    int32_t v[AMJ_MAX_ATTRS];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x) {
+        for (int c = 0; c < P.probe_ncols; c++) {
+            const int a = P.probe_attr[c];
+            const int32_t x = P.probe_col[c][P.row_lo + i];
+#pragma unroll
+            for (int t = 0; t < AMJ_MAX_ATTRS; t++)
+                if (t == a) v[t] = x;
+        }
+        uint32_t s, aux;
+        uint8_t m8;
+        sizes[i] = level_lookup(P.lv[0], [&](int a) {
+            int32_t r = 0;
+#pragma unroll
+            for (int t = 0; t < AMJ_MAX_ATTRS; t++)
+                if (t == a) r = v[t];
+            return r;
+        }, s, aux, m8);
+    }
+}
+
 template <int MODE, bool WS>
 __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_constant__ ProbeLaunch L) {
     extern __shared__ __align__(16) char smem[];
@@ -151,9 +259,10 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
             u_emitted = u_written = 0;
 
             // ---- acquire the next unit
-            int have = 0;          // 1 probe batch, 2 task
+            int have = 0;          // 1 probe batch, 2 task, 3 level-0 chunk
             uint64_t row0 = 0;
             uint32_t tslot = 0;
+            unsigned long long l0c = 0;
             if (MODE == PM_RESIDUAL) {
                 if (lane == 0) res_next = atomicAdd(&L.st->next_batch, 1ull);
                 res_next = __shfl_sync(AMJ_FULL_MASK, res_next, 0);
@@ -163,6 +272,9 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
                 if (bp.kind == 0) {
                     have = 1;
                     row0 = P.row_lo + (uint64_t)bp.id * 32;
+                } else if (bp.kind == 2) {
+                    have = 3;
+                    l0c = bp.id;
                 } else {
                     have = 2;
                     tslot = bp.id;
@@ -172,11 +284,18 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
                 if (lane == 0) b = atomicAdd(&L.st->next_batch, 1ull);
                 b = __shfl_sync(AMJ_FULL_MASK, b, 0);
                 if (b < L.batch_count) {
-                    row0 = P.row_lo + b * L.batch_stride * 32;
-                    if (row0 < P.row_hi) {
-                        have = 1;
-                        u_kind = 0;
-                        u_id = (uint32_t)(b * L.batch_stride);
+                    if (P.lbs) {
+                        have = 3;
+                        l0c = b;
+                        u_kind = 2;
+                        u_id = (uint32_t)b;
+                    } else {
+                        row0 = P.row_lo + b * L.batch_stride * 32;
+                        if (row0 < P.row_hi) {
+                            have = 1;
+                            u_kind = 0;
+                            u_id = (uint32_t)(b * L.batch_stride);
+                        }
                     }
                 }
                 if (!have) {
@@ -193,6 +312,10 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
             }
             u_live = true;
 
+            if (have == 3) {
+                depth = load_l0_chunk<MODE, WS>(L, wbase, l0c, lane) ? 0 : -1;
+                continue;
+            }
             if (have == 1) {
                 // ---- depth 0: 32 probe tuples, coalesced column loads
                 Frontier F = frontier_at(wbase, P, 0);

@@ -56,6 +56,11 @@ struct ProbePlan {
     // DRO: units that overflowed the output are recorded for the residual pass
     uint32_t dro;                       // 1: main pass of direct result output
     uint32_t unit_cap;
+    // work sharing at level 0: the level-0 candidates of rows row_lo..row_hi-1
+    // form one space (l0_start[r - row_lo] = first candidate of row r,
+    // l0_start[rows] = total); units are 32-candidate chunks of it
+    const unsigned long long *l0_start;
+    uint32_t lbs;
 };
 
 struct ProbeState {
@@ -79,8 +84,8 @@ struct Task {
 // DRO breakpoint: a unit (probe batch or task) whose output did not fit; the
 // residual pass re-enumerates it, skipping the `written` rows it already wrote.
 struct Breakpoint {
-    uint32_t kind;      // 0 probe batch, 1 task
-    uint32_t id;        // batch number or task slot
+    uint32_t kind;      // 0 probe batch, 1 task, 2 level-0 chunk
+    uint32_t id;        // batch number, task slot or chunk number
     unsigned long long written;
 };
 

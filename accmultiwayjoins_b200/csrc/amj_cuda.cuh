@@ -126,6 +126,7 @@ struct amj_ctx {
     amj::DevStatus *h_status = nullptr;    // pinned host mirror
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaStream_t side_stream[2] = {nullptr, nullptr};   // ooc copy / prefetch streams
+    unsigned long long launches = 0;                     // kernels launched through this context
 };
 
 struct amj_rel {
@@ -140,6 +141,8 @@ struct amj_rel {
 };
 
 namespace amj {
+
+inline void note_launch(amj_ctx *ctx) { ctx->launches++; }
 
 // Stream-ordered device allocation on the context stream.
 int dev_alloc(amj_ctx *ctx, void **p, size_t bytes);

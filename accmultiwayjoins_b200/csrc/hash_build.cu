@@ -186,25 +186,32 @@ static int build_bucket(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, u
     AMJ_TRY(b.alloc(ctx, n));
     const bool pairs = ncols <= 2;
     if (pairs) {
+        note_launch(ctx);
         pack_pairs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_cols[0], ncols > 1 ? d_cols[1] : nullptr, n,
                                                                       a.p);
     } else {
         if (key_mode != KEY_SINGLE) return fail(AMJ_EUNSUPPORTED, "bucket index: pair key needs a 2-column relation");
+        note_launch(ctx);
         pack_key_rowid_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_cols[0], n, a.p);
     }
     AMJ_CUDA_TRY(cudaGetLastError());
     uint64_t *sorted = nullptr;
     AMJ_TRY(radix_sort_u64(ctx, a.p, b.p, n, key_mode == KEY_PAIR ? SK_PAIR_HASH : SK_LOW32, 0, bits, &sorted));
     if (pairs) {
+        note_launch(ctx);
         unpack_pairs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, out->cols[0].p,
                                                                         ncols > 1 ? out->cols[1].p : nullptr);
     } else {
+        note_launch(ctx);
         unpack_pairs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, out->cols[0].p, nullptr);
-        for (int c = 1; c < ncols; c++)
+        for (int c = 1; c < ncols; c++) {
+            note_launch(ctx);
             gather_col_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, d_cols[c], out->cols[c].p);
+        }
     }
     AMJ_CUDA_TRY(cudaGetLastError());
     AMJ_CUDA_TRY(cudaMemsetAsync(out->buc_ptrs.p, 0, (B + 1) * sizeof(uint32_t), ctx->stream));
+    note_launch(ctx);
     bucket_hist_sorted_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(
         sorted, n, pairs ? key_mode : KEY_SINGLE, out->mask, out->buc_ptrs.p);
     AMJ_CUDA_TRY(cudaGetLastError());
@@ -231,7 +238,9 @@ int build_hash_index(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, uint
         if (cap > (1ull << 31)) return fail(AMJ_EINVAL, "open addressing: capacity too large");
         out->mask = (uint32_t)(cap - 1);
         AMJ_TRY(out->slots.alloc(ctx, cap));
+        note_launch(ctx);
         fill_slots_kernel<<<grid_for(ctx, cap), 256, 0, ctx->stream>>>(out->slots.p, cap);
+        note_launch(ctx);
         oa_insert_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_cols[0], ncols > 1 ? d_cols[1] : nullptr, n,
                                                                      key_mode, out->mask, out->slots.p, ctx->d_status);
         AMJ_CUDA_TRY(cudaGetLastError());
@@ -243,7 +252,9 @@ int build_hash_index(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, uint
         if (nb * CUCKOO_SLOTS > (1ull << 31)) return fail(AMJ_EINVAL, "cuckoo: capacity too large");
         out->mask = (uint32_t)(nb - 1);
         AMJ_TRY(out->slots.alloc(ctx, nb * CUCKOO_SLOTS));
+        note_launch(ctx);
         fill_slots_kernel<<<grid_for(ctx, nb * CUCKOO_SLOTS), 256, 0, ctx->stream>>>(out->slots.p, nb * CUCKOO_SLOTS);
+        note_launch(ctx);
         cuckoo_insert_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(
             d_cols[0], ncols > 1 ? d_cols[1] : nullptr, n, key_mode, out->mask, out->slots.p, 256, ctx->d_status);
         AMJ_CUDA_TRY(cudaGetLastError());
@@ -269,12 +280,15 @@ extern "C" int amj_bucket_build(amj_ctx *ctx, const int32_t *d_keys, uint64_t n,
         DBuf<uint64_t> a, b;
         AMJ_TRY(a.alloc(ctx, n));
         AMJ_TRY(b.alloc(ctx, n));
+        note_launch(ctx);
         pack_key_rowid_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_keys, n, a.p);
         AMJ_CUDA_TRY(cudaGetLastError());
         uint64_t *sorted = nullptr;
         AMJ_TRY(radix_sort_u64(ctx, a.p, b.p, n, SK_LOW32, 0, log2_exact(buckets), &sorted));
+        note_launch(ctx);
         unpack_pairs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, d_hash_keys,
                                                                         (int32_t *)d_idx_in_origin);
+        note_launch(ctx);
         bucket_hist_sorted_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, KEY_SINGLE, mask, d_buc_ptrs);
         AMJ_CUDA_TRY(cudaGetLastError());
     }

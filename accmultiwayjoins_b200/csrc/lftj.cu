@@ -54,6 +54,13 @@ struct TriArgs {
     int32_t *out[3];
     uint64_t out_cap;
     int small_sum;   // merge by one lane when |X|+|Y| <= small_sum
+    // heavy vertices (bitmap kernel): R's level-0 entries with at least
+    // heavy_deg children whose T-children span at most bitmap_bits values
+    TrieRef R;
+    uint64_t r_lo, r_hi;          // R level-1 slice handled by this launch
+    unsigned long long *cursor0;  // level-0 claim cursor of the bitmap kernel
+    uint32_t heavy_deg;           // 0: no bitmap kernel
+    uint32_t bitmap_bits;
 };
 
 __device__ __forceinline__ void child_range(const TrieRef &t, int32_t v, uint64_t &s, uint64_t &e) {
@@ -174,6 +181,160 @@ __device__ __forceinline__ void warp_intersect(const int32_t *X, uint64_t nx, co
     }
 }
 
+// A level-0 value a of R is "heavy" when it has at least heavy_deg children in
+// R and its children in T span at most bitmap_bits values: its edges are
+// then joined by the bitmap kernel, all others by the warp kernel.
+__device__ __forceinline__ bool heavy_vertex(const TriArgs &A, uint64_t r_deg, uint64_t ta, uint64_t ea,
+                                             int32_t &lo, uint32_t &span) {
+    if (A.heavy_deg == 0 || r_deg < A.heavy_deg || ea <= ta) return false;
+    lo = A.T.data1[ta];
+    const int64_t sp = (int64_t)A.T.data1[ea - 1] - (int64_t)lo + 1;
+    span = (uint32_t)sp;
+    return sp > 0 && sp <= (int64_t)A.bitmap_bits;
+}
+
+constexpr int BM_THREADS = 1024;
+constexpr int BM_UNROLL = 8;
+
+// Bitmap kernel: one block per heavy vertex a at a time.  The children of a
+// in T are set in a shared-memory bitmap (one bit per value in their span,
+// up to 2^20 values = 128 KB); then the children lists of every b in a's
+// R-children are streamed through the block, 1024 edges per batch, with a
+// block scan over their lengths so every thread takes one candidate c per
+// step (load-balanced, coalesced) and tests bit c.  Each child list is read
+// once per (a,b) and tested with one shared-memory load, instead of a
+// galloping search per needle window.
+template <bool WRITE>
+__global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __grid_constant__ TriArgs A) {
+    extern __shared__ __align__(16) unsigned char bm_smem[];
+    const uint32_t words = (A.bitmap_bits + 31) / 32;
+    uint32_t *bits = (uint32_t *)bm_smem;
+    unsigned long long *pre = (unsigned long long *)(bm_smem + (size_t)words * 4);  // inclusive
+    unsigned long long *hab = pre + BM_THREADS;
+    uint32_t *sbeg = (uint32_t *)(hab + BM_THREADS);
+    int32_t *bval = (int32_t *)(sbeg + BM_THREADS);
+    __shared__ unsigned long long s_i;
+    __shared__ unsigned long long s_wsum[BM_THREADS / 32 + 1];
+    __shared__ uint32_t s_next;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (uint32_t w = tid; w < words; w += BM_THREADS) bits[w] = 0u;
+    unsigned long long cnt = 0, chk = 0;
+    __syncthreads();
+    while (true) {
+        if (tid == 0) s_i = atomicAdd(A.cursor0, 1ull);
+        __syncthreads();
+        const unsigned long long i = s_i;
+        __syncthreads();
+        if (i >= A.R.len0) break;
+        const uint64_t rs = A.R.off0[i], re = A.R.off0[i + 1];
+        const uint64_t es = rs > A.r_lo ? rs : A.r_lo, ee = re < A.r_hi ? re : A.r_hi;
+        if (es >= ee) continue;
+        const int32_t a = A.R.data0[i];
+        uint64_t ta, ea;
+        child_range(A.T, a, ta, ea);
+        int32_t lo = 0;
+        uint32_t span = 0;
+        if (!heavy_vertex(A, re - rs, ta, ea, lo, span)) continue;
+        for (uint64_t k = ta + tid; k < ea; k += BM_THREADS) {
+            const uint32_t r = (uint32_t)(A.T.data1[k] - lo);
+            atomicOr(&bits[r >> 5], 1u << (r & 31));
+        }
+        const uint64_t ha = amj_hash_step(AMJ_CHECKSUM_SEED, a);
+        __syncthreads();
+        for (uint64_t bs = es; bs < ee; bs += BM_THREADS) {
+            const uint64_t j = bs + tid;
+            unsigned long long len = 0;
+            uint64_t sb = 0, eb = 0;
+            int32_t b = 0;
+            if (j < ee) {
+                b = A.R.data1[j];
+                child_range(A.S, b, sb, eb);
+                len = eb - sb;
+            }
+            // block inclusive scan of len
+            unsigned long long incl = warp_inclusive_scan(len, lane);
+            if (lane == 31) s_wsum[warp] = incl;
+            __syncthreads();
+            if (warp == 0) {
+                unsigned long long w = lane < BM_THREADS / 32 ? s_wsum[lane] : 0ull;
+                unsigned long long wi = warp_inclusive_scan(w, lane);
+                s_wsum[lane] = wi - w;
+                if (lane == 31) s_wsum[BM_THREADS / 32] = wi;
+            }
+            __syncthreads();
+            pre[tid] = s_wsum[warp] + incl;
+            sbeg[tid] = (uint32_t)sb;
+            hab[tid] = amj_hash_step(ha, b);
+            bval[tid] = b;
+            const uint32_t nb = (uint32_t)((ee - bs) < BM_THREADS ? (ee - bs) : BM_THREADS);
+            __syncthreads();
+            // warps claim child lists of the batch one at a time and stream
+            // each list 32 x BM_UNROLL values per step (all loads in flight
+            // before the bit tests); the owner of a value is the list itself
+            if (tid == 0) s_next = 0;
+            __syncthreads();
+            while (true) {
+                uint32_t li = 0;
+                if (lane == 0) li = atomicAdd(&s_next, 1u);
+                li = __shfl_sync(AMJ_FULL_MASK, li, 0);
+                if (li >= nb) break;
+                const unsigned long long lbeg = li ? pre[li - 1] : 0ull;
+                const uint32_t len = (uint32_t)(pre[li] - lbeg);
+                const int32_t *lst = A.S.data1 + sbeg[li];
+                const uint64_t hb = hab[li];
+                for (uint32_t k0 = 0; k0 < len; k0 += 32 * BM_UNROLL) {
+                    int32_t cv[BM_UNROLL];
+#pragma unroll
+                    for (int u = 0; u < BM_UNROLL; u++) {
+                        const uint32_t k = k0 + u * 32 + lane;
+                        cv[u] = k < len ? lst[k] : lo - 1;
+                    }
+#pragma unroll
+                    for (int u = 0; u < BM_UNROLL; u++) {
+                        const int32_t c = cv[u];
+                        const int64_t r = (int64_t)c - (int64_t)lo;
+                        const bool hit = r >= 0 && r < (int64_t)span &&
+                                         ((bits[(uint32_t)r >> 5] >> ((uint32_t)r & 31)) & 1u);
+                        if (!WRITE) {
+                            if (hit) {
+                                cnt++;
+                                chk += amj_hash_step(hb, c);
+                            }
+                        } else {
+                            const unsigned m = __ballot_sync(AMJ_FULL_MASK, hit);
+                            if (m) {
+                                unsigned long long base = 0;
+                                if (lane == 0) base = atomicAdd(A.out_cursor, (unsigned long long)__popc(m));
+                                base = __shfl_sync(AMJ_FULL_MASK, base, 0);
+                                if (hit) {
+                                    cnt++;
+                                    chk += amj_hash_step(hb, c);
+                                    const unsigned long long p = base + __popc(m & lanemask_lt());
+                                    if (p < A.out_cap) {
+                                        A.out[0][p] = a; A.out[1][p] = bval[li]; A.out[2][p] = c;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        for (uint64_t k = ta + tid; k < ea; k += BM_THREADS) {
+            const uint32_t r = (uint32_t)(A.T.data1[k] - lo);
+            bits[r >> 5] = 0u;
+        }
+        __syncthreads();
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if (lane == 0 && cnt) {
+        atomicAdd(A.count, cnt);
+        atomicAdd(A.checksum, chk);
+    }
+}
+
 template <bool WRITE>
 __global__ __launch_bounds__(256) void lftj_tri_dfs_kernel(const __grid_constant__ TriArgs A) {
     const int lane = threadIdx.x & 31;
@@ -192,6 +353,13 @@ __global__ __launch_bounds__(256) void lftj_tri_dfs_kernel(const __grid_constant
             b = A.r_dst[j];
             child_range(A.S, b, sb, eb);
             if (eb > sb) child_range(A.T, a, ta, ea);
+            if (A.heavy_deg && ea > ta) {
+                uint64_t rs, re;
+                child_range(A.R, a, rs, re);
+                int32_t lo;
+                uint32_t span;
+                if (heavy_vertex(A, re - rs, ta, ea, lo, span)) sb = eb = 0;  // the bitmap kernel owns this edge
+            }
         }
         const uint64_t lb = eb - sb, la = ea - ta;
         const bool active = valid && lb && la;
@@ -386,7 +554,7 @@ __global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const 
 // ---- host side ----
 
 struct LftjCounters {
-    unsigned long long cursor, count, checksum, out_cursor;
+    unsigned long long cursor, count, checksum, out_cursor, cursor0;
 };
 
 static TrieRef trie_ref(const Trie2 &t) {
@@ -406,7 +574,7 @@ static TrieRef trie_ref(const Trie2 &t) {
 // written too (out_cap rows available).
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
-                  uint64_t r_lo, uint64_t r_hi) {
+                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg) {
     TriArgs A{};
     if (r_hi > R.len1) r_hi = R.len1;
     if (r_lo > r_hi) r_lo = r_hi;
@@ -415,6 +583,9 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
     A.r_n = r_hi - r_lo;
     A.S = trie_ref(S);
     A.T = trie_ref(T);
+    A.R = trie_ref(R);
+    A.r_lo = r_lo;
+    A.r_hi = r_hi;
     A.small_sum = small_sum;
     DBuf<LftjCounters> ctr;
     AMJ_TRY(ctr.alloc(ctx, 1));
@@ -423,6 +594,7 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
     A.count = &ctr.p->count;
     A.checksum = &ctr.p->checksum;
     A.out_cursor = &ctr.p->out_cursor;
+    A.cursor0 = &ctr.p->cursor0;
     const bool write = out != nullptr;
     if (write) {
         for (int i = 0; i < 3; i++) A.out[i] = out[i];
@@ -430,11 +602,26 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
     }
     if (A.r_n) {
         if (algo == AMJ_LFTJ_DFS) {
+            if (heavy_deg) {
+                // the bitmap kernel takes the heavy vertices; its shared memory: bitmap + 1024 x 24 B
+                const uint32_t bits_max = 1u << 20;
+                const size_t smem = (size_t)bits_max / 8 + (size_t)BM_THREADS * (8 + 8 + 4 + 4);
+                if (smem <= (size_t)ctx->max_smem_optin) {
+                    A.heavy_deg = heavy_deg;
+                    A.bitmap_bits = bits_max;
+                    auto kb = write ? lftj_tri_bitmap_kernel<true> : lftj_tri_bitmap_kernel<false>;
+                    AMJ_CUDA_TRY(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                    note_launch(ctx);
+                    kb<<<(unsigned)ctx->num_sms, BM_THREADS, smem, ctx->stream>>>(A);
+                    AMJ_CUDA_TRY(cudaGetLastError());
+                }
+            }
             int per_sm = 0;
             AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                 &per_sm, write ? lftj_tri_dfs_kernel<true> : lftj_tri_dfs_kernel<false>, 256, 0));
             if (per_sm < 1) per_sm = 1;
             const unsigned grid = (unsigned)(ctx->num_sms * per_sm);
+            note_launch(ctx);
             if (write) lftj_tri_dfs_kernel<true><<<grid, 256, 0, ctx->stream>>>(A);
             else lftj_tri_dfs_kernel<false><<<grid, 256, 0, ctx->stream>>>(A);
             AMJ_CUDA_TRY(cudaGetLastError());
@@ -442,6 +629,7 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
             DBuf<unsigned long long> cand;
             AMJ_TRY(cand.alloc(ctx, A.r_n + 1));
             const unsigned g1 = (unsigned)std::min<uint64_t>((A.r_n + 255) / 256, (uint64_t)ctx->num_sms * 16);
+            note_launch(ctx);
             lftj_tri_bfs_count_kernel<<<g1, 256, 0, ctx->stream>>>(A, cand.p);
             AMJ_CUDA_TRY(cudaGetLastError());
             AMJ_TRY(scan_exclusive_u64(ctx, (const uint64_t *)cand.p, (uint64_t *)cand.p, A.r_n,
@@ -457,6 +645,7 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
                 if (per_sm < 1) per_sm = 1;
                 const uint64_t tiles = (total + BFS_TILE - 1) / BFS_TILE;
                 const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)ctx->num_sms * per_sm);
+                note_launch(ctx);
                 if (write)
                     lftj_tri_bfs_expand_kernel<true><<<grid, BFS_THREADS, 0, ctx->stream>>>(A, cand.p, total);
                 else

@@ -17,7 +17,7 @@
 namespace amj {
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
-                  uint64_t r_lo, uint64_t r_hi);
+                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg);
 }
 
 using namespace amj;
@@ -64,6 +64,8 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     // ws=0: every (a,b) pair intersected by its own lane; ws=1: long pairs
     // shared by the whole warp
     const int small_sum = ws ? 48 : 0x7fffffff;
+    // ws=1 also hands vertices with many children to the block-wide bitmap kernel
+    const uint32_t heavy_deg = ws ? (ctx->opts.lftj_heavy_degree ? ctx->opts.lftj_heavy_degree : 32u) : 0u;
     const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
     const uint64_t nr = R->len1;
     uint64_t slice = nr;
@@ -78,14 +80,14 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     for (uint64_t lo = 0; rc == AMJ_OK && (lo < nr || (lo == 0 && nr == 0)); lo += slice) {
         const uint64_t hi = std::min(nr, lo + slice);
         uint64_t c = 0, h = 0, w = 0;
-        rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, lo, hi);
+        rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, lo, hi, heavy_deg);
         if (rc != AMJ_OK) break;
         if (materialize) {
             int32_t *cols[3] = {nullptr, nullptr, nullptr};
             for (int a = 0; a < 3 && rc == AMJ_OK; a++) rc = dev_alloc(ctx, (void **)&cols[a], (c ? c : 1) * 4);
             uint64_t c2 = 0, h2 = 0;
             if (rc == AMJ_OK)
-                rc = lftj_triangle(ctx, *R, *S, *T, algo, cols, c, &c2, &h2, &w, small_sum, lo, hi);
+                rc = lftj_triangle(ctx, *R, *S, *T, algo, cols, c, &c2, &h2, &w, small_sum, lo, hi, heavy_deg);
             if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
                 rc = fail(AMJ_ECUDA, "LFTJ: write pass disagrees with count pass");
             if (rc == AMJ_OK && ooc) {

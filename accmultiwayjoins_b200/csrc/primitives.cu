@@ -102,15 +102,18 @@ static int scan_exclusive_impl(amj_ctx *ctx, const T *in, T *out, uint64_t n, T 
     const uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (tiles > 0x7fffffffull) return fail(AMJ_EINVAL, "scan: input too large");
     if (tiles == 1) {
+        note_launch(ctx);
         scan_tiles_kernel<T><<<1, SCAN_THREADS, 0, ctx->stream>>>(in, out, n, nullptr, d_total);
         AMJ_CUDA_TRY(cudaGetLastError());
         return AMJ_OK;
     }
     DBuf<T> partial;
     AMJ_TRY(partial.alloc(ctx, tiles));
+    note_launch(ctx);
     scan_reduce_kernel<T><<<(unsigned)tiles, SCAN_THREADS, 0, ctx->stream>>>(in, n, partial.p);
     AMJ_CUDA_TRY(cudaGetLastError());
     AMJ_TRY(scan_exclusive_impl<T>(ctx, partial.p, partial.p, tiles, nullptr));
+    note_launch(ctx);
     scan_tiles_kernel<T><<<(unsigned)tiles, SCAN_THREADS, 0, ctx->stream>>>(in, out, n, partial.p, d_total);
     AMJ_CUDA_TRY(cudaGetLastError());
     return AMJ_OK;
@@ -261,10 +264,12 @@ static int radix_sort_impl(amj_ctx *ctx, uint64_t *d_a, uint64_t *d_b, uint64_t 
         const int shift = lo_bit + p * width;
         const int bits = (hi_bit - shift) < width ? (hi_bit - shift) : width;
         if (bits <= 0) break;
+        note_launch(ctx);
         rs_upsweep_kernel<KK><<<nblocks, RS_THREADS, 0, ctx->stream>>>(src, (uint32_t)n, shift, bits, counts.p,
                                                                        nblocks);
         AMJ_CUDA_TRY(cudaGetLastError());
         AMJ_TRY(scan_exclusive_u32(ctx, counts.p, counts.p, (uint64_t)(1u << bits) * nblocks, nullptr));
+        note_launch(ctx);
         rs_downsweep_kernel<KK><<<nblocks, RS_THREADS, 0, ctx->stream>>>(src, dst, (uint32_t)n, shift, bits,
                                                                          counts.p, nblocks);
         AMJ_CUDA_TRY(cudaGetLastError());

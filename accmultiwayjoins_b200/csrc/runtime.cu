@@ -83,9 +83,36 @@ int status_check(amj_ctx *ctx, const char *what) {
     return fail(code, msg);
 }
 
+// A wait on a flag that nothing sets: it must give up after limit_ns, record
+// AMJ_ETIMEOUT in the status block and return, leaving the context usable.
+__global__ void bounded_wait_kernel(const unsigned int *flag, unsigned long long limit_ns, DevStatus *st) {
+    const unsigned long long t0 = globaltimer_ns();
+    while (ld_volatile_u32(flag) == 0u) {
+        if (globaltimer_ns() - t0 > limit_ns) {
+            report_error(st, (unsigned)-AMJ_ETIMEOUT, SITE_TEST_WAIT, limit_ns);
+            return;
+        }
+        __nanosleep(1000);
+    }
+}
+
 }  // namespace amj
 
 using namespace amj;
+
+extern "C" int amj_selftest_bounded_wait(amj_ctx *ctx, uint32_t limit_ms) {
+    if (!ctx || limit_ms == 0 || limit_ms > 60000) return fail(AMJ_EINVAL, "selftest_bounded_wait: bad arguments");
+    DBuf<unsigned int> flag;
+    AMJ_TRY(flag.alloc(ctx, 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(flag.p, 0, sizeof(unsigned int), ctx->stream));
+    AMJ_TRY(status_reset(ctx));
+    note_launch(ctx);
+    bounded_wait_kernel<<<1, 32, 0, ctx->stream>>>(flag.p, (unsigned long long)limit_ms * 1000000ull, ctx->d_status);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    int rc = status_check(ctx, "selftest_bounded_wait");
+    (void)status_reset(ctx);
+    return rc;
+}
 
 extern "C" const char *amj_last_error(void) { return g_last_error.c_str(); }
 extern "C" const char *amj_version(void) { return "amj 0.1.0 (sm_100a)"; }
@@ -168,6 +195,12 @@ extern "C" int amj_ctx_set_stream(amj_ctx *c, void *s) {
 extern "C" int amj_ctx_sync(amj_ctx *c) {
     if (!c) return fail(AMJ_EINVAL, "ctx_sync: null ctx");
     AMJ_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return AMJ_OK;
+}
+
+extern "C" int amj_ctx_launch_count(const amj_ctx *c, uint64_t *out) {
+    if (!c || !out) return fail(AMJ_EINVAL, "ctx_launch_count: null argument");
+    *out = c->launches;
     return AMJ_OK;
 }
 

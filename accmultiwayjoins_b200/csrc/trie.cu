@@ -112,6 +112,7 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
     AMJ_TRY(mm.alloc(ctx, 8));
     const uint32_t init[4] = {0xffffffffu, 0u, 0xffffffffu, 0u};
     AMJ_CUDA_TRY(cudaMemcpyAsync(mm.p, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    note_launch(ctx);
     minmax_pairs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_c0, d_c1, n, mm.p);
     AMJ_CUDA_TRY(cudaGetLastError());
     uint32_t h_mm[4];
@@ -123,6 +124,7 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
     DBuf<uint64_t> a, b;
     AMJ_TRY(a.alloc(ctx, n));
     AMJ_TRY(b.alloc(ctx, n));
+    note_launch(ctx);
     pack_trie_keys_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_c0, d_c1, n, min0, min1, bits1, a.p);
     AMJ_CUDA_TRY(cudaGetLastError());
     uint64_t *sorted = nullptr;
@@ -132,6 +134,7 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
     AMJ_TRY(out->src1.alloc(ctx, n));
     DBuf<uint32_t> head;
     AMJ_TRY(head.alloc(ctx, n + 1));
+    note_launch(ctx);
     unpack_trie_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, min0, min1, bits1, out->data1.p,
                                                                    out->src1.p, head.p);
     AMJ_CUDA_TRY(cudaGetLastError());
@@ -142,6 +145,7 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
     out->len0 = len0;
     AMJ_TRY(out->data0.alloc(ctx, len0));
     AMJ_TRY(out->off0.alloc(ctx, (uint64_t)len0 + 1));
+    note_launch(ctx);
     scatter_level0_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, head.p, head.p, n, min0, bits1,
                                                                       out->data0.p, out->off0.p, len0);
     AMJ_CUDA_TRY(cudaGetLastError());
@@ -152,6 +156,7 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
         out->rp_count = range;
         AMJ_TRY(out->rowptr.alloc(ctx, range + 1));
         AMJ_CUDA_TRY(cudaMemsetAsync(out->rowptr.p, 0, (range + 1) * sizeof(uint64_t), ctx->stream));
+        note_launch(ctx);
         dense_counts_kernel<<<grid_for(ctx, len0), 256, 0, ctx->stream>>>(out->data0.p, out->off0.p, len0,
                                                                           out->rp_min, out->rowptr.p);
         AMJ_CUDA_TRY(cudaGetLastError());
@@ -190,6 +195,18 @@ extern "C" int amj_trie_view(const amj_trie *t, uint64_t *len0, uint64_t *len1, 
     if (d_data0) *d_data0 = t->t.data0.p;
     if (d_offsets0) *d_offsets0 = t->t.off0.p;
     if (d_data1) *d_data1 = t->t.data1.p;
+    return AMJ_OK;
+}
+
+extern "C" int amj_trie_download(const amj_trie *t, int32_t *data0, uint64_t *offsets0, int32_t *data1) {
+    if (!t || !data0 || !offsets0 || !data1) return fail(AMJ_EINVAL, "trie_download: null argument");
+    amj_ctx *ctx = t->ctx;
+    if (t->t.len0)
+        AMJ_CUDA_TRY(cudaMemcpyAsync(data0, t->t.data0.p, t->t.len0 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (t->t.len1)
+        AMJ_CUDA_TRY(cudaMemcpyAsync(data1, t->t.data1.p, t->t.len1 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(offsets0, t->t.off0.p, (t->t.len0 + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return AMJ_OK;
 }
 

@@ -89,6 +89,9 @@ typedef struct amj_opts {
     uint64_t task_capacity;    /* work-sharing queue capacity in tasks (0: 1<<20) */
     uint64_t ooc_slice_rows;   /* ooc probe slice rows (0: derived from budget)   */
     uint64_t mem_budget;       /* device bytes the ooc planner may use (0: free/2) */
+    uint32_t lftj_heavy_degree; /* ALFTJ ws=1: children count from which a vertex is
+                                   joined by the block-wide bitmap kernel (0: 32)  */
+    float    dro_headroom;     /* DRO output estimate multiplier (0: 1.05)        */
 } amj_opts;
 
 typedef struct amj_result {
@@ -113,6 +116,8 @@ void amj_ctx_destroy(amj_ctx *ctx);
 int  amj_ctx_set_stream(amj_ctx *ctx, void *cuda_stream);
 int  amj_ctx_sync(amj_ctx *ctx);
 const char *amj_stat_name(int i);
+/* number of kernels this context has launched (all entry points) */
+int  amj_ctx_launch_count(const amj_ctx *ctx, uint64_t *out);
 
 /* ---- relations (MHJ-GPU/Relation.cuh:9-38) ---- */
 int  amj_rel_create(amj_ctx *ctx, uint64_t n, int ncols, const uint32_t *attrs,
@@ -157,11 +162,20 @@ int  amj_trie_build(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint
 int  amj_trie_view(const amj_trie *t, uint64_t *len0, uint64_t *len1,
                    const int32_t **d_data0, const uint64_t **d_offsets0,
                    const int32_t **d_data1);
+/* copy a trie's three arrays to host memory (len0, len0+1, len1 entries) */
+int  amj_trie_download(const amj_trie *t, int32_t *data0, uint64_t *offsets0, int32_t *data1);
 /* .tr serialisation, byte layout of IndexedTrie::serialization
  * (LFTJ-GPU/IndexedTrie.cuh:122-156) with attrs {a0,a1} */
 int  amj_trie_save(const amj_trie *t, const char *path, uint32_t a0, uint32_t a1);
 int  amj_trie_load(amj_ctx *ctx, const char *path, amj_trie **out, uint32_t *a0, uint32_t *a1);
 void amj_trie_release(amj_trie *t);
+
+/* ---- failure detection self-test ----
+ * Launches a kernel that waits on a device flag nothing sets.  The wait is
+ * bounded by limit_ms (%globaltimer); the call must return AMJ_ETIMEOUT and
+ * the context must stay usable.  The same bounded-wait-and-report pattern
+ * guards every device-side wait of the operators (work-sharing queue). */
+int  amj_selftest_bounded_wait(amj_ctx *ctx, uint32_t limit_ms);
 
 /* ---- seeded synthetic data (host, deterministic, OpenMP) ---- */
 int  amj_gen_uniform_i32(int32_t *out, uint64_t n, int64_t lo, int64_t hi_excl,

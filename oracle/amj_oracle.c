@@ -70,12 +70,14 @@ static int cmp_i64(const void *a, const void *b) {
     return x < y ? -1 : x > y;
 }
 
-/* pack (c0, c1) so that signed lexicographic order is integer order */
+/* pack (c0, c1) so that signed int64 order is (c0, c1) lexicographic order:
+ * c0 in the high half keeps its two's-complement sign bit, c1 in the low half
+ * is sign-flipped so its unsigned magnitude orders like the signed value */
 static int64_t pack_pair(int32_t a, int32_t b) {
-    return (int64_t)(((uint64_t)(uint32_t)a << 32) | (uint32_t)b) ^ (int64_t)0x8000000080000000ull;
+    return (int64_t)(((uint64_t)(uint32_t)a << 32) | ((uint32_t)b ^ 0x80000000u));
 }
-static int32_t pair_c0(int64_t p) { return (int32_t)(uint32_t)(((uint64_t)p ^ 0x8000000080000000ull) >> 32); }
-static int32_t pair_c1(int64_t p) { return (int32_t)(uint32_t)((uint64_t)p ^ 0x8000000080000000ull); }
+static int32_t pair_c0(int64_t p) { return (int32_t)(uint32_t)((uint64_t)p >> 32); }
+static int32_t pair_c1(int64_t p) { return (int32_t)((uint32_t)(uint64_t)p ^ 0x80000000u); }
 
 int orc_trie_build(const int32_t *c0, const int32_t *c1, uint64_t n, int32_t *data0, uint64_t *off0, int32_t *data1,
                    uint64_t *len0) {

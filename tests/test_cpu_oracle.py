@@ -1,0 +1,158 @@
+"""The CPU oracle pinned against the reference's MHJ-CPU, the committed
+golden fixtures (outputs of MHJ-CPU run here) and brute force."""
+import json
+import os
+from collections import defaultdict
+
+import numpy as np
+import pytest
+
+from accmultiwayjoins_b200 import data
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden.json")
+M64 = (1 << 64) - 1
+
+
+def mix(z):
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+    return z ^ (z >> 31)
+
+
+def tuple_hash(vals):
+    h = 0x9E3779B97F4A7C15
+    for v in vals:
+        h = mix(h ^ (int(v) & 0xFFFFFFFF))
+    return h
+
+
+def brute_join(relations):
+    """Nested-loop natural join of small relations, in query order."""
+    k = 1 + max(a for _, attrs in relations for a in attrs)
+    rows = []
+    cols0, attrs0 = relations[0]
+    for i in range(len(cols0[0])):
+        t = [None] * k
+        for c, a in zip(cols0, attrs0):
+            t[a] = int(c[i])
+        rows.append(t)
+    for cols, attrs in relations[1:]:
+        new = []
+        for t in rows:
+            for i in range(len(cols[0])):
+                ok = all(t[a] is None or t[a] == int(c[i]) for c, a in zip(cols, attrs))
+                if ok:
+                    u = list(t)
+                    for c, a in zip(cols, attrs):
+                        u[a] = int(c[i])
+                    new.append(u)
+        rows = new
+    return len(rows), sum(tuple_hash(t) for t in rows) & M64, sorted(tuple(t) for t in rows)
+
+
+def load_golden():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+def make_case(case):
+    kind = case["kind"]
+    if kind == "chain":
+        return data.chain_relations(case["n"], case["key_range"], case["nrels"], seed=case["seed"])
+    if kind == "star":
+        fact, dims = data.star_relations(case["fact_rows"], case["dims"], theta=case["theta"], seed=case["seed"])
+        return [fact] + dims
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("case", load_golden()["cases"], ids=lambda c: c["name"])
+def test_oracle_matches_golden(built, case):
+    rels = make_case(case)
+    cnt, chk = O.mhj(rels)
+    assert cnt == case["count"]
+    assert f"{chk:016x}" == case["checksum"]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference MHJ-CPU harness not built (reference sources absent)")
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_oracle_matches_reference_mhj_cpu(built, seed):
+    rels = data.chain_relations(20000, 1 << 12, 3, seed=seed)
+    ref_cnt, ref_chk, _ = O.mhj_reference(rels, nthreads=4)
+    assert O.mhj(rels) == (ref_cnt, ref_chk)
+    fact, dims = data.star_relations(30000, [2000, 500, 100, 10], seed=seed)
+    rels = [fact] + dims
+    ref_cnt, ref_chk, _ = O.mhj_reference(rels, nthreads=3)
+    assert O.mhj(rels) == (ref_cnt, ref_chk)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference MHJ-CPU harness not built (reference sources absent)")
+def test_reference_tuples_equal_oracle_tuples(built):
+    rels = data.chain_relations(3000, 1 << 9, 4, seed=5)
+    cnt, chk, _, cols = O.mhj_reference(rels, nthreads=2, tuples=True)
+    ocnt, ochk, ocols = O.mhj(rels, tuples=True)
+    assert (cnt, chk) == (ocnt, ochk)
+    a = np.stack(cols, 1)
+    b = np.stack(ocols, 1)
+    assert np.array_equal(a[np.lexsort(a.T[::-1])], b[np.lexsort(b.T[::-1])])
+
+
+def test_oracle_matches_brute_force_small(built):
+    rels = data.chain_relations(60, 12, 3, seed=9)
+    cnt, chk, tuples = brute_join(rels)
+    assert O.mhj(rels) == (cnt, chk)
+    ocnt, ochk, ocols = O.mhj(rels, tuples=True)
+    got = sorted(tuple(int(x) for x in r) for r in np.stack(ocols, 1))
+    assert got == tuples
+
+
+def test_oracle_negative_and_duplicate_keys(built):
+    r1 = ([np.array([-5, -5, 7, 2**31 - 1], np.int32), np.array([-1, -1, 3, -2**31], np.int32)], [0, 1])
+    r2 = ([np.array([-1, -1, -2**31, 3], np.int32), np.array([10, 11, 12, 13], np.int32)], [1, 2])
+    rels = [r1, r2]
+    cnt, chk, _ = brute_join(rels)
+    assert O.mhj(rels) == (cnt, chk)
+
+
+def test_triangle_and_four_restatements_agree_with_join_patterns(built):
+    s, d = data.rmat(9, 5000, 0.57, 0.19, 0.19, seed=4)
+    tri = O.triangle(s, d)
+    assert tri == O.mhj([([s, d], [0, 1]), ([s, d], [1, 2]), ([s, d], [0, 2])])
+    four = O.four_clique(s, d)
+    pat = [(0, 1), (1, 2), (2, 3), (0, 3), (0, 2), (1, 3)]
+    assert four == O.mhj([([s, d], list(p)) for p in pat])
+
+
+def test_triangle_bag_semantics_with_duplicates(built):
+    s = np.array([0, 0, 1, 0, 0], np.int32)
+    d = np.array([1, 2, 2, 1, 2], np.int32)
+    rels = [([s, d], [0, 1]), ([s, d], [1, 2]), ([s, d], [0, 2])]
+    cnt, chk, _ = brute_join(rels)
+    assert O.triangle(s, d) == (cnt, chk)
+
+
+def test_trie_build_oracle_is_a_csr(built):
+    s, d = data.rmat(10, 8000, 0.57, 0.19, 0.19, seed=2)
+    d0, o0, d1 = O.trie_build(s, d)
+    order = np.lexsort((d, s))
+    assert np.array_equal(d1, d[order])
+    assert np.array_equal(d0, np.unique(s))
+    counts = np.bincount(np.searchsorted(d0, s), minlength=len(d0))
+    assert np.array_equal(np.diff(o0.astype(np.int64)), counts)
+
+
+def test_bucket_build_oracle(built):
+    keys = data.uniform(5000, -1000, 1000, seed=3)
+    hk, idx, bp = O.bucket_build(keys, 1024)
+    assert bp[0] == 0 and bp[-1] == 5000
+    for b in range(1024):
+        seg = idx[bp[b]:bp[b + 1]]
+        assert np.all(np.diff(seg.astype(np.int64)) > 0)
+        assert np.all((keys[seg].astype(np.int64) & 1023) == b)
+    assert np.array_equal(hk, keys[idx])
+
+
+def test_checksum_definition_matches_python(built):
+    cols = [data.uniform(100, -50, 50, seed=1, stream=s) for s in range(3)]
+    want = sum(tuple_hash(t) for t in zip(*cols)) & M64
+    assert data.checksum(cols) == want

@@ -1,0 +1,395 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle: counts,
+checksums and, at small sizes, sorted tuples; edge cases; every switch of
+exec-AMHJ / exec-LFTJ; full-size property checks."""
+import ctypes as C
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from accmultiwayjoins_b200 import AmjError, Context, _lib as L, data
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden", "golden.json")
+
+
+def sorted_rows(cols):
+    a = np.stack([np.asarray(c, np.int64) for c in cols], 1)
+    if a.shape[0] == 0:
+        return a
+    return a[np.lexsort(a.T[::-1])]
+
+
+def rels_on(ctx, rels):
+    return [ctx.relation(c, a) for c, a in rels]
+
+
+# ------------------------------------------------------------ building blocks
+
+@pytest.mark.parametrize("n,B,lo,hi", [(0, 1, 0, 1), (1, 1, 5, 6), (1000, 512, 0, 1000), (1 << 20, 1 << 19, 0, 1 << 18),
+                                       (3_000_000, 1 << 21, -(1 << 30), 1 << 30), (100000, 1 << 16, 7, 8)])
+def test_bucket_build_matches_oracle(ctx, n, B, lo, hi):
+    import torch
+    keys = data.uniform(n, lo, hi, seed=5) if n else np.zeros(0, np.int32)
+    dk = torch.from_numpy(keys).cuda() if n else torch.zeros(1, dtype=torch.int32, device="cuda")
+    hk = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    idx = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    bp = torch.empty(B + 1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    L.check(L.load().amj_bucket_build(ctx.handle, dk.data_ptr(), n, B, hk.data_ptr(), idx.data_ptr(), bp.data_ptr()))
+    ohk, oidx, obp = O.bucket_build(keys, B)
+    assert np.array_equal(bp.cpu().numpy().view(np.uint32), obp)
+    assert np.array_equal(hk.cpu().numpy()[:n], ohk)
+    assert np.array_equal(idx.cpu().numpy()[:n].view(np.uint32), oidx)
+
+
+def trie_arrays(ctx, s, d):
+    import torch
+    lib = L.load()
+    ds, dd = torch.from_numpy(s).cuda(), torch.from_numpy(d).cuda()
+    h = C.c_void_p()
+    L.check(lib.amj_trie_build(ctx.handle, ds.data_ptr(), dd.data_ptr(), len(s), C.byref(h)))
+    l0, l1 = C.c_uint64(), C.c_uint64()
+    L.check(lib.amj_trie_view(h, C.byref(l0), C.byref(l1), None, None, None))
+    a0 = np.empty(max(l0.value, 1), np.int32)
+    ao = np.empty(l0.value + 1, np.uint64)
+    a1 = np.empty(max(l1.value, 1), np.int32)
+    L.check(lib.amj_trie_download(h, a0.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  ao.ctypes.data_as(C.POINTER(C.c_uint64)), a1.ctypes.data_as(C.POINTER(C.c_int32))))
+    return h, a0[:l0.value], ao, a1[:l1.value]
+
+
+@pytest.mark.parametrize("case", ["small", "1M", "dups_negative"])
+def test_trie_build_matches_oracle(ctx, case):
+    if case == "small":
+        s, d = data.rmat(8, 2000, 0.57, 0.19, 0.19, 3)
+    elif case == "1M":
+        s, d = data.rmat(16, 1 << 20, 0.57, 0.19, 0.19, 3)
+    else:
+        s = data.uniform(50000, -(1 << 31), 1 << 31, seed=1)
+        s[::3] = s[0]
+        d = data.uniform(50000, -40, 40, seed=2)
+    h, a0, ao, a1 = trie_arrays(ctx, s, d)
+    L.load().amj_trie_release(h)
+    o0, oo, o1 = O.trie_build(s, d)
+    assert np.array_equal(a0, o0) and np.array_equal(ao, oo) and np.array_equal(a1, o1)
+
+
+def test_trie_tr_file_round_trip(ctx, tmp_path):
+    lib = L.load()
+    s, d = data.rmat(10, 8000, 0.57, 0.19, 0.19, 4)
+    h, a0, ao, a1 = trie_arrays(ctx, s, d)
+    p = str(tmp_path / "t.tr").encode()
+    L.check(lib.amj_trie_save(h, p, 0, 1))
+    h2 = C.c_void_p()
+    x0, x1 = C.c_uint32(), C.c_uint32()
+    L.check(lib.amj_trie_load(ctx.handle, p, C.byref(h2), C.byref(x0), C.byref(x1)))
+    assert (x0.value, x1.value) == (0, 1)
+    l0, l1 = C.c_uint64(), C.c_uint64()
+    L.check(lib.amj_trie_view(h2, C.byref(l0), C.byref(l1), None, None, None))
+    b0 = np.empty(l0.value, np.int32)
+    bo = np.empty(l0.value + 1, np.uint64)
+    b1 = np.empty(l1.value, np.int32)
+    L.check(lib.amj_trie_download(h2, b0.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  bo.ctypes.data_as(C.POINTER(C.c_uint64)), b1.ctypes.data_as(C.POINTER(C.c_int32))))
+    assert np.array_equal(a0, b0) and np.array_equal(ao, bo) and np.array_equal(a1, b1)
+    lib.amj_trie_release(h)
+    lib.amj_trie_release(h2)
+
+
+# ------------------------------------------------------------------- AMHJ
+
+SWITCHES = [dict(ws=0, dro=0, fib=0), dict(ws=1, dro=0, fib=0), dict(ws=0, dro=1, fib=0), dict(ws=1, dro=1, fib=0),
+            dict(ws=1, dro=0, fib=1)]
+
+
+@pytest.mark.parametrize("layout", ["bucket", "oa", "cuckoo"])
+@pytest.mark.parametrize("sw", SWITCHES, ids=lambda s: "ws{ws}dro{dro}fib{fib}".format(**s))
+@pytest.mark.parametrize("materialize", [False, True])
+def test_amhj_chain_all_switches(layout, sw, materialize):
+    with Context(0, layout=layout) as ctx:
+        rels = data.chain_relations(20000, 1 << 12, 3, seed=11)
+        got = ctx.amhj("NORMAL", rels_on(ctx, rels), materialize=materialize, **sw)
+        cnt, chk, cols = O.mhj(rels, tuples=True)
+        assert (got.count, got.checksum) == (cnt, chk)
+        if materialize:
+            assert np.array_equal(sorted_rows(got.columns), sorted_rows(cols))
+            assert data.checksum(got.columns) == chk
+
+
+@pytest.mark.parametrize("case", json.load(open(GOLDEN))["cases"], ids=lambda c: c["name"])
+def test_amhj_golden(ctx, case):
+    if case["kind"] == "chain":
+        rels = data.chain_relations(case["n"], case["key_range"], case["nrels"], seed=case["seed"])
+    else:
+        fact, dims = data.star_relations(case["fact_rows"], case["dims"], theta=case["theta"], seed=case["seed"])
+        rels = [fact] + dims
+    for ws in (0, 1):
+        got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=ws)
+        assert got.count == case["count"]
+        assert f"{got.checksum:016x}" == case["checksum"]
+
+
+@pytest.mark.parametrize("layout", ["bucket", "oa", "cuckoo"])
+def test_amhj_star(layout):
+    with Context(0, layout=layout) as ctx:
+        fact, dims = data.star_relations(200000, [20000, 4000, 2000, 200], theta=1.1, seed=8)
+        rels = [fact] + dims
+        for sw in SWITCHES:
+            got = ctx.amhj("NORMAL", rels_on(ctx, rels), **sw)
+            assert (got.count, got.checksum) == O.mhj(rels)
+
+
+@pytest.mark.parametrize("qt", ["TRI", "FOUR"])
+@pytest.mark.parametrize("reorder", [True, False])
+def test_amhj_tri_four(ctx, qt, reorder):
+    s, d = data.rmat(10, 6000, 0.57, 0.19, 0.19, seed=21)
+    e = ctx.relation([s, d], [0, 1])
+    want = O.triangle(s, d) if qt == "TRI" else O.four_clique(s, d)
+    for sw in SWITCHES:
+        got = ctx.amhj(qt, [e], reorder=reorder, **sw)
+        assert (got.count, got.checksum) == want, sw
+    got = ctx.amhj(qt, [e], materialize=True, reorder=reorder)
+    assert data.checksum(got.columns) == want[1]
+
+
+def test_amhj_dro_residual_resume():
+    """An estimate far too small forces breakpoints and the residual pass."""
+    with Context(0, dro_headroom=0.01) as ctx:
+        rels = data.chain_relations(50000, 1 << 12, 3, seed=12)
+        for ws in (0, 1):
+            got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=ws, dro=1, materialize=True)
+            cnt, chk, cols = O.mhj(rels, tuples=True)
+            assert (got.count, got.checksum) == (cnt, chk)
+            assert got.stats["residual_units"] > 0 and got.stats["rows_written_residual"] > 0
+            assert np.array_equal(sorted_rows(got.columns), sorted_rows(cols))
+
+
+def test_amhj_work_sharing_on_skew():
+    """Zipf keys make a few huge buckets; small tasks force many splits."""
+    with Context(0, task_chunk=32) as ctx:
+        n = 60000
+        r1 = ([data.uniform(n, 0, 1000, 1), data.zipf(n, 1000, 1.4, 2)], [0, 1])
+        r2 = ([data.zipf(n, 1000, 1.4, 3), data.uniform(n, 0, 50, 4)], [1, 2])
+        r3 = ([data.uniform(n, 0, 50, 5), data.uniform(n, 0, 1 << 20, 6)], [2, 3])
+        rels = [r1, r2, r3]
+        want = O.mhj(rels)
+        for dro in (0, 1):
+            got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=1, dro=dro, materialize=bool(dro))
+            assert (got.count, got.checksum) == want
+            assert got.stats["tasks_pushed"] > 0 or got.stats["fallbacks"] > 0
+            assert got.stats["tasks_popped"] == got.stats["tasks_pushed"]
+
+
+@pytest.mark.parametrize("streamed", [False, True])
+@pytest.mark.parametrize("materialize", [False, True])
+def test_amhj_out_of_core(streamed, materialize):
+    with Context(0, ooc_slice_rows=3000) as ctx:
+        rels = data.chain_relations(20000, 1 << 11, 3, seed=13)
+        handles = [ctx.relation(rels[0][0], rels[0][1], streamed=streamed)] + rels_on(ctx, rels[1:])
+        for sw in SWITCHES[:4]:
+            got = ctx.amhj("NORMAL", handles, ooc=1, materialize=materialize, **sw)
+            cnt, chk = O.mhj(rels)
+            assert (got.count, got.checksum) == (cnt, chk)
+            assert got.stats["slices"] == 7
+            if materialize:
+                assert data.checksum(got.columns) == chk
+
+
+def test_amhj_edge_cases(ctx):
+    z = np.zeros(0, np.int32)
+    one = ([np.array([3], np.int32), np.array([4], np.int32)], [0, 1])
+    cases = [
+        [([z, z], [0, 1]), ([z, z], [1, 2])],
+        [one, ([z, z], [1, 2])],
+        [([z, z], [0, 1]), one and ([np.array([4], np.int32), np.array([9], np.int32)], [1, 2])],
+        [one, ([np.array([4, 4, 4], np.int32), np.array([7, 8, 9], np.int32)], [1, 2])],
+        # every key equal: one bucket holds the whole relation
+        [([np.full(3000, 5, np.int32), np.arange(3000, dtype=np.int32)], [0, 1]),
+         ([np.arange(3000, dtype=np.int32) % 7, np.full(3000, -1, np.int32)], [1, 2])],
+        # extreme values
+        [([np.array([-2**31, 2**31 - 1, 0], np.int32), np.array([2**31 - 1, -2**31, -1], np.int32)], [0, 1]),
+         ([np.array([2**31 - 1, -2**31, -1], np.int32), np.array([1, 2, 3], np.int32)], [1, 2])],
+    ]
+    for rels in cases:
+        want = O.mhj(rels)
+        for sw in SWITCHES:
+            got = ctx.amhj("NORMAL", rels_on(ctx, rels), materialize=True, **sw)
+            assert (got.count, got.checksum) == want, (rels, sw)
+
+
+def test_amhj_single_relation(ctx):
+    rels = [([data.uniform(100, 0, 10, 1), data.uniform(100, 0, 10, 2)], [0, 1])]
+    got = ctx.amhj("NORMAL", rels_on(ctx, rels), materialize=True)
+    assert (got.count, got.checksum) == O.mhj(rels)
+
+
+def test_amhj_rejects_bad_queries(ctx):
+    a = ctx.relation([np.arange(4, dtype=np.int32), np.arange(4, dtype=np.int32)], [0, 2])
+    b = ctx.relation([np.arange(4, dtype=np.int32), np.arange(4, dtype=np.int32)], [3, 4])
+    with pytest.raises(AmjError) as e:
+        ctx.amhj("NORMAL", [a, b])
+    assert e.value.status == L.AMJ_EINVAL
+    c = ctx.relation([np.arange(4, dtype=np.int32), np.arange(4, dtype=np.int32)], [0, 1])
+    d = ctx.relation([np.arange(4, dtype=np.int32), np.arange(4, dtype=np.int32)], [2, 3])
+    with pytest.raises(AmjError) as e:
+        ctx.amhj("NORMAL", [c, d])
+    assert e.value.status == L.AMJ_EUNSUPPORTED
+
+
+# ------------------------------------------------------------------- ALFTJ
+
+@pytest.mark.parametrize("algo", ["DFS", "BFS"])
+@pytest.mark.parametrize("ws", [0, 1])
+@pytest.mark.parametrize("heavy", [0, 1, 8])
+def test_lftj_triangle_small(algo, ws, heavy):
+    with Context(0, lftj_heavy_degree=heavy) as ctx:
+        for seed, scale, ne in [(1, 8, 1500), (2, 12, 50000)]:
+            s, d = data.rmat(scale, ne, 0.57, 0.19, 0.19, seed)
+            e = ctx.relation([s, d], [0, 1])
+            got = ctx.lftj([e], algo=algo, ws=ws)
+            assert (got.count, got.checksum) == O.triangle(s, d)
+
+
+@pytest.mark.parametrize("algo", ["DFS", "BFS"])
+def test_lftj_materialized_tuples(ctx, algo):
+    s, d = data.rmat(11, 20000, 0.57, 0.19, 0.19, 5)
+    e = ctx.relation([s, d], [0, 1])
+    cnt, chk, cols = O.triangle(s, d, tuples=True)
+    for ws in (0, 1):
+        got = ctx.lftj([e], algo=algo, ws=ws, materialize=True)
+        assert (got.count, got.checksum) == (cnt, chk)
+        assert np.array_equal(sorted_rows(got.columns), sorted_rows(cols))
+
+
+def test_lftj_three_relations_and_cross_operator(ctx):
+    s, d = data.rmat(11, 20000, 0.57, 0.19, 0.19, 6)
+    want = O.triangle(s, d)
+    # three relations (0,1), (2,1) given with swapped column order, (0,2)
+    R = ctx.relation([s, d], [0, 1])
+    S = ctx.relation([d, s], [2, 1])
+    T = ctx.relation([s, d], [0, 2])
+    for algo in ("DFS", "BFS"):
+        got = ctx.lftj([S, T, R], algo=algo)
+        assert (got.count, got.checksum) == want
+    e = ctx.relation([s, d], [0, 1])
+    amhj = ctx.amhj("TRI", [e], ws=1)
+    dfs = ctx.lftj([e], algo="DFS")
+    bfs = ctx.lftj([e], algo="BFS")
+    assert (amhj.count, amhj.checksum) == (dfs.count, dfs.checksum) == (bfs.count, bfs.checksum) == want
+
+
+def test_lftj_out_of_core_slices():
+    with Context(0, ooc_slice_rows=5000) as ctx:
+        s, d = data.rmat(11, 30000, 0.57, 0.19, 0.19, 7)
+        e = ctx.relation([s, d], [0, 1])
+        want = O.triangle(s, d)
+        for algo in ("DFS", "BFS"):
+            got = ctx.lftj([e], algo=algo, ooc=1, materialize=True)
+            assert (got.count, got.checksum) == want
+            assert data.checksum(got.columns) == want[1]
+            assert got.stats["slices"] > 1
+
+
+def test_lftj_rejects_two_relations_and_edge_cases(ctx):
+    e = ctx.relation([np.array([0], np.int32), np.array([1], np.int32)], [0, 1])
+    with pytest.raises(AmjError) as x:
+        ctx.lftj([e, e], algo="DFS")
+    assert x.value.status == L.AMJ_EINVAL
+    empty = ctx.relation([np.zeros(0, np.int32), np.zeros(0, np.int32)], [0, 1])
+    for algo in ("DFS", "BFS"):
+        assert ctx.lftj([empty], algo=algo).count == 0
+        assert ctx.lftj([e], algo=algo).count == 0
+
+
+# ---------------------------------------------------------- full size
+
+def test_c1_chain_full_size(ctx):
+    rels = data.chain_relations(1_000_000, 1 << 18, 3, seed=1)
+    want = O.mhj(rels)
+    got = ctx.amhj("NORMAL", rels_on(ctx, rels))
+    assert (got.count, got.checksum) == want
+    got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=1, dro=1, materialize=True)
+    assert (got.count, got.checksum) == want
+    assert data.checksum(got.columns) == want[1]
+
+
+def test_c2_triangle_full_size(ctx):
+    s, d = data.rmat(20, 1 << 24, 0.57, 0.19, 0.19, 20)
+    want = O.triangle(s, d)
+    e = ctx.relation([s, d], [0, 1])
+    for algo in ("DFS", "BFS"):
+        got = ctx.lftj([e], algo=algo)
+        assert (got.count, got.checksum) == want
+    got = ctx.amhj("TRI", [e], ws=1)
+    assert (got.count, got.checksum) == want
+
+
+# ----------------------------------------------------- failure detection
+
+def test_bounded_wait_times_out_and_context_survives(ctx):
+    lib = L.load()
+    st = lib.amj_selftest_bounded_wait(ctx.handle, 200)
+    assert st == L.AMJ_ETIMEOUT
+    assert b"bounded wait" in lib.amj_last_error()
+    rels = data.chain_relations(1000, 256, 3, seed=1)
+    got = ctx.amhj("NORMAL", rels_on(ctx, rels))
+    assert (got.count, got.checksum) == O.mhj(rels)
+
+
+def test_work_sharing_queue_overflow_falls_back():
+    """A one-slot task queue under direct output cannot hold the splits the
+    residual replay relies on: the overflow is detected on the device and the
+    direct output is redone without work sharing, still exact."""
+    with Context(0, task_chunk=32, task_capacity=1, dro_headroom=0.5) as ctx:
+        n = 20000
+        rels = [([data.uniform(n, 0, 100, 1), data.zipf(n, 100, 1.5, 2)], [0, 1]),
+                ([data.zipf(n, 100, 1.5, 3), data.uniform(n, 0, 1000, 4)], [1, 2])]
+        want = O.mhj(rels)
+        got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=1, dro=1, materialize=True)
+        assert (got.count, got.checksum) == want
+        assert got.stats["fallbacks"] >= 1
+        assert data.checksum(got.columns) == want[1]
+        got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=1)   # count mode keeps unsplit work local
+        assert (got.count, got.checksum) == want
+
+
+# ------------------------------------------------------------------- CLIs
+
+def test_cli_exec_amhj_and_exec_lftj(tmp_path):
+    rels = data.chain_relations(5000, 1 << 10, 3, seed=2)
+    d = tmp_path / "chain"
+    d.mkdir()
+    # file names sort as r0, r1, r2 only by attribute: write them in query order with --order
+    for i, (cols, attrs) in enumerate(rels):
+        data.write_db(str(d / data.db_name(len(cols[0]), attrs)), cols)
+    names = sorted(os.listdir(d))
+    order = [names.index(data.db_name(len(c[0]), a)) for c, a in rels]
+    pos = [order.index(i) for i in range(len(names))]
+    exe = os.path.join(ROOT, "accmultiwayjoins_b200", "bin", "exec-AMHJ")
+    r = subprocess.run([exe, "NORMAL", str(d), "0", "1", "0", "0", "--order", ",".join(map(str, pos))],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    cnt, chk = O.mhj(rels)
+    assert out["count"] == cnt and out["checksum"] == f"{chk:016x}"
+    s, dd = data.rmat(10, 8000, 0.57, 0.19, 0.19, 3)
+    g = tmp_path / "graph"
+    g.mkdir()
+    data.write_db(str(g / data.db_name(len(s), [0, 1])), [s, dd])
+    want = O.triangle(s, dd)
+    for algo in ("0", "1"):
+        exe = os.path.join(ROOT, "accmultiwayjoins_b200", "bin", "exec-LFTJ")
+        r = subprocess.run([exe, str(g), algo, "0", "1"], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        out = json.loads(r.stdout.strip().splitlines()[-1])
+        assert out["count"] == want[0] and out["checksum"] == f"{want[1]:016x}"
+    exe = os.path.join(ROOT, "accmultiwayjoins_b200", "bin", "exec-AMHJ")
+    r = subprocess.run([exe, "TRI", str(g / data.db_name(len(s), [0, 1])), "0", "1", "0", "0"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert json.loads(r.stdout.strip().splitlines()[-1])["count"] == want[0]
