@@ -281,7 +281,7 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
         unsigned long long total = 0;
         AMJ_CUDA_TRY(cudaMemcpyAsync(&total, l0.p + rows, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
         AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-        nchunks = (total + 31) / 32;
+        nchunks = (total + L0_CHUNK - 1) / L0_CHUNK;
         if (nchunks > 0xffffffffull) return fail(AMJ_EUNSUPPORTED, "AMHJ: more than 2^37 level-0 candidates in one slice");
         P.lbs = 1;
         PL.batch_count = nchunks;

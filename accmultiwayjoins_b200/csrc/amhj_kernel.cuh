@@ -135,40 +135,17 @@ __device__ __forceinline__ uint64_t warp_row_of(const unsigned long long *E, uin
     return lo + (uint64_t)__popc(__ballot_sync(AMJ_FULL_MASK, le)) - 1;
 }
 
-// Depth-0 frontier of level-0 chunk `c`: lane j takes candidate 32c + j of the
-// concatenated level-0 ranges; its entry is that single candidate of its row.
+constexpr uint32_t L0_CHUNK = 1024;   // level-0 candidates per work-sharing unit
+
+// Depth-0 frontier for rows [rb, re) of a level-0 chunk [g0, g1): lane i
+// takes row rb+i with its candidate range clipped to the chunk.
 template <int MODE, bool WS>
-__device__ __forceinline__ bool load_l0_chunk(const ProbeLaunch &L, char *wbase, unsigned long long c, int lane) {
+__device__ __forceinline__ void load_l0_group(const ProbeLaunch &L, char *wbase, unsigned long long g0,
+                                              unsigned long long g1, uint64_t rb, uint64_t re, int lane) {
     const ProbePlan &P = L.P;
-    const uint64_t rows = P.row_hi - P.row_lo;
-    const unsigned long long total = P.l0_start[rows];
-    const unsigned long long g0 = c * 32ull;
-    if (g0 >= total) return false;
-    const unsigned long long g = g0 + lane;
-    const bool valid = g < total;
-    // row of the chunk's first candidate, then each lane's row from a window of 32 row starts
-    const uint64_t r0 = warp_row_of(P.l0_start, rows, g0, lane);
-    const uint64_t wr = r0 + lane;
-    const unsigned long long ws = wr < rows ? P.l0_start[wr] : ~0ull;
-    int pos = 0;
-#pragma unroll
-    for (int step = 16; step > 0; step >>= 1) {
-        const int cand = pos + step;
-        const unsigned long long v = __shfl_sync(AMJ_FULL_MASK, ws, cand & 31);
-        if (v <= g) pos = cand;
-    }
-    uint64_t row = r0 + pos;
-    if (valid && pos == 31 && row + 1 < rows && P.l0_start[row + 1] <= g) {
-        // more than 32 rows lie inside this chunk: plain binary search
-        uint64_t lo = row + 1, hi = rows;
-        while (hi - lo > 1) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (P.l0_start[mid] <= g) lo = mid;
-            else hi = mid;
-        }
-        row = lo;
-    }
     Frontier F = frontier_at(wbase, P, 0);
+    const uint64_t row = rb + lane;
+    const bool valid = row < re;
     const uint64_t prow = P.row_lo + row;
     for (int cc = 0; cc < P.probe_ncols; cc++)
         F.vals[P.probe_attr[cc] * 32 + lane] = valid ? P.probe_col[cc][prow] : 0;
@@ -176,16 +153,26 @@ __device__ __forceinline__ bool load_l0_chunk(const ProbeLaunch &L, char *wbase,
     uint32_t s = 0, aux = 0, sz = 0;
     uint8_t m8 = 0;
     if (valid) {
-        const uint32_t k = (uint32_t)(g - P.l0_start[row]);
-        level_lookup(P.lv[0], [&](int a) { return F.vals[a * 32 + lane]; }, s, aux, m8);
-        if (P.lv[0].layout == AMJ_LAYOUT_CUCKOO) {
-            uint32_t m = m8;
-            for (uint32_t t = 0; t < k; t++) m &= m - 1;
-            m8 = (uint8_t)(m & (~m + 1u));   // keep the k-th matching slot only
-        } else {
-            s += k;
+        const unsigned long long e0 = P.l0_start[row], e1 = P.l0_start[row + 1];
+        const unsigned long long lo = e0 > g0 ? e0 : g0, hi = e1 < g1 ? e1 : g1;
+        if (hi > lo) {
+            const uint32_t k0 = (uint32_t)(lo - e0);
+            sz = (uint32_t)(hi - lo);
+            level_lookup(P.lv[0], [&](int a) { return F.vals[a * 32 + lane]; }, s, aux, m8);
+            if (P.lv[0].layout == AMJ_LAYOUT_CUCKOO) {
+                uint32_t m = m8;
+                for (uint32_t t = 0; t < k0; t++) m &= m - 1;   // drop the first k0 matches
+                uint32_t keep = 0;
+                for (uint32_t t = 0; t < sz; t++) {
+                    const uint32_t low = m & (~m + 1u);
+                    keep |= low;
+                    m &= m - 1;
+                }
+                m8 = (uint8_t)keep;
+            } else {
+                s += k0;
+            }
         }
-        sz = 1;
     }
     F.s[lane] = s;
     F.aux[lane] = aux;
@@ -198,7 +185,6 @@ __device__ __forceinline__ bool load_l0_chunk(const ProbeLaunch &L, char *wbase,
         F.meta[2] = 32;
     }
     __syncwarp();
-    return true;
 }
 
 // level-0 candidate counts of probe rows row_lo..row_hi-1
@@ -240,8 +226,19 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
     unsigned long long u_emitted = 0, u_written = 0, u_skip = 0;
     bool u_over = false, u_live = false;
     unsigned long long res_next = 0;   // residual: next breakpoint index
+    // level-0 chunk in progress: candidates [c_g0, c_g1), rows c_row .. c_rend-1 still to load
+    unsigned long long c_g0 = 0, c_g1 = 0;
+    uint64_t c_row = 0, c_rend = 0;
 
     while (true) {
+        if (depth < 0 && c_row < c_rend) {
+            // ---- next 32 rows of the current level-0 chunk (same unit)
+            const uint64_t re = (c_row + 32 < c_rend) ? c_row + 32 : c_rend;
+            load_l0_group<MODE, WS>(L, wbase, c_g0, c_g1, c_row, re, lane);
+            c_row = re;
+            depth = 0;
+            continue;
+        }
         if (depth < 0) {
             // ---- unit finished: record a breakpoint if its output overflowed
             if (MODE == PM_WRITE && P.dro && u_live && u_over && lane == 0) {
@@ -313,8 +310,17 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
             u_live = true;
 
             if (have == 3) {
-                depth = load_l0_chunk<MODE, WS>(L, wbase, l0c, lane) ? 0 : -1;
-                continue;
+                const uint64_t rows = P.row_hi - P.row_lo;
+                const unsigned long long total = P.l0_start[rows];
+                c_g0 = l0c * (unsigned long long)L0_CHUNK;
+                c_g1 = c_g0 + L0_CHUNK < total ? c_g0 + L0_CHUNK : total;
+                if (c_g0 < total) {
+                    c_row = warp_row_of(P.l0_start, rows, c_g0, lane);
+                    c_rend = warp_row_of(P.l0_start, rows, c_g1 - 1, lane) + 1;
+                } else {
+                    c_row = c_rend = 0;
+                }
+                continue;   // the first group is loaded at the top of the loop
             }
             if (have == 1) {
                 // ---- depth 0: 32 probe tuples, coalesced column loads

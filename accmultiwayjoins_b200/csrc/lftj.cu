@@ -195,6 +195,7 @@ __device__ __forceinline__ bool heavy_vertex(const TriArgs &A, uint64_t r_deg, u
 
 constexpr int BM_THREADS = 1024;
 constexpr int BM_UNROLL = 8;
+constexpr uint32_t BM_SEG = 1024;   // values of one child list per warp work item
 
 // Bitmap kernel: one block per heavy vertex a at a time.  The children of a
 // in T are set in a shared-memory bitmap (one bit per value in their span,
@@ -213,9 +214,11 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
     unsigned long long *hab = pre + BM_THREADS;
     uint32_t *sbeg = (uint32_t *)(hab + BM_THREADS);
     int32_t *bval = (int32_t *)(sbeg + BM_THREADS);
+    uint32_t *segpre = (uint32_t *)(bval + BM_THREADS);
     __shared__ unsigned long long s_i;
     __shared__ unsigned long long s_wsum[BM_THREADS / 32 + 1];
     __shared__ uint32_t s_next;
+    __shared__ uint32_t s_ssum[BM_THREADS / 32 + 1];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (uint32_t w = tid; w < words; w += BM_THREADS) bits[w] = 0u;
     unsigned long long cnt = 0, chk = 0;
@@ -251,36 +254,55 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
                 child_range(A.S, b, sb, eb);
                 len = eb - sb;
             }
-            // block inclusive scan of len
+            // block inclusive scans of len and of the list's segment count
+            const uint32_t nseg = (uint32_t)((len + BM_SEG - 1) / BM_SEG);
             unsigned long long incl = warp_inclusive_scan(len, lane);
-            if (lane == 31) s_wsum[warp] = incl;
+            uint32_t sincl = warp_inclusive_scan(nseg, lane);
+            if (lane == 31) {
+                s_wsum[warp] = incl;
+                s_ssum[warp] = sincl;
+            }
             __syncthreads();
             if (warp == 0) {
                 unsigned long long w = lane < BM_THREADS / 32 ? s_wsum[lane] : 0ull;
                 unsigned long long wi = warp_inclusive_scan(w, lane);
                 s_wsum[lane] = wi - w;
-                if (lane == 31) s_wsum[BM_THREADS / 32] = wi;
+                uint32_t sw = lane < BM_THREADS / 32 ? s_ssum[lane] : 0u;
+                uint32_t swi = warp_inclusive_scan(sw, lane);
+                s_ssum[lane] = swi - sw;
+                if (lane == 31) s_ssum[BM_THREADS / 32] = swi;
             }
             __syncthreads();
             pre[tid] = s_wsum[warp] + incl;
+            segpre[tid] = s_ssum[warp] + sincl;
             sbeg[tid] = (uint32_t)sb;
             hab[tid] = amj_hash_step(ha, b);
             bval[tid] = b;
+            const uint32_t total_seg = s_ssum[BM_THREADS / 32];
             const uint32_t nb = (uint32_t)((ee - bs) < BM_THREADS ? (ee - bs) : BM_THREADS);
-            __syncthreads();
-            // warps claim child lists of the batch one at a time and stream
-            // each list 32 x BM_UNROLL values per step (all loads in flight
-            // before the bit tests); the owner of a value is the list itself
             if (tid == 0) s_next = 0;
             __syncthreads();
+            // warps claim segments of at most BM_SEG values of the child lists
+            // (balanced across warps whatever the list lengths) and stream each
+            // 32 x BM_UNROLL values per step, all loads in flight before the tests
             while (true) {
-                uint32_t li = 0;
-                if (lane == 0) li = atomicAdd(&s_next, 1u);
-                li = __shfl_sync(AMJ_FULL_MASK, li, 0);
-                if (li >= nb) break;
+                uint32_t sg = 0;
+                if (lane == 0) sg = atomicAdd(&s_next, 1u);
+                sg = __shfl_sync(AMJ_FULL_MASK, sg, 0);
+                if (sg >= total_seg) break;
+                uint32_t slo = 0, shi = nb - 1;
+                while (slo < shi) {
+                    const uint32_t mid = (slo + shi) >> 1;
+                    if (segpre[mid] > sg) shi = mid;
+                    else slo = mid + 1;
+                }
+                const uint32_t li = slo;
+                const uint32_t first_seg = li ? segpre[li - 1] : 0u;
                 const unsigned long long lbeg = li ? pre[li - 1] : 0ull;
-                const uint32_t len = (uint32_t)(pre[li] - lbeg);
-                const int32_t *lst = A.S.data1 + sbeg[li];
+                const uint32_t llen = (uint32_t)(pre[li] - lbeg);
+                const uint32_t kbeg = (sg - first_seg) * BM_SEG;
+                const uint32_t len = (llen - kbeg) < BM_SEG ? (llen - kbeg) : BM_SEG;
+                const int32_t *lst = A.S.data1 + sbeg[li] + kbeg;
                 const uint64_t hb = hab[li];
                 for (uint32_t k0 = 0; k0 < len; k0 += 32 * BM_UNROLL) {
                     int32_t cv[BM_UNROLL];
@@ -605,7 +627,7 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
             if (heavy_deg) {
                 // the bitmap kernel takes the heavy vertices; its shared memory: bitmap + 1024 x 24 B
                 const uint32_t bits_max = 1u << 20;
-                const size_t smem = (size_t)bits_max / 8 + (size_t)BM_THREADS * (8 + 8 + 4 + 4);
+                const size_t smem = (size_t)bits_max / 8 + (size_t)BM_THREADS * (8 + 8 + 4 + 4 + 4);
                 if (smem <= (size_t)ctx->max_smem_optin) {
                     A.heavy_deg = heavy_deg;
                     A.bitmap_bits = bits_max;

@@ -170,19 +170,28 @@ def test_amhj_dro_residual_resume():
 
 
 def test_amhj_work_sharing_on_skew():
-    """Zipf keys make a few huge buckets; small tasks force many splits."""
+    """Zipf keys make a few huge buckets (about 9M output tuples); small tasks
+    force splits below level 0 and level-0 chunks balance the probe side."""
     with Context(0, task_chunk=32) as ctx:
-        n = 60000
-        r1 = ([data.uniform(n, 0, 1000, 1), data.zipf(n, 1000, 1.4, 2)], [0, 1])
-        r2 = ([data.zipf(n, 1000, 1.4, 3), data.uniform(n, 0, 50, 4)], [1, 2])
-        r3 = ([data.uniform(n, 0, 50, 5), data.uniform(n, 0, 1 << 20, 6)], [2, 3])
+        n = 20000
+        r1 = ([data.uniform(n, 0, 1000, 1), data.zipf(n, 1000, 1.2, 2)], [0, 1])
+        r2 = ([data.zipf(n, 1000, 1.2, 3), data.uniform(n, 0, 1 << 16, 4)], [1, 2])
+        r3 = ([data.uniform(n, 0, 1 << 16, 5), data.uniform(n, 0, 1 << 20, 6)], [2, 3])
         rels = [r1, r2, r3]
         want = O.mhj(rels)
         for dro in (0, 1):
             got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=1, dro=dro, materialize=bool(dro))
             assert (got.count, got.checksum) == want
-            assert got.stats["tasks_pushed"] > 0 or got.stats["fallbacks"] > 0
             assert got.stats["tasks_popped"] == got.stats["tasks_pushed"]
+            if dro:
+                assert data.checksum(got.columns) == want[1]
+        # a chain whose level-1 buckets are large: the task queue is used
+        q = [([data.uniform(100, 0, 100, 1), data.uniform(100, 0, 100, 2)], [0, 1]),
+             ([data.uniform(2000, 0, 100, 3), data.uniform(2000, 0, 4, 4)], [1, 2]),
+             ([data.uniform(20000, 0, 4, 5), data.uniform(20000, 0, 1 << 20, 6)], [2, 3])]
+        got = ctx.amhj("NORMAL", rels_on(ctx, q), ws=1)
+        assert (got.count, got.checksum) == O.mhj(q)
+        assert got.stats["tasks_pushed"] > 0 and got.stats["tasks_popped"] == got.stats["tasks_pushed"]
 
 
 @pytest.mark.parametrize("streamed", [False, True])
@@ -346,15 +355,15 @@ def test_work_sharing_queue_overflow_falls_back():
     residual replay relies on: the overflow is detected on the device and the
     direct output is redone without work sharing, still exact."""
     with Context(0, task_chunk=32, task_capacity=1, dro_headroom=0.5) as ctx:
-        n = 20000
-        rels = [([data.uniform(n, 0, 100, 1), data.zipf(n, 100, 1.5, 2)], [0, 1]),
-                ([data.zipf(n, 100, 1.5, 3), data.uniform(n, 0, 1000, 4)], [1, 2])]
-        want = O.mhj(rels)
-        got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=1, dro=1, materialize=True)
+        q = [([data.uniform(100, 0, 100, 1), data.uniform(100, 0, 100, 2)], [0, 1]),
+             ([data.uniform(2000, 0, 100, 3), data.uniform(2000, 0, 4, 4)], [1, 2]),
+             ([data.uniform(20000, 0, 4, 5), data.uniform(20000, 0, 1 << 20, 6)], [2, 3])]
+        want = O.mhj(q)
+        got = ctx.amhj("NORMAL", rels_on(ctx, q), ws=1, dro=1, materialize=True)
         assert (got.count, got.checksum) == want
         assert got.stats["fallbacks"] >= 1
         assert data.checksum(got.columns) == want[1]
-        got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=1)   # count mode keeps unsplit work local
+        got = ctx.amhj("NORMAL", rels_on(ctx, q), ws=1)   # count mode keeps unsplit work local
         assert (got.count, got.checksum) == want
 
 
