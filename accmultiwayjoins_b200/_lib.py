@@ -103,6 +103,7 @@ SIGNATURES = {
                                    C.POINTER(amj_result)]),
     "amj_result_release": (None, [C.POINTER(amj_result)]),
     "amj_bucket_build": (C.c_int, [_P, _P, C.c_uint64, C.c_uint64, _P, _P, _P]),
+    "amj_bucket_build_static": (C.c_int, [_P, C.c_uint64, C.c_uint64, _P, _P, _P, _P]),
     "amj_trie_build": (C.c_int, [_P, _P, _P, C.c_uint64, C.POINTER(_P)]),
     "amj_trie_view": (C.c_int, [_P, _U64P, _U64P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "amj_trie_download": (C.c_int, [_P, _I32P, _U64P, _I32P]),

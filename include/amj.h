@@ -151,6 +151,24 @@ void amj_result_release(amj_result *res);
 int  amj_bucket_build(amj_ctx *ctx, const int32_t *d_keys, uint64_t n, uint64_t buckets,
                       int32_t *d_hash_keys, uint32_t *d_idx_in_origin, uint32_t *d_buc_ptrs);
 
+/* amj_bucket_build_static: the same bucket-CSR build, for callers that may
+ * not allocate device memory (inside a stream capture that must stay free of
+ * allocation nodes, under an engine that owns all device memory through its
+ * own pool, or on a latency-critical path that cannot wait on the driver's
+ * allocator).  No counterpart in the reference.  It allocates nothing: its
+ * scratch is a fixed area inside the library (about 16.3 MB, resident on
+ * every device that loads the library until exit), so n is limited to
+ * AMJ_BUCKET_STATIC_MAX_KEYS and buckets to AMJ_BUCKET_STATIC_MAX_BUCKETS
+ * (larger requests return AMJ_EINVAL).  Runs on `stream` (a cudaStream_t, 0
+ * for the default stream) of the current device and synchronises it before
+ * returning.  All calls share the one scratch area: calls that overlap on the
+ * GPU race.  The first call on a device looks up the area's address; make it
+ * before any stream capture begins. */
+#define AMJ_BUCKET_STATIC_MAX_KEYS    (1u << 20)
+#define AMJ_BUCKET_STATIC_MAX_BUCKETS (1u << 20)
+int  amj_bucket_build_static(const int32_t *d_keys, uint64_t n, uint64_t buckets, int32_t *d_hash_keys,
+                             uint32_t *d_idx_in_origin, uint32_t *d_buc_ptrs, void *stream);
+
 /* amj_trie_build: 2-level IndexedTrie of the pairs (c0[i], c1[i]): the
  * distinct c0 values ascending (level 0), their child offsets, and the c1
  * values sorted inside each c0 group (level 1, duplicates kept).
