@@ -283,8 +283,8 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
             if (tid == 0) s_next = 0;
             __syncthreads();
             // warps claim segments of at most BM_SEG values of the child lists
-            // (balanced across warps whatever the list lengths) and stream each
-            // 32 x BM_UNROLL values per step, all loads in flight before the tests
+            // (balanced across warps whatever the list lengths) and stream each,
+            // 32 x BM_UNROLL values per step with all loads in flight before the tests
             while (true) {
                 uint32_t sg = 0;
                 if (lane == 0) sg = atomicAdd(&s_next, 1u);
@@ -304,41 +304,49 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
                 const uint32_t len = (llen - kbeg) < BM_SEG ? (llen - kbeg) : BM_SEG;
                 const int32_t *lst = A.S.data1 + sbeg[li] + kbeg;
                 const uint64_t hb = hab[li];
-                for (uint32_t k0 = 0; k0 < len; k0 += 32 * BM_UNROLL) {
-                    int32_t cv[BM_UNROLL];
-#pragma unroll
-                    for (int u = 0; u < BM_UNROLL; u++) {
-                        const uint32_t k = k0 + u * 32 + lane;
-                        cv[u] = k < len ? lst[k] : lo - 1;
-                    }
-#pragma unroll
-                    for (int u = 0; u < BM_UNROLL; u++) {
-                        const int32_t c = cv[u];
-                        const int64_t r = (int64_t)c - (int64_t)lo;
-                        const bool hit = r >= 0 && r < (int64_t)span &&
-                                         ((bits[(uint32_t)r >> 5] >> ((uint32_t)r & 31)) & 1u);
-                        if (!WRITE) {
+                // value c of the list is a hit when lo <= c < lo + span and its bit is set
+                auto test = [&](int32_t c) -> bool {
+                    const uint32_t r = (uint32_t)c - (uint32_t)lo;
+                    return c >= lo && r < span && ((bits[r >> 5] >> (r & 31)) & 1u);
+                };
+                auto emit = [&](bool hit, int32_t c) {
+                    if (!WRITE) {
+                        if (hit) {
+                            cnt++;
+                            chk += amj_hash_step(hb, c);
+                        }
+                    } else {
+                        const unsigned m = __ballot_sync(AMJ_FULL_MASK, hit);
+                        if (m) {
+                            unsigned long long base = 0;
+                            if (lane == 0) base = atomicAdd(A.out_cursor, (unsigned long long)__popc(m));
+                            base = __shfl_sync(AMJ_FULL_MASK, base, 0);
                             if (hit) {
                                 cnt++;
                                 chk += amj_hash_step(hb, c);
-                            }
-                        } else {
-                            const unsigned m = __ballot_sync(AMJ_FULL_MASK, hit);
-                            if (m) {
-                                unsigned long long base = 0;
-                                if (lane == 0) base = atomicAdd(A.out_cursor, (unsigned long long)__popc(m));
-                                base = __shfl_sync(AMJ_FULL_MASK, base, 0);
-                                if (hit) {
-                                    cnt++;
-                                    chk += amj_hash_step(hb, c);
-                                    const unsigned long long p = base + __popc(m & lanemask_lt());
-                                    if (p < A.out_cap) {
-                                        A.out[0][p] = a; A.out[1][p] = bval[li]; A.out[2][p] = c;
-                                    }
+                                const unsigned long long p = base + __popc(m & lanemask_lt());
+                                if (p < A.out_cap) {
+                                    A.out[0][p] = a; A.out[1][p] = bval[li]; A.out[2][p] = c;
                                 }
                             }
                         }
                     }
+                };
+                uint32_t k0 = 0;
+                // full blocks of 32 x BM_UNROLL values: all loads issued before the tests
+                for (; k0 + 32 * BM_UNROLL <= len; k0 += 32 * BM_UNROLL) {
+                    int32_t cv[BM_UNROLL];
+#pragma unroll
+                    for (int u = 0; u < BM_UNROLL; u++) cv[u] = lst[k0 + u * 32 + lane];
+#pragma unroll
+                    for (int u = 0; u < BM_UNROLL; u++) emit(test(cv[u]), cv[u]);
+                }
+                // the rest (all of a short list) 32 values at a time
+                for (; k0 < len; k0 += 32) {
+                    const uint32_t k = k0 + lane;
+                    const bool in = k < len;
+                    const int32_t c = in ? lst[k] : 0;
+                    emit(in && test(c), c);
                 }
             }
             __syncthreads();
