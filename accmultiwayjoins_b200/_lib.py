@@ -67,6 +67,7 @@ class amj_result(C.Structure):
         ("probe_ms", C.c_double),
         ("total_ms", C.c_double),
         ("stats", C.c_uint64 * 8),
+        ("kernel_ms", C.c_double * 4),
         ("priv", C.c_void_p),
     ]
 

@@ -40,6 +40,7 @@ class Result:
     probe_ms: float
     total_ms: float
     stats: dict
+    kernel_ms: tuple = ()
     columns: Optional[list] = None  # k numpy int32 arrays (attribute order) when materialised
 
     def tuples(self) -> np.ndarray:
@@ -152,7 +153,8 @@ class Context:
                     cols.append(np.zeros(0, np.int32))
         out = Result(count=int(res.count), checksum=int(res.checksum), num_attrs=int(res.num_attrs),
                      build_ms=float(res.build_ms), probe_ms=float(res.probe_ms), total_ms=float(res.total_ms),
-                     stats={STAT_NAMES[i]: int(res.stats[i]) for i in range(8)}, columns=cols)
+                     stats={STAT_NAMES[i]: int(res.stats[i]) for i in range(8)},
+                     kernel_ms=tuple(float(res.kernel_ms[i]) for i in range(4)), columns=cols)
         L.load().amj_result_release(C.byref(res))
         return out
 

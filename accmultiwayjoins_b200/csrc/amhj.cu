@@ -191,11 +191,19 @@ static int launch_probe_t(amj_ctx *ctx, const ProbeLaunch &PL, size_t smem) {
     return AMJ_OK;
 }
 
-static int launch_probe(amj_ctx *ctx, const ProbeLaunch &PL, int mode, bool ws) {
+static int launch_probe_raw(amj_ctx *ctx, const ProbeLaunch &PL, int mode, bool ws) {
     const size_t smem = (size_t)PROBE_WARPS * PL.P.warp_bytes;
     if (mode == PM_COUNT) return ws ? launch_probe_t<PM_COUNT, true>(ctx, PL, smem) : launch_probe_t<PM_COUNT, false>(ctx, PL, smem);
     if (mode == PM_WRITE) return ws ? launch_probe_t<PM_WRITE, true>(ctx, PL, smem) : launch_probe_t<PM_WRITE, false>(ctx, PL, smem);
     return ws ? launch_probe_t<PM_RESIDUAL, true>(ctx, PL, smem) : launch_probe_t<PM_RESIDUAL, false>(ctx, PL, smem);
+}
+
+// probe launch bracketed by the context's kernel-timing events
+static int launch_probe(amj_ctx *ctx, const ProbeLaunch &PL, int mode, bool ws) {
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
+    AMJ_TRY(launch_probe_raw(ctx, PL, mode, ws));
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
+    return AMJ_OK;
 }
 
 static int reset_state(amj_ctx *ctx, ProbeState *st, unsigned int *ready, uint32_t task_cap) {
@@ -204,9 +212,13 @@ static int reset_state(amj_ctx *ctx, ProbeState *st, unsigned int *ready, uint32
     return AMJ_OK;
 }
 
-static int read_state(amj_ctx *ctx, const ProbeState *d, ProbeState *h, const char *what) {
+// read the probe state back after the last launch; adds that launch's
+// kernel time to *kslot when given
+static int read_state(amj_ctx *ctx, const ProbeState *d, ProbeState *h, const char *what, double *kslot = nullptr) {
     AMJ_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(ProbeState), cudaMemcpyDeviceToHost, ctx->stream));
-    return status_check(ctx, what);
+    AMJ_TRY(status_check(ctx, what));
+    if (kslot) *kslot += event_ms(ctx->kev[0], ctx->kev[1]);
+    return AMJ_OK;
 }
 
 static int alloc_cols(amj_ctx *ctx, int k, uint64_t rows, int32_t **cols) {
@@ -291,7 +303,7 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
         P.dro = 0;
         AMJ_TRY(reset_state(ctx, PL.st, ws ? PL.task_ready : nullptr, task_cap));
         AMJ_TRY(launch_probe(ctx, PL, PM_COUNT, ws));
-        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ count"));
+        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ count", &res->kernel_ms[0]));
         pr->count = h.count;
         pr->checksum = h.checksum;
         res->stats[0] += h.tasks_pushed;
@@ -303,7 +315,7 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
         P.dro = 0;
         AMJ_TRY(reset_state(ctx, PL.st, ws ? PL.task_ready : nullptr, task_cap));
         AMJ_TRY(launch_probe(ctx, PL, PM_COUNT, ws));
-        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ count"));
+        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ count", &res->kernel_ms[0]));
         const uint64_t total = h.count;
         res->stats[0] += h.tasks_pushed;
         res->stats[1] += h.tasks_popped;
@@ -312,7 +324,7 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
         P.out_cap = total;
         AMJ_TRY(reset_state(ctx, PL.st, ws ? PL.task_ready : nullptr, task_cap));
         AMJ_TRY(launch_probe(ctx, PL, PM_WRITE, ws));
-        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ write"));
+        AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ write", &res->kernel_ms[1]));
         if (h.count != total || h.out_cursor != total)
             return fail(AMJ_ECUDA, "AMHJ: write pass disagrees with count pass");
         pr->count = total;
@@ -355,7 +367,7 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
     P.unit_cap = (uint32_t)std::min<uint64_t>(unit_cap, 0xffffffffull);
     AMJ_TRY(reset_state(ctx, PL.st, ws ? PL.task_ready : nullptr, task_cap));
     int rc = launch_probe(ctx, PL, PM_WRITE, ws);
-    if (rc == AMJ_OK) rc = read_state(ctx, PL.st, &h, "AMHJ DRO main write");
+    if (rc == AMJ_OK) rc = read_state(ctx, PL.st, &h, "AMHJ DRO main write", &res->kernel_ms[1]);
     if (rc != AMJ_OK) {
         for (int a = 0; a < k; a++) dev_free(ctx, main_cols[a]);
         if (rc == AMJ_EOVERFLOW && ws) {
@@ -401,7 +413,7 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
     AMJ_CUDA_TRY(cudaMemsetAsync(PL.st, 0, sizeof(ProbeState), ctx->stream));
     PL.batch_count = n_units;
     AMJ_TRY(launch_probe(ctx, PL, PM_RESIDUAL, ws));
-    AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ DRO residual write"));
+    AMJ_TRY(read_state(ctx, PL.st, &h, "AMHJ DRO residual write", &res->kernel_ms[1]));
     if (h.out_cursor != total - written)
         return fail(AMJ_ECUDA, "AMHJ DRO: residual pass wrote " + std::to_string(h.out_cursor) + " rows, expected " +
                                    std::to_string(total - written));

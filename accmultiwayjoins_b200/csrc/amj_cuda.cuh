@@ -127,6 +127,7 @@ struct amj_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaStream_t side_stream[2] = {nullptr, nullptr};   // ooc copy / prefetch streams
     unsigned long long launches = 0;                     // kernels launched through this context
+    cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};   // per-kernel timing
 };
 
 struct amj_rel {

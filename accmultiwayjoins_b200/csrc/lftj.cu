@@ -604,7 +604,8 @@ static TrieRef trie_ref(const Trie2 &t) {
 // written too (out_cap rows available).
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
-                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg) {
+                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms) {
+    bool timed[2] = {false, false};
     TriArgs A{};
     if (r_hi > R.len1) r_hi = R.len1;
     if (r_lo > r_hi) r_lo = r_hi;
@@ -642,8 +643,11 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
                     auto kb = write ? lftj_tri_bitmap_kernel<true> : lftj_tri_bitmap_kernel<false>;
                     AMJ_CUDA_TRY(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                     note_launch(ctx);
+                    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
                     kb<<<(unsigned)ctx->num_sms, BM_THREADS, smem, ctx->stream>>>(A);
                     AMJ_CUDA_TRY(cudaGetLastError());
+                    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
+                    timed[0] = true;
                 }
             }
             int per_sm = 0;
@@ -652,16 +656,22 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
             if (per_sm < 1) per_sm = 1;
             const unsigned grid = (unsigned)(ctx->num_sms * per_sm);
             note_launch(ctx);
+            AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[2], ctx->stream));
             if (write) lftj_tri_dfs_kernel<true><<<grid, 256, 0, ctx->stream>>>(A);
             else lftj_tri_dfs_kernel<false><<<grid, 256, 0, ctx->stream>>>(A);
             AMJ_CUDA_TRY(cudaGetLastError());
+            AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[3], ctx->stream));
+            timed[1] = true;
         } else {
             DBuf<unsigned long long> cand;
             AMJ_TRY(cand.alloc(ctx, A.r_n + 1));
             const unsigned g1 = (unsigned)std::min<uint64_t>((A.r_n + 255) / 256, (uint64_t)ctx->num_sms * 16);
             note_launch(ctx);
+            AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
             lftj_tri_bfs_count_kernel<<<g1, 256, 0, ctx->stream>>>(A, cand.p);
             AMJ_CUDA_TRY(cudaGetLastError());
+            AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
+            timed[0] = true;
             AMJ_TRY(scan_exclusive_u64(ctx, (const uint64_t *)cand.p, (uint64_t *)cand.p, A.r_n,
                                        (uint64_t *)cand.p + A.r_n));
             unsigned long long total = 0;
@@ -676,11 +686,14 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
                 const uint64_t tiles = (total + BFS_TILE - 1) / BFS_TILE;
                 const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)ctx->num_sms * per_sm);
                 note_launch(ctx);
+                AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[2], ctx->stream));
                 if (write)
                     lftj_tri_bfs_expand_kernel<true><<<grid, BFS_THREADS, 0, ctx->stream>>>(A, cand.p, total);
                 else
                     lftj_tri_bfs_expand_kernel<false><<<grid, BFS_THREADS, 0, ctx->stream>>>(A, cand.p, total);
                 AMJ_CUDA_TRY(cudaGetLastError());
+                AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[3], ctx->stream));
+                timed[1] = true;
             }
         }
     }
@@ -690,6 +703,10 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
     *count = h.count;
     *checksum = h.checksum;
     if (written) *written = write ? (h.out_cursor < out_cap ? h.out_cursor : out_cap) : 0;
+    if (kernel_ms) {
+        if (timed[0]) kernel_ms[0] += event_ms(ctx->kev[0], ctx->kev[1]);
+        if (timed[1]) kernel_ms[1] += event_ms(ctx->kev[2], ctx->kev[3]);
+    }
     return AMJ_OK;
 }
 

@@ -17,7 +17,7 @@
 namespace amj {
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
-                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg);
+                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms);
 }
 
 using namespace amj;
@@ -80,14 +80,16 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     for (uint64_t lo = 0; rc == AMJ_OK && (lo < nr || (lo == 0 && nr == 0)); lo += slice) {
         const uint64_t hi = std::min(nr, lo + slice);
         uint64_t c = 0, h = 0, w = 0;
-        rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, lo, hi, heavy_deg);
+        rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, lo, hi, heavy_deg,
+                           out->kernel_ms);
         if (rc != AMJ_OK) break;
         if (materialize) {
             int32_t *cols[3] = {nullptr, nullptr, nullptr};
             for (int a = 0; a < 3 && rc == AMJ_OK; a++) rc = dev_alloc(ctx, (void **)&cols[a], (c ? c : 1) * 4);
             uint64_t c2 = 0, h2 = 0;
             if (rc == AMJ_OK)
-                rc = lftj_triangle(ctx, *R, *S, *T, algo, cols, c, &c2, &h2, &w, small_sum, lo, hi, heavy_deg);
+                rc = lftj_triangle(ctx, *R, *S, *T, algo, cols, c, &c2, &h2, &w, small_sum, lo, hi, heavy_deg,
+                                   out->kernel_ms + 2);
             if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
                 rc = fail(AMJ_ECUDA, "LFTJ: write pass disagrees with count pass");
             if (rc == AMJ_OK && ooc) {

@@ -147,7 +147,7 @@ extern "C" int amj_ctx_create(int device, const amj_opts *opts, amj_ctx **out) {
     for (int i = 0; rc == AMJ_OK && i < 2; i++)
         if (cudaStreamCreateWithFlags(&c->side_stream[i], cudaStreamNonBlocking) != cudaSuccess) rc = AMJ_ECUDA;
     for (int i = 0; rc == AMJ_OK && i < 4; i++)
-        if (cudaEventCreate(&c->ev[i]) != cudaSuccess) rc = AMJ_ECUDA;
+        if (cudaEventCreate(&c->ev[i]) != cudaSuccess || cudaEventCreate(&c->kev[i]) != cudaSuccess) rc = AMJ_ECUDA;
     if (rc == AMJ_OK && cudaMalloc((void **)&c->d_status, sizeof(DevStatus)) != cudaSuccess) rc = AMJ_ENOMEM;
     if (rc == AMJ_OK && cudaMallocHost((void **)&c->h_status, sizeof(DevStatus)) != cudaSuccess) rc = AMJ_ENOMEM;
     if (rc == AMJ_OK && cudaMemset(c->d_status, 0, sizeof(DevStatus)) != cudaSuccess) rc = AMJ_ECUDA;
@@ -172,8 +172,10 @@ extern "C" void amj_ctx_destroy(amj_ctx *c) {
     if (!c) return;
     (void)cudaSetDevice(c->device);
     if (c->stream) (void)cudaStreamSynchronize(c->stream);
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 4; i++) {
         if (c->ev[i]) (void)cudaEventDestroy(c->ev[i]);
+        if (c->kev[i]) (void)cudaEventDestroy(c->kev[i]);
+    }
     for (int i = 0; i < 2; i++)
         if (c->side_stream[i]) (void)cudaStreamDestroy(c->side_stream[i]);
     if (c->d_status) (void)cudaFree(c->d_status);

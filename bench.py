@@ -9,22 +9,28 @@ the radix sort, then the leapfrog intersection, returning count and
 checksum.  The unit of work is one output tuple (one triangle).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--algo DFS|BFS|AMHJ]
+                  [--algo DFS|BFS|AMHJ] [--scale S] [--workload triangle|chain]
+
+--scale S runs the same workload on a smaller R-MAT graph (2^S vertices,
+2^(S+4) edges), for profiling.  --workload chain runs the 3-way chain join
+R1(a,b) R2(b,c) R3(c,d) (3 x 1M rows, keys uniform in [0, 2^18), seeds 1-3)
+through AMHJ (count + checksum, hash builds included), with the reference's
+own MHJ-CPU (compiled from its sources into oracle/_ref) as CPU baseline.
 
 * value: tuples/s with the input resident on the device (whole job: sum of
   the ranks' tuples / max over ranks of the timed K steps).
 * e2e: the same metric through the C ABI with host buffers: every step copies
-  the edge relation from pinned host memory to the device, runs the query and
+  the relations from pinned host memory to the device, runs the query and
   reads the 16-byte (count, checksum) result back.
-* roofline: the intersection kernel, HBM-bound; algorithmic bytes per launch
-  = every edge read once (8 B) + two row-pointer pairs per edge (32 B) + the
-  shorter child list of every edge read once (4 B x min(d+(a), d+(b))).
-* cpu_baseline: the CPU oracle's triangle restatement on all host cores over
-  the full workload (the reference has no CPU triangle implementation; its
-  MHJ-CPU hard-codes a single-key compare that is wrong for cyclic queries).
+* roofline: the intersection kernels (triangle) or the probe kernel (chain),
+  timed with CUDA events inside the library; algorithmic bytes per launch
+  as documented below; traffic from the committed ncu capture.
+* cpu_baseline: triangle: the oracle's restatement on all host cores (the
+  reference has no CPU triangle; its MHJ-CPU hard-codes a single-key compare
+  that is wrong for cyclic queries); chain: the reference MHJ-CPU.
 
 With N > 1 (torchrun) every rank runs its own independent instance of the
-workload (graph seed 20 + rank): per-GPU work is fixed, no data-path
+workload (seed offset by rank): per-GPU work is fixed, no data-path
 collective; the ranks' counts are summed once after timing.
 """
 from __future__ import annotations
@@ -32,6 +38,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -43,7 +50,7 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-SCALE, NEDGES, RMAT_ABC, SEED = 20, 1 << 24, (0.57, 0.19, 0.19), 20
+SCALE, RMAT_ABC, SEED = 20, (0.57, 0.19, 0.19), 20
 METRIC = "join output tuples/sec"
 L2_FLUSH_BYTES = 256 << 20
 
@@ -109,166 +116,269 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def workload(rank: int):
-    from accmultiwayjoins_b200 import data
-    return data.rmat(SCALE, NEDGES, *RMAT_ABC, seed=SEED + rank)
+# ------------------------------------------------------------------ workloads
+
+class Triangle:
+    def __init__(self, args, rank):
+        from accmultiwayjoins_b200 import data
+        self.scale = args.scale
+        self.nedges = 1 << (self.scale + 4)
+        self.algo = args.algo
+        self.src, self.dst = data.rmat(self.scale, self.nedges, *RMAT_ABC, seed=SEED + rank)
+        self.E = int(self.src.shape[0])
+        self.h2d = 8 * self.E
+
+    def describe(self, rank_note):
+        return (f"triangle R(a,b)S(b,c)T(a,c), R-MAT scale {self.scale}, {self.nedges} edges "
+                f"(0.57,0.19,0.19,0.05), seed {SEED}{rank_note}; "
+                f"{'AMHJ TRI' if self.algo == 'AMHJ' else 'ALFTJ-' + self.algo} count+checksum incl. index build")
+
+    def device_relations(self, ctx, dev):
+        import torch
+        return [ctx.relation([torch.from_numpy(self.src).to(dev), torch.from_numpy(self.dst).to(dev)], [0, 1])]
+
+    def host_relations(self, ctx, pinned):
+        return [ctx.relation([pinned[0], pinned[1]], [0, 1])]
+
+    def host_columns(self):
+        return [self.src, self.dst]
+
+    def run(self, ctx, rels):
+        if self.algo == "AMHJ":
+            return ctx.amhj("TRI", rels, ws=1)
+        return ctx.lftj(rels, algo=self.algo, ws=1)
+
+    def algorithmic_bytes(self):
+        """Per intersection: every edge once (8 B), two row-pointer pairs
+        (32 B) and the shorter child list of the edge once (4 B each)."""
+        deg = np.bincount(self.src, minlength=1 << self.scale).astype(np.int64)
+        shorter = np.minimum(deg[self.src], deg[self.dst])
+        return self.E * (8 + 32) + 4 * int(shorter.sum())
+
+    def kernel_name(self):
+        return "lftj_tri_bitmap_kernel + lftj_tri_dfs_kernel (intersection)"
+
+    def cpu_baseline(self):
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        cnt, chk = O.triangle(self.src, self.dst, nthreads=cores)
+        sec = time.perf_counter() - t0
+        return cnt, chk, sec, cores, "port", "the full workload once (oracle triangle restatement)"
 
 
-def algorithmic_bytes(src, dst) -> int:
-    deg = np.bincount(src, minlength=1 << SCALE).astype(np.int64)
-    shorter = np.minimum(deg[src], deg[dst])
-    return int(src.shape[0]) * (8 + 32) + 4 * int(shorter.sum())
+class Chain:
+    B = 1 << 19   # buckets = floorPow2(1e6)
 
+    def __init__(self, args, rank):
+        from accmultiwayjoins_b200 import data
+        self.rels = data.chain_relations(1_000_000, 1 << 18, 3, seed=1 + 3 * rank)
+        self.h2d = sum(4 * len(c[0]) * len(c) for c, _ in self.rels)
+
+    def describe(self, rank_note):
+        return ("3-way chain R1(a,b)R2(b,c)R3(c,d), 3 x 1M rows, keys U[0,2^18), seeds 1,2,3" + rank_note +
+                "; AMHJ NORMAL count+checksum incl. hash builds")
+
+    def device_relations(self, ctx, dev):
+        import torch
+        return [ctx.relation([torch.from_numpy(c).to(dev) for c in cols], a) for cols, a in self.rels]
+
+    def host_relations(self, ctx, pinned):
+        out, i = [], 0
+        for cols, a in self.rels:
+            out.append(ctx.relation(pinned[i:i + len(cols)], a))
+            i += len(cols)
+        return out
+
+    def host_columns(self):
+        return [c for cols, _ in self.rels for c in cols]
+
+    def run(self, ctx, rels):
+        return ctx.amhj("NORMAL", rels)
+
+    def algorithmic_bytes(self):
+        """Per probe row: its two columns (8 B) and its level-0 bucket bounds
+        (8 B); per level-0 candidate its two co-located columns (8 B) and, for
+        a match, its level-1 bucket bounds (8 B); per level-1 candidate its
+        two columns (8 B)."""
+        (p0, p1), _ = self.rels[0]
+        (b0, b1), _ = self.rels[1]
+        (c0, _), _ = self.rels[2]
+        m = self.B - 1
+        n1 = np.bincount(b0 & m, minlength=self.B).astype(np.int64)
+        n2 = np.bincount(c0 & m, minlength=self.B).astype(np.int64)
+        cand0 = int(n1[p1 & m].sum())
+        per_key = np.zeros(1 << 18, np.int64)        # level-1 candidates behind each level-1 key
+        np.add.at(per_key, b0, n2[b1 & m])
+        match0 = int(np.bincount(b0, minlength=1 << 18)[p1].sum())
+        cand1 = int(per_key[p1].sum())
+        return len(p0) * 16 + cand0 * 8 + match0 * 8 + cand1 * 8
+
+    def kernel_name(self):
+        return "amhj_probe_kernel (count pass)"
+
+    def cpu_baseline(self):
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        if O.ref_available():
+            cnt, chk, sec = O.mhj_reference(self.rels, nthreads=cores)
+            return cnt, chk, sec, cores, "reference", "the full workload once (reference MHJ-CPU, TBJ call timed)"
+        t0 = time.perf_counter()
+        cnt, chk = O.mhj(self.rels, nthreads=cores)
+        return cnt, chk, time.perf_counter() - t0, cores, "port", "the full workload once (oracle restatement)"
+
+
+def make_workload(args, rank):
+    return Chain(args, rank) if args.workload == "chain" else Triangle(args, rank)
+
+
+def profiled_traffic(args):
+    """DRAM bytes per measured launch from the committed ncu capture of the
+    full-size triangle workload, or None."""
+    if args.workload != "triangle" or args.scale != SCALE or args.algo != "DFS":
+        return None
+    p = os.path.join(ROOT, "profiles", "lftj_intersect_c2_traffic.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_intersection:\s*([0-9]+)", open(p).read())
+    return int(m.group(1)) if m else None
+
+
+# ------------------------------------------------------------------ arms
 
 def run_reference(args, rank, world):
-    """CPU arm: the oracle's triangle restatement on all host threads."""
+    """CPU arm: the reference's CPU implementation of the workload (MHJ-CPU
+    for the chain; the oracle's triangle restatement for the triangle) on all
+    host threads.  Rank 0 only."""
     if rank != 0:
         return
-    from oracle import oracle as O
-    src, dst = workload(0)
-    cores = os.cpu_count() or 1
+    wl = make_workload(args, 0)
     times = []
-    count = 0
+    cnt = 0
+    kind = sample = None
+    cores = os.cpu_count() or 1
     for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        count, chk = O.triangle(src, dst, nthreads=cores)
-        dt = time.perf_counter() - t0
+        cnt, _, sec, cores, kind, sample = wl.cpu_baseline()
         if i >= args.warmup:
-            times.append(dt)
+            times.append(sec)
     sec = sum(times) / len(times)
-    value = count / sec
+    value = cnt / sec
     line = {
         "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT)", "impl": "reference",
-        "config": {"workload": f"triangle R(a,b)S(b,c)T(a,c), R-MAT scale {SCALE}, {NEDGES} edges "
-                               f"(0.57,0.19,0.19,0.05), seed {SEED}", "edges_after_cleaning": int(src.shape[0]),
-                   "algo": "CPU merge-intersection restatement", "l2": "n/a (CPU)"},
-        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": "port",
-                         "sample": "the full workload per step"},
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": wl.describe(""), "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 def run_ours(args, rank, world, local_rank):
-    import torch
     import ctypes as C
+    import torch
     from accmultiwayjoins_b200 import Context, _lib as L
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    src, dst = workload(rank)
-    E = int(src.shape[0])
+    wl = make_workload(args, rank)
     stream = torch.cuda.current_stream(dev)
     ctx = Context(local_rank)
     lib = L.load()
+    # run the library on torch's stream so torch's CUDA events see its kernels
     L.check(lib.amj_ctx_set_stream(ctx.handle, C.c_void_p(stream.cuda_stream)), "set_stream")
-    rel = ctx.relation([torch.from_numpy(src).to(dev), torch.from_numpy(dst).to(dev)], [0, 1])
+    rels = wl.device_relations(ctx, dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
-    algo = args.algo
-
-    def step():
-        if algo == "AMHJ":
-            return ctx.amhj("TRI", [rel], ws=1)
-        return ctx.lftj([rel], algo=algo, ws=1)
 
     for _ in range(args.warmup):
-        r = step()
+        r = wl.run(ctx, rels)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     sampler = ClockSampler(local_rank)
     sampler.start()
-    launches0 = C.c_uint64()
-    L.check(lib.amj_ctx_launch_count(ctx.handle, C.byref(launches0)))
+    l0 = C.c_uint64()
+    L.check(lib.amj_ctx_launch_count(ctx.handle, C.byref(l0)))
     torch.cuda.synchronize()
-    evs = []
-    probe_ms = []
-    build_ms = []
-    count = 0
+    evs, probe_ms, build_ms, kern_ms = [], [], [], []
     t_wall0 = time.perf_counter()
     for _ in range(args.steps):
-        flush.zero_()  # L2 flush (256 MB) outside the timed events
+        flush.zero_()  # L2 flush (256 MB write) outside the timed events
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        r = step()
+        r = wl.run(ctx, rels)
         b.record(stream)
         evs.append((a, b))
         probe_ms.append(r.probe_ms)
         build_ms.append(r.build_ms)
-        count = r.count
-        checksum = r.checksum
+        kern_ms.append(r.kernel_ms[0] + r.kernel_ms[1])
+        count, checksum = r.count, r.checksum
     torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
     t_wall = time.perf_counter() - t_wall0
-    launches1 = C.c_uint64()
-    L.check(lib.amj_ctx_launch_count(ctx.handle, C.byref(launches1)))
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    ms = sum(step_ms) / len(step_ms)
-    # e2e through the C ABI with host buffers
-    hs = torch.from_numpy(src).pin_memory()
-    hd = torch.from_numpy(dst).pin_memory()
+    l1 = C.c_uint64()
+    L.check(lib.amj_ctx_launch_count(ctx.handle, C.byref(l1)))
+    ms = sum(a.elapsed_time(b) for a, b in evs) / len(evs)
+
+    # end to end through the C ABI from pinned host buffers
+    pinned = [torch.from_numpy(c).pin_memory().numpy() for c in wl.host_columns()]
     e2e_ms = []
     for i in range(args.warmup + args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        hr = ctx.relation([hs.numpy(), hd.numpy()], [0, 1])
-        if algo == "AMHJ":
-            rr = ctx.amhj("TRI", [hr], ws=1)
-        else:
-            rr = ctx.lftj([hr], algo=algo, ws=1)
-        assert (rr.count, rr.checksum) == (count, checksum)
-        hr.release()
+        hr = wl.host_relations(ctx, pinned)
+        rr = wl.run(ctx, hr)
+        for h in hr:
+            h.release()
         dt = (time.perf_counter() - t0) * 1e3
+        assert (rr.count, rr.checksum) == (count, checksum)
         if i >= args.warmup:
             e2e_ms.append(dt)
     clocks = sampler.stop()
     e2e_mean = sum(e2e_ms) / len(e2e_ms)
 
-    # whole job: max time over ranks, tuples summed over ranks
     tot_count, max_ms, max_e2e = count, ms, e2e_mean
     if world > 1:
-        t = torch.tensor([float(count), ms, e2e_mean], dtype=torch.float64, device=dev)
-        cnt = torch.tensor([count], dtype=torch.float64, device=dev)
+        cnt = torch.tensor([float(count)], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(cnt)
-        mx = t.clone()
+        mx = torch.tensor([ms, e2e_mean], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
-        tot_count, max_ms, max_e2e = int(cnt.item()), mx[1].item(), mx[2].item()
+        tot_count, max_ms, max_e2e = int(cnt.item()), mx[0].item(), mx[1].item()
     if rank != 0:
+        ctx.close()
         return
     hbm, peak_kind = peaks()
-    alg_bytes = algorithmic_bytes(src, dst)
-    kern_ms = sum(probe_ms) / len(probe_ms)
-    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9 if algo == "DFS" else None
+    alg = wl.algorithmic_bytes()
+    kms = sum(kern_ms) / len(kern_ms)
+    achieved = alg / (kms * 1e-3) / 1e9 if kms > 0 else None
+    rank_note = "+rank" if world > 1 else ""
     line = {
         "metric": METRIC, "value": tot_count / (max_ms * 1e-3), "unit": "tuples/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT)",
-        "config": {"workload": f"triangle R(a,b)S(b,c)T(a,c), R-MAT scale {SCALE}, {NEDGES} edges "
-                               f"(0.57,0.19,0.19,0.05), seed {SEED}+rank; ALFTJ-{algo} count+checksum incl. trie build",
-                   "edges_after_cleaning": E, "triangles_per_rank": count,
-                   "l2": "flushed between steps (256 MB write)", "parallelism": f"independent instance per GPU x{world}"},
-        "e2e": {"value": tot_count / (max_e2e * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": 8 * E,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+        "config": {"workload": wl.describe(rank_note), "tuples_per_rank": count,
+                   "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"independent instance per GPU x{world}"},
+        "e2e": {"value": tot_count / (max_e2e * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": wl.h2d,
                 "d2h_bytes_per_step": 16, "ms_per_step": max_e2e},
-        "gpu_launches": int(launches1.value - launches0.value),
-        "phase_ms": {"build": sum(build_ms) / len(build_ms), "intersect": kern_ms},
+        "gpu_launches": int(l1.value - l0.value),
+        "phase_ms": {"build": sum(build_ms) / len(build_ms), "join": sum(probe_ms) / len(probe_ms),
+                     "join_kernels": kms},
         "clocks": clocks,
         "wall_s_timed": t_wall,
     }
+    if isinstance(wl, Triangle):
+        line["config"]["edges_after_cleaning"] = wl.E
     if achieved is not None:
         line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                            "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
-                            "kernel": "lftj_tri_dfs_kernel", "alg_bytes_per_launch": alg_bytes}
+                            "frac": achieved / hbm, "traffic": profiled_traffic(args), "peak_kind": peak_kind,
+                            "kernel": wl.kernel_name(), "alg_bytes_per_launch": alg}
     if not args.no_cpu_baseline:
-        from oracle import oracle as O
-        cores = os.cpu_count() or 1
-        t0 = time.perf_counter()
-        c_cnt, c_chk = O.triangle(src, dst, nthreads=cores)
-        sec = time.perf_counter() - t0
-        line["cpu_baseline"] = {"value": c_cnt / sec, "unit": "tuples/s", "cores": cores, "kind": "port",
-                                "sample": "the full workload once (oracle triangle restatement)",
-                                "matches_gpu": bool((c_cnt, c_chk) == (count, checksum))}
+        c_cnt, c_chk, sec, cores, kind, sample = wl.cpu_baseline()
+        line["cpu_baseline"] = {"value": c_cnt / sec, "unit": "tuples/s", "cores": cores, "kind": kind,
+                                "sample": sample, "matches_gpu": bool((c_cnt, c_chk) == (count, checksum))}
     print(json.dumps(line), flush=True)
     ctx.close()
 
@@ -280,9 +390,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--algo", default="DFS", choices=["DFS", "BFS", "AMHJ"])
+    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain"])
+    ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    if args.impl == "ours":
+        args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
