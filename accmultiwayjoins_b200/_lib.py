@@ -66,7 +66,7 @@ class amj_result(C.Structure):
         ("build_ms", C.c_double),
         ("probe_ms", C.c_double),
         ("total_ms", C.c_double),
-        ("stats", C.c_uint64 * 8),
+        ("stats", C.c_uint64 * 12),
         ("kernel_ms", C.c_double * 4),
         ("priv", C.c_void_p),
     ]

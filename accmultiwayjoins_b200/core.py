@@ -28,7 +28,7 @@ _ALGO = {"BFS": L.AMJ_LFTJ_BFS, "DFS": L.AMJ_LFTJ_DFS, 0: L.AMJ_LFTJ_BFS, 1: L.A
 _LAYOUT = {"bucket": L.AMJ_LAYOUT_BUCKET, "oa": L.AMJ_LAYOUT_OPEN_ADDR, "open_addr": L.AMJ_LAYOUT_OPEN_ADDR,
            "cuckoo": L.AMJ_LAYOUT_CUCKOO}
 STAT_NAMES = ["tasks_pushed", "tasks_popped", "residual_units", "rows_written_main", "rows_written_residual",
-              "estimate", "fallbacks", "slices"]
+              "estimate", "fallbacks", "slices", "fib_keys", "fib_rows_cached", "fib_rows_served", "batch_queries"]
 
 
 @dataclass
@@ -153,7 +153,7 @@ class Context:
                     cols.append(np.zeros(0, np.int32))
         out = Result(count=int(res.count), checksum=int(res.checksum), num_attrs=int(res.num_attrs),
                      build_ms=float(res.build_ms), probe_ms=float(res.probe_ms), total_ms=float(res.total_ms),
-                     stats={STAT_NAMES[i]: int(res.stats[i]) for i in range(8)},
+                     stats={STAT_NAMES[i]: int(res.stats[i]) for i in range(len(STAT_NAMES))},
                      kernel_ms=tuple(float(res.kernel_ms[i]) for i in range(4)), columns=cols)
         L.load().amj_result_release(C.byref(res))
         return out

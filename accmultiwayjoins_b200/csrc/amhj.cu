@@ -155,6 +155,11 @@ struct ExecScratch {
     DBuf<Task> tasks;
     DBuf<unsigned int> ready;
     DBuf<Breakpoint> units;
+    // frequent-item buffer
+    DBuf<int32_t> fib_keys;
+    DBuf<uint32_t> fib_idx;
+    DBuf<unsigned long long> fib_off;
+    DBuf<int32_t> fib_cols[AMJ_MAX_ATTRS];
 };
 
 double event_ms(cudaEvent_t a, cudaEvent_t b) {
@@ -308,6 +313,7 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
         pr->checksum = h.checksum;
         res->stats[0] += h.tasks_pushed;
         res->stats[1] += h.tasks_popped;
+        res->stats[10] += h.fib_rows;
         return AMJ_OK;
     }
     if (!dro) {
@@ -319,6 +325,7 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
         const uint64_t total = h.count;
         res->stats[0] += h.tasks_pushed;
         res->stats[1] += h.tasks_popped;
+        res->stats[10] += h.fib_rows;
         AMJ_TRY(alloc_cols(ctx, k, total, pr->cols));
         for (int a = 0; a < k; a++) P.out[a] = pr->cols[a];
         P.out_cap = total;
@@ -418,6 +425,221 @@ static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bo
         return fail(AMJ_ECUDA, "AMHJ DRO: residual pass wrote " + std::to_string(h.out_cursor) + " rows, expected " +
                                    std::to_string(total - written));
     res->stats[4] += h.out_cursor;
+    return AMJ_OK;
+}
+
+// ---------------------------------------------------------------- FIB --
+// Frequent-item buffering (reference AMHJ_WS_FIB, MHJ-GPU/Joins/AMHJ_WS_FIB.cuh,
+// SubfixBuffer.cuh:65-98): the suffix of the query below some level d,
+// when it depends on nothing but the key bound at d, is the same for every
+// partial tuple arriving with the same key.  The frequent keys of level d
+// (those of its largest buckets, read off the bucket index instead of a CPU
+// Topkapi sketch) get their suffix tuples materialised once, by the same
+// probe kernel run on a probe relation made of those keys; the main probe
+// then emits a cached key's suffix tuples directly.  The checksum needs the
+// tuples themselves (a tuple's hash chains its prefix into its suffix), so
+// the cache holds tuples, not counts.
+
+constexpr uint32_t FIB_MAX_KEYS = 256;
+constexpr uint32_t FIB_MIN_BUCKET = 16;
+constexpr uint64_t FIB_MAX_ROWS = 1ull << 26;
+
+// the shallowest level d >= 1 with at least two levels below it whose suffix
+// depends only on the key attribute of level d; -1 if none
+static int fib_choose_level(const HostPlan &hp, uint32_t *suffix_attrs) {
+    for (int d = 1; d + 1 < hp.L; d++) {
+        const LevelSpec &ld = hp.lv[d];
+        if (ld.key_mode != KEY_SINGLE) continue;
+        const int ka = ld.attr[0];
+        uint32_t suffix = 0;
+        bool ok = true;
+        for (int e = d; e < hp.L && ok; e++) {
+            const LevelSpec &le = hp.lv[e];
+            for (int c = 0; c < le.ncols; c++) {
+                const int a = le.attr[c];
+                if ((le.cmp_mask >> c) & 1) {
+                    if (a != ka && !((suffix >> a) & 1)) ok = false;
+                }
+            }
+            for (int c = 0; c < le.ncols; c++)
+                if ((le.bind_mask >> c) & 1) suffix |= 1u << le.attr[c];
+        }
+        if (ok) {
+            *suffix_attrs = suffix;
+            return d;
+        }
+    }
+    return -1;
+}
+
+__global__ void fib_bucket_sizes_kernel(const uint32_t *__restrict__ buc_ptrs, uint64_t B,
+                                        uint64_t *__restrict__ items) {
+    for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < B; b += (uint64_t)gridDim.x * blockDim.x)
+        items[b] = ((uint64_t)(buc_ptrs[b + 1] - buc_ptrs[b]) << 32) | b;
+}
+
+__global__ void fib_first_keys_kernel(const uint64_t *__restrict__ items, uint32_t n,
+                                      const uint32_t *__restrict__ buc_ptrs, const int32_t *__restrict__ key_col,
+                                      int32_t *__restrict__ keys) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) keys[i] = (items[i] >> 32) ? key_col[buc_ptrs[(uint32_t)items[i]]] : OA_EMPTY_KEY;
+}
+
+// cache index of every suffix tuple (via the key hash set), packed with its row
+__global__ void fib_pack_kernel(const int32_t *__restrict__ key_col, uint64_t n, const int32_t *__restrict__ set_keys,
+                                const uint32_t *__restrict__ set_idx, uint32_t mask, uint64_t *__restrict__ items,
+                                unsigned long long *__restrict__ counts) {
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
+        const int32_t key = key_col[r];
+        uint32_t s = hash_key(key) & mask, idx = 0;
+        for (uint32_t t = 0; t <= mask; t++) {
+            if (set_keys[s] == key) {
+                idx = set_idx[s];
+                break;
+            }
+            s = (s + 1) & mask;
+        }
+        items[r] = ((uint64_t)idx << 32) | (uint32_t)r;
+        atomicAdd(&counts[idx], 1ull);
+    }
+}
+
+__global__ void fib_gather_kernel(const uint64_t *__restrict__ items, uint64_t n, const int32_t *__restrict__ src,
+                                  int32_t *__restrict__ dst) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[(uint32_t)items[i]];
+}
+
+static unsigned fib_grid(amj_ctx *ctx, uint64_t n) {
+    uint64_t g = (n + 255) / 256, cap = (uint64_t)ctx->num_sms * 16;
+    return (unsigned)(g == 0 ? 1 : (g > cap ? cap : g));
+}
+
+static int build_fib(amj_ctx *ctx, const HostPlan &hp, const std::vector<const HashIndex *> &lvix, ProbeLaunch &PL,
+                     ExecScratch &X, amj_result *res) {
+    ProbePlan &P = PL.P;
+    P.fib_level = -1;
+    uint32_t suffix = 0;
+    const int d = fib_choose_level(hp, &suffix);
+    if (d < 0) return AMJ_OK;
+    const HashIndex &ix = *lvix[d];
+    if (ix.layout != AMJ_LAYOUT_BUCKET || ix.n < FIB_MIN_BUCKET) return AMJ_OK;
+    // 1. frequent keys: first keys of the largest buckets
+    const uint64_t B = (uint64_t)ix.mask + 1;
+    DBuf<uint64_t> a, b;
+    AMJ_TRY(a.alloc(ctx, B));
+    AMJ_TRY(b.alloc(ctx, B));
+    note_launch(ctx);
+    fib_bucket_sizes_kernel<<<fib_grid(ctx, B), 256, 0, ctx->stream>>>(ix.buc_ptrs.p, B, a.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    uint64_t *sorted = nullptr;
+    AMJ_TRY(radix_sort_u64(ctx, a.p, b.p, B, SK_IDENT, 32, 64, &sorted));
+    const uint32_t take = (uint32_t)std::min<uint64_t>(B, FIB_MAX_KEYS);
+    std::vector<uint64_t> top(take);
+    AMJ_CUDA_TRY(cudaMemcpyAsync(top.data(), sorted + (B - take), take * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    DBuf<int32_t> keys_d;
+    AMJ_TRY(keys_d.alloc(ctx, take));
+    note_launch(ctx);
+    fib_first_keys_kernel<<<(take + 255) / 256, 256, 0, ctx->stream>>>(sorted + (B - take), take, ix.buc_ptrs.p,
+                                                                       ix.cols[0].p, keys_d.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    std::vector<int32_t> keys(take);
+    AMJ_CUDA_TRY(cudaMemcpyAsync(keys.data(), keys_d.p, take * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    std::vector<int32_t> freq;
+    for (uint32_t i = 0; i < take; i++)
+        if ((top[i] >> 32) >= FIB_MIN_BUCKET && keys[i] != OA_EMPTY_KEY) freq.push_back(keys[i]);
+    std::sort(freq.begin(), freq.end());
+    freq.erase(std::unique(freq.begin(), freq.end()), freq.end());
+    if (freq.empty()) return AMJ_OK;
+    const uint32_t K = (uint32_t)freq.size();
+    AMJ_CUDA_TRY(cudaMemcpyAsync(keys_d.p, freq.data(), K * 4, cudaMemcpyHostToDevice, ctx->stream));
+    // 2. their suffix tuples: the sub-plan below level d probed by the keys
+    ProbeLaunch SL = PL;
+    ProbePlan &S = SL.P;
+    S.L = (int8_t)(hp.L - d);
+    for (int l = 0; l < S.L; l++) S.lv[l] = P.lv[d + l];
+    S.probe_ncols = 1;
+    S.probe_col[0] = keys_d.p;
+    S.probe_attr[0] = (int8_t)hp.lv[d].attr[0];
+    S.row_lo = 0;
+    S.row_hi = K;
+    S.warp_bytes = (uint32_t)S.L * S.depth_bytes;
+    S.lbs = 0;
+    S.dro = 0;
+    S.fib_level = -1;
+    SL.batch_stride = 1;
+    SL.batch_count = (K + 31) / 32;
+    ProbeState h{};
+    AMJ_CUDA_TRY(cudaMemsetAsync(SL.st, 0, sizeof(ProbeState), ctx->stream));
+    AMJ_TRY(launch_probe(ctx, SL, PM_COUNT, false));
+    AMJ_TRY(read_state(ctx, SL.st, &h, "FIB suffix count"));
+    const uint64_t T = h.count;
+    if (T == 0 || T > FIB_MAX_ROWS) return AMJ_OK;
+    const int k = hp.k;
+    int32_t *tcols[AMJ_MAX_ATTRS] = {};
+    std::vector<DBuf<int32_t>> tmp(k);
+    for (int at = 0; at < k; at++) {
+        AMJ_TRY(tmp[at].alloc(ctx, T));
+        tcols[at] = tmp[at].p;
+        S.out[at] = tcols[at];
+    }
+    S.out_cap = T;
+    AMJ_CUDA_TRY(cudaMemsetAsync(SL.st, 0, sizeof(ProbeState), ctx->stream));
+    AMJ_TRY(launch_probe(ctx, SL, PM_WRITE, false));
+    AMJ_TRY(read_state(ctx, SL.st, &h, "FIB suffix write"));
+    if (h.out_cursor != T) return fail(AMJ_ECUDA, "FIB: suffix write disagrees with its count");
+    // 3. group the suffix tuples by key: hash set of the keys, sort by cache index
+    uint32_t slots = 512;
+    while (slots < 2 * K) slots <<= 1;
+    std::vector<int32_t> skey(slots, OA_EMPTY_KEY);
+    std::vector<uint32_t> sidx(slots, 0);
+    for (uint32_t i = 0; i < K; i++) {
+        uint32_t s = hash_key(freq[i]) & (slots - 1);
+        while (skey[s] != OA_EMPTY_KEY) s = (s + 1) & (slots - 1);
+        skey[s] = freq[i];
+        sidx[s] = i;
+    }
+    AMJ_TRY(X.fib_keys.alloc(ctx, slots));
+    AMJ_TRY(X.fib_idx.alloc(ctx, slots));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(X.fib_keys.p, skey.data(), slots * 4, cudaMemcpyHostToDevice, ctx->stream));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(X.fib_idx.p, sidx.data(), slots * 4, cudaMemcpyHostToDevice, ctx->stream));
+    DBuf<uint64_t> ia, ib;
+    DBuf<unsigned long long> counts;
+    AMJ_TRY(ia.alloc(ctx, T));
+    AMJ_TRY(ib.alloc(ctx, T));
+    AMJ_TRY(counts.alloc(ctx, K));
+    AMJ_CUDA_TRY(cudaMemsetAsync(counts.p, 0, K * 8, ctx->stream));
+    note_launch(ctx);
+    fib_pack_kernel<<<fib_grid(ctx, T), 256, 0, ctx->stream>>>(tcols[hp.lv[d].attr[0]], T, X.fib_keys.p, X.fib_idx.p,
+                                                                slots - 1, ia.p, counts.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    uint64_t *by_key = nullptr;
+    int kbits = 1;
+    while ((1u << kbits) < K) kbits++;
+    AMJ_TRY(radix_sort_u64(ctx, ia.p, ib.p, T, SK_IDENT, 32, 32 + kbits, &by_key));
+    for (int at = 0; at < k; at++) {
+        if (!((suffix >> at) & 1)) continue;
+        AMJ_TRY(X.fib_cols[at].alloc(ctx, T));
+        note_launch(ctx);
+        fib_gather_kernel<<<fib_grid(ctx, T), 256, 0, ctx->stream>>>(by_key, T, tcols[at], X.fib_cols[at].p);
+        AMJ_CUDA_TRY(cudaGetLastError());
+        P.fib_cols[at] = X.fib_cols[at].p;
+    }
+    std::vector<unsigned long long> cnt(K), off(K + 1, 0);
+    AMJ_CUDA_TRY(cudaMemcpyAsync(cnt.data(), counts.p, K * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (uint32_t i = 0; i < K; i++) off[i + 1] = off[i] + cnt[i];
+    AMJ_TRY(X.fib_off.alloc(ctx, K + 1));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(X.fib_off.p, off.data(), (K + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    P.fib_keys = X.fib_keys.p;
+    P.fib_slot_idx = X.fib_idx.p;
+    P.fib_off = X.fib_off.p;
+    P.fib_mask = slots - 1;
+    P.fib_suffix_attrs = suffix;
+    P.fib_level = d;
+    res->stats[8] = K;
+    res->stats[9] = T;
     return AMJ_OK;
 }
 
@@ -637,6 +859,8 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
         PL.task_ready = X.ready.p;
     }
     AMJ_TRY(status_reset(ctx));
+    P.fib_level = -1;
+    if (fib && !dro && hp.L >= 3) AMJ_TRY(build_fib(ctx, hp, lvix, PL, X, out));
 
     int rc = AMJ_OK;
     if (hp.L == 0) {

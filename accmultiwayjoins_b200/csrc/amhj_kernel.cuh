@@ -218,7 +218,7 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
     const int lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
     char *wbase = smem + (threadIdx.x >> 5) * P.warp_bytes;
-    unsigned long long cnt = 0, chk = 0;
+    unsigned long long cnt = 0, chk = 0, fib_served = 0;
     int depth = -1;
 
     // unit bookkeeping for direct result output
@@ -391,8 +391,9 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
         if (lane == 0) F.meta[0] = cursor + 32;
         const LevelDesc &lv = P.lv[depth];
         const unsigned long long j = cursor + lane;
-        bool matched = false;
+        bool matched = false, cached = false;
         int o = 0;
+        uint32_t cslot = 0;
         int32_t cv[4] = {0, 0, 0, 0};
         if (j < total) {
             int lo = 0, hi = n - 1;
@@ -403,12 +404,49 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
             }
             o = lo;
             const unsigned long long start = o ? F.psum[o - 1] : 0ull;
-            const uint32_t slot = candidate_slot(lv, F.s[o], F.aux[o], F.m8[o], (uint32_t)(j - start));
-            load_candidate(lv, slot, lv.cmp_mask | lv.bind_mask, cv);
-            matched = true;
+            if (depth == P.fib_level && (F.m8[o] & FIB_FLAG)) {
+                cached = true;
+                cslot = F.s[o] + (uint32_t)(j - start);
+            } else {
+                const uint32_t slot = candidate_slot(lv, F.s[o], F.aux[o], F.m8[o], (uint32_t)(j - start));
+                load_candidate(lv, slot, lv.cmp_mask | lv.bind_mask, cv);
+                matched = true;
 #pragma unroll
-            for (int c = 0; c < 4; c++)
-                if (c < lv.ncols && ((lv.cmp_mask >> c) & 1)) matched &= (cv[c] == F.vals[lv.attr[c] * 32 + o]);
+                for (int c = 0; c < 4; c++)
+                    if (c < lv.ncols && ((lv.cmp_mask >> c) & 1)) matched &= (cv[c] == F.vals[lv.attr[c] * 32 + o]);
+            }
+        }
+        if (depth == P.fib_level) {
+            // frequent-item buffering: cached suffix tuples are emitted here
+            const unsigned cm = __ballot_sync(AMJ_FULL_MASK, cached);
+            if (cm) {
+                int32_t tv[AMJ_MAX_ATTRS];
+                uint64_t h = AMJ_CHECKSUM_SEED;
+                if (cached) {
+#pragma unroll
+                    for (int a = 0; a < AMJ_MAX_ATTRS; a++) {
+                        if (a < P.k) {
+                            const int32_t v = ((P.fib_suffix_attrs >> a) & 1u) ? P.fib_cols[a][cslot] : F.vals[a * 32 + o];
+                            tv[a] = v;
+                            h = amj_hash_step(h, v);
+                        }
+                    }
+                    cnt++;
+                    chk += h;
+                    fib_served++;
+                }
+                if (MODE == PM_WRITE) {
+                    unsigned long long base = 0;
+                    if (lane == 0) base = atomicAdd(&L.st->out_cursor, (unsigned long long)__popc(cm));
+                    base = __shfl_sync(AMJ_FULL_MASK, base, 0);
+                    const unsigned long long pos = base + __popc(cm & lt);
+                    if (cached && pos < P.out_cap) {
+#pragma unroll
+                        for (int a = 0; a < AMJ_MAX_ATTRS; a++)
+                            if (a < P.k) P.out[a][pos] = tv[a];
+                    }
+                }
+            }
         }
         const unsigned mm = __ballot_sync(AMJ_FULL_MASK, matched);
         const int idx = __popc(mm & lt);
@@ -494,8 +532,17 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
 #pragma unroll
             for (int c = 0; c < 4; c++)
                 if (c < lv.ncols && ((lv.bind_mask >> c) & 1)) C.vals[lv.attr[c] * 32 + idx] = cv[c];
-            sz = level_lookup(nl, [&](int a) { return C.vals[a * 32 + idx]; }, s, aux, m8);
-            sz = maybe_split<MODE, WS>(L, nl, C.vals + idx, s, sz, depth + 1);
+            int fi = -1;
+            if (depth + 1 == P.fib_level) fi = fib_find(P, C.vals[nl.key_attr[0] * 32 + idx]);
+            if (fi >= 0) {
+                s = (uint32_t)P.fib_off[fi];
+                sz = (uint32_t)(P.fib_off[fi + 1] - P.fib_off[fi]);
+                aux = (uint32_t)fi;
+                m8 = FIB_FLAG;
+            } else {
+                sz = level_lookup(nl, [&](int a) { return C.vals[a * 32 + idx]; }, s, aux, m8);
+                sz = maybe_split<MODE, WS>(L, nl, C.vals + idx, s, sz, depth + 1);
+            }
             C.s[idx] = s;
             C.aux[idx] = aux;
             C.m8[idx] = m8;
@@ -514,10 +561,12 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
 
     cnt = warp_sum(cnt);
     chk = warp_sum(chk);
+    fib_served = warp_sum(fib_served);
     if (lane == 0 && (cnt || chk)) {
         atomicAdd(&L.st->count, cnt);
         atomicAdd(&L.st->checksum, chk);
     }
+    if (lane == 0 && fib_served) atomicAdd(&L.st->fib_rows, fib_served);
 }
 
 }  // namespace amj

@@ -61,6 +61,15 @@ struct ProbePlan {
     // l0_start[rows] = total); units are 32-candidate chunks of it
     const unsigned long long *l0_start;
     uint32_t lbs;
+    // frequent-item buffering: a depth-fib_level entry whose key is one of
+    // the cached frequent keys takes its suffix tuples from the cache
+    const int32_t *fib_keys;               // hash set of frequent keys, fib_mask+1 slots
+    const uint32_t *fib_slot_idx;          // cache index of the key in each slot
+    const unsigned long long *fib_off;     // suffix tuples of key i: [fib_off[i], fib_off[i+1])
+    const int32_t *fib_cols[AMJ_MAX_ATTRS];
+    uint32_t fib_mask;
+    uint32_t fib_suffix_attrs;             // attributes the cached tuples provide
+    int32_t fib_level;                     // -1: off
 };
 
 struct ProbeState {
@@ -73,6 +82,7 @@ struct ProbeState {
     unsigned int busy;
     unsigned int n_units;
     unsigned long long tasks_pushed, tasks_popped;
+    unsigned long long fib_rows;
 };
 
 struct Task {
@@ -115,6 +125,20 @@ __device__ __forceinline__ Frontier frontier_at(char *wbase, const ProbePlan &P,
     p += 32;
     f.m8 = (uint8_t *)p;
     return f;
+}
+
+constexpr uint8_t FIB_FLAG = 0x80;   // frontier entry served from the frequent-item cache
+
+// cache index of a frequent key, or -1
+__device__ __forceinline__ int fib_find(const ProbePlan &P, int32_t key) {
+    uint32_t s = hash_key(key) & P.fib_mask;
+    for (uint32_t n = 0; n <= P.fib_mask; n++) {
+        const int32_t k = P.fib_keys[s];
+        if (k == key) return (int)P.fib_slot_idx[s];
+        if (k == OA_EMPTY_KEY) return -1;
+        s = (s + 1) & P.fib_mask;
+    }
+    return -1;
 }
 
 __host__ __device__ inline uint32_t frontier_bytes(int k) { return 128u * k + 128 + 128 + 256 + 32 + 32; }

@@ -207,9 +207,10 @@ extern "C" int amj_ctx_launch_count(const amj_ctx *c, uint64_t *out) {
 }
 
 extern "C" const char *amj_stat_name(int i) {
-    static const char *names[8] = {"tasks_pushed", "tasks_popped", "residual_units", "rows_written_main",
-                                   "rows_written_residual", "estimate", "fib_hits", "slices"};
-    return (i >= 0 && i < 8) ? names[i] : "";
+    static const char *names[12] = {"tasks_pushed", "tasks_popped", "residual_units", "rows_written_main",
+                                    "rows_written_residual", "estimate", "fallbacks", "slices",
+                                    "fib_keys", "fib_rows_cached", "fib_rows_served", "batch_queries"};
+    return (i >= 0 && i < 12) ? names[i] : "";
 }
 
 // ---- relations ----

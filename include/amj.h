@@ -104,7 +104,7 @@ typedef struct amj_result {
     double   build_ms;                /* index build, device time              */
     double   probe_ms;                /* join, device time                     */
     double   total_ms;                /* whole call, device time               */
-    uint64_t stats[8];                /* operator counters, see amj_stat_name  */
+    uint64_t stats[12];               /* operator counters, see amj_stat_name  */
     double   kernel_ms[4];            /* device time of the main kernels: ALFTJ DFS
                                          [0] bitmap [1] warp intersection, BFS
                                          [0] candidate count [1] expand ([2], [3]

@@ -194,6 +194,65 @@ def test_amhj_work_sharing_on_skew():
         assert got.stats["tasks_pushed"] > 0 and got.stats["tasks_popped"] == got.stats["tasks_pushed"]
 
 
+def fib_chain(n, dom):
+    """A 4-way chain whose middle join attribute (2) is Zipf-skewed on both
+    sides: the partial tuples reaching R2 concentrate on a few keys, each with
+    a large bucket, so their suffix tuples are worth caching."""
+    r0 = ([data.uniform(n, 0, 5000, 1), data.uniform(n, 0, dom, 2)], [0, 1])
+    r1 = ([data.uniform(n, 0, dom, 3), data.zipf(n, dom, 1.1, 4)], [1, 2])
+    r2 = ([data.zipf(n, dom, 1.1, 5), data.uniform(n, 0, 4000, 6)], [2, 3])
+    r3 = ([data.uniform(n, 0, 4000, 7), data.uniform(n, 0, 1 << 20, 8)], [3, 4])
+    return [r0, r1, r2, r3]
+
+
+def test_amhj_fib_caches_frequent_suffixes():
+    """Frequent-item buffering: same count/checksum as fib=0 and the oracle,
+    and the cache is used (850M tuples, most of them served from it)."""
+    with Context(0) as ctx:
+        rels = fib_chain(20000, 2000)
+        want = O.mhj(rels)
+        rs = rels_on(ctx, rels)
+        off = ctx.amhj("NORMAL", rs, ws=1, fib=0)
+        on = ctx.amhj("NORMAL", rs, ws=1, fib=1)
+        assert (off.count, off.checksum) == want
+        assert (on.count, on.checksum) == want
+        assert on.stats["fib_keys"] > 0 and on.stats["fib_rows_cached"] > 0
+        assert on.stats["fib_rows_served"] > want[0] // 4
+        assert off.stats["fib_keys"] == 0
+
+
+@pytest.mark.parametrize("layout", ["bucket", "oa", "cuckoo"])
+def test_amhj_fib_materialized_and_other_layouts(layout):
+    """Materialised tuples with the cache on; the open-addressing and cuckoo
+    layouts run without a cache and still agree."""
+    with Context(0, layout=layout) as ctx:
+        rels = fib_chain(4000, 2000)
+        cnt, chk, cols = O.mhj(rels, tuples=True)
+        got = ctx.amhj("NORMAL", rels_on(ctx, rels), fib=1, materialize=True)
+        assert (got.count, got.checksum) == (cnt, chk)
+        assert np.array_equal(sorted_rows(got.columns), sorted_rows(cols))
+        if layout == "bucket":
+            assert got.stats["fib_rows_served"] > 0
+
+
+def test_amhj_fib_star_and_out_of_core():
+    """A star join with a shared key (every level keyed on attribute 0) is
+    cacheable below level 1; the cache also serves every slice of an
+    out-of-core run."""
+    n = 5000
+    rels = [([data.zipf(n, 3000, 0.8, 1), data.uniform(n, 0, 1 << 20, 2)], [0, 1]),
+            ([data.uniform(3000, 0, 3000, 3), data.uniform(3000, 0, 1 << 20, 4)], [0, 2]),
+            ([data.zipf(n, 3000, 0.8, 5), data.uniform(n, 0, 1 << 20, 6)], [0, 3]),
+            ([data.zipf(n, 3000, 0.8, 7), data.uniform(n, 0, 1 << 20, 8)], [0, 4])]
+    want = O.mhj(rels)
+    with Context(0, ooc_slice_rows=4096) as ctx:
+        rs = rels_on(ctx, rels)
+        for ooc in (0, 1):
+            got = ctx.amhj("NORMAL", rs, ooc=ooc, fib=1)
+            assert (got.count, got.checksum) == want, ooc
+            assert got.stats["fib_keys"] > 0
+
+
 @pytest.mark.parametrize("streamed", [False, True])
 @pytest.mark.parametrize("materialize", [False, True])
 def test_amhj_out_of_core(streamed, materialize):
