@@ -72,6 +72,44 @@ class amj_result(C.Structure):
     ]
 
 
+class amj_batch_opts(C.Structure):
+    _fields_ = [
+        ("layout", C.c_int),
+        ("load_factor", C.c_float),
+        ("block_size", C.c_int),
+        ("task_chunk", C.c_int),
+        ("use_graph", C.c_int),
+    ]
+
+
+class amj_batch_stats(C.Structure):
+    _fields_ = [
+        ("build_ms", C.c_double),
+        ("probe_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("launches", C.c_uint64),
+        ("tasks_pushed", C.c_uint64),
+        ("tasks_popped", C.c_uint64),
+        ("units", C.c_uint64),
+        ("build_rows", C.c_uint64),
+        ("build_jobs", C.c_uint64),
+        ("graph", C.c_int32),
+        ("pad", C.c_int32),
+    ]
+
+
+class amj_batch_tune_grid(C.Structure):
+    _fields_ = [
+        ("layout", C.c_int),
+        ("n_load_factor", C.c_int),
+        ("n_block_size", C.c_int),
+        ("n_task_chunk", C.c_int),
+        ("load_factor", C.c_float * 8),
+        ("block_size", C.c_int * 8),
+        ("task_chunk", C.c_int * 8),
+    ]
+
+
 class AmjError(RuntimeError):
     """A libamj call returned a non-zero status."""
 
@@ -103,6 +141,13 @@ SIGNATURES = {
     "amj_lftj_execute": (C.c_int, [_P, C.POINTER(_P), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.POINTER(amj_result)]),
     "amj_result_release": (None, [C.POINTER(amj_result)]),
+    "amj_batch_create": (C.c_int, [_P, C.POINTER(_P)]),
+    "amj_batch_submit": (C.c_int, [_P, C.c_int, C.POINTER(_P), C.c_int, C.c_int, _U32P]),
+    "amj_batch_size": (C.c_int, [_P, _U32P]),
+    "amj_batch_run": (C.c_int, [_P, C.POINTER(amj_batch_opts), _U64P, _U64P, C.POINTER(amj_batch_stats)]),
+    "amj_batch_tune": (C.c_int, [_P, C.POINTER(amj_batch_tune_grid), C.c_uint32, C.c_int, C.POINTER(amj_batch_opts),
+                                 C.POINTER(C.c_double)]),
+    "amj_batch_destroy": (C.c_int, [_P]),
     "amj_bucket_build": (C.c_int, [_P, _P, C.c_uint64, C.c_uint64, _P, _P, _P]),
     "amj_bucket_build_static": (C.c_int, [_P, C.c_uint64, C.c_uint64, _P, _P, _P, _P]),
     "amj_trie_build": (C.c_int, [_P, _P, _P, C.c_uint64, C.POINTER(_P)]),

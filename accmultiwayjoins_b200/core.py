@@ -6,7 +6,9 @@ operator API for this path:
   (MHJ-GPU/exec_AMHJ.cu:218-246) / ``OOC<..>::execute`` (MHJ-GPU/ooc.cuh:77-82);
 * ``Context.lftj(relations, algo, ooc, ws)`` is
   ``exec-LFTJ <path> <0=BFS|1=DFS> <ooc> <ws>`` (LFTJ-GPU/exec_LFTJ.cu:261-268) /
-  ``OOCWrapper::execute_with_{BFS,DFS}`` (LFTJ-GPU/ooc_wrapper.cuh:404-427).
+  ``OOCWrapper::execute_with_{BFS,DFS}`` (LFTJ-GPU/ooc_wrapper.cuh:404-427);
+* ``Context.batch()`` collects many AMHJ queries and runs them in one build
+  pass and one persistent probe launch (no reference counterpart).
 
 Every call goes through libamj.so; nothing here computes a join.  Errors
 raise ``AmjError`` carrying the C status instead of exiting the process as
@@ -113,6 +115,111 @@ class Relation:
             pass
 
 
+@dataclass
+class BatchRun:
+    counts: list
+    checksums: list
+    build_ms: float
+    probe_ms: float
+    total_ms: float
+    launches: int
+    tasks_pushed: int
+    tasks_popped: int
+    units: int
+    build_rows: int
+    build_jobs: int
+    graph: bool
+
+
+class Batch:
+    """Many AMHJ queries run together (amj_batch).  ``submit`` compiles a
+    query exactly as ``Context.amhj`` would; ``run`` returns every query's
+    count and checksum, which equal the one-query-per-call results."""
+
+    def __init__(self, ctx: "Context"):
+        self.ctx = ctx
+        h = C.c_void_p()
+        self.handle = None
+        L.check(L.load().amj_batch_create(ctx.handle, C.byref(h)), "batch_create")
+        self.handle = h
+        self._rels = []   # keeps the relations alive while the batch may read them
+
+    def submit(self, query_type, relations: Sequence[Relation], reorder: bool = True) -> int:
+        qt = _QUERY[query_type] if isinstance(query_type, str) else int(query_type)
+        arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
+        qid = C.c_uint32()
+        flags = 0 if reorder else L.AMJ_F_NO_REORDER
+        L.check(L.load().amj_batch_submit(self.handle, qt, arr, len(relations), flags, C.byref(qid)), "batch_submit")
+        self._rels.extend(relations)
+        return int(qid.value)
+
+    def __len__(self) -> int:
+        n = C.c_uint32()
+        L.check(L.load().amj_batch_size(self.handle, C.byref(n)), "batch_size")
+        return int(n.value)
+
+    @staticmethod
+    def _opts(layout="bucket", load_factor=0.0, block_size=256, task_chunk=1024, use_graph=False):
+        o = L.amj_batch_opts()
+        o.layout = _LAYOUT[layout] if isinstance(layout, str) else int(layout)
+        o.load_factor = load_factor
+        o.block_size = block_size
+        o.task_chunk = task_chunk
+        o.use_graph = 1 if use_graph else 0
+        return o
+
+    def run(self, layout="bucket", load_factor=0.0, block_size=256, task_chunk=1024, use_graph=False,
+            opts: Optional[L.amj_batch_opts] = None) -> BatchRun:
+        n = len(self)
+        counts = (C.c_uint64 * max(n, 1))()
+        chks = (C.c_uint64 * max(n, 1))()
+        st = L.amj_batch_stats()
+        o = opts if opts is not None else self._opts(layout, load_factor, block_size, task_chunk, use_graph)
+        L.check(L.load().amj_batch_run(self.handle, C.byref(o), counts, chks, C.byref(st)), "batch_run")
+        return BatchRun(counts=[int(counts[i]) for i in range(n)], checksums=[int(chks[i]) for i in range(n)],
+                        build_ms=st.build_ms, probe_ms=st.probe_ms, total_ms=st.total_ms, launches=int(st.launches),
+                        tasks_pushed=int(st.tasks_pushed), tasks_popped=int(st.tasks_popped), units=int(st.units),
+                        build_rows=int(st.build_rows), build_jobs=int(st.build_jobs), graph=bool(st.graph))
+
+    def tune(self, sample_every: int = 1, reps: int = 1, layout="bucket", load_factors=(), block_sizes=(),
+             task_chunks=(), use_graph=False):
+        """Autotune load factor x block size x task chunk on a sample of the
+        batch; returns (amj_batch_opts, best median ms on the sample)."""
+        g = L.amj_batch_tune_grid()
+        g.layout = _LAYOUT[layout] if isinstance(layout, str) else int(layout)
+        g.n_load_factor, g.n_block_size, g.n_task_chunk = len(load_factors), len(block_sizes), len(task_chunks)
+        for i, v in enumerate(load_factors):
+            g.load_factor[i] = v
+        for i, v in enumerate(block_sizes):
+            g.block_size[i] = v
+        for i, v in enumerate(task_chunks):
+            g.task_chunk[i] = v
+        best = L.amj_batch_opts()
+        best.use_graph = 1 if use_graph else 0
+        ms = C.c_double()
+        L.check(L.load().amj_batch_tune(self.handle, C.byref(g), int(sample_every), int(reps), C.byref(best),
+                                        C.byref(ms)), "batch_tune")
+        return best, float(ms.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().amj_batch_destroy(self.handle)
+            self.handle = None
+            self._rels = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Context:
     """One CUDA device and stream (amj_ctx)."""
 
@@ -134,6 +241,7 @@ class Context:
         h = C.c_void_p()
         self.handle = None
         self._relations = weakref.WeakSet()
+        self._batches = weakref.WeakSet()
         L.check(lib.amj_ctx_create(device, C.byref(o), C.byref(h)), "ctx_create")
         self.handle = h
 
@@ -181,11 +289,18 @@ class Context:
                                      C.byref(res)), "lftj_execute")
         return self._result(res, materialize)
 
+    def batch(self) -> Batch:
+        b = Batch(self)
+        self._batches.add(b)
+        return b
+
     def sync(self):
         L.check(L.load().amj_ctx_sync(self.handle), "ctx_sync")
 
     def close(self):
         if getattr(self, "handle", None):
+            for b in list(getattr(self, "_batches", ())):
+                b.close()
             for r in list(self._relations):
                 r.release()
             L.load().amj_ctx_destroy(self.handle)

@@ -16,7 +16,7 @@
 //    one bucket instead of a scan of every row sharing the first value;
 //  - such filters move to the earliest level at which their attributes are
 //    bound (AMJ_F_NO_REORDER keeps the query order).
-#include "amhj_kernel.cuh"
+#include "amhj_host.h"
 
 #include <algorithm>
 #include <cstring>
@@ -26,30 +26,13 @@
 
 namespace amj {
 
-struct LevelSpec {
-    const amj_rel *rel;
-    int ncols;
-    int src_col[4];    // relation column feeding index column c (index column 0 is the key)
-    int attr[4];       // attribute of index column c
-    int key_mode;
-    uint8_t cmp_mask, bind_mask;
-};
-
-struct HostPlan {
-    const amj_rel *probe = nullptr;
-    int probe_attr[AMJ_MAX_COLS] = {};
-    int L = 0, k = 0;
-    LevelSpec lv[AMJ_MAX_BUILD_TABLES];
-    int last_src[AMJ_MAX_ATTRS] = {};
-};
-
 struct RelAttrs {
     const amj_rel *rel;
     int ncols;
     int attr[AMJ_MAX_COLS];
 };
 
-static int compile_plan(int query_type, amj_rel *const *rels, int nrels, int flags, HostPlan *hp) {
+int compile_plan(int query_type, amj_rel *const *rels, int nrels, int flags, HostPlan *hp) {
     std::vector<RelAttrs> tabs;
     if (query_type == AMJ_QUERY_NORMAL) {
         if (nrels < 1) return fail(AMJ_EINVAL, "AMHJ: no relations");
@@ -139,15 +122,6 @@ static int compile_plan(int query_type, amj_rel *const *rels, int nrels, int fla
     return AMJ_OK;
 }
 
-struct IndexKey {
-    const amj_rel *rel;
-    int src[4];
-    int ncols, key_mode, layout;
-    bool operator<(const IndexKey &o) const {
-        return std::tie(rel, src[0], src[1], src[2], src[3], ncols, key_mode, layout) <
-               std::tie(o.rel, o.src[0], o.src[1], o.src[2], o.src[3], o.ncols, o.key_mode, o.layout);
-    }
-};
 
 struct ExecScratch {
     std::map<IndexKey, HashIndex> indexes;
@@ -643,21 +617,43 @@ static int build_fib(amj_ctx *ctx, const HostPlan &hp, const std::vector<const H
     return AMJ_OK;
 }
 
-static int fill_level(const LevelSpec &ls, const HashIndex &ix, LevelDesc *d) {
+void fill_level_desc(const LevelSpec &ls, int layout, int key_mode, uint32_t mask, const uint32_t *buc_ptrs,
+                     const int32_t *const *cols, const int2 *slots, LevelDesc *d) {
     std::memset(d, 0, sizeof(*d));
-    d->buc_ptrs = ix.buc_ptrs.p;
-    for (int c = 0; c < 4; c++) d->col[c] = ix.cols[c].p;
-    d->slots = ix.slots.p;
-    d->mask = ix.mask;
-    d->layout = (int8_t)ix.layout;
-    d->key_mode = (int8_t)ix.key_mode;
+    d->buc_ptrs = buc_ptrs;
+    for (int c = 0; c < 4; c++) d->col[c] = cols[c];
+    d->slots = slots;
+    d->mask = mask;
+    d->layout = (int8_t)layout;
+    d->key_mode = (int8_t)key_mode;
     d->ncols = (int8_t)ls.ncols;
     d->key_attr[0] = (int8_t)ls.attr[0];
     d->key_attr[1] = (int8_t)(ls.ncols > 1 ? ls.attr[1] : 0);
     d->cmp_mask = ls.cmp_mask;
     d->bind_mask = ls.bind_mask;
     for (int c = 0; c < 4; c++) d->attr[c] = (int8_t)(c < ls.ncols ? ls.attr[c] : 0);
-    return AMJ_OK;
+}
+
+static void fill_level(const LevelSpec &ls, const HashIndex &ix, LevelDesc *d) {
+    const int32_t *cols[4] = {ix.cols[0].p, ix.cols[1].p, ix.cols[2].p, ix.cols[3].p};
+    fill_level_desc(ls, ix.layout, ix.key_mode, ix.mask, ix.buc_ptrs.p, cols, ix.slots.p, d);
+}
+
+void plan_common(const HostPlan &hp, const amj_opts &o, ProbePlan *P) {
+    P->L = (int8_t)hp.L;
+    P->k = (int8_t)hp.k;
+    P->probe_ncols = (int8_t)hp.probe->ncols;
+    for (int c = 0; c < hp.probe->ncols && c < AMJ_MAX_COLS; c++) {
+        P->probe_col[c] = hp.probe->d_cols[c];
+        P->probe_attr[c] = (int8_t)hp.probe_attr[c];
+    }
+    for (int a = 0; a < AMJ_MAX_ATTRS; a++) P->last_src[a] = (int8_t)hp.last_src[a];
+    P->task_chunk = (uint32_t)o.task_chunk;
+    P->task_cap = (uint32_t)std::min<uint64_t>(o.task_capacity, 0x7fffffffull);
+    P->spin_limit_ns = (uint64_t)o.spin_limit_ms * 1000000ull;
+    P->depth_bytes = frontier_bytes(hp.k);
+    P->warp_bytes = (uint32_t)hp.L * P->depth_bytes;
+    P->fib_level = -1;
 }
 
 // ---- out-of-core (reference OOC::execute ooc=1, MHJ-GPU/ooc.cuh:166-306) ----
@@ -835,20 +831,8 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
     ProbeLaunch PL;
     std::memset(&PL, 0, sizeof(PL));
     ProbePlan &P = PL.P;
-    P.L = (int8_t)hp.L;
-    P.k = (int8_t)hp.k;
-    P.probe_ncols = (int8_t)hp.probe->ncols;
-    for (int c = 0; c < hp.probe->ncols && c < AMJ_MAX_COLS; c++) {
-        P.probe_col[c] = hp.probe->d_cols[c];
-        P.probe_attr[c] = (int8_t)hp.probe_attr[c];
-    }
-    for (int a = 0; a < AMJ_MAX_ATTRS; a++) P.last_src[a] = (int8_t)hp.last_src[a];
+    plan_common(hp, ctx->opts, &P);
     for (int l = 0; l < hp.L; l++) fill_level(hp.lv[l], *lvix[l], &P.lv[l]);
-    P.task_chunk = (uint32_t)ctx->opts.task_chunk;
-    P.task_cap = (uint32_t)std::min<uint64_t>(ctx->opts.task_capacity, 0x7fffffffull);
-    P.spin_limit_ns = (uint64_t)ctx->opts.spin_limit_ms * 1000000ull;
-    P.depth_bytes = frontier_bytes(hp.k);
-    P.warp_bytes = (uint32_t)hp.L * P.depth_bytes;
     AMJ_TRY(X.st.alloc(ctx, 1));
     PL.st = X.st.p;
     PL.status = ctx->d_status;
@@ -859,7 +843,6 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
         PL.task_ready = X.ready.p;
     }
     AMJ_TRY(status_reset(ctx));
-    P.fib_level = -1;
     if (fib && !dro && hp.L >= 3) AMJ_TRY(build_fib(ctx, hp, lvix, PL, X, out));
 
     int rc = AMJ_OK;

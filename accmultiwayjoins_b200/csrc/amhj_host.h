@@ -1,0 +1,48 @@
+// Host-side AMHJ plan types shared by the single-query operator (amhj.cu)
+// and the batched executor (amhj_batch.cu).
+#pragma once
+#include "amhj_kernel.cuh"
+
+#include <tuple>
+
+namespace amj {
+
+struct LevelSpec {
+    const amj_rel *rel;
+    int ncols;
+    int src_col[4];    // relation column feeding index column c (index column 0 is the key)
+    int attr[4];       // attribute of index column c
+    int key_mode;
+    uint8_t cmp_mask, bind_mask;
+};
+
+struct HostPlan {
+    const amj_rel *probe = nullptr;
+    int probe_attr[AMJ_MAX_COLS] = {};
+    int L = 0, k = 0;
+    LevelSpec lv[AMJ_MAX_BUILD_TABLES];
+    int last_src[AMJ_MAX_ATTRS] = {};
+};
+
+struct IndexKey {
+    const amj_rel *rel;
+    int src[4];
+    int ncols, key_mode, layout;
+    bool operator<(const IndexKey &o) const {
+        return std::tie(rel, src[0], src[1], src[2], src[3], ncols, key_mode, layout) <
+               std::tie(o.rel, o.src[0], o.src[1], o.src[2], o.src[3], o.ncols, o.key_mode, o.layout);
+    }
+};
+
+// Compile a query (reference exec_AMHJ.cu:70-89, TRI/FOUR :32-69) into the
+// probe relation and the ordered build levels.
+int compile_plan(int query_type, amj_rel *const *rels, int nrels, int flags, HostPlan *hp);
+
+// Level descriptor of index `layout` over the given device arrays.
+void fill_level_desc(const LevelSpec &ls, int layout, int key_mode, uint32_t mask, const uint32_t *buc_ptrs,
+                     const int32_t *const *cols, const int2 *slots, LevelDesc *d);
+
+// Plan fields that depend only on the query and the options (levels excluded).
+void plan_common(const HostPlan &hp, const amj_opts &o, ProbePlan *P);
+
+}  // namespace amj

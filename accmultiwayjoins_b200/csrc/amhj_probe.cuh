@@ -39,7 +39,7 @@ struct LevelDesc {
     int8_t attr[4];
 };
 
-struct ProbePlan {
+struct alignas(16) ProbePlan {
     uint64_t row_lo, row_hi;            // probe rows handled by this launch
     const int32_t *probe_col[AMJ_MAX_COLS];
     int8_t probe_attr[AMJ_MAX_COLS];
@@ -71,6 +71,7 @@ struct ProbePlan {
     uint32_t fib_suffix_attrs;             // attributes the cached tuples provide
     int32_t fib_level;                     // -1: off
 };
+static_assert(sizeof(ProbePlan) % 16 == 0, "plans are copied as 16-byte words");
 
 struct ProbeState {
     unsigned long long next_batch;
@@ -88,7 +89,8 @@ struct ProbeState {
 struct Task {
     int32_t vals[AMJ_MAX_ATTRS];
     uint32_t s, aux, sz;
-    uint8_t depth, m8, pad[2];
+    uint8_t depth, m8;
+    uint16_t qid;       // query of a batched launch (0 for a single query)
 };
 
 // DRO breakpoint: a unit (probe batch or task) whose output did not fit; the

@@ -80,6 +80,93 @@ def star_relations(fact_rows: int, dim_rows, theta: float = 1.1, seed: int = 3):
     return (fact_cols, list(range(d))), dims
 
 
+def _log_uniform(rng, lo: float, hi: float) -> float:
+    return float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+
+
+def query_mix(count: int, seed: int = 4, min_rows: int = 10_000, max_rows: int = 4_000_000, min_dom_bits: int = 12,
+              max_dom_bits: int = 24, theta_range=(0.5, 1.5), out_cap: int = 1 << 24):
+    """The heterogeneous query mix of the batched workload, one query at a time.
+
+    Each query is a chain or a star of 2-5 relations, or a triangle, drawn
+    with numpy's PCG64 seeded `seed`.  Relation sizes are log-uniform in
+    [min_rows, max_rows]; join-key domains log-uniform in
+    [2^min_dom_bits, 2^max_dom_bits]; half the queries are uniform, half
+    Zipf with theta uniform in theta_range.
+
+    * chain R0(0,1) R1(1,2) ..: the build side of every join (column 0 of
+      R1..) is Zipf in a Zipf query, the probe side uniform, so the expected
+      output is n0 * prod(n_j / D_j) whatever the skew.  While that exceeds
+      out_cap the domains are doubled (up to 2^max_dom_bits), then the largest
+      relation halved.
+    * star F(0..d-1) D_j(j, d+j): dimensions with unique keys (a permutation
+      of [0, m_j)), foreign keys uniform or Zipf over [0, m_j): |OUT| = |F|.
+    * triangle: the TRI query over a cleaned R-MAT edge relation
+      (0.57, 0.19, 0.19) with E generated edges and scale log2(E / 8).
+
+    Yields dicts with shape, qt, rels (list of (columns, attrs)) and theta."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    for q in range(count):
+        shape = ("chain", "star", "triangle")[int(rng.integers(0, 3))]
+        zipfian = bool(rng.integers(0, 2))
+        theta = float(rng.uniform(*theta_range)) if zipfian else 0.0
+        qseed = seed * 1_000_003 + q
+        if shape == "triangle":
+            e = int(_log_uniform(rng, min_rows, max_rows))
+            scale = max(8, int(round(np.log2(max(e, 256) / 8))))
+            s, d = rmat(scale, e, 0.57, 0.19, 0.19, qseed)
+            yield dict(shape=shape, qt="TRI", rels=[([s, d], [0, 1])], theta=0.0)
+            continue
+        r = int(rng.integers(2, 6))
+        sizes = [int(_log_uniform(rng, min_rows, max_rows)) for _ in range(r)]
+        if shape == "star":
+            d = r - 1
+            fact_cols, dims = [], []
+            for j in range(d):
+                m = sizes[j + 1]
+                keys = permutation(m, qseed, 100 + j)
+                payload = uniform(m, 0, 1 << 30, qseed, 200 + j)
+                dims.append(([keys, payload], [j, d + j]))
+                if zipfian:
+                    fact_cols.append(zipf(sizes[0], m, theta, qseed, 400 + j,
+                                          rank_to_key=permutation(m, qseed, 300 + j)))
+                else:
+                    fact_cols.append(uniform(sizes[0], 0, m, qseed, 400 + j))
+            yield dict(shape=shape, qt="NORMAL", rels=[(fact_cols, list(range(d)))] + dims, theta=theta)
+            continue
+        doms = [int(_log_uniform(rng, 1 << min_dom_bits, 1 << max_dom_bits)) for _ in range(r - 1)]
+
+        def expected():
+            e = float(sizes[0])
+            for j in range(1, r):
+                e *= sizes[j] / doms[j - 1]
+            return e
+
+        while expected() > out_cap:
+            grow = [j for j in range(r - 1) if doms[j] < (1 << max_dom_bits)]
+            if grow:
+                for j in grow:
+                    doms[j] = min(doms[j] * 2, 1 << max_dom_bits)
+                continue
+            big = int(np.argmax(sizes))
+            if sizes[big] <= min_rows:
+                break
+            sizes[big] = max(min_rows, sizes[big] // 2)
+        rels = []
+        for i in range(r):
+            if i == 0:
+                c0 = uniform(sizes[i], 0, 1 << max_dom_bits, qseed, 10 * i)
+            elif zipfian:
+                c0 = zipf(sizes[i], doms[i - 1], theta, qseed, 10 * i,
+                          rank_to_key=permutation(doms[i - 1], qseed, 10 * i + 2))
+            else:
+                c0 = uniform(sizes[i], 0, doms[i - 1], qseed, 10 * i)
+            hi = doms[i] if i < r - 1 else (1 << max_dom_bits)
+            c1 = uniform(sizes[i], 0, hi, qseed, 10 * i + 1)
+            rels.append(([c0, c1], [i, i + 1]))
+        yield dict(shape=shape, qt="NORMAL", rels=rels, theta=theta)
+
+
 def db_name(n: int, attrs) -> str:
     return f"{n}_" + "_".join(str(a) for a in attrs) + ".db"
 

@@ -79,6 +79,7 @@ extern "C" {
 typedef struct amj_ctx  amj_ctx;
 typedef struct amj_rel  amj_rel;
 typedef struct amj_trie amj_trie;
+typedef struct amj_batch amj_batch;
 
 typedef struct amj_opts {
     int      block_size;       /* threads per block of the probe kernels (0: 256) */
@@ -147,6 +148,59 @@ int  amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels,
                       int algo, int ooc, int ws, int flags, amj_result *out);
 
 void amj_result_release(amj_result *res);
+
+/* ---- batched AMHJ: many queries, one build pass, one persistent probe launch ----
+ * No reference counterpart: the reference runs one query per exec-AMHJ
+ * process (MHJ-GPU/exec_AMHJ.cu:218-246).  Queries are compiled as
+ * amj_amhj_execute compiles them (same query types, AMJ_F_NO_REORDER
+ * allowed) and produce the same count and checksum; they are count-only
+ * (no materialisation, ooc, dro or fib).  Relations must stay alive and on
+ * the device until the batch is destroyed; their contents may change between
+ * runs (a replayed graph reads them again). */
+typedef struct amj_batch_opts {
+    int      layout;        /* AMJ_LAYOUT_BUCKET or AMJ_LAYOUT_OPEN_ADDR (0: bucket)     */
+    float    load_factor;   /* rows per table slot: bucket directory floorPow2(n / lf),
+                               open addressing capacity ceilPow2(n / lf)
+                               (0: the reference's floorPow2(n) and n / 0.5)             */
+    int      block_size;    /* probe threads per block: 128, 256 or 512 (0: 256)        */
+    int      task_chunk;    /* work-sharing task size in candidates, >= 32 (0: 1024)   */
+    int      use_graph;     /* 1: capture the device sequence into a CUDA graph on the
+                               first run with these options and replay it afterwards   */
+} amj_batch_opts;
+
+typedef struct amj_batch_stats {
+    double   build_ms, probe_ms, total_ms;   /* device time of the run               */
+    uint64_t launches;                       /* kernels in one run                   */
+    uint64_t tasks_pushed, tasks_popped;     /* work-sharing tasks                   */
+    uint64_t units;                          /* level-0 units of 1024 candidates     */
+    uint64_t build_rows, build_jobs;         /* rows indexed, distinct indexes       */
+    int32_t  graph;                          /* 1: the run replayed a captured graph */
+    int32_t  pad;
+} amj_batch_stats;
+
+/* autotuner grid; a zero count takes the default list
+ * (load factor {0.5, 0.7, 0.85}, block {128, 256, 512}, chunk {32 .. 1024}) */
+typedef struct amj_batch_tune_grid {
+    int   layout;
+    int   n_load_factor, n_block_size, n_task_chunk;
+    float load_factor[8];
+    int   block_size[8];
+    int   task_chunk[8];
+} amj_batch_tune_grid;
+
+int  amj_batch_create(amj_ctx *ctx, amj_batch **out);
+int  amj_batch_submit(amj_batch *b, int query_type, amj_rel *const *rels, int nrels,
+                      int flags, uint32_t *qid);
+int  amj_batch_size(const amj_batch *b, uint32_t *queries);
+/* counts / checksums: one entry per submitted query (either may be NULL) */
+int  amj_batch_run(amj_batch *b, const amj_batch_opts *opts, uint64_t *counts,
+                   uint64_t *checksums, amj_batch_stats *stats);
+/* every grid point on every `sample_every`-th query: one warm-up and `reps`
+ * timed runs each; *best gets the point with the least median device time
+ * (best->use_graph is kept as passed in) */
+int  amj_batch_tune(amj_batch *b, const amj_batch_tune_grid *grid, uint32_t sample_every,
+                    int reps, amj_batch_opts *best, double *best_ms);
+int  amj_batch_destroy(amj_batch *b);
 
 /* ---- building blocks on device pointers, enqueued on the context stream ----
  * amj_bucket_build: bucket-CSR index of n keys with `buckets` (a power of two)
