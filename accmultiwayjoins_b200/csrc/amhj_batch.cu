@@ -224,6 +224,7 @@ struct amj_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t cap_stream = nullptr;
 
     void drop_graph() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -542,10 +543,17 @@ static int batch_run(amj_batch *b, const amj_batch_opts &o, uint64_t *counts, ui
     bool replay = false;
     if (o.use_graph) {
         if (!b->exec) {
-            AMJ_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            // capture on a private stream (the context stream may be the
+            // legacy default stream, which cannot capture); only the replay
+            // runs on the context stream
+            if (!b->cap_stream) AMJ_CUDA_TRY(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+            cudaStream_t user = ctx->stream;
+            AMJ_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+            ctx->stream = b->cap_stream;
             const int rc = batch_record(b, true);
+            ctx->stream = user;
             cudaGraph_t g = nullptr;
-            const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+            const cudaError_t ce = cudaStreamEndCapture(b->cap_stream, &g);
             if (rc != AMJ_OK) {
                 if (g) cudaGraphDestroy(g);
                 return rc;
@@ -717,6 +725,7 @@ extern "C" int amj_batch_destroy(amj_batch *b) {
     b->unprepare();
     for (auto &e : b->ev)
         if (e) cudaEventDestroy(e);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
     delete b;
     return AMJ_OK;
 }

@@ -9,13 +9,16 @@ the radix sort, then the leapfrog intersection, returning count and
 checksum.  The unit of work is one output tuple (one triangle).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--algo DFS|BFS|AMHJ] [--scale S] [--workload triangle|chain]
+                  [--algo DFS|BFS|AMHJ] [--scale S] [--workload triangle|chain|batch]
 
 --scale S runs the same workload on a smaller R-MAT graph (2^S vertices,
 2^(S+4) edges), for profiling.  --workload chain runs the 3-way chain join
 R1(a,b) R2(b,c) R3(c,d) (3 x 1M rows, keys uniform in [0, 2^18), seeds 1-3)
 through AMHJ (count + checksum, hash builds included), with the reference's
 own MHJ-CPU (compiled from its sources into oracle/_ref) as CPU baseline.
+--workload batch runs 512 heterogeneous queries as one batch (autotuned,
+CUDA-graph replay) and reports, beside its tuples/s, the one-query-per-call
+tuples/s on the same queries and p50/p99 latencies of both forms.
 
 * value: tuples/s with the input resident on the device (whole job: sum of
   the ranks' tuples / max over ranks of the timed K steps).
@@ -228,6 +231,186 @@ class Chain:
         return cnt, chk, time.perf_counter() - t0, cores, "port", "the full workload once (oracle restatement)"
 
 
+class BatchMix:
+    """The batched workload: a heterogeneous mix of chain / star / triangle
+    queries (sizes log-uniform 10K-4M rows, key domains 2^12-2^24, uniform or
+    Zipf theta in [0.5, 1.5]; accmultiwayjoins_b200.data.query_mix, seed 4)
+    run as one amj_batch: one build pass and one persistent probe launch,
+    captured once into a CUDA graph and replayed every step."""
+
+    def __init__(self, args, rank):
+        from accmultiwayjoins_b200 import data
+        t0 = time.perf_counter()
+        self.queries = list(data.query_mix(args.queries, seed=4 + 1000 * rank, min_rows=args.min_rows,
+                                           max_rows=args.max_rows))
+        self.gen_s = time.perf_counter() - t0
+        self.rows = sum(len(cols[0]) for q in self.queries for cols, _ in q["rels"])
+        self.h2d = sum(4 * len(c) for q in self.queries for cols, _ in q["rels"] for c in cols)
+
+    def describe(self, rank_note):
+        shapes = {}
+        for q in self.queries:
+            shapes[q["shape"]] = shapes.get(q["shape"], 0) + 1
+        return (f"batched: {len(self.queries)} heterogeneous queries {shapes}, {self.rows} relation rows "
+                f"(log-uniform sizes in [{self.queries and min(len(c[0]) for q in self.queries for c, _ in q['rels'])}, "
+                f"4M], key domains 2^12-2^24, uniform or Zipf theta in [0.5,1.5], seed 4{rank_note}); "
+                f"one build pass + one persistent probe launch per step, CUDA graph replay")
+
+    def cpu_sample(self, budget_s=15.0):
+        """The oracle (and the reference MHJ-CPU where it applies: acyclic
+        single-key chains and stars) on the first queries until budget_s of
+        CPU time is spent."""
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        spent, tuples, n, kinds = 0.0, 0, 0, set()
+        for q in self.queries:
+            t0 = time.perf_counter()
+            if q["qt"] == "TRI":
+                s, d = q["rels"][0][0]
+                cnt, _ = O.triangle(s, d, nthreads=cores)
+                kinds.add("port")
+            elif O.ref_available() and len(q["rels"]) >= 3:
+                cnt, _, _ = O.mhj_reference(q["rels"], nthreads=cores)
+                kinds.add("reference")
+            else:
+                cnt, _ = O.mhj(q["rels"], nthreads=cores)
+                kinds.add("port")
+            spent += time.perf_counter() - t0
+            tuples += cnt
+            n += 1
+            if spent >= budget_s:
+                break
+        kind = "reference" if kinds == {"reference"} else "port"
+        sample = (f"first {n} of {len(self.queries)} queries, one query at a time (reference MHJ-CPU for chains and "
+                  f"stars of 3+ relations, the oracle's restatement for triangles and two-relation joins)")
+        return tuples, spent, cores, kind, sample
+
+
+def pct(xs, p):
+    xs = sorted(xs)
+    return xs[min(len(xs) - 1, int(round(p / 100.0 * (len(xs) - 1))))]
+
+
+def run_batch(args, rank, world, local_rank):
+    import ctypes as C
+    import torch
+    from accmultiwayjoins_b200 import Context, _lib as L
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = BatchMix(args, rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx = Context(local_rank)
+    lib = L.load()
+    L.check(lib.amj_ctx_set_stream(ctx.handle, C.c_void_p(stream.cuda_stream)), "set_stream")
+    host_cols = [c for q in wl.queries for cols, _ in q["rels"] for c in cols]
+    dcols = [torch.from_numpy(c).to(dev) for c in host_cols]
+    it = iter(dcols)
+    qrels = [[ctx.relation([next(it) for _ in cols], a) for cols, a in q["rels"]] for q in wl.queries]
+    b = ctx.batch()
+    for q, rels in zip(wl.queries, qrels):
+        b.submit(q["qt"], rels)
+    torch.cuda.synchronize()
+
+    # plain: one query per call, inputs resident, each call's wall latency
+    plain_lat, plain_tuples, plain_res = [], 0, []
+    for q, rels in list(zip(wl.queries, qrels))[:8]:
+        ctx.amhj(q["qt"], rels)
+    for q, rels in zip(wl.queries, qrels):
+        t0 = time.perf_counter()
+        r = ctx.amhj(q["qt"], rels)
+        plain_lat.append((time.perf_counter() - t0) * 1e3)
+        plain_tuples += r.count
+        plain_res.append((r.count, r.checksum))
+    plain_s = sum(plain_lat) / 1e3
+
+    # autotune on every 8th query, then the batched steps (graph replay)
+    t0 = time.perf_counter()
+    if args.tune:
+        opts, tune_ms = b.tune(sample_every=8, reps=1)
+    else:
+        opts, tune_ms = Batch_default_opts(L), None
+    tune_s = time.perf_counter() - t0
+    opts.use_graph = 1
+    for _ in range(args.warmup):
+        r = b.run(opts=opts)
+    assert list(zip(r.counts, r.checksums)) == plain_res, "batched results differ from one query per call"
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    l0 = C.c_uint64()
+    L.check(lib.amj_ctx_launch_count(ctx.handle, C.byref(l0)))
+    dev_ms, wall_ms = [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        r = b.run(opts=opts)
+        wall_ms.append((time.perf_counter() - t1) * 1e3)
+        dev_ms.append(r.total_ms)
+    l1 = C.c_uint64()
+    L.check(lib.amj_ctx_launch_count(ctx.handle, C.byref(l1)))
+    total = sum(r.counts)
+
+    # end to end: every step copies all relation columns from pinned host
+    # memory into the device columns the batch reads, replays, reads results
+    pinned = [torch.from_numpy(c).pin_memory() for c in host_cols]
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for d, h in zip(dcols, pinned):
+            d.copy_(h, non_blocking=True)
+        re_ = b.run(opts=opts)
+        if i >= args.warmup:
+            e2e_ms.append((time.perf_counter() - t1) * 1e3)
+    assert re_.counts == r.counts and re_.checksums == r.checksums
+    clocks = sampler.stop()
+    ms = sum(dev_ms) / len(dev_ms)
+    e2e = sum(e2e_ms) / len(e2e_ms)
+    if rank != 0:
+        b.close()
+        ctx.close()
+        return
+    line = {
+        "metric": METRIC, "value": total / (ms * 1e-3), "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic (seeded)",
+        "config": {"workload": wl.describe(""), "queries": len(wl.queries), "output_tuples": total,
+                   "l2": "inputs far larger than L2 (%.1f GB of relations)" % (wl.h2d / 1e9),
+                   "opts": {"layout": int(opts.layout), "load_factor": float(opts.load_factor),
+                            "block_size": int(opts.block_size), "task_chunk": int(opts.task_chunk),
+                            "use_graph": int(opts.use_graph)},
+                   "tuned_on": "every 8th query, full grid" if args.tune else "defaults",
+                   "tune_s": tune_s, "tune_best_sample_ms": tune_ms, "generation_s": wl.gen_s},
+        "e2e": {"value": total / (e2e * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": wl.h2d,
+                "d2h_bytes_per_step": 16 * len(wl.queries), "ms_per_step": e2e},
+        "batched_vs_plain": {
+            "plain_value": plain_tuples / plain_s, "plain_ms_total": plain_s * 1e3,
+            "batched_over_plain": (total / (ms * 1e-3)) / (plain_tuples / plain_s),
+            "latency_ms": {"plain": {"p50": pct(plain_lat, 50), "p99": pct(plain_lat, 99)},
+                           "batched": {"p50": pct(wall_ms, 50), "p99": pct(wall_ms, 99),
+                                       "note": "every query of a batch completes with the batch"}}},
+        "phase_ms": {"build": r.build_ms, "probe": r.probe_ms},
+        "gpu_launches": int(l1.value - l0.value),
+        "batch_stats": {"launches_per_run": r.launches, "graph": r.graph, "units": r.units,
+                        "tasks_pushed": r.tasks_pushed, "build_rows": r.build_rows, "build_jobs": r.build_jobs},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        tuples, sec, cores, kind, sample = wl.cpu_sample()
+        line["cpu_baseline"] = {"value": tuples / sec, "unit": "tuples/s", "cores": cores, "kind": kind,
+                                "sample": sample}
+    print(json.dumps(line), flush=True)
+    b.close()
+    ctx.close()
+
+
+def Batch_default_opts(L):
+    o = L.amj_batch_opts()
+    o.block_size, o.task_chunk = 256, 1024
+    return o
+
+
 def make_workload(args, rank):
     return Chain(args, rank) if args.workload == "chain" else Triangle(args, rank)
 
@@ -251,6 +434,26 @@ def run_reference(args, rank, world):
     for the chain; the oracle's triangle restatement for the triangle) on all
     host threads.  Rank 0 only."""
     if rank != 0:
+        return
+    if args.workload == "batch":
+        wl = BatchMix(args, 0)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            tuples, sec, cores, kind, sample = wl.cpu_sample(budget_s=10.0)
+            if i >= args.warmup:
+                vals.append((tuples, sec))
+        tuples = sum(t for t, _ in vals)
+        sec = sum(t for _, t in vals)
+        value = tuples / sec
+        line = {
+            "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec / len(vals) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+            "impl": "reference", "config": {"workload": wl.describe(""), "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
         return
     wl = make_workload(args, 0)
     times = []
@@ -390,7 +593,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--algo", default="DFS", choices=["DFS", "BFS", "AMHJ"])
-    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain"])
+    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain", "batch"])
+    ap.add_argument("--queries", type=int, default=512, help="batch workload: queries per batch")
+    ap.add_argument("--min-rows", type=int, default=10_000, help="batch workload: smallest relation")
+    ap.add_argument("--max-rows", type=int, default=4_000_000, help="batch workload: largest relation")
+    ap.add_argument("--no-tune", dest="tune", action="store_false", help="batch workload: skip the autotuner")
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -407,7 +614,10 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    run_ours(args, rank, world, local_rank)
+    if args.workload == "batch":
+        run_batch(args, rank, world, local_rank)
+    else:
+        run_ours(args, rank, world, local_rank)
     if world > 1:
         import torch
         torch.distributed.destroy_process_group()

@@ -174,6 +174,10 @@ def mhj_reference(relations, nthreads=0, tuples=False):
     Returns (count, checksum, seconds[, columns])."""
     lib = ref()
     nt = len(relations)
+    if nt < 3:
+        # a two-relation join (one build table) crashes TBJ as compiled here
+        # (SIGSEGV in the host process)
+        raise ValueError("the reference MHJ-CPU needs at least three relations")
     lens = (C.c_uint64 * nt)()
     ncols = (C.c_int * nt)()
     attrs = (C.c_uint32 * (8 * nt))()
