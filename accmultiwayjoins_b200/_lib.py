@@ -79,6 +79,7 @@ class amj_batch_opts(C.Structure):
         ("block_size", C.c_int),
         ("task_chunk", C.c_int),
         ("use_graph", C.c_int),
+        ("grid_blocks", C.c_int),
     ]
 
 
@@ -107,6 +108,49 @@ class amj_batch_tune_grid(C.Structure):
         ("load_factor", C.c_float * 8),
         ("block_size", C.c_int * 8),
         ("task_chunk", C.c_int * 8),
+    ]
+
+
+class amj_serve_opts(C.Structure):
+    _fields_ = [
+        ("lanes", C.c_int),
+        ("max_batch", C.c_uint32),
+        ("mem_budget", C.c_uint64),
+        ("batch", amj_batch_opts),
+        ("ooc_lane", C.c_int),
+        ("ooc_mem", C.c_uint64),
+        ("ooc_slice_rows", C.c_uint64),
+    ]
+
+
+class amj_serve_result(C.Structure):
+    _fields_ = [
+        ("count", C.c_uint64),
+        ("checksum", C.c_uint64),
+        ("status", C.c_int32),
+        ("path", C.c_int32),
+        ("spilled", C.c_int32),
+        ("batch_id", C.c_uint32),
+        ("batch_size", C.c_uint32),
+        ("pad", C.c_int32),
+        ("queue_ms", C.c_double),
+        ("exec_ms", C.c_double),
+        ("latency_ms", C.c_double),
+    ]
+
+
+class amj_serve_stats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_uint64),
+        ("completed", C.c_uint64),
+        ("rejected", C.c_uint64),
+        ("spilled", C.c_uint64),
+        ("batches", C.c_uint64),
+        ("ooc_runs", C.c_uint64),
+        ("budget_bytes", C.c_uint64),
+        ("peak_reserved_bytes", C.c_uint64),
+        ("max_inflight_batches", C.c_uint32),
+        ("lanes", C.c_uint32),
     ]
 
 
@@ -148,6 +192,11 @@ SIGNATURES = {
     "amj_batch_tune": (C.c_int, [_P, C.POINTER(amj_batch_tune_grid), C.c_uint32, C.c_int, C.POINTER(amj_batch_opts),
                                  C.POINTER(C.c_double)]),
     "amj_batch_destroy": (C.c_int, [_P]),
+    "amj_server_create": (C.c_int, [_P, C.POINTER(amj_serve_opts), C.POINTER(_P)]),
+    "amj_server_submit": (C.c_int, [_P, C.c_int, C.POINTER(_P), C.c_int, C.c_int, C.c_int, _U64P]),
+    "amj_server_wait": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.POINTER(amj_serve_result)]),
+    "amj_server_stats": (C.c_int, [_P, C.POINTER(amj_serve_stats)]),
+    "amj_server_destroy": (C.c_int, [_P]),
     "amj_bucket_build": (C.c_int, [_P, _P, C.c_uint64, C.c_uint64, _P, _P, _P]),
     "amj_bucket_build_static": (C.c_int, [_P, C.c_uint64, C.c_uint64, _P, _P, _P, _P]),
     "amj_trie_build": (C.c_int, [_P, _P, _P, C.c_uint64, C.POINTER(_P)]),

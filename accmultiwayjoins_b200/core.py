@@ -8,7 +8,10 @@ operator API for this path:
   ``exec-LFTJ <path> <0=BFS|1=DFS> <ooc> <ws>`` (LFTJ-GPU/exec_LFTJ.cu:261-268) /
   ``OOCWrapper::execute_with_{BFS,DFS}`` (LFTJ-GPU/ooc_wrapper.cuh:404-427);
 * ``Context.batch()`` collects many AMHJ queries and runs them in one build
-  pass and one persistent probe launch (no reference counterpart).
+  pass and one persistent probe launch (no reference counterpart);
+* ``Context.server()`` serves AMHJ requests over resident relations by
+  continuous batching, with admission by device memory and an out-of-core
+  lane (no reference counterpart).
 
 Every call goes through libamj.so; nothing here computes a join.  Errors
 raise ``AmjError`` carrying the C status instead of exiting the process as
@@ -159,13 +162,14 @@ class Batch:
         return int(n.value)
 
     @staticmethod
-    def _opts(layout="bucket", load_factor=0.0, block_size=256, task_chunk=1024, use_graph=False):
+    def _opts(layout="bucket", load_factor=0.0, block_size=256, task_chunk=1024, use_graph=False, grid_blocks=0):
         o = L.amj_batch_opts()
         o.layout = _LAYOUT[layout] if isinstance(layout, str) else int(layout)
         o.load_factor = load_factor
         o.block_size = block_size
         o.task_chunk = task_chunk
         o.use_graph = 1 if use_graph else 0
+        o.grid_blocks = grid_blocks
         return o
 
     def run(self, layout="bucket", load_factor=0.0, block_size=256, task_chunk=1024, use_graph=False,
@@ -206,6 +210,83 @@ class Batch:
             L.load().amj_batch_destroy(self.handle)
             self.handle = None
             self._rels = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class ServeResult:
+    ticket: int
+    count: int
+    checksum: int
+    path: str            # "batch" or "ooc"
+    spilled: bool
+    batch_id: int
+    batch_size: int
+    queue_ms: float
+    exec_ms: float
+    latency_ms: float
+
+
+class Server:
+    """Request server (amj_server): submit() returns a ticket at once, wait()
+    returns that request's result.  The relations of a request are kept alive
+    here until its result has been waited for."""
+
+    def __init__(self, ctx: "Context", lanes: int = 2, max_batch: int = 256, mem_budget: int = 0,
+                 ooc_lane: bool = True, ooc_mem: int = 0, ooc_slice_rows: int = 0, **batch_kw):
+        o = L.amj_serve_opts()
+        o.lanes, o.max_batch, o.mem_budget = lanes, max_batch, mem_budget
+        o.batch = Batch._opts(**batch_kw)
+        o.ooc_lane, o.ooc_mem, o.ooc_slice_rows = int(bool(ooc_lane)), ooc_mem, ooc_slice_rows
+        h = C.c_void_p()
+        self.handle = None
+        L.check(L.load().amj_server_create(ctx.handle, C.byref(o), C.byref(h)), "server_create")
+        self.handle = h
+        self.ctx = ctx
+        self._held = {}
+
+    def submit(self, query_type, relations: Sequence[Relation], ooc: bool = False, reorder: bool = True) -> int:
+        qt = _QUERY[query_type] if isinstance(query_type, str) else int(query_type)
+        arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
+        t = C.c_uint64()
+        flags = 0 if reorder else L.AMJ_F_NO_REORDER
+        L.check(L.load().amj_server_submit(self.handle, qt, arr, len(relations), flags, int(bool(ooc)), C.byref(t)),
+                "server_submit")
+        self._held[int(t.value)] = list(relations)
+        return int(t.value)
+
+    def wait(self, ticket: int, timeout_ms: int = 600_000) -> ServeResult:
+        r = L.amj_serve_result()
+        st = L.load().amj_server_wait(self.handle, ticket, timeout_ms, C.byref(r))
+        if st != L.AMJ_ETIMEOUT:
+            self._held.pop(ticket, None)
+        L.check(st, "server_wait")
+        return ServeResult(ticket=ticket, count=int(r.count), checksum=int(r.checksum),
+                           path="ooc" if r.path == 1 else "batch", spilled=bool(r.spilled), batch_id=int(r.batch_id),
+                           batch_size=int(r.batch_size), queue_ms=r.queue_ms, exec_ms=r.exec_ms,
+                           latency_ms=r.latency_ms)
+
+    def stats(self) -> dict:
+        s = L.amj_serve_stats()
+        L.check(L.load().amj_server_stats(self.handle, C.byref(s)), "server_stats")
+        return {name: int(getattr(s, name)) for name, _ in L.amj_serve_stats._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().amj_server_destroy(self.handle)
+            self.handle = None
+            self._held = {}
 
     def __enter__(self):
         return self
@@ -293,6 +374,11 @@ class Context:
         b = Batch(self)
         self._batches.add(b)
         return b
+
+    def server(self, **kw) -> Server:
+        srv = Server(self, **kw)
+        self._batches.add(srv)
+        return srv
 
     def sync(self):
         L.check(L.load().amj_ctx_sync(self.handle), "ctx_sync")

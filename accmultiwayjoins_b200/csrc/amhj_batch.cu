@@ -20,7 +20,7 @@
 //
 // Sizes are known on the host once the queries are submitted, so the whole
 // device sequence needs no host round trip and can be captured.
-#include "amhj_host.h"
+#include "amhj_batch.h"
 
 #include <algorithm>
 #include <cstring>
@@ -224,7 +224,11 @@ struct amj_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t done_ev = nullptr;
     cudaStream_t cap_stream = nullptr;
+    // pinned host copy of the results: counts[nq], checksums[nq], units, state
+    unsigned long long *h_out = nullptr;
+    bool replayed = false;
 
     void drop_graph() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -254,6 +258,8 @@ struct amj_batch {
         st.release();
         tasks.release();
         ready.release();
+        if (h_out) cudaFreeHost(h_out);
+        h_out = nullptr;
     }
 };
 
@@ -264,7 +270,9 @@ static unsigned batch_grid_for(amj_ctx *ctx, uint64_t n) {
     return (unsigned)(g == 0 ? 1 : (g > cap ? cap : g));
 }
 
-static int normalize_opts(const amj_batch_opts *in, amj_batch_opts *o) {
+static uint64_t ctx_task_capacity(const amj_ctx *ctx) { return std::min<uint64_t>(ctx->opts.task_capacity, 0x7fffffffull); }
+
+int normalize_batch_opts(const amj_batch_opts *in, amj_batch_opts *o) {
     std::memset(o, 0, sizeof(*o));
     if (in) *o = *in;
     if (o->layout == 0) o->layout = AMJ_LAYOUT_BUCKET;
@@ -276,6 +284,7 @@ static int normalize_opts(const amj_batch_opts *in, amj_batch_opts *o) {
         return fail(AMJ_EINVAL, "batch: block size must be 128, 256 or 512");
     if (o->task_chunk == 0) o->task_chunk = 1024;
     if (o->task_chunk < 32 || o->task_chunk > (1 << 20)) return fail(AMJ_EINVAL, "batch: task chunk out of range");
+    if (o->grid_blocks < 0) return fail(AMJ_EINVAL, "batch: negative grid size");
     return AMJ_OK;
 }
 
@@ -440,6 +449,9 @@ static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
     if (b->block == 128) AMJ_TRY(batch_kernel_setup<128>(ctx, b->smem, &b->grid));
     else if (b->block == 256) AMJ_TRY(batch_kernel_setup<256>(ctx, b->smem, &b->grid));
     else AMJ_TRY(batch_kernel_setup<512>(ctx, b->smem, &b->grid));
+    if (o.grid_blocks > 0 && (unsigned)o.grid_blocks < b->grid) b->grid = (unsigned)o.grid_blocks;
+    const size_t hbytes = (2 * (size_t)nq + 1) * sizeof(unsigned long long) + sizeof(ProbeState);
+    AMJ_CUDA_TRY(cudaMallocHost((void **)&b->h_out, hbytes));
     AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     b->popts = o;
     b->prepared = true;
@@ -529,18 +541,21 @@ static int batch_record(amj_batch *b, bool capturing) {
 
 static bool same_opts(const amj_batch_opts &a, const amj_batch_opts &b) {
     return a.layout == b.layout && a.load_factor == b.load_factor && a.block_size == b.block_size &&
-           a.task_chunk == b.task_chunk;
+           a.task_chunk == b.task_chunk && a.grid_blocks == b.grid_blocks;
 }
 
-static int batch_run(amj_batch *b, const amj_batch_opts &o, uint64_t *counts, uint64_t *checksums,
-                     amj_batch_stats *stats) {
+// Enqueue one run on the context stream: the device sequence (replayed
+// graph or eager launches), then the results into pinned host memory and the
+// completion event.  Returns without waiting.
+int batch_launch(amj_batch *b, const amj_batch_opts &o) {
     amj_ctx *ctx = b->ctx;
     AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
     if (!b->prepared || !same_opts(o, b->popts)) AMJ_TRY(batch_prepare(b, o));
     for (auto &e : b->ev)
         if (!e) AMJ_CUDA_TRY(cudaEventCreate(&e));
+    if (!b->done_ev) AMJ_CUDA_TRY(cudaEventCreateWithFlags(&b->done_ev, cudaEventDisableTiming));
     AMJ_TRY(status_reset(ctx));
-    bool replay = false;
+    b->replayed = false;
     if (o.use_graph) {
         if (!b->exec) {
             // capture on a private stream (the context stream may be the
@@ -568,21 +583,37 @@ static int batch_run(amj_batch *b, const amj_batch_opts &o, uint64_t *counts, ui
         }
         AMJ_CUDA_TRY(cudaGraphLaunch(b->exec, ctx->stream));
         ctx->launches += b->launches_per_run;
-        replay = true;
+        b->replayed = true;
     } else {
         AMJ_TRY(batch_record(b, false));
     }
     const uint32_t nq = (uint32_t)b->qs.size();
-    std::vector<unsigned long long> hc(nq), hk(nq);
-    ProbeState hs;
-    AMJ_CUDA_TRY(cudaMemcpyAsync(hc.data(), b->q_count.p, nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaMemcpyAsync(hk.data(), b->q_checksum.p, nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaMemcpyAsync(&hs, b->st.p, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+    unsigned long long *h = b->h_out;
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h, b->q_count.p, nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h + nq, b->q_checksum.p, nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h + 2 * nq, b->unit_base.p + nq, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h + 2 * nq + 1, b->st.p, sizeof(ProbeState), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaEventRecord(b->done_ev, ctx->stream));
+    return AMJ_OK;
+}
+
+// whether the last launched run has completed (no waiting)
+bool batch_done(amj_batch *b) { return b->done_ev && cudaEventQuery(b->done_ev) == cudaSuccess; }
+
+// Wait for the last launched run and return its results.
+int batch_collect(amj_batch *b, uint64_t *counts, uint64_t *checksums, amj_batch_stats *stats) {
+    amj_ctx *ctx = b->ctx;
+    AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
+    AMJ_CUDA_TRY(cudaEventSynchronize(b->done_ev));
     AMJ_TRY(status_check(ctx, "batched AMHJ"));
+    const uint32_t nq = (uint32_t)b->qs.size();
+    const unsigned long long *h = b->h_out;
+    ProbeState hs;
+    std::memcpy(&hs, h + 2 * nq + 1, sizeof(hs));
     if (hs.q_tail > b->task_cap) return fail(AMJ_EOVERFLOW, "batch: work-sharing queue overflowed");
     for (uint32_t q = 0; q < nq; q++) {
-        if (counts) counts[q] = hc[q];
-        if (checksums) checksums[q] = hk[q];
+        if (counts) counts[q] = h[q];
+        if (checksums) checksums[q] = h[nq + q];
     }
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
@@ -596,15 +627,36 @@ static int batch_run(amj_batch *b, const amj_batch_opts &o, uint64_t *counts, ui
         stats->launches = b->launches_per_run;
         stats->tasks_pushed = hs.tasks_pushed;
         stats->tasks_popped = hs.tasks_popped;
-        unsigned long long units = 0;
-        AMJ_CUDA_TRY(cudaMemcpyAsync(&units, b->unit_base.p + nq, 8, cudaMemcpyDeviceToHost, ctx->stream));
-        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-        stats->units = units;
-        stats->graph = replay ? 1 : 0;
+        stats->units = h[2 * nq];
+        stats->graph = b->replayed ? 1 : 0;
         stats->build_rows = b->bucket_rows + b->oa_rows;
         stats->build_jobs = b->jobs.size();
     }
     return AMJ_OK;
+}
+
+static int batch_run(amj_batch *b, const amj_batch_opts &o, uint64_t *counts, uint64_t *checksums,
+                     amj_batch_stats *stats) {
+    AMJ_TRY(batch_launch(b, o));
+    return batch_collect(b, counts, checksums, stats);
+}
+
+// Device bytes a run of these queries allocates, from the relation sizes
+// (an upper bound of batch_prepare's buffers plus the sort's scratch).
+uint64_t batch_estimate_bytes(const amj_batch *b, const amj_batch_opts &o) {
+    const double lf = o.load_factor > 0.f ? o.load_factor : 1.0;
+    uint64_t rows = 0, buckets = 0, probe = 0;
+    for (const auto &q : b->qs) {
+        probe += q.hp.probe->n;
+        for (int l = 0; l < q.hp.L; l++) {
+            rows += q.hp.lv[l].rel->n;
+            buckets += (uint64_t)((double)q.hp.lv[l].rel->n / lf) + 1;
+        }
+    }
+    const uint64_t per_row = 16 + 4 * 4 + 1;   // sort items (2 x 8 B), up to 4 gathered columns, sort counts
+    return rows * per_row + buckets * (o.layout == AMJ_LAYOUT_OPEN_ADDR ? 16 : 4) + probe * 16 +
+           (uint64_t)b->qs.size() * (sizeof(ProbePlan) + 64) + (uint64_t)(ctx_task_capacity(b->ctx)) * 52 +
+           (64ull << 20);
 }
 
 }  // namespace amj
@@ -623,7 +675,8 @@ extern "C" int amj_batch_submit(amj_batch *b, int query_type, amj_rel *const *re
     if (b->qs.size() >= 0xffffu) return fail(AMJ_EUNSUPPORTED, "batch_submit: at most 65535 queries per batch");
     for (int i = 0; i < nrels; i++) {
         if (!rels[i]) return fail(AMJ_EINVAL, "batch_submit: null relation");
-        if (rels[i]->ctx != b->ctx) return fail(AMJ_EINVAL, "batch_submit: relation of another context");
+        if (rels[i]->ctx->device != b->ctx->device)
+            return fail(AMJ_EINVAL, "batch_submit: relation on another device");
         if (rels[i]->where == AMJ_MEM_HOST_STREAMED)
             return fail(AMJ_EUNSUPPORTED, "batch_submit: relations must be resident on the device");
     }
@@ -643,7 +696,7 @@ extern "C" int amj_batch_run(amj_batch *b, const amj_batch_opts *opts, uint64_t 
                              amj_batch_stats *stats) {
     if (!b) return fail(AMJ_EINVAL, "batch_run: null batch");
     amj_batch_opts o;
-    AMJ_TRY(normalize_opts(opts, &o));
+    AMJ_TRY(normalize_batch_opts(opts, &o));
     return batch_run(b, o, counts, checksums, stats);
 }
 
@@ -695,7 +748,7 @@ extern "C" int amj_batch_tune(amj_batch *b, const amj_batch_tune_grid *grid, uin
                 o.block_size = g.block_size[j];
                 o.task_chunk = g.task_chunk[t];
                 amj_batch_opts n;
-                AMJ_TRY(normalize_opts(&o, &n));
+                AMJ_TRY(normalize_batch_opts(&o, &n));
                 amj_batch_stats st;
                 AMJ_TRY(batch_run(&sub, n, nullptr, nullptr, &st));   // warm-up
                 std::vector<double> ms;
@@ -726,6 +779,7 @@ extern "C" int amj_batch_destroy(amj_batch *b) {
     for (auto &e : b->ev)
         if (e) cudaEventDestroy(e);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    if (b->done_ev) cudaEventDestroy(b->done_ev);
     delete b;
     return AMJ_OK;
 }

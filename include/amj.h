@@ -166,6 +166,8 @@ typedef struct amj_batch_opts {
     int      task_chunk;    /* work-sharing task size in candidates, >= 32 (0: 1024)   */
     int      use_graph;     /* 1: capture the device sequence into a CUDA graph on the
                                first run with these options and replay it afterwards   */
+    int      grid_blocks;   /* probe blocks (0: as many as are resident on the device);
+                               a share of the device lets batches run side by side     */
 } amj_batch_opts;
 
 typedef struct amj_batch_stats {
@@ -201,6 +203,60 @@ int  amj_batch_run(amj_batch *b, const amj_batch_opts *opts, uint64_t *counts,
 int  amj_batch_tune(amj_batch *b, const amj_batch_tune_grid *grid, uint32_t sample_every,
                     int reps, amj_batch_opts *best, double *best_ms);
 int  amj_batch_destroy(amj_batch *b);
+
+/* ---- request server: resident relations, continuous batching, ooc spill ----
+ * No reference counterpart.  A host thread takes submitted AMHJ queries in
+ * arrival order and runs them as batches on `lanes` contexts of the same
+ * device (each batch on a share of the SMs, so batches overlap); a request is
+ * admitted when its estimated device memory fits the budget left by the
+ * batches in flight.  Requests over host-resident relations
+ * (AMJ_MEM_HOST_STREAMED), requests submitted with ooc = 1, and requests too
+ * large for the whole budget run through the out-of-core operator on their
+ * own lane (context, stream and host thread), streaming probe slices from
+ * pinned host memory.  Results are the same as one amj_amhj_execute call per
+ * query (count and checksum). */
+typedef struct amj_server amj_server;
+
+typedef struct amj_serve_opts {
+    int      lanes;           /* batches in flight at once (0: 2)                        */
+    uint32_t max_batch;       /* queries per batch (0: 256)                               */
+    uint64_t mem_budget;      /* device bytes for batches in flight (0: 80% of the free
+                                 memory at creation, minus the ooc lane's share)          */
+    amj_batch_opts batch;     /* options of every batch (use_graph ignored; grid_blocks 0:
+                                 twice the SM count divided by the lanes)                 */
+    int      ooc_lane;        /* 1: run out-of-core and spilled requests on their own lane */
+    uint64_t ooc_mem;         /* device bytes of the ooc lane's slices (0: free / 8)       */
+    uint64_t ooc_slice_rows;  /* ooc probe slice rows (0: derived from ooc_mem)            */
+} amj_serve_opts;
+
+typedef struct amj_serve_result {
+    uint64_t count, checksum;
+    int32_t  status;          /* AMJ_OK or the error of the request's batch / ooc run */
+    int32_t  path;            /* 0 batched, 1 out-of-core lane                         */
+    int32_t  spilled;         /* 1: sent to the out-of-core lane by admission           */
+    uint32_t batch_id, batch_size;
+    int32_t  pad;
+    double   queue_ms;        /* submit -> launch                                      */
+    double   exec_ms;         /* launch -> result                                      */
+    double   latency_ms;      /* submit -> result                                      */
+} amj_serve_result;
+
+typedef struct amj_serve_stats {
+    uint64_t submitted, completed, rejected, spilled, batches, ooc_runs;
+    uint64_t budget_bytes, peak_reserved_bytes;
+    uint32_t max_inflight_batches, lanes;
+} amj_serve_stats;
+
+int  amj_server_create(amj_ctx *ctx, const amj_serve_opts *opts, amj_server **out);
+/* relations must stay alive until the request's result has been waited for */
+int  amj_server_submit(amj_server *s, int query_type, amj_rel *const *rels, int nrels,
+                       int flags, int ooc, uint64_t *ticket);
+/* waits up to timeout_ms (AMJ_ETIMEOUT otherwise); returns the request's
+ * status and releases the ticket */
+int  amj_server_wait(amj_server *s, uint64_t ticket, uint32_t timeout_ms, amj_serve_result *out);
+int  amj_server_stats(amj_server *s, amj_serve_stats *out);
+/* finishes every submitted request, then stops the server threads */
+int  amj_server_destroy(amj_server *s);
 
 /* ---- building blocks on device pointers, enqueued on the context stream ----
  * amj_bucket_build: bucket-CSR index of n keys with `buckets` (a power of two)
