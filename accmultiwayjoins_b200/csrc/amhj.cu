@@ -706,6 +706,12 @@ int amhj_ooc_execute(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch *X, const amj_re
             registered[c] = cudaHostRegister((void *)probe->h_cols[c], n * sizeof(int32_t),
                                              cudaHostRegisterReadOnly) == cudaSuccess;
         (void)cudaGetLastError();
+        // the staging buffers are stream-ordered allocations of the context
+        // stream; the side stream may write them only after they exist
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            cleanup();
+            return fail(AMJ_ECUDA, "ooc: synchronising the staging allocations failed");
+        }
     }
     auto stage_copy = [&](uint64_t s) -> int {
         const int b = (int)(s & 1);
@@ -751,7 +757,8 @@ int amhj_ooc_execute(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch *X, const amj_re
             for (int a = 0; a < k; a++) dev_free(ctx, pr.cols[a]);
         }
     }
-    if (rc == AMJ_OK) (void)cudaStreamSynchronize(ctx->side_stream[0]);
+    // no staging copy may outlive its buffer, on the error paths too
+    if (host) (void)cudaStreamSynchronize(ctx->side_stream[0]);
     cleanup();
     if (rc != AMJ_OK) return rc;
     out->count = count;

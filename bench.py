@@ -405,6 +405,123 @@ def run_batch(args, rank, world, local_rank):
     ctx.close()
 
 
+class ServeMix:
+    """The serving workload: a Poisson request stream (default 200 requests/s)
+    of scaled skewed-clique and star queries against relations kept resident
+    in HBM, plus out-of-core 4-way chain joins interleaved every few seconds
+    whose probe relation stays in pinned host memory.
+
+    Resident templates (each request picks one uniformly, seed 5):
+    * FOUR (4-clique) over R-MAT graphs of scale 10, 11, 12 (16 edges per
+      vertex, quadrant probabilities 0.6/0.15/0.15/0.1);
+    * 4-way star: fact of 50K / 200K / 1M rows of Zipf(1.1) foreign keys into
+      dimensions of 1M / 200K / 100K / 10K rows scaled by fact rows / 60M.
+    Out-of-core: R1(a,b) R2(b,c) R3(c,d) R4(d,e) of --ooc-rows rows each, keys
+    uniform in [0, rows) (about one match per probe row per join)."""
+
+    def __init__(self, args, rank):
+        from accmultiwayjoins_b200 import data
+        self.args = args
+        self.templates = []
+        for sc in (10, 11, 12):
+            s_, d_ = data.rmat(sc, (1 << sc) * 16, 0.6, 0.15, 0.15, seed=5 + sc + 100 * rank)
+            self.templates.append(("FOUR", f"4-clique R-MAT scale {sc}", [([s_, d_], [0, 1])]))
+        for fr in (50_000, 200_000, 1_000_000):
+            dims = [max(100, m * fr // 60_000_000) for m in (1_000_000, 200_000, 100_000, 10_000)]
+            fact, dd = data.star_relations(fr, dims, theta=1.1, seed=7 + fr + rank)
+            self.templates.append(("NORMAL", f"star fact {fr} dims {dims}", [fact] + dd))
+        n = args.ooc_rows
+        self.ooc = [([data.uniform(n, 0, n, 31 + i + 10 * rank, 0), data.uniform(n, 0, n, 31 + i + 10 * rank, 1)],
+                     [i, i + 1]) for i in range(4)] if n else None
+
+    def describe(self, rank_note):
+        return (f"serving: Poisson {self.args.rate:g} requests/s of {len(self.templates)} resident templates "
+                f"(FOUR on R-MAT scale 10-12, 4-way star with 50K-1M fact rows) plus an out-of-core 4-way chain "
+                f"join of 4 x {self.args.ooc_rows} rows (probe in pinned host memory) every "
+                f"{self.args.ooc_every:g} s{rank_note}; continuous batching, {self.args.lanes} lanes")
+
+
+def run_serve(args, rank, world, local_rank):
+    import torch
+    from accmultiwayjoins_b200 import Context
+
+    torch.cuda.set_device(local_rank)
+    wl = ServeMix(args, rank)
+    ctx = Context(local_rank, ooc_slice_rows=args.ooc_slice)
+    trels = [[ctx.relation(c, a) for c, a in rels] for _, _, rels in wl.templates]
+    alone = []
+    for (qt, _, _), r in zip(wl.templates, trels):
+        x = ctx.amhj(qt, r)
+        alone.append((x.count, x.checksum))
+    ooc_rels, ooc_want = None, None
+    if wl.ooc:
+        pinned = [torch.from_numpy(c).pin_memory() for c in wl.ooc[0][0]]
+        ooc_rels = [ctx.relation([p.numpy() for p in pinned], wl.ooc[0][1], streamed=True)]
+        ooc_rels += [ctx.relation(c, a) for c, a in wl.ooc[1:]]
+        x = ctx.amhj("NORMAL", ooc_rels, ooc=1)
+        ooc_want = (x.count, x.checksum)
+    srv = ctx.server(lanes=args.lanes, max_batch=args.max_batch, ooc_lane=True)
+    rng = np.random.Generator(np.random.PCG64(5 + rank))
+
+    def stream(seconds):
+        """Submit a Poisson stream for `seconds`; returns [(template or -1, ticket)]."""
+        out = []
+        t_end = time.perf_counter() + seconds
+        t_next = time.perf_counter()
+        t_ooc = time.perf_counter() + args.ooc_every / 2
+        while True:
+            t_next += rng.exponential(1.0 / args.rate)
+            if t_next >= t_end:
+                break
+            while time.perf_counter() < t_next:
+                time.sleep(0.0001)
+            if ooc_rels is not None and time.perf_counter() >= t_ooc:
+                out.append((-1, srv.submit("NORMAL", ooc_rels, ooc=True)))
+                t_ooc += args.ooc_every
+            i = int(rng.integers(0, len(wl.templates)))
+            out.append((i, srv.submit(wl.templates[i][0], trels[i])))
+        return out
+
+    warm = stream(args.warmup * 0.5)
+    for _, t in warm:
+        srv.wait(t)
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    t0 = time.perf_counter()
+    timed = stream(float(args.steps))
+    res = [(i, srv.wait(t)) for i, t in timed]
+    clocks = sampler.stop()
+    for i, r in res:
+        assert (r.count, r.checksum) == (ooc_want if i < 0 else alone[i]), "served result differs from alone"
+    st = srv.stats()
+    srv.close()
+    # the window runs from the first timed submission until every timed request has completed
+    total = sum(r.count for _, r in res)
+    wall = time.perf_counter() - t0
+    lat = [r.latency_ms for i, r in res if i >= 0]
+    olat = [r.latency_ms for i, r in res if i < 0]
+    bsz = [r.batch_size for i, r in res if i >= 0]
+    line = {
+        "metric": METRIC, "value": total / wall, "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+        "config": {"workload": wl.describe(""), "step": "one second of the request stream",
+                   "requests": len(res), "ooc_requests": len(olat), "output_tuples": total,
+                   "l2": "resident relations and ooc inputs larger than L2"},
+        "e2e": {"value": total / wall, "unit": "tuples/s",
+                "h2d_bytes_per_step": int(len(olat) * 8 * args.ooc_rows / args.steps),
+                "d2h_bytes_per_step": int(16 * len(res) / args.steps),
+                "note": "requests submitted from the host, results read back; resident relations are not re-copied"},
+        "latency_ms": {"resident": {"p50": pct(lat, 50), "p99": pct(lat, 99)},
+                       "ooc": {"p50": pct(olat, 50), "p99": pct(olat, 99)} if olat else None},
+        "serve_stats": {**st, "mean_batch_size": sum(bsz) / max(1, len(bsz))},
+        "gpu_launches": None,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def Batch_default_opts(L):
     o = L.amj_batch_opts()
     o.block_size, o.task_chunk = 256, 1024
@@ -593,7 +710,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--algo", default="DFS", choices=["DFS", "BFS", "AMHJ"])
-    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain", "batch"])
+    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain", "batch", "serve"])
+    ap.add_argument("--rate", type=float, default=200.0, help="serve workload: requests per second")
+    ap.add_argument("--lanes", type=int, default=3, help="serve workload: batches in flight")
+    ap.add_argument("--max-batch", type=int, default=128, help="serve workload: requests per batch")
+    ap.add_argument("--ooc-rows", type=int, default=64 << 20, help="serve workload: rows per ooc relation")
+    ap.add_argument("--ooc-every", type=float, default=2.5, help="serve workload: seconds between ooc joins")
+    ap.add_argument("--ooc-slice", type=int, default=8 << 20, help="serve workload: ooc probe slice rows")
     ap.add_argument("--queries", type=int, default=512, help="batch workload: queries per batch")
     ap.add_argument("--min-rows", type=int, default=10_000, help="batch workload: smallest relation")
     ap.add_argument("--max-rows", type=int, default=4_000_000, help="batch workload: largest relation")
@@ -616,6 +739,8 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.workload == "batch":
         run_batch(args, rank, world, local_rank)
+    elif args.workload == "serve":
+        run_serve(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
     if world > 1:

@@ -268,6 +268,25 @@ def test_amhj_out_of_core(streamed, materialize):
                 assert data.checksum(got.columns) == chk
 
 
+def test_amhj_out_of_core_streamed_large_slices():
+    """Host-streamed probe whose staging buffers are fresh pool allocations
+    (4M rows, 1M-row slices, pinned and pageable host columns): equal to the
+    device-resident join."""
+    import torch
+    n = 1 << 22
+    rels = [([data.uniform(n, 0, n, 31 + i, 0), data.uniform(n, 0, n, 31 + i, 1)], [i, i + 1]) for i in range(4)]
+    with Context(0, ooc_slice_rows=1 << 20) as ctx:
+        dev = [ctx.relation(c, a) for c, a in rels]
+        want = ctx.amhj("NORMAL", dev)
+        pinned = [torch.from_numpy(c).pin_memory() for c in rels[0][0]]
+        for cols in (rels[0][0], [p.numpy() for p in pinned]):
+            probe = ctx.relation(cols, rels[0][1], streamed=True)
+            for ws in (0, 1):
+                got = ctx.amhj("NORMAL", [probe] + dev[1:], ooc=1, ws=ws)
+                assert (got.count, got.checksum) == (want.count, want.checksum)
+                assert got.stats["slices"] == 4
+
+
 def test_amhj_edge_cases(ctx):
     z = np.zeros(0, np.int32)
     one = ([np.array([3], np.int32), np.array([4], np.int32)], [0, 1])
