@@ -149,6 +149,7 @@ class amj_serve_stats(C.Structure):
         ("ooc_runs", C.c_uint64),
         ("budget_bytes", C.c_uint64),
         ("peak_reserved_bytes", C.c_uint64),
+        ("launches", C.c_uint64),
         ("max_inflight_batches", C.c_uint32),
         ("lanes", C.c_uint32),
     ]

@@ -230,6 +230,8 @@ struct amj_batch {
     unsigned long long *h_out = nullptr;
     bool replayed = false;
 
+    size_t h_out_bytes = 0;
+
     void drop_graph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -260,6 +262,14 @@ struct amj_batch {
         ready.release();
         if (h_out) cudaFreeHost(h_out);
         h_out = nullptr;
+        h_out_bytes = 0;
+    }
+    // forget the plan but keep every buffer for the next prepare (they only grow)
+    void invalidate() {
+        drop_graph();
+        prepared = false;
+        jobs.clear();
+        job_rb.clear();
     }
 };
 
@@ -300,9 +310,17 @@ static int batch_kernel_setup(amj_ctx *ctx, size_t smem, unsigned *grid) {
 }
 
 // Plan the batch for the given options: jobs, plans, sizes, device buffers.
+// grow-only device buffer
+template <typename T>
+static int ensure(amj_ctx *ctx, DBuf<T> &buf, size_t n) {
+    if (buf.p && buf.n >= n) return AMJ_OK;
+    buf.release();
+    return buf.alloc(ctx, n);
+}
+
 static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
     amj_ctx *ctx = b->ctx;
-    b->unprepare();
+    b->invalidate();
     const uint32_t nq = (uint32_t)b->qs.size();
     if (nq == 0) return fail(AMJ_EINVAL, "batch: no queries submitted");
     // ---- jobs: one per distinct index; bucket-layout jobs first
@@ -385,30 +403,30 @@ static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
 
     // ---- device buffers of the build
     const uint32_t njobs = (uint32_t)b->jobs.size();
-    AMJ_TRY(b->d_jobs.alloc(ctx, std::max<uint32_t>(njobs, 1)));
-    AMJ_TRY(b->d_job_rb.alloc(ctx, std::max<uint32_t>(njobs, 1)));
+    AMJ_TRY(ensure(ctx, b->d_jobs, std::max<uint32_t>(njobs, 1)));
+    AMJ_TRY(ensure(ctx, b->d_job_rb, std::max<uint32_t>(njobs, 1)));
     AMJ_CUDA_TRY(cudaMemcpyAsync(b->d_jobs.p, b->jobs.data(), njobs * sizeof(BatchJob), cudaMemcpyHostToDevice,
                                  ctx->stream));
     AMJ_CUDA_TRY(cudaMemcpyAsync(b->d_job_rb.p, b->job_rb.data(), njobs * sizeof(unsigned long long),
                                  cudaMemcpyHostToDevice, ctx->stream));
     const uint64_t br = std::max<uint64_t>(b->bucket_rows, 1);
-    AMJ_TRY(b->items_a.alloc(ctx, br));
-    AMJ_TRY(b->items_b.alloc(ctx, br));
-    for (int c = 0; c < b->ncols_max; c++) AMJ_TRY(b->gcols[c].alloc(ctx, br));
-    AMJ_TRY(b->gptrs.alloc(ctx, b->total_buckets + 1));
-    if (b->total_slots) AMJ_TRY(b->gslots.alloc(ctx, b->total_slots));
+    AMJ_TRY(ensure(ctx, b->items_a, br));
+    AMJ_TRY(ensure(ctx, b->items_b, br));
+    for (int c = 0; c < b->ncols_max; c++) AMJ_TRY(ensure(ctx, b->gcols[c], br));
+    AMJ_TRY(ensure(ctx, b->gptrs, b->total_buckets + 1));
+    if (b->total_slots) AMJ_TRY(ensure(ctx, b->gslots, b->total_slots));
 
     // ---- plans
     std::vector<unsigned long long> qrow(nq + 1, 0);
     for (uint32_t q = 0; q < nq; q++) qrow[q + 1] = qrow[q] + b->qs[q].hp.probe->n;
     b->probe_rows = qrow[nq];
-    AMJ_TRY(b->qrow.alloc(ctx, nq + 1));
-    AMJ_TRY(b->sizes.alloc(ctx, b->probe_rows + 1));
-    AMJ_TRY(b->l0.alloc(ctx, b->probe_rows + 1));
-    AMJ_TRY(b->unit_base.alloc(ctx, nq + 1));
-    AMJ_TRY(b->q_count.alloc(ctx, nq));
-    AMJ_TRY(b->q_checksum.alloc(ctx, nq));
-    AMJ_TRY(b->plans.alloc(ctx, nq));
+    AMJ_TRY(ensure(ctx, b->qrow, nq + 1));
+    AMJ_TRY(ensure(ctx, b->sizes, b->probe_rows + 1));
+    AMJ_TRY(ensure(ctx, b->l0, b->probe_rows + 1));
+    AMJ_TRY(ensure(ctx, b->unit_base, nq + 1));
+    AMJ_TRY(ensure(ctx, b->q_count, nq));
+    AMJ_TRY(ensure(ctx, b->q_checksum, nq));
+    AMJ_TRY(ensure(ctx, b->plans, nq));
     AMJ_CUDA_TRY(cudaMemcpyAsync(b->qrow.p, qrow.data(), (nq + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice,
                                  ctx->stream));
     amj_opts po = ctx->opts;
@@ -437,9 +455,9 @@ static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
     AMJ_CUDA_TRY(cudaMemcpyAsync(b->plans.p, hplans.data(), nq * sizeof(ProbePlan), cudaMemcpyHostToDevice,
                                  ctx->stream));
     b->task_cap = hplans[0].task_cap;
-    AMJ_TRY(b->st.alloc(ctx, 1));
-    AMJ_TRY(b->tasks.alloc(ctx, b->task_cap));
-    AMJ_TRY(b->ready.alloc(ctx, b->task_cap));
+    AMJ_TRY(ensure(ctx, b->st, 1));
+    AMJ_TRY(ensure(ctx, b->tasks, b->task_cap));
+    AMJ_TRY(ensure(ctx, b->ready, b->task_cap));
 
     // ---- probe launch shape
     b->block = (uint32_t)o.block_size;
@@ -451,8 +469,14 @@ static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
     else AMJ_TRY(batch_kernel_setup<512>(ctx, b->smem, &b->grid));
     if (o.grid_blocks > 0 && (unsigned)o.grid_blocks < b->grid) b->grid = (unsigned)o.grid_blocks;
     const size_t hbytes = (2 * (size_t)nq + 1) * sizeof(unsigned long long) + sizeof(ProbeState);
-    AMJ_CUDA_TRY(cudaMallocHost((void **)&b->h_out, hbytes));
-    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (b->h_out_bytes < hbytes) {
+        // pinned memory is kept across runs: freeing it synchronises the device
+        if (b->h_out) cudaFreeHost(b->h_out);
+        b->h_out = nullptr;
+        b->h_out_bytes = 0;
+        AMJ_CUDA_TRY(cudaMallocHost((void **)&b->h_out, hbytes));
+        b->h_out_bytes = hbytes;
+    }
     b->popts = o;
     b->prepared = true;
     return AMJ_OK;
@@ -597,6 +621,12 @@ int batch_launch(amj_batch *b, const amj_batch_opts &o) {
     return AMJ_OK;
 }
 
+// drop the submitted queries, keep the buffers for the next ones
+void batch_clear(amj_batch *b) {
+    b->invalidate();
+    b->qs.clear();
+}
+
 // whether the last launched run has completed (no waiting)
 bool batch_done(amj_batch *b) { return b->done_ev && cudaEventQuery(b->done_ev) == cudaSuccess; }
 
@@ -687,7 +717,7 @@ extern "C" int amj_batch_submit(amj_batch *b, int query_type, amj_rel *const *re
     AMJ_TRY(compile_plan(query_type, rels, nrels, flags, &q.hp));
     if (q.hp.L == 0) return fail(AMJ_EUNSUPPORTED, "batch_submit: a query needs at least one build relation");
     b->qs.push_back(q);
-    b->unprepare();
+    b->invalidate();
     if (qid) *qid = (uint32_t)(b->qs.size() - 1);
     return AMJ_OK;
 }

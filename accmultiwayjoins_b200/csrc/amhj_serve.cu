@@ -100,9 +100,10 @@ void finish(amj_server *s, ServeReq *r, int status) {
     s->st.completed++;
 }
 
-// Launch the requests of one lane as a batch.  Called without the lock.
+// Launch the requests of one lane as a batch.  Called without the lock.  The
+// lane's batch object is reused: its device and pinned buffers only grow.
 int launch_lane(amj_server *s, Lane &ln) {
-    AMJ_TRY(amj_batch_create(ln.ctx, &ln.b));
+    batch_clear(ln.b);
     for (ServeReq *r : ln.reqs)
         AMJ_TRY(amj_batch_submit(ln.b, r->qt, r->rels.data(), (int)r->rels.size(), r->flags & AMJ_F_NO_REORDER,
                                  nullptr));
@@ -119,8 +120,6 @@ void server_loop(amj_server *s) {
             lk.unlock();
             std::vector<uint64_t> cnt(ln.reqs.size()), chk(ln.reqs.size());
             const int rc = batch_collect(ln.b, cnt.data(), chk.data(), nullptr);
-            amj_batch_destroy(ln.b);
-            ln.b = nullptr;
             lk.lock();
             for (size_t i = 0; i < ln.reqs.size(); i++) {
                 ln.reqs[i]->count = cnt[i];
@@ -185,10 +184,6 @@ void server_loop(amj_server *s) {
             const int rc = launch_lane(s, ln);
             lk.lock();
             if (rc != AMJ_OK) {
-                if (ln.b) {
-                    amj_batch_destroy(ln.b);
-                    ln.b = nullptr;
-                }
                 for (ServeReq *r : ln.reqs) finish(s, r, rc);
                 ln.reqs.clear();
                 s->reserved -= ln.reserved;
@@ -267,8 +262,13 @@ extern "C" int amj_server_create(amj_ctx *ctx, const amj_serve_opts *opts, amj_s
     for (int i = 0; i < s->opts.lanes; i++) {
         Lane ln;
         int rc = amj_ctx_create(ctx->device, &lo, &ln.ctx);
+        if (rc == AMJ_OK) rc = amj_batch_create(ln.ctx, &ln.b);
         if (rc != AMJ_OK) {
-            for (Lane &l : s->lanes) amj_ctx_destroy(l.ctx);
+            if (ln.ctx) amj_ctx_destroy(ln.ctx);
+            for (Lane &l : s->lanes) {
+                amj_batch_destroy(l.b);
+                amj_ctx_destroy(l.ctx);
+            }
             return rc;
         }
         s->lanes.push_back(ln);
@@ -279,7 +279,10 @@ extern "C" int amj_server_create(amj_ctx *ctx, const amj_serve_opts *opts, amj_s
         if (s->opts.ooc_slice_rows) oo.ooc_slice_rows = s->opts.ooc_slice_rows;
         int rc = amj_ctx_create(ctx->device, &oo, &s->ooc_ctx);
         if (rc != AMJ_OK) {
-            for (Lane &l : s->lanes) amj_ctx_destroy(l.ctx);
+            for (Lane &l : s->lanes) {
+                amj_batch_destroy(l.b);
+                amj_ctx_destroy(l.ctx);
+            }
             return rc;
         }
     }
@@ -360,6 +363,9 @@ extern "C" int amj_server_stats(amj_server *s, amj_serve_stats *out) {
     *out = s->st;
     out->budget_bytes = s->budget;
     out->peak_reserved_bytes = s->peak_reserved;
+    out->launches = 0;
+    for (const Lane &ln : s->lanes) out->launches += ln.ctx->launches;
+    if (s->ooc_ctx) out->launches += s->ooc_ctx->launches;
     out->lanes = (uint32_t)s->lanes.size();
     return AMJ_OK;
 }

@@ -485,6 +485,7 @@ def run_serve(args, rank, world, local_rank):
     warm = stream(args.warmup * 0.5)
     for _, t in warm:
         srv.wait(t)
+    st_warm = srv.stats()
     sampler = ClockSampler(local_rank)
     sampler.start()
     t0 = time.perf_counter()
@@ -494,6 +495,7 @@ def run_serve(args, rank, world, local_rank):
     for i, r in res:
         assert (r.count, r.checksum) == (ooc_want if i < 0 else alone[i]), "served result differs from alone"
     st = srv.stats()
+    launches_timed = st["launches"] - st_warm["launches"]
     srv.close()
     # the window runs from the first timed submission until every timed request has completed
     total = sum(r.count for _, r in res)
@@ -515,7 +517,7 @@ def run_serve(args, rank, world, local_rank):
         "latency_ms": {"resident": {"p50": pct(lat, 50), "p99": pct(lat, 99)},
                        "ooc": {"p50": pct(olat, 50), "p99": pct(olat, 99)} if olat else None},
         "serve_stats": {**st, "mean_batch_size": sum(bsz) / max(1, len(bsz))},
-        "gpu_launches": None,
+        "gpu_launches": launches_timed,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)

@@ -244,6 +244,7 @@ typedef struct amj_serve_result {
 typedef struct amj_serve_stats {
     uint64_t submitted, completed, rejected, spilled, batches, ooc_runs;
     uint64_t budget_bytes, peak_reserved_bytes;
+    uint64_t launches;        /* kernels launched by the lanes and the ooc lane   */
     uint32_t max_inflight_batches, lanes;
 } amj_serve_stats;
 
