@@ -145,9 +145,9 @@ double event_ms(cudaEvent_t a, cudaEvent_t b) {
     return (double)ms;
 }
 
-template <int MODE, bool WS>
+template <int MODE, bool WS, bool WT>
 static int launch_probe_t(amj_ctx *ctx, const ProbeLaunch &PL, size_t smem) {
-    auto kern = amhj_probe_kernel<MODE, WS>;
+    auto kern = amhj_probe_kernel<MODE, WS, WT>;
     AMJ_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PROBE_THREADS, smem));
@@ -172,9 +172,14 @@ static int launch_probe_t(amj_ctx *ctx, const ProbeLaunch &PL, size_t smem) {
 
 static int launch_probe_raw(amj_ctx *ctx, const ProbeLaunch &PL, int mode, bool ws) {
     const size_t smem = (size_t)PROBE_WARPS * PL.P.warp_bytes;
-    if (mode == PM_COUNT) return ws ? launch_probe_t<PM_COUNT, true>(ctx, PL, smem) : launch_probe_t<PM_COUNT, false>(ctx, PL, smem);
-    if (mode == PM_WRITE) return ws ? launch_probe_t<PM_WRITE, true>(ctx, PL, smem) : launch_probe_t<PM_WRITE, false>(ctx, PL, smem);
-    return ws ? launch_probe_t<PM_RESIDUAL, true>(ctx, PL, smem) : launch_probe_t<PM_RESIDUAL, false>(ctx, PL, smem);
+    const bool wt = PL.P.has_inl != 0;
+#define AMJ_LAUNCH(M)                                                                              \
+    return ws ? (wt ? launch_probe_t<M, true, true>(ctx, PL, smem) : launch_probe_t<M, true, false>(ctx, PL, smem)) \
+              : (wt ? launch_probe_t<M, false, true>(ctx, PL, smem) : launch_probe_t<M, false, false>(ctx, PL, smem))
+    if (mode == PM_COUNT) AMJ_LAUNCH(PM_COUNT);
+    if (mode == PM_WRITE) AMJ_LAUNCH(PM_WRITE);
+    AMJ_LAUNCH(PM_RESIDUAL);
+#undef AMJ_LAUNCH
 }
 
 // probe launch bracketed by the context's kernel-timing events
@@ -542,6 +547,7 @@ static int build_fib(amj_ctx *ctx, const HostPlan &hp, const std::vector<const H
     S.lbs = 0;
     S.dro = 0;
     S.fib_level = -1;
+    plan_inline(S);
     SL.batch_stride = 1;
     SL.batch_count = (K + 31) / 32;
     ProbeState h{};
@@ -840,6 +846,7 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
     ProbePlan &P = PL.P;
     plan_common(hp, ctx->opts, &P);
     for (int l = 0; l < hp.L; l++) fill_level(hp.lv[l], *lvix[l], &P.lv[l]);
+    plan_inline(P);
     AMJ_TRY(X.st.alloc(ctx, 1));
     PL.st = X.st.p;
     PL.status = ctx->d_status;

@@ -206,6 +206,7 @@ struct amj_batch {
     uint64_t bucket_rows = 0, oa_rows = 0, total_buckets = 0, total_slots = 0, probe_rows = 0;
     int sort_bits = 0, ncols_max = 1;
     uint32_t block = 256, warp_stride = 0;
+    bool weighted = false;   // some query has inlined filter levels
     unsigned grid = 0;
     size_t smem = 0;
     DBuf<BatchJob> d_jobs;
@@ -298,9 +299,9 @@ int normalize_batch_opts(const amj_batch_opts *in, amj_batch_opts *o) {
     return AMJ_OK;
 }
 
-template <int T>
+template <int T, bool WT>
 static int batch_kernel_setup(amj_ctx *ctx, size_t smem, unsigned *grid) {
-    auto kern = amhj_batch_kernel<T>;
+    auto kern = amhj_batch_kernel<T, WT>;
     AMJ_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem));
@@ -450,6 +451,7 @@ static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
             else
                 fill_level_desc(hp.lv[l], J.layout, J.key_mode, J.mask, nullptr, gc, b->gslots.p + J.base, &P.lv[l]);
         }
+        plan_inline(P);
         max_warp_bytes = std::max(max_warp_bytes, P.warp_bytes);
     }
     AMJ_CUDA_TRY(cudaMemcpyAsync(b->plans.p, hplans.data(), nq * sizeof(ProbePlan), cudaMemcpyHostToDevice,
@@ -464,9 +466,17 @@ static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
     b->warp_stride = (BATCH_PLAN_BYTES + max_warp_bytes + 15) / 16 * 16;
     b->smem = (size_t)(b->block / 32) * b->warp_stride;
     if (b->smem > (size_t)ctx->max_smem_optin) return fail(AMJ_EUNSUPPORTED, "batch: frontier exceeds shared memory");
-    if (b->block == 128) AMJ_TRY(batch_kernel_setup<128>(ctx, b->smem, &b->grid));
-    else if (b->block == 256) AMJ_TRY(batch_kernel_setup<256>(ctx, b->smem, &b->grid));
-    else AMJ_TRY(batch_kernel_setup<512>(ctx, b->smem, &b->grid));
+    b->weighted = false;
+    for (const ProbePlan &P : hplans) b->weighted |= P.has_inl != 0;
+    if (b->weighted) {
+        if (b->block == 128) AMJ_TRY((batch_kernel_setup<128, true>(ctx, b->smem, &b->grid)));
+        else if (b->block == 256) AMJ_TRY((batch_kernel_setup<256, true>(ctx, b->smem, &b->grid)));
+        else AMJ_TRY((batch_kernel_setup<512, true>(ctx, b->smem, &b->grid)));
+    } else {
+        if (b->block == 128) AMJ_TRY((batch_kernel_setup<128, false>(ctx, b->smem, &b->grid)));
+        else if (b->block == 256) AMJ_TRY((batch_kernel_setup<256, false>(ctx, b->smem, &b->grid)));
+        else AMJ_TRY((batch_kernel_setup<512, false>(ctx, b->smem, &b->grid)));
+    }
     if (o.grid_blocks > 0 && (unsigned)o.grid_blocks < b->grid) b->grid = (unsigned)o.grid_blocks;
     const size_t hbytes = (2 * (size_t)nq + 1) * sizeof(unsigned long long) + sizeof(ProbeState);
     if (b->h_out_bytes < hbytes) {
@@ -554,9 +564,15 @@ static int batch_record(amj_batch *b, bool capturing) {
     L.spin_limit_ns = (uint64_t)ctx->opts.spin_limit_ms * 1000000ull;
     L.warp_stride = b->warp_stride;
     note_launch(ctx);
-    if (b->block == 128) amhj_batch_kernel<128><<<b->grid, 128, b->smem, s>>>(L);
-    else if (b->block == 256) amhj_batch_kernel<256><<<b->grid, 256, b->smem, s>>>(L);
-    else amhj_batch_kernel<512><<<b->grid, 512, b->smem, s>>>(L);
+    if (b->weighted) {
+        if (b->block == 128) amhj_batch_kernel<128, true><<<b->grid, 128, b->smem, s>>>(L);
+        else if (b->block == 256) amhj_batch_kernel<256, true><<<b->grid, 256, b->smem, s>>>(L);
+        else amhj_batch_kernel<512, true><<<b->grid, 512, b->smem, s>>>(L);
+    } else {
+        if (b->block == 128) amhj_batch_kernel<128, false><<<b->grid, 128, b->smem, s>>>(L);
+        else if (b->block == 256) amhj_batch_kernel<256, false><<<b->grid, 256, b->smem, s>>>(L);
+        else amhj_batch_kernel<512, false><<<b->grid, 512, b->smem, s>>>(L);
+    }
     AMJ_CUDA_TRY(cudaGetLastError());
     AMJ_TRY(mark(b->ev[2], s, capturing));
     b->launches_per_run = ctx->launches - l0;

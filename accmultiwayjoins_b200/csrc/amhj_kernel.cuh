@@ -32,7 +32,7 @@ struct ProbeLaunch {
 };
 
 __device__ __forceinline__ bool ws_push(const ProbePlan &P, const WsQueue &Q, const int32_t *vals, uint32_t s,
-                                        uint32_t sz, uint8_t depth, uint16_t qid) {
+                                        uint32_t sz, uint8_t depth, uint16_t qid, uint32_t w) {
     ProbeState *st = Q.st;
     if (ld_volatile_u32(&st->q_tail) >= P.task_cap) return false;
     const uint32_t slot = atomicAdd(&st->q_tail, 1u);
@@ -45,6 +45,7 @@ __device__ __forceinline__ bool ws_push(const ProbePlan &P, const WsQueue &Q, co
     t->depth = depth;
     t->m8 = 0;
     t->qid = qid;
+    t->w = w;
     __threadfence();
     atomicExch(&Q.ready[slot], 1u);
     atomicAdd(&st->tasks_pushed, 1ull);
@@ -58,18 +59,18 @@ __device__ __forceinline__ bool ws_push(const ProbePlan &P, const WsQueue &Q, co
 template <int MODE, bool WS>
 __device__ __forceinline__ uint32_t maybe_split(const ProbePlan &P, const WsQueue &Q, const LevelDesc &lv,
                                                 const int32_t *vals, uint32_t s, uint32_t sz, int depth,
-                                                uint16_t qid) {
+                                                uint16_t qid, uint32_t w) {
     if (!WS || lv.layout == AMJ_LAYOUT_CUCKOO) return sz;
     const uint32_t chunk = P.task_chunk;
     if (sz <= 2 * chunk) return sz;
     const uint32_t rem = sz - chunk, half = rem / 2;
     if (MODE == PM_RESIDUAL) return chunk;
     // push the tail first so a failure leaves a contiguous kept range
-    if (!ws_push(P, Q, vals, s + chunk + half, rem - half, (uint8_t)depth, qid)) {
+    if (!ws_push(P, Q, vals, s + chunk + half, rem - half, (uint8_t)depth, qid, w)) {
         if (P.dro) report_error(Q.status, (unsigned)-AMJ_EOVERFLOW, SITE_WS_QUEUE, sz);
         return sz;
     }
-    if (!ws_push(P, Q, vals, s + chunk, half, (uint8_t)depth, qid)) {
+    if (!ws_push(P, Q, vals, s + chunk, half, (uint8_t)depth, qid, w)) {
         if (P.dro) report_error(Q.status, (unsigned)-AMJ_EOVERFLOW, SITE_WS_QUEUE, sz);
         return chunk + half;
     }
@@ -82,11 +83,15 @@ static __device__ int ws_acquire(const WsQueue &Q, uint32_t cap, uint64_t spin_l
     ProbeState *st = Q.st;
     bool busy = true;
     unsigned long long t0 = globaltimer_ns();
+    // an idle warp backs off exponentially (64 ns .. 8 us) so that its polling
+    // does not take issue slots from the warps that still work on the SM
+    unsigned int backoff = 64;
     while (true) {
         uint32_t h = ld_volatile_u32(&st->q_head);
         uint32_t t = ld_volatile_u32(&st->q_tail);
         if (t > cap) t = cap;
         if (h < t) {
+            backoff = 64;
             if (!busy) {
                 atomicAdd(&st->busy, 1u);
                 busy = true;
@@ -127,7 +132,8 @@ static __device__ int ws_acquire(const WsQueue &Q, uint32_t cap, uint64_t spin_l
             report_error(Q.status, (unsigned)-AMJ_ETIMEOUT, SITE_WS_IDLE, 0);
             return 0;
         }
-        __nanosleep(256);
+        __nanosleep(backoff);
+        if (backoff < 8192) backoff <<= 1;
     }
 }
 
@@ -210,6 +216,7 @@ __device__ __forceinline__ void load_l0_group(const ProbePlan &P, char *wbase, u
     F.s[lane] = s;
     F.aux[lane] = aux;
     F.m8[lane] = m8;
+    F.w[lane] = 1;
     const unsigned long long ps = warp_inclusive_scan((unsigned long long)sz, lane);
     F.psum[lane] = ps;
     if (lane == 31) {
@@ -233,11 +240,12 @@ __device__ __forceinline__ void load_probe_batch(const ProbePlan &P, const WsQue
     uint8_t m8 = 0;
     if (valid) {
         sz = level_lookup(P.lv[0], [&](int a) { return F.vals[a * 32 + lane]; }, s, aux, m8);
-        sz = maybe_split<MODE, WS>(P, Q, P.lv[0], F.vals + lane, s, sz, 0, qid);
+        sz = maybe_split<MODE, WS>(P, Q, P.lv[0], F.vals + lane, s, sz, 0, qid, 1u);
     }
     F.s[lane] = s;
     F.aux[lane] = aux;
     F.m8[lane] = m8;
+    F.w[lane] = 1;
     const unsigned long long ps = warp_inclusive_scan((unsigned long long)sz, lane);
     F.psum[lane] = ps;
     if (lane == 31) {
@@ -267,10 +275,11 @@ __device__ __forceinline__ int load_task(const ProbePlan &P, const WsQueue &Q, c
     if (lane < P.k) F.vals[lane * 32] = t.vals[lane];
     __syncwarp();
     if (lane == 0) {
-        const uint32_t sz = maybe_split<MODE, WS>(P, Q, P.lv[td], F.vals, t.s, t.sz, td, t.qid);
+        const uint32_t sz = maybe_split<MODE, WS>(P, Q, P.lv[td], F.vals, t.s, t.sz, td, t.qid, t.w);
         F.s[0] = t.s;
         F.aux[0] = t.aux;
         F.m8[0] = t.m8;
+        F.w[0] = t.w;
         F.psum[0] = sz;
         F.meta[0] = 0;
         F.meta[1] = sz;
@@ -291,9 +300,99 @@ struct UnitOut {
     bool over = false;
 };
 
-// Expand one 32-candidate chunk of the frontier at `depth`: compare, then
-// emit at the last level or build the next depth's frontier.
-template <int MODE, bool WS>
+// Rows of an inlined filter level that equal the tuple on every column.
+template <class Get>
+__device__ __forceinline__ uint32_t filter_count(const LevelDesc &fl, Get &&get) {
+    uint32_t s, aux;
+    uint8_t m8;
+    const uint32_t sz = level_lookup(fl, get, s, aux, m8);
+    int32_t want[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) want[c] = c < fl.ncols ? get(fl.attr[c]) : 0;
+    uint32_t m = 0;
+    for (uint32_t i = 0; i < sz; i++) {
+        int32_t v[4] = {0, 0, 0, 0};
+        load_candidate(fl, candidate_slot(fl, s, aux, m8, i), fl.cmp_mask, v);
+        bool eq = true;
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < fl.ncols && ((fl.cmp_mask >> c) & 1)) eq &= v[c] == want[c];
+        m += eq ? 1u : 0u;
+    }
+    return m;
+}
+
+// Emit this step's tuples: lane tuple tv (hash h) stands for `wt` identical
+// tuples (wt = 0: none).  Count mode adds them up; the write modes place them
+// at consecutive positions of the output (the residual pass skips the ones
+// the main pass wrote).
+template <int MODE>
+__device__ __forceinline__ void emit_weighted(const ProbePlan &P, const WsQueue &Q, int lane, const int32_t *tv,
+                                              uint64_t h, uint32_t wt, ProbeAcc &acc, UnitOut &u) {
+    if (MODE == PM_COUNT) {
+        acc.cnt += wt;
+        acc.chk += (unsigned long long)wt * h;
+        return;
+    }
+    const unsigned long long mine = wt;
+    const unsigned long long incl = warp_inclusive_scan(mine, lane);
+    const unsigned long long tot = __shfl_sync(AMJ_FULL_MASK, incl, 31);
+    if (!tot) return;
+    const unsigned long long excl = incl - mine;
+    if (MODE == PM_WRITE) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&Q.st->out_cursor, tot);
+        base = __shfl_sync(AMJ_FULL_MASK, base, 0);
+        acc.cnt += wt;
+        acc.chk += (unsigned long long)wt * h;
+        for (uint32_t r = 0; r < wt; r++) {
+            const unsigned long long pos = base + excl + r;
+            if (pos < P.out_cap) {
+#pragma unroll
+                for (int a = 0; a < AMJ_MAX_ATTRS; a++)
+                    if (a < P.k) P.out[a][pos] = tv[a];
+            }
+        }
+        if (!u.over) {
+            if (base + tot <= P.out_cap) u.written += tot;
+            else {
+                u.written += base < P.out_cap ? P.out_cap - base : 0ull;
+                u.over = true;
+            }
+        }
+        u.emitted += tot;
+        return;
+    }
+    // residual: this lane's copies are tuples [start, start + wt) of the unit
+    const unsigned long long start = u.emitted + excl;
+    unsigned long long keep = 0;
+    if (wt) keep = start >= u.skip ? wt : (start + wt > u.skip ? start + wt - u.skip : 0ull);
+    const unsigned long long kincl = warp_inclusive_scan(keep, lane);
+    const unsigned long long ktot = __shfl_sync(AMJ_FULL_MASK, kincl, 31);
+    if (ktot) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&Q.st->out_cursor, ktot);
+        base = __shfl_sync(AMJ_FULL_MASK, base, 0);
+        acc.cnt += keep;
+        acc.chk += keep * h;
+        for (unsigned long long r = 0; r < keep; r++) {
+            const unsigned long long pos = base + (kincl - keep) + r;
+            if (pos < P.out_cap) {
+#pragma unroll
+                for (int a = 0; a < AMJ_MAX_ATTRS; a++)
+                    if (a < P.k) P.out[a][pos] = tv[a];
+            }
+        }
+    }
+    u.emitted += tot;
+}
+
+// Expand one 32-candidate chunk of the frontier at `depth`: compare, run the
+// inlined filters that follow the level, then emit (no frontier level left)
+// or build the frontier of the next level that is one.
+// WT: the plan has inlined filter levels, so entries carry weights; without
+// them every level is a frontier depth and every weight is 1.
+template <int MODE, bool WS, bool WT>
 __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q, uint16_t qid, char *wbase, int lane,
                                            unsigned lt, int &depth, ProbeAcc &acc, UnitOut &u) {
     Frontier F = frontier_at(wbase, P, depth);
@@ -301,7 +400,7 @@ __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q,
     const int n = (int)F.meta[2];
     __syncwarp();
     if (cursor >= total) {
-        depth--;
+        depth = WT ? P.prev_lv[depth] : depth - 1;
         return;
     }
     if (lane == 0) F.meta[0] = cursor + 32;
@@ -338,7 +437,9 @@ __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q,
         if (cm) {
             int32_t tv[AMJ_MAX_ATTRS];
             uint64_t h = AMJ_CHECKSUM_SEED;
+            uint32_t cw = 0;
             if (cached) {
+                cw = WT ? F.w[o] : 1u;
 #pragma unroll
                 for (int a = 0; a < AMJ_MAX_ATTRS; a++) {
                     if (a < P.k) {
@@ -347,109 +448,58 @@ __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q,
                         h = amj_hash_step(h, v);
                     }
                 }
-                acc.cnt++;
-                acc.chk += h;
-                acc.fib++;
+                acc.fib += cw;
             }
-            if (MODE == PM_WRITE) {
-                unsigned long long base = 0;
-                if (lane == 0) base = atomicAdd(&Q.st->out_cursor, (unsigned long long)__popc(cm));
-                base = __shfl_sync(AMJ_FULL_MASK, base, 0);
-                const unsigned long long pos = base + __popc(cm & lt);
-                if (cached && pos < P.out_cap) {
-#pragma unroll
-                    for (int a = 0; a < AMJ_MAX_ATTRS; a++)
-                        if (a < P.k) P.out[a][pos] = tv[a];
-                }
-            }
+            emit_weighted<MODE>(P, Q, lane, tv, h, cw, acc, u);
         }
     }
-    const unsigned mm = __ballot_sync(AMJ_FULL_MASK, matched);
+    // the tuple's value of attribute a: this level's bound columns, else the frontier
+    auto val = [&](int a) -> int32_t {
+        int32_t v = F.vals[a * 32 + o];
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < lv.ncols && ((lv.bind_mask >> c) & 1) && lv.attr[c] == a) v = cv[c];
+        return v;
+    };
+    const int nd = WT ? (int)P.next_lv[depth] : depth + 1;
+    uint32_t wt = matched ? (WT ? F.w[o] : 1u) : 0u;
+    if (WT)
+        for (int l = depth + 1; l < nd && wt; l++) wt *= filter_count(P.lv[l], val);
+    const bool live = wt != 0;
+    const unsigned mm = __ballot_sync(AMJ_FULL_MASK, live);
     const int idx = __popc(mm & lt);
 
-    if (depth == P.L - 1) {
-        // ---- emit
+    if (nd == P.L) {
+        // ---- no frontier level left: emit
+        if (!mm) return;
         int32_t tv[AMJ_MAX_ATTRS];
         uint64_t h = AMJ_CHECKSUM_SEED;
-        if (matched) {
+        if (live) {
 #pragma unroll
             for (int a = 0; a < AMJ_MAX_ATTRS; a++) {
                 if (a < P.k) {
-                    const int src = P.last_src[a];
-                    const int32_t v = src < 0 ? F.vals[a * 32 + o]
-                                              : (src == 0 ? cv[0] : src == 1 ? cv[1] : src == 2 ? cv[2] : cv[3]);
-                    tv[a] = v;
-                    h = amj_hash_step(h, v);
+                    tv[a] = val(a);
+                    h = amj_hash_step(h, tv[a]);
                 }
             }
         }
-        if (MODE == PM_COUNT) {
-            if (matched) {
-                acc.cnt++;
-                acc.chk += h;
-            }
-        } else if (mm) {
-            const int tot = __popc(mm);
-            if (MODE == PM_WRITE) {
-                unsigned long long base = 0;
-                if (lane == 0) base = atomicAdd(&Q.st->out_cursor, (unsigned long long)tot);
-                base = __shfl_sync(AMJ_FULL_MASK, base, 0);
-                const unsigned long long pos = base + idx;
-                if (matched) {
-                    acc.cnt++;
-                    acc.chk += h;
-                    if (pos < P.out_cap) {
-#pragma unroll
-                        for (int a = 0; a < AMJ_MAX_ATTRS; a++)
-                            if (a < P.k) P.out[a][pos] = tv[a];
-                    }
-                }
-                if (!u.over) {
-                    if (base + tot <= P.out_cap) u.written += tot;
-                    else {
-                        u.written += base < P.out_cap ? P.out_cap - base : 0ull;
-                        u.over = true;
-                    }
-                }
-                u.emitted += tot;
-            } else {
-                // residual: skip what the main pass wrote
-                const bool keep = matched && (u.emitted + idx >= u.skip);
-                const unsigned km = __ballot_sync(AMJ_FULL_MASK, keep);
-                if (km) {
-                    unsigned long long base = 0;
-                    if (lane == 0) base = atomicAdd(&Q.st->out_cursor, (unsigned long long)__popc(km));
-                    base = __shfl_sync(AMJ_FULL_MASK, base, 0);
-                    const unsigned long long pos = base + __popc(km & lt);
-                    if (keep) {
-                        acc.cnt++;
-                        acc.chk += h;
-                        if (pos < P.out_cap) {
-#pragma unroll
-                            for (int a = 0; a < AMJ_MAX_ATTRS; a++)
-                                if (a < P.k) P.out[a][pos] = tv[a];
-                        }
-                    }
-                }
-                u.emitted += tot;
-            }
-        }
+        emit_weighted<MODE>(P, Q, lane, tv, h, wt, acc, u);
         return;
     }
     if (!mm) return;
 
-    // ---- matches become the next frontier
-    Frontier C = frontier_at(wbase, P, depth + 1);
-    const LevelDesc &nl = P.lv[depth + 1];
+    // ---- live tuples become the frontier of level nd
+    Frontier C = frontier_at(wbase, P, nd);
+    const LevelDesc &nl = P.lv[nd];
     uint32_t s = 0, aux = 0, sz = 0;
     uint8_t m8 = 0;
-    if (matched) {
+    if (live) {
         for (int a = 0; a < P.k; a++) C.vals[a * 32 + idx] = F.vals[a * 32 + o];
 #pragma unroll
         for (int c = 0; c < 4; c++)
             if (c < lv.ncols && ((lv.bind_mask >> c) & 1)) C.vals[lv.attr[c] * 32 + idx] = cv[c];
         int fi = -1;
-        if (depth + 1 == P.fib_level) fi = fib_find(P, C.vals[nl.key_attr[0] * 32 + idx]);
+        if (nd == P.fib_level) fi = fib_find(P, C.vals[nl.key_attr[0] * 32 + idx]);
         if (fi >= 0) {
             s = (uint32_t)P.fib_off[fi];
             sz = (uint32_t)(P.fib_off[fi + 1] - P.fib_off[fi]);
@@ -457,14 +507,15 @@ __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q,
             m8 = FIB_FLAG;
         } else {
             sz = level_lookup(nl, [&](int a) { return C.vals[a * 32 + idx]; }, s, aux, m8);
-            sz = maybe_split<MODE, WS>(P, Q, nl, C.vals + idx, s, sz, depth + 1, qid);
+            sz = maybe_split<MODE, WS>(P, Q, nl, C.vals + idx, s, sz, nd, qid, wt);
         }
         C.s[idx] = s;
         C.aux[idx] = aux;
         C.m8[idx] = m8;
+        if (WT) C.w[idx] = wt;
     }
-    const unsigned long long ps = warp_inclusive_scan((unsigned long long)(matched ? sz : 0u), lane);
-    if (matched) C.psum[idx] = ps;
+    const unsigned long long ps = warp_inclusive_scan((unsigned long long)(live ? sz : 0u), lane);
+    if (live) C.psum[idx] = ps;
     const unsigned long long ctot = __shfl_sync(AMJ_FULL_MASK, ps, 31);
     if (lane == 0) {
         C.meta[0] = 0;
@@ -472,7 +523,7 @@ __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q,
         C.meta[2] = (unsigned long long)__popc(mm);
     }
     __syncwarp();
-    if (ctot) depth++;
+    if (ctot) depth = nd;
 }
 
 // level-0 candidate count of probe row i (relative to row_lo) of a plan
@@ -503,7 +554,7 @@ static __global__ void amhj_l0_sizes_kernel(const __grid_constant__ ProbePlan P,
         sizes[i] = l0_size_of(P, i);
 }
 
-template <int MODE, bool WS>
+template <int MODE, bool WS, bool WT>
 __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_constant__ ProbeLaunch L) {
     extern __shared__ __align__(16) char smem[];
     const ProbePlan &P = L.P;
@@ -612,7 +663,7 @@ __global__ __launch_bounds__(PROBE_THREADS) void amhj_probe_kernel(const __grid_
             }
             continue;
         }
-        probe_step<MODE, WS>(P, Q, 0, wbase, lane, lt, depth, acc, u);
+        probe_step<MODE, WS, WT>(P, Q, 0, wbase, lane, lt, depth, acc, u);
     }
 
     const unsigned long long cnt = warp_sum(acc.cnt), chk = warp_sum(acc.chk), fib = warp_sum(acc.fib);
@@ -654,7 +705,7 @@ __device__ __forceinline__ void batch_flush(const BatchLaunch &B, int q, ProbeAc
     acc.cnt = acc.chk = 0;
 }
 
-template <int THREADS>
+template <int THREADS, bool WT>
 __global__ __launch_bounds__(THREADS) void amhj_batch_kernel(const __grid_constant__ BatchLaunch B) {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31;
@@ -708,7 +759,7 @@ __global__ __launch_bounds__(THREADS) void amhj_batch_kernel(const __grid_consta
             }
             continue;
         }
-        probe_step<PM_COUNT, true>(P, B.Q, (uint16_t)cur, wbase, lane, lt, depth, acc, u);
+        probe_step<PM_COUNT, true, WT>(P, B.Q, (uint16_t)cur, wbase, lane, lt, depth, acc, u);
     }
     batch_flush(B, cur, acc, lane);
 }

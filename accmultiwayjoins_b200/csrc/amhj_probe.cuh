@@ -46,6 +46,16 @@ struct alignas(16) ProbePlan {
     int8_t probe_ncols, L, k, pad0;
     int8_t last_src[AMJ_MAX_ATTRS];     // output attr a: -1 from the tuple, c >= 0 from last level column c
     LevelDesc lv[AMJ_MAX_BUILD_TABLES];
+    // Inline filters: a level that binds nothing and is looked up by the
+    // pair of its columns (C(0,2) of the triangle, D/E/F of the 4-clique) is
+    // evaluated by the lane that created the partial tuple instead of
+    // becoming a frontier depth; its number of exact matches multiplies the
+    // tuple's weight.  next_lv[d] / prev_lv[d]: the next / previous level
+    // that is a frontier depth (L / -1 at the ends).
+    uint8_t inl[AMJ_MAX_BUILD_TABLES];
+    int8_t next_lv[AMJ_MAX_BUILD_TABLES];
+    int8_t prev_lv[AMJ_MAX_BUILD_TABLES];
+    uint8_t has_inl;                    // any level inlined: run the weighted kernels
     int32_t *out[AMJ_MAX_ATTRS];
     uint64_t out_cap;
     uint32_t task_chunk;
@@ -89,6 +99,7 @@ struct ProbeState {
 struct Task {
     int32_t vals[AMJ_MAX_ATTRS];
     uint32_t s, aux, sz;
+    uint32_t w;         // weight (multiplicity) of the entry
     uint8_t depth, m8;
     uint16_t qid;       // query of a batched launch (0 for a single query)
 };
@@ -102,11 +113,12 @@ struct Breakpoint {
 };
 
 // ---- shared-memory frontier of one depth ----
-// vals[k][32] int32 | s[32] u32 | aux[32] u32 | psum[32] u64 | m8[32] u8 | meta
+// vals[k][32] int32 | s[32] u32 | aux[32] u32 | w[32] u32 | psum[32] u64 | meta | m8[32] u8
 struct Frontier {
     int32_t *vals;
     uint32_t *s;
     uint32_t *aux;
+    uint32_t *w;                // weight: how many identical tuples the entry stands for
     unsigned long long *psum;
     uint8_t *m8;
     unsigned long long *meta;   // [0] cursor, [1] total, [2] n
@@ -120,6 +132,8 @@ __device__ __forceinline__ Frontier frontier_at(char *wbase, const ProbePlan &P,
     f.s = (uint32_t *)p;
     p += 128;
     f.aux = (uint32_t *)p;
+    p += 128;
+    f.w = (uint32_t *)p;
     p += 128;
     f.psum = (unsigned long long *)p;
     p += 256;
@@ -143,7 +157,30 @@ __device__ __forceinline__ int fib_find(const ProbePlan &P, int32_t key) {
     return -1;
 }
 
-__host__ __device__ inline uint32_t frontier_bytes(int k) { return 128u * k + 128 + 128 + 256 + 32 + 32; }
+__host__ __device__ inline uint32_t frontier_bytes(int k) { return 128u * k + 128 + 128 + 128 + 256 + 32 + 32; }
+
+// Fill inl / next_lv / prev_lv of a plan whose levels are set.  Level 0 is
+// never inlined (the probe rows create its entries).
+__host__ inline void plan_inline(ProbePlan &P) {
+    for (int l = 0; l < AMJ_MAX_BUILD_TABLES; l++) {
+        P.inl[l] = 0;
+        P.next_lv[l] = (int8_t)P.L;
+        P.prev_lv[l] = -1;
+    }
+    P.has_inl = 0;
+    for (int l = 1; l < P.L; l++) {
+        P.inl[l] = (P.lv[l].bind_mask == 0 && P.lv[l].key_mode == KEY_PAIR) ? 1 : 0;
+        P.has_inl |= P.inl[l];
+    }
+    for (int l = 0; l < P.L; l++) {
+        int n = l + 1;
+        while (n < P.L && P.inl[n]) n++;
+        P.next_lv[l] = (int8_t)n;
+        int p = l - 1;
+        while (p >= 0 && P.inl[p]) p--;
+        P.prev_lv[l] = (int8_t)p;
+    }
+}
 
 // Look up the candidate range of table `lv` for a tuple whose values are
 // given by get(attr).  Returns the range size.
