@@ -170,6 +170,54 @@ class Triangle:
         return cnt, chk, sec, cores, "port", "the full workload once (oracle triangle restatement)"
 
 
+class Clique4:
+    """The skewed 4-clique: AMHJ FOUR (ws=1, fib=1) over an R-MAT graph of
+    scale S (2^S vertices, 2^(S+4) edges, quadrant probabilities
+    0.6/0.15/0.15/0.1), cleaned as the triangle graph.  The full size is
+    scale 22 (64 Mi edges)."""
+
+    def __init__(self, args, rank):
+        from accmultiwayjoins_b200 import data
+        self.scale = args.scale
+        self.src, self.dst = data.rmat(self.scale, 1 << (self.scale + 4), 0.6, 0.15, 0.15, seed=22 + rank)
+        self.E = int(self.src.shape[0])
+        self.h2d = 8 * self.E
+
+    def describe(self, rank_note):
+        return (f"4-clique FOUR (ws=1 fib=1), R-MAT scale {self.scale}, {1 << (self.scale + 4)} edges "
+                f"(0.6,0.15,0.15,0.1), seed 22{rank_note}; AMHJ count+checksum incl. hash builds")
+
+    def device_relations(self, ctx, dev):
+        import torch
+        return [ctx.relation([torch.from_numpy(self.src).to(dev), torch.from_numpy(self.dst).to(dev)], [0, 1])]
+
+    def host_relations(self, ctx, pinned):
+        return [ctx.relation([pinned[0], pinned[1]], [0, 1])]
+
+    def host_columns(self):
+        return [self.src, self.dst]
+
+    def run(self, ctx, rels):
+        return ctx.amhj("FOUR", rels, ws=1, fib=1)
+
+    def algorithmic_bytes(self):
+        return None
+
+    def kernel_name(self):
+        return "amhj_probe_kernel (count pass)"
+
+    def cpu_baseline(self):
+        """The oracle's 4-clique restatement on a scale-14 graph of the same
+        generator (the full graph would take hours on the CPU)."""
+        from accmultiwayjoins_b200 import data
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        s, d = data.rmat(14, 1 << 18, 0.6, 0.15, 0.15, seed=22)
+        t0 = time.perf_counter()
+        cnt, chk = O.four_clique(s, d, nthreads=cores)
+        return cnt, chk, time.perf_counter() - t0, cores, "port", "R-MAT scale 14 of the same generator (oracle restatement)"
+
+
 class Chain:
     B = 1 << 19   # buckets = floorPow2(1e6)
 
@@ -300,7 +348,7 @@ def run_batch(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     wl = BatchMix(args, rank)
     stream = torch.cuda.current_stream(dev)
-    ctx = Context(local_rank)
+    ctx = Context(local_rank, spin_limit_ms=args.spin_limit_ms)
     lib = L.load()
     L.check(lib.amj_ctx_set_stream(ctx.handle, C.c_void_p(stream.cuda_stream)), "set_stream")
     host_cols = [c for q in wl.queries for cols, _ in q["rels"] for c in cols]
@@ -447,7 +495,7 @@ def run_serve(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     wl = ServeMix(args, rank)
-    ctx = Context(local_rank, ooc_slice_rows=args.ooc_slice)
+    ctx = Context(local_rank, ooc_slice_rows=args.ooc_slice, spin_limit_ms=args.spin_limit_ms)
     trels = [[ctx.relation(c, a) for c, a in rels] for _, _, rels in wl.templates]
     alone = []
     for (qt, _, _), r in zip(wl.templates, trels):
@@ -531,6 +579,8 @@ def Batch_default_opts(L):
 
 
 def make_workload(args, rank):
+    if args.workload == "four":
+        return Clique4(args, rank)
     return Chain(args, rank) if args.workload == "chain" else Triangle(args, rank)
 
 
@@ -553,6 +603,48 @@ def run_reference(args, rank, world):
     for the chain; the oracle's triangle restatement for the triangle) on all
     host threads.  Rank 0 only."""
     if rank != 0:
+        return
+    if args.workload == "serve":
+        # the reference serves nothing: its CPU join (MHJ-CPU for the stars,
+        # the oracle's restatement for the 4-cliques) runs the resident
+        # templates one request after another, drawn as the stream draws them
+        from oracle import oracle as O
+        wl = ServeMix(args, 0)
+        cores = os.cpu_count() or 1
+        rng = np.random.Generator(np.random.PCG64(5))
+        vals = []
+        for i in range(args.warmup + args.steps):
+            t_end = time.perf_counter() + 1.0
+            tuples, sec, n = 0, 0.0, 0
+            while time.perf_counter() < t_end:
+                qt, _, rels = wl.templates[int(rng.integers(0, len(wl.templates)))]
+                t0 = time.perf_counter()
+                if qt == "FOUR":
+                    cnt, _ = O.four_clique(*rels[0][0])
+                elif O.ref_available():
+                    cnt, _, _ = O.mhj_reference(rels, nthreads=cores)
+                else:
+                    cnt, _ = O.mhj(rels, nthreads=cores)
+                sec += time.perf_counter() - t0
+                tuples += cnt
+                n += 1
+            if i >= args.warmup:
+                vals.append((tuples, sec, n))
+        tuples = sum(v[0] for v in vals)
+        sec = sum(v[1] for v in vals)
+        value = tuples / sec
+        sample = (f"{sum(v[2] for v in vals)} requests of the resident templates, one after another, over "
+                  f"{args.steps} s (reference MHJ-CPU for the stars, the oracle's 4-clique restatement)")
+        line = {
+            "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec / len(vals), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+            "impl": "reference", "config": {"workload": wl.describe(""), "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
         return
     if args.workload == "batch":
         wl = BatchMix(args, 0)
@@ -605,7 +697,7 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     wl = make_workload(args, rank)
     stream = torch.cuda.current_stream(dev)
-    ctx = Context(local_rank)
+    ctx = Context(local_rank, spin_limit_ms=args.spin_limit_ms)
     lib = L.load()
     # run the library on torch's stream so torch's CUDA events see its kernels
     L.check(lib.amj_ctx_set_stream(ctx.handle, C.c_void_p(stream.cuda_stream)), "set_stream")
@@ -674,7 +766,7 @@ def run_ours(args, rank, world, local_rank):
     hbm, peak_kind = peaks()
     alg = wl.algorithmic_bytes()
     kms = sum(kern_ms) / len(kern_ms)
-    achieved = alg / (kms * 1e-3) / 1e9 if kms > 0 else None
+    achieved = alg / (kms * 1e-3) / 1e9 if (kms > 0 and alg) else None
     rank_note = "+rank" if world > 1 else ""
     line = {
         "metric": METRIC, "value": tot_count / (max_ms * 1e-3), "unit": "tuples/s", "n_gpus": world,
@@ -712,7 +804,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--algo", default="DFS", choices=["DFS", "BFS", "AMHJ"])
-    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain", "batch", "serve"])
+    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain", "four", "batch", "serve"])
+    ap.add_argument("--spin-limit-ms", type=int, default=5000, help="bound on every device-side wait")
     ap.add_argument("--rate", type=float, default=200.0, help="serve workload: requests per second")
     ap.add_argument("--lanes", type=int, default=3, help="serve workload: batches in flight")
     ap.add_argument("--max-batch", type=int, default=128, help="serve workload: requests per batch")
