@@ -656,7 +656,7 @@ int batch_collect(amj_batch *b, uint64_t *counts, uint64_t *checksums, amj_batch
     const unsigned long long *h = b->h_out;
     ProbeState hs;
     std::memcpy(&hs, h + 2 * nq + 1, sizeof(hs));
-    if (hs.q_tail > b->task_cap) return fail(AMJ_EOVERFLOW, "batch: work-sharing queue overflowed");
+    // a full work-sharing queue only means some ranges were not split: results stay exact
     for (uint32_t q = 0; q < nq; q++) {
         if (counts) counts[q] = h[q];
         if (checksums) checksums[q] = h[nq + q];

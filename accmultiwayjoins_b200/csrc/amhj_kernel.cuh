@@ -31,12 +31,21 @@ struct ProbeLaunch {
     uint64_t batch_count;    // number of batches
 };
 
+// Work-sharing queue.  Slots are handed out in order by q_tail to pushers and
+// by q_head as tickets to idle warps; ticket x takes the task of slot x.
+// `busy` counts the warps at work plus the tasks pushed but not yet finished:
+// a pusher adds the task's share before publishing it and the warp that takes
+// the task inherits it, so busy == 0 means no work is left anywhere.
 __device__ __forceinline__ bool ws_push(const ProbePlan &P, const WsQueue &Q, const int32_t *vals, uint32_t s,
                                         uint32_t sz, uint8_t depth, uint16_t qid, uint32_t w) {
     ProbeState *st = Q.st;
     if (ld_volatile_u32(&st->q_tail) >= P.task_cap) return false;
+    atomicAdd(&st->busy, 1u);
     const uint32_t slot = atomicAdd(&st->q_tail, 1u);
-    if (slot >= P.task_cap) return false;
+    if (slot >= P.task_cap) {
+        atomicSub(&st->busy, 1u);
+        return false;
+    }
     Task *t = &Q.tasks[slot];
     for (int a = 0; a < P.k; a++) t->vals[a] = vals[a * 32];
     t->s = s;
@@ -77,63 +86,38 @@ __device__ __forceinline__ uint32_t maybe_split(const ProbePlan &P, const WsQueu
     return chunk;
 }
 
-// Idle protocol of work sharing, run by lane 0.  Returns 1 with a task slot,
-// 0 when all work is done (or on error / timeout).
+// Idle protocol of work sharing, run by lane 0 of a warp whose own work is
+// done.  Returns 1 with a task slot, 0 when all work is done (or on error /
+// timeout).  One atomic takes a ticket; the warp then waits for that slot's
+// task or for the end of all work, backing off exponentially (64 ns .. 4 us)
+// so that waiting warps leave the issue slots to the working ones.
 static __device__ int ws_acquire(const WsQueue &Q, uint32_t cap, uint64_t spin_limit_ns, uint32_t &slot_out) {
     ProbeState *st = Q.st;
-    bool busy = true;
-    unsigned long long t0 = globaltimer_ns();
-    // an idle warp backs off exponentially (64 ns .. 8 us) so that its polling
-    // does not take issue slots from the warps that still work on the SM
+    __threadfence();
+    atomicSub(&st->busy, 1u);
+    const uint32_t x = atomicAdd(&st->q_head, 1u);
+    const unsigned long long t0 = globaltimer_ns();
     unsigned int backoff = 64;
     while (true) {
-        uint32_t h = ld_volatile_u32(&st->q_head);
-        uint32_t t = ld_volatile_u32(&st->q_tail);
-        if (t > cap) t = cap;
-        if (h < t) {
-            backoff = 64;
-            if (!busy) {
-                atomicAdd(&st->busy, 1u);
-                busy = true;
-                __threadfence();
-            }
-            if (atomicCAS(&st->q_head, h, h + 1) == h) {
-                // wait for the pusher to publish the task
-                unsigned long long w0 = globaltimer_ns();
-                while (ld_volatile_u32(&Q.ready[h]) == 0u) {
-                    if (globaltimer_ns() - w0 > spin_limit_ns) {
-                        report_error(Q.status, (unsigned)-AMJ_ETIMEOUT, SITE_WS_SLOT, h);
-                        return 0;
-                    }
-                    __nanosleep(64);
-                }
-                __threadfence();
-                atomicAdd(&st->tasks_popped, 1ull);
-                slot_out = h;
-                return 1;
-            }
-            continue;
-        }
-        if (busy) {
+        if (x < cap && ld_volatile_u32(&Q.ready[x]) != 0u) {
             __threadfence();
-            atomicSub(&st->busy, 1u);
-            busy = false;
-            t0 = globaltimer_ns();
+            atomicAdd(&st->tasks_popped, 1ull);
+            slot_out = x;
+            return 1;
         }
         if (ld_volatile_u32(&st->busy) == 0u) {
+            // nothing at work and nothing pending: the ticket's task never comes
             __threadfence();
-            h = ld_volatile_u32(&st->q_head);
-            t = ld_volatile_u32(&st->q_tail);
-            if (t > cap) t = cap;
-            if (h >= t) return 0;
+            if (x < cap && ld_volatile_u32(&Q.ready[x]) != 0u) continue;
+            return 0;
         }
         if (ld_volatile_u32(&Q.status->code) != 0u) return 0;
         if (globaltimer_ns() - t0 > spin_limit_ns) {
-            report_error(Q.status, (unsigned)-AMJ_ETIMEOUT, SITE_WS_IDLE, 0);
+            report_error(Q.status, (unsigned)-AMJ_ETIMEOUT, SITE_WS_IDLE, x);
             return 0;
         }
         __nanosleep(backoff);
-        if (backoff < 8192) backoff <<= 1;
+        if (backoff < 4096) backoff <<= 1;
     }
 }
 
@@ -326,10 +310,18 @@ __device__ __forceinline__ uint32_t filter_count(const LevelDesc &fl, Get &&get)
 // tuples (wt = 0: none).  Count mode adds them up; the write modes place them
 // at consecutive positions of the output (the residual pass skips the ones
 // the main pass wrote).
-template <int MODE>
+template <int MODE, bool WT = true>
 __device__ __forceinline__ void emit_weighted(const ProbePlan &P, const WsQueue &Q, int lane, const int32_t *tv,
                                               uint64_t h, uint32_t wt, ProbeAcc &acc, UnitOut &u) {
     if (MODE == PM_COUNT) {
+        if (!WT) {
+            // weights are 0 or 1
+            if (wt) {
+                acc.cnt++;
+                acc.chk += h;
+            }
+            return;
+        }
         acc.cnt += wt;
         acc.chk += (unsigned long long)wt * h;
         return;
@@ -453,13 +445,10 @@ __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q,
             emit_weighted<MODE>(P, Q, lane, tv, h, cw, acc, u);
         }
     }
-    // the tuple's value of attribute a: this level's bound columns, else the frontier
+    // the tuple's value of attribute a: this level's bound column, else the frontier
     auto val = [&](int a) -> int32_t {
-        int32_t v = F.vals[a * 32 + o];
-#pragma unroll
-        for (int c = 0; c < 4; c++)
-            if (c < lv.ncols && ((lv.bind_mask >> c) & 1) && lv.attr[c] == a) v = cv[c];
-        return v;
+        const int bc = P.bind_col[depth][a];
+        return bc < 0 ? F.vals[a * 32 + o] : (bc == 0 ? cv[0] : bc == 1 ? cv[1] : bc == 2 ? cv[2] : cv[3]);
     };
     const int nd = WT ? (int)P.next_lv[depth] : depth + 1;
     uint32_t wt = matched ? (WT ? F.w[o] : 1u) : 0u;
@@ -483,7 +472,7 @@ __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q,
                 }
             }
         }
-        emit_weighted<MODE>(P, Q, lane, tv, h, wt, acc, u);
+        emit_weighted<MODE, WT>(P, Q, lane, tv, h, wt, acc, u);
         return;
     }
     if (!mm) return;

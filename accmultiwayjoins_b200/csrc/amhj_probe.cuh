@@ -56,6 +56,9 @@ struct alignas(16) ProbePlan {
     int8_t next_lv[AMJ_MAX_BUILD_TABLES];
     int8_t prev_lv[AMJ_MAX_BUILD_TABLES];
     uint8_t has_inl;                    // any level inlined: run the weighted kernels
+    // bind_col[d][a]: the column of level d that binds attribute a, or -1
+    // (the value then comes from the frontier)
+    int8_t bind_col[AMJ_MAX_BUILD_TABLES][AMJ_MAX_ATTRS];
     int32_t *out[AMJ_MAX_ATTRS];
     uint64_t out_cap;
     uint32_t task_chunk;
@@ -167,6 +170,11 @@ __host__ inline void plan_inline(ProbePlan &P) {
         P.next_lv[l] = (int8_t)P.L;
         P.prev_lv[l] = -1;
     }
+    for (int l = 0; l < AMJ_MAX_BUILD_TABLES; l++)
+        for (int a = 0; a < AMJ_MAX_ATTRS; a++) P.bind_col[l][a] = -1;
+    for (int l = 0; l < P.L; l++)
+        for (int c = 0; c < P.lv[l].ncols; c++)
+            if ((P.lv[l].bind_mask >> c) & 1) P.bind_col[l][P.lv[l].attr[c]] = (int8_t)c;
     P.has_inl = 0;
     for (int l = 1; l < P.L; l++) {
         P.inl[l] = (P.lv[l].bind_mask == 0 && P.lv[l].key_mode == KEY_PAIR) ? 1 : 0;
