@@ -52,6 +52,7 @@ class amj_opts(C.Structure):
         ("mem_budget", C.c_uint64),
         ("lftj_heavy_degree", C.c_uint32),
         ("dro_headroom", C.c_float),
+        ("max_blocks", C.c_uint32),
     ]
 
 

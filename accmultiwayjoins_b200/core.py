@@ -305,8 +305,8 @@ class Context:
     """One CUDA device and stream (amj_ctx)."""
 
     def __init__(self, device: int = 0, layout: str = "bucket", load_factor: float = 0.5, task_chunk: int = 1024,
-                 spin_limit_ms: int = 5000, task_capacity: int = 1 << 20, ooc_slice_rows: int = 0,
-                 mem_budget: int = 0, lftj_heavy_degree: int = 0, dro_headroom: float = 0.0):
+                 spin_limit_ms: int = 5000, task_capacity: int = 1 << 22, ooc_slice_rows: int = 0,
+                 mem_budget: int = 0, lftj_heavy_degree: int = 0, dro_headroom: float = 0.0, max_blocks: int = 0):
         lib = L.load()
         o = L.amj_opts()
         o.block_size = 256
@@ -319,6 +319,7 @@ class Context:
         o.mem_budget = mem_budget
         o.lftj_heavy_degree = lftj_heavy_degree
         o.dro_headroom = dro_headroom
+        o.max_blocks = max_blocks
         h = C.c_void_p()
         self.handle = None
         self._relations = weakref.WeakSet()

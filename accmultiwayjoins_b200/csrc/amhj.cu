@@ -153,6 +153,7 @@ static int launch_probe_t(amj_ctx *ctx, const ProbeLaunch &PL, size_t smem) {
     AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PROBE_THREADS, smem));
     if (per_sm < 1) return fail(AMJ_EUNSUPPORTED, "AMHJ: probe frontier does not fit in shared memory");
     uint64_t grid = (uint64_t)ctx->num_sms * per_sm;
+    if (ctx->opts.max_blocks && grid > ctx->opts.max_blocks) grid = ctx->opts.max_blocks;
     const uint64_t need = (PL.batch_count + PROBE_WARPS - 1) / PROBE_WARPS;
     if (!WS && MODE != PM_RESIDUAL && need < grid) grid = need ? need : 1;
     if (MODE == PM_RESIDUAL) {

@@ -252,12 +252,17 @@ extern "C" int amj_server_create(amj_ctx *ctx, const amj_serve_opts *opts, amj_s
     uint64_t ooc_reserve = 0;
     if (s->opts.ooc_lane) ooc_reserve = s->opts.ooc_mem ? s->opts.ooc_mem : (uint64_t)(fr / 8);
     s->budget = s->opts.mem_budget ? s->opts.mem_budget : (uint64_t)(fr * 0.8) - ooc_reserve;
-    // each lane's batches use a share of the resident probe blocks
-    if (s->bopts.grid_blocks == 0 && s->opts.lanes > 1) {
-        int sms = 0;
-        AMJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-        s->bopts.grid_blocks = std::max(1, sms * 2 / s->opts.lanes);
-    }
+    // The persistent kernels of the lanes and of the ooc lane run at the same
+    // time; their idle warps wait for their own unstarted blocks, so all of
+    // them must be resident together.  Each gets an equal share of four probe
+    // blocks per SM: with the default 256-thread blocks (at most 64 registers
+    // a thread, frontiers of at most 61 KB for a batch of 8-attribute queries
+    // and 29 KB for an ooc chain) one block of each fits an SM together.
+    int sms = 0;
+    AMJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    const int kernels = s->opts.lanes + (s->opts.ooc_lane ? 1 : 0);
+    const int share = std::max(1, 4 / kernels) * sms;
+    if (s->bopts.grid_blocks == 0 && kernels > 1) s->bopts.grid_blocks = share;
     amj_opts lo = ctx->opts;
     for (int i = 0; i < s->opts.lanes; i++) {
         Lane ln;
@@ -276,6 +281,7 @@ extern "C" int amj_server_create(amj_ctx *ctx, const amj_serve_opts *opts, amj_s
     if (s->opts.ooc_lane) {
         amj_opts oo = ctx->opts;
         oo.mem_budget = ooc_reserve;
+        if (kernels > 1 && oo.max_blocks == 0) oo.max_blocks = (uint32_t)share;
         if (s->opts.ooc_slice_rows) oo.ooc_slice_rows = s->opts.ooc_slice_rows;
         int rc = amj_ctx_create(ctx->device, &oo, &s->ooc_ctx);
         if (rc != AMJ_OK) {

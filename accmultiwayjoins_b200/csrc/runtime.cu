@@ -135,7 +135,7 @@ extern "C" int amj_ctx_create(int device, const amj_opts *opts, amj_ctx **out) {
     if (c->opts.load_factor <= 0.f || c->opts.load_factor >= 1.f) c->opts.load_factor = 0.5f;
     if (c->opts.task_chunk <= 0) c->opts.task_chunk = 1024;
     if (c->opts.spin_limit_ms == 0) c->opts.spin_limit_ms = 5000;
-    if (c->opts.task_capacity == 0) c->opts.task_capacity = 1ull << 20;
+    if (c->opts.task_capacity == 0) c->opts.task_capacity = 1ull << 22;
     cudaDeviceProp prop;
     AMJ_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
     c->num_sms = prop.multiProcessorCount;

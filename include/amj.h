@@ -87,12 +87,16 @@ typedef struct amj_opts {
     float    load_factor;      /* open addressing load factor (0: 0.5)            */
     int      task_chunk;       /* work-sharing task size in candidates (0: 1024)  */
     uint32_t spin_limit_ms;    /* bound on every device-side wait (0: 5000)       */
-    uint64_t task_capacity;    /* work-sharing queue capacity in tasks (0: 1<<20) */
+    uint64_t task_capacity;    /* work-sharing queue capacity in tasks (0: 1<<22) */
     uint64_t ooc_slice_rows;   /* ooc probe slice rows (0: derived from budget)   */
     uint64_t mem_budget;       /* device bytes the ooc planner may use (0: free/2) */
     uint32_t lftj_heavy_degree; /* ALFTJ ws=1: children count from which a vertex is
                                    joined by the block-wide bitmap kernel (0: 32)  */
     float    dro_headroom;     /* DRO output estimate multiplier (0: 1.05)        */
+    uint32_t max_blocks;       /* cap on the blocks of the persistent probe kernels
+                                  (0: every block that fits on the device); kernels
+                                  of several contexts running at once must fit
+                                  together, since idle warps wait for the others  */
 } amj_opts;
 
 typedef struct amj_result {
