@@ -362,10 +362,13 @@ class Context:
         return self._result(res, materialize)
 
     def lftj(self, relations: Sequence[Relation], algo="DFS", ooc: int = 0, ws: int = 1,
-             materialize: bool = False) -> Result:
+             materialize: bool = False, clique4: bool = False) -> Result:
+        """clique4: one edge relation joined as the 4-clique (FOUR pattern) instead of the triangle."""
         lib = L.load()
         arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
         flags = (L.AMJ_F_MATERIALIZE | L.AMJ_F_HOST_RESULT) if materialize else 0
+        if clique4:
+            flags |= L.AMJ_F_CLIQUE4
         res = L.amj_result()
         L.check(lib.amj_lftj_execute(self.handle, arr, len(relations), _ALGO[algo], int(ooc), int(ws), flags,
                                      C.byref(res)), "lftj_execute")

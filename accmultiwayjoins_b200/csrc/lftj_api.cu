@@ -15,6 +15,8 @@
 #include <vector>
 
 namespace amj {
+int lftj_clique4(amj_ctx *ctx, const Trie2 &T, int32_t *const *out, uint64_t out_cap, uint64_t *count,
+                 uint64_t *checksum, uint64_t *written, double *kernel_ms);
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
                   uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms);
@@ -29,6 +31,57 @@ static int build_rel_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t) {
     return build_trie2(ctx, r->d_cols[swap ? 1 : 0], r->d_cols[swap ? 0 : 1], r->n, t);
 }
 
+// The 4-clique over one edge relation (AMJ_F_CLIQUE4): a count pass, then
+// with AMJ_F_MATERIALIZE a write pass into exactly allocated columns.
+static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int flags,
+                                amj_result *out) {
+    if (nrels != 1) return fail(AMJ_EUNSUPPORTED, "LFTJ 4-clique: one edge relation");
+    if (algo != AMJ_LFTJ_DFS) return fail(AMJ_EUNSUPPORTED, "LFTJ 4-clique: DFS only");
+    if (ooc) return fail(AMJ_EUNSUPPORTED, "LFTJ 4-clique: no out-of-core form");
+    result_init(out, 4);
+    cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
+    AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
+    Trie2 t;
+    AMJ_TRY(build_rel_trie(ctx, rels[0], &t));
+    AMJ_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
+    uint64_t c = 0, h = 0;
+    AMJ_TRY(lftj_clique4(ctx, t, nullptr, 0, &c, &h, nullptr, &out->kernel_ms[0]));
+    out->count = c;
+    out->checksum = h;
+    const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
+    if (materialize) {
+        int32_t *cols[4] = {nullptr, nullptr, nullptr, nullptr};
+        int rc = AMJ_OK;
+        for (int a = 0; a < 4 && rc == AMJ_OK; a++) rc = dev_alloc(ctx, (void **)&cols[a], (c ? c : 1) * 4);
+        uint64_t c2 = 0, h2 = 0, w = 0;
+        if (rc == AMJ_OK) rc = lftj_clique4(ctx, t, cols, c, &c2, &h2, &w, &out->kernel_ms[1]);
+        if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
+            rc = fail(AMJ_ECUDA, "LFTJ 4-clique: write pass disagrees with count pass");
+        if (rc != AMJ_OK) {
+            for (int a = 0; a < 4; a++) dev_free(ctx, cols[a]);
+            return rc;
+        }
+        auto *o = new ResultOwner();
+        o->ctx = ctx;
+        out->priv = o;
+        out->rows = c;
+        for (int a = 0; a < 4; a++) out->cols[a] = cols[a];
+    }
+    AMJ_CUDA_TRY(cudaEventRecord(e2, ctx->stream));
+    AMJ_CUDA_TRY(cudaEventSynchronize(e2));
+    out->build_ms = event_ms(e0, e1);
+    out->probe_ms = event_ms(e1, e2);
+    out->total_ms = event_ms(e0, e2);
+    if (materialize) {
+        const int rc = finish_result_columns(ctx, out, flags);
+        if (rc != AMJ_OK) {
+            amj_result_release(out);
+            return rc;
+        }
+    }
+    return AMJ_OK;
+}
+
 extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int ws, int flags,
                                 amj_result *out) {
     if (!ctx || !out || !rels || nrels <= 0) return fail(AMJ_EINVAL, "lftj_execute: bad arguments");
@@ -38,6 +91,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         if (!rels[i]) return fail(AMJ_EINVAL, "lftj_execute: null relation");
     if (nrels > 3) return fail(AMJ_EUNSUPPORTED, "lftj_execute: at most 3 relations (MAX_NUM_TABLES)");
     AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (flags & AMJ_F_CLIQUE4) return lftj_clique4_execute(ctx, rels, nrels, algo, ooc, flags, out);
     result_init(out, 3);
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));

@@ -70,6 +70,8 @@ extern "C" {
 #define AMJ_F_MATERIALIZE  0x1  /* write the result tuples (else count+checksum) */
 #define AMJ_F_HOST_RESULT  0x2  /* copy materialised columns to host memory      */
 #define AMJ_F_NO_REORDER   0x4  /* keep fully-bound tables at their query position */
+#define AMJ_F_CLIQUE4      0x8  /* amj_lftj_execute, one relation: the 4-clique (the
+                                   FOUR pattern) instead of the triangle, DFS only */
 
 /* ---- relation residency ---- */
 #define AMJ_MEM_DEVICE 0   /* columns are device pointers, borrowed            */

@@ -342,6 +342,38 @@ def test_lftj_triangle_small(algo, ws, heavy):
             assert (got.count, got.checksum) == O.triangle(s, d)
 
 
+@pytest.mark.parametrize("scale,ne,seed", [(8, 1500, 1), (12, 60000, 2), (14, 1 << 18, 22)])
+def test_lftj_clique4_matches_oracle_and_amhj_four(ctx, scale, ne, seed):
+    """The ALFTJ 4-clique equals the oracle and AMHJ FOUR on the same relation
+    (skewed R-MAT, 0.6/0.15/0.15/0.1); the largest case has hub edges that
+    take the warp-cooperative path."""
+    s, d = data.rmat(scale, ne, 0.6, 0.15, 0.15, seed)
+    e = ctx.relation([s, d], [0, 1])
+    want = O.four_clique(s, d)
+    got = ctx.lftj([e], algo="DFS", clique4=True)
+    assert (got.count, got.checksum) == want
+    four = ctx.amhj("FOUR", [e], ws=1)
+    assert (four.count, four.checksum) == want
+
+
+def test_lftj_clique4_materialized_and_rejections(ctx):
+    s, d = data.rmat(11, 20000, 0.6, 0.15, 0.15, 7)
+    e = ctx.relation([s, d], [0, 1])
+    got = ctx.lftj([e], algo="DFS", clique4=True, materialize=True)
+    cnt, chk = O.four_clique(s, d)
+    assert got.count == cnt and len(got.columns) == 4
+    assert data.checksum(got.columns) == chk
+    m = ctx.amhj("FOUR", [e], materialize=True)
+    assert np.array_equal(sorted_rows(got.columns), sorted_rows(m.columns))
+    with pytest.raises(AmjError):
+        ctx.lftj([e], algo="BFS", clique4=True)
+    with pytest.raises(AmjError):
+        ctx.lftj([e], algo="DFS", clique4=True, ooc=1)
+    empty = ctx.relation([np.zeros(0, np.int32), np.zeros(0, np.int32)], [0, 1])
+    r = ctx.lftj([empty], clique4=True)
+    assert (r.count, r.checksum) == (0, 0)
+
+
 @pytest.mark.parametrize("algo", ["DFS", "BFS"])
 def test_lftj_materialized_tuples(ctx, algo):
     s, d = data.rmat(11, 20000, 0.57, 0.19, 0.19, 5)
