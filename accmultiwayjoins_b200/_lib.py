@@ -37,6 +37,7 @@ AMJ_QUERY_NORMAL, AMJ_QUERY_TRI, AMJ_QUERY_FOUR = 0, 1, 2
 AMJ_LFTJ_BFS, AMJ_LFTJ_DFS = 0, 1
 AMJ_LAYOUT_BUCKET, AMJ_LAYOUT_OPEN_ADDR, AMJ_LAYOUT_CUCKOO = 0, 1, 2
 AMJ_F_MATERIALIZE, AMJ_F_HOST_RESULT, AMJ_F_NO_REORDER, AMJ_F_CLIQUE4 = 0x1, 0x2, 0x4, 0x8
+AMJ_F_KEEP_ORDER, AMJ_F_DEGREE_ORDER = 0x10, 0x20
 AMJ_MEM_DEVICE, AMJ_MEM_HOST, AMJ_MEM_HOST_STREAMED = 0, 1, 2
 
 

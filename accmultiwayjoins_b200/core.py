@@ -362,13 +362,19 @@ class Context:
         return self._result(res, materialize)
 
     def lftj(self, relations: Sequence[Relation], algo="DFS", ooc: int = 0, ws: int = 1,
-             materialize: bool = False, clique4: bool = False) -> Result:
-        """clique4: one edge relation joined as the 4-clique (FOUR pattern) instead of the triangle."""
+             materialize: bool = False, clique4: bool = False, degree_order=None) -> Result:
+        """clique4: one edge relation joined as the 4-clique (FOUR pattern) instead of the triangle.
+        degree_order: None for the operator's choice, True / False to force joining (or not) the
+        degree-ordered copy of an oriented self-joined relation (same results either way)."""
         lib = L.load()
         arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
         flags = (L.AMJ_F_MATERIALIZE | L.AMJ_F_HOST_RESULT) if materialize else 0
         if clique4:
             flags |= L.AMJ_F_CLIQUE4
+        if degree_order is True:
+            flags |= L.AMJ_F_DEGREE_ORDER
+        elif degree_order is False:
+            flags |= L.AMJ_F_KEEP_ORDER
         res = L.amj_result()
         L.check(lib.amj_lftj_execute(self.handle, arr, len(relations), _ALGO[algo], int(ooc), int(ws), flags,
                                      C.byref(res)), "lftj_execute")

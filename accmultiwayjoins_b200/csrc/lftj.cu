@@ -51,7 +51,34 @@ struct TriArgs {
     unsigned long long *cursor0;  // level-0 claim cursor of the bitmap kernel
     uint32_t heavy_deg;           // 0: no bitmap kernel
     uint32_t bitmap_bits;
+    int sorted_out;               // the tries hold a degree-ordered copy of an oriented relation:
+                                  // every triangle is listed with its values in increasing order
 };
+
+// A triangle found as (a, b, c) in the tuple the query lists: attribute order,
+// or increasing order for a degree-ordered copy of an oriented relation
+// (whose triangles, in attribute order, are exactly the increasing triples).
+__device__ __forceinline__ void tri_order(const TriArgs &A, int32_t &a, int32_t &b, int32_t &c) {
+    if (!A.sorted_out) return;
+    int32_t t;
+    if (a > b) { t = a; a = b; b = t; }
+    if (b > c) { t = b; b = c; c = t; }
+    if (a > b) { t = a; a = b; b = t; }
+}
+
+// checksum term of the triangle (a, b, c); hab is the hash of (a, b)
+__device__ __forceinline__ uint64_t tri_chk(const TriArgs &A, uint64_t hab, int32_t a, int32_t b, int32_t c) {
+    if (!A.sorted_out) return amj_hash_step(hab, c);
+    tri_order(A, a, b, c);
+    return amj_hash_step(amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a), b), c);
+}
+
+__device__ __forceinline__ void tri_store(const TriArgs &A, unsigned long long p, int32_t a, int32_t b, int32_t c) {
+    tri_order(A, a, b, c);
+    A.out[0][p] = a;
+    A.out[1][p] = b;
+    A.out[2][p] = c;
+}
 
 // A level-0 value a of R is "heavy" when it has at least heavy_deg children in
 // R and its children in T span at most bitmap_bits values: its edges are
@@ -185,7 +212,7 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
                     if (!WRITE) {
                         if (hit) {
                             cnt++;
-                            chk += amj_hash_step(hb, c);
+                            chk += tri_chk(A, hb, a, bval[li], c);
                         }
                     } else {
                         const unsigned m = __ballot_sync(AMJ_FULL_MASK, hit);
@@ -195,11 +222,9 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
                             base = __shfl_sync(AMJ_FULL_MASK, base, 0);
                             if (hit) {
                                 cnt++;
-                                chk += amj_hash_step(hb, c);
+                                chk += tri_chk(A, hb, a, bval[li], c);
                                 const unsigned long long p = base + __popc(m & lanemask_lt());
-                                if (p < A.out_cap) {
-                                    A.out[0][p] = a; A.out[1][p] = bval[li]; A.out[2][p] = c;
-                                }
+                                if (p < A.out_cap) tri_store(A, p, a, bval[li], c);
                             }
                         }
                     }
@@ -275,7 +300,7 @@ __global__ __launch_bounds__(256) void lftj_tri_dfs_kernel(const __grid_constant
                     const int32_t x = A.S.data1[p], y = A.T.data1[q];
                     if (x == y) {
                         cnt++;
-                        chk += amj_hash_step(hab, x);
+                        chk += tri_chk(A, hab, a, b, x);
                         p++;
                         q++;
                     } else if (x < y) p++;
@@ -305,12 +330,10 @@ __global__ __launch_bounds__(256) void lftj_tri_dfs_kernel(const __grid_constant
                 while (p < eb && q < ea) {
                     const int32_t x = A.S.data1[p], y = A.T.data1[q];
                     if (x == y) {
-                        if (pos < A.out_cap) {
-                            A.out[0][pos] = a; A.out[1][pos] = b; A.out[2][pos] = x;
-                        }
+                        if (pos < A.out_cap) tri_store(A, pos, a, b, x);
                         pos++;
                         cnt++;
-                        chk += amj_hash_step(hab, x);
+                        chk += tri_chk(A, hab, a, b, x);
                         p++; q++;
                     } else if (x < y) p++;
                     else q++;
@@ -330,17 +353,15 @@ __global__ __launch_bounds__(256) void lftj_tri_dfs_kernel(const __grid_constant
             if (!WRITE) {
                 warp_intersect(A.S.data1 + wsb, web - wsb, A.T.data1 + wta, wea - wta, lane, [&](int32_t c) {
                     cnt++;
-                    chk += amj_hash_step(whab, c);
+                    chk += tri_chk(A, whab, wa, wb, c);
                 });
             } else {
                 // one reservation per round: count this round's matches with a ballot inside emit
                 warp_intersect(A.S.data1 + wsb, web - wsb, A.T.data1 + wta, wea - wta, lane, [&](int32_t c) {
                     cnt++;
-                    chk += amj_hash_step(whab, c);
+                    chk += tri_chk(A, whab, wa, wb, c);
                     const unsigned long long p = atomicAdd(A.out_cursor, 1ull);
-                    if (p < A.out_cap) {
-                        A.out[0][p] = wa; A.out[1][p] = wb; A.out[2][p] = c;
-                    }
+                    if (p < A.out_cap) tri_store(A, p, wa, wb, c);
                 });
             }
         }
@@ -434,12 +455,10 @@ __global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const 
             const bool found = lo < (s_short ? ea : eb) && hay[lo] == c;
             if (found) {
                 cnt++;
-                chk += amj_hash_step(amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a), b), c);
+                chk += tri_chk(A, amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a), b), a, b, c);
                 if (WRITE) {
                     const unsigned long long p = atomicAdd(A.out_cursor, 1ull);
-                    if (p < A.out_cap) {
-                        A.out[0][p] = a; A.out[1][p] = b; A.out[2][p] = c;
-                    }
+                    if (p < A.out_cap) tri_store(A, p, a, b, c);
                 }
             }
         }
@@ -465,9 +484,10 @@ struct LftjCounters {
 // written too (out_cap rows available).
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
-                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms) {
+                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out) {
     bool timed[2] = {false, false};
     TriArgs A{};
+    A.sorted_out = sorted_out;
     if (r_hi > R.len1) r_hi = R.len1;
     if (r_lo > r_hi) r_lo = r_hi;
     A.r_src = R.src1.p + r_lo;

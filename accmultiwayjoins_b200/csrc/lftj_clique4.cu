@@ -32,6 +32,7 @@ struct C4Args {
     uint64_t out_cap;
     int32_t *scratch;           // per warp: scratch_cap values
     uint64_t scratch_cap;
+    int sorted_out;             // degree-ordered copy of an oriented relation: list tuples increasing
 };
 
 __device__ __forceinline__ uint64_t umin(uint64_t x, uint64_t y) { return x < y ? x : y; }
@@ -45,7 +46,18 @@ template <bool WRITE>
 __device__ __forceinline__ void c4_emit(const C4Args &A, int32_t a, int32_t b, int32_t c, int32_t d, uint64_t habc,
                                         unsigned long long &cnt, unsigned long long &chk) {
     cnt++;
-    chk += amj_hash_step(habc, d);
+    if (A.sorted_out) {
+        // sorting network of four
+        int32_t t;
+        if (a > b) { t = a; a = b; b = t; }
+        if (c > d) { t = c; c = d; d = t; }
+        if (a > c) { t = a; a = c; c = t; }
+        if (b > d) { t = b; b = d; d = t; }
+        if (b > c) { t = b; b = c; c = t; }
+        chk += amj_hash_step(amj_hash_step(amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a), b), c), d);
+    } else {
+        chk += amj_hash_step(habc, d);
+    }
     if (WRITE) {
         const unsigned long long p = atomicAdd(A.out_cursor, 1ull);
         if (p < A.out_cap) {
@@ -220,7 +232,7 @@ struct C4Counters {
 // One 4-clique pass over the trie T of the edge relation: count and checksum,
 // and the tuples when `out` is given (out_cap rows).
 int lftj_clique4(amj_ctx *ctx, const Trie2 &T, int32_t *const *out, uint64_t out_cap, uint64_t *count,
-                 uint64_t *checksum, uint64_t *written, double *kernel_ms) {
+                 uint64_t *checksum, uint64_t *written, double *kernel_ms, int sorted_out) {
     DBuf<C4Counters> ctr;
     AMJ_TRY(ctr.alloc(ctx, 1));
     AMJ_CUDA_TRY(cudaMemsetAsync(ctr.p, 0, sizeof(C4Counters), ctx->stream));
@@ -263,6 +275,7 @@ int lftj_clique4(amj_ctx *ctx, const Trie2 &T, int32_t *const *out, uint64_t out
     }
     A.scratch = scratch.p;
     A.scratch_cap = cap;
+    A.sorted_out = sorted_out;
     AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
     note_launch(ctx);
     kern<<<(unsigned)blocks, 256, 0, ctx->stream>>>(A);

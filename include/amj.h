@@ -72,6 +72,11 @@ extern "C" {
 #define AMJ_F_NO_REORDER   0x4  /* keep fully-bound tables at their query position */
 #define AMJ_F_CLIQUE4      0x8  /* amj_lftj_execute, one relation: the 4-clique (the
                                    FOUR pattern) instead of the triangle, DFS only */
+#define AMJ_F_KEEP_ORDER   0x10 /* amj_lftj_execute, one relation: join the relation as
+                                   given, never its degree-ordered copy             */
+#define AMJ_F_DEGREE_ORDER 0x20 /* amj_lftj_execute, one oriented relation: join its
+                                   degree-ordered copy (the default for BFS and the
+                                   4-clique; DFS triangles keep the relation's order) */
 
 /* ---- relation residency ---- */
 #define AMJ_MEM_DEVICE 0   /* columns are device pointers, borrowed            */

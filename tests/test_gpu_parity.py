@@ -356,6 +356,28 @@ def test_lftj_clique4_matches_oracle_and_amhj_four(ctx, scale, ne, seed):
     assert (four.count, four.checksum) == want
 
 
+@pytest.mark.parametrize("algo", ["DFS", "BFS", "clique4"])
+def test_lftj_degree_order_gives_the_same_bag(ctx, algo):
+    """An oriented relation may be joined through its degree-ordered copy (the
+    default for BFS and the 4-clique): same count, checksum and tuples.  A
+    relation that is not oriented is always joined as given."""
+    s, d = data.rmat(13, 100000, 0.57, 0.19, 0.19, 9)
+    e = ctx.relation([s, d], [0, 1])
+    c4 = algo == "clique4"
+    run = dict(algo="DFS" if c4 else algo, clique4=c4)
+    want = O.four_clique(s, d) if c4 else O.triangle(s, d)
+    for dego in (None, True, False):
+        r = ctx.lftj([e], degree_order=dego, **run)
+        assert (r.count, r.checksum) == want, dego
+    m1 = ctx.lftj([e], degree_order=True, materialize=True, **run)
+    m0 = ctx.lftj([e], degree_order=False, materialize=True, **run)
+    assert np.array_equal(sorted_rows(m1.columns), sorted_rows(m0.columns))
+    if not c4:
+        rev = ctx.relation([d, s], [0, 1])   # every edge v > u: not oriented
+        r = ctx.lftj([rev], degree_order=True, **run)
+        assert (r.count, r.checksum) == O.triangle(d, s)
+
+
 def test_lftj_clique4_materialized_and_rejections(ctx):
     s, d = data.rmat(11, 20000, 0.6, 0.15, 0.15, 7)
     e = ctx.relation([s, d], [0, 1])
