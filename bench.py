@@ -171,21 +171,25 @@ class Triangle:
 
 
 class Clique4:
-    """The skewed 4-clique: AMHJ FOUR (ws=1, fib=1) over an R-MAT graph of
-    scale S (2^S vertices, 2^(S+4) edges, quadrant probabilities
-    0.6/0.15/0.15/0.1), cleaned as the triangle graph.  The full size is
-    scale 22 (64 Mi edges)."""
+    """The skewed 4-clique over an R-MAT graph of scale S (2^S vertices,
+    2^(S+4) edges, quadrant probabilities 0.6/0.15/0.15/0.1), cleaned as the
+    triangle graph; the full size is scale 22 (64 Mi edges).  --algo AMHJ
+    runs the configured operator, AMHJ FOUR with ws=1 fib=1 (about 6 minutes
+    a query at full size); the default runs the ALFTJ 4-clique, which gives
+    the same count and checksum."""
 
     def __init__(self, args, rank):
         from accmultiwayjoins_b200 import data
         self.scale = args.scale
+        self.algo = args.algo
         self.src, self.dst = data.rmat(self.scale, 1 << (self.scale + 4), 0.6, 0.15, 0.15, seed=22 + rank)
         self.E = int(self.src.shape[0])
         self.h2d = 8 * self.E
 
     def describe(self, rank_note):
-        return (f"4-clique FOUR (ws=1 fib=1), R-MAT scale {self.scale}, {1 << (self.scale + 4)} edges "
-                f"(0.6,0.15,0.15,0.1), seed 22{rank_note}; AMHJ count+checksum incl. hash builds")
+        op = "AMHJ FOUR (ws=1 fib=1), hash builds" if self.algo == "AMHJ" else "ALFTJ 4-clique (DFS), trie build"
+        return (f"4-clique, R-MAT scale {self.scale}, {1 << (self.scale + 4)} edges "
+                f"(0.6,0.15,0.15,0.1), seed 22{rank_note}; {op} included, count+checksum")
 
     def device_relations(self, ctx, dev):
         import torch
@@ -198,13 +202,15 @@ class Clique4:
         return [self.src, self.dst]
 
     def run(self, ctx, rels):
-        return ctx.amhj("FOUR", rels, ws=1, fib=1)
+        if self.algo == "AMHJ":
+            return ctx.amhj("FOUR", rels, ws=1, fib=1)
+        return ctx.lftj(rels, algo="DFS", clique4=True)
 
     def algorithmic_bytes(self):
         return None
 
     def kernel_name(self):
-        return "amhj_probe_kernel (count pass)"
+        return "amhj_probe_kernel (count pass)" if self.algo == "AMHJ" else "lftj_clique4_kernel"
 
     def cpu_baseline(self):
         """The oracle's 4-clique restatement on a scale-14 graph of the same
