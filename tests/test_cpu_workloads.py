@@ -1,0 +1,54 @@
+"""Host-side pieces of the batched and served workloads, without a GPU: the
+seeded query mix (shapes, sizes, domains, skew, output bound), and the
+bench's percentile helper."""
+import numpy as np
+
+from accmultiwayjoins_b200 import data
+from oracle import oracle as O
+
+
+def test_query_mix_is_seeded_and_within_bounds():
+    a = list(data.query_mix(24, seed=3, min_rows=1000, max_rows=20000, out_cap=1 << 22))
+    b = list(data.query_mix(24, seed=3, min_rows=1000, max_rows=20000, out_cap=1 << 22))
+    assert [q["shape"] for q in a] == [q["shape"] for q in b]
+    for qa, qb in zip(a, b):
+        for (ca, aa), (cb, ab) in zip(qa["rels"], qb["rels"]):
+            assert aa == ab and all(np.array_equal(x, y) for x, y in zip(ca, cb))
+    shapes = {q["shape"] for q in a}
+    assert shapes <= {"chain", "star", "triangle"} and len(shapes) == 3
+    for q in a:
+        if q["shape"] == "triangle":
+            (s, d), at = q["rels"][0]
+            assert at == [0, 1] and q["qt"] == "TRI" and np.all(s < d)
+            continue
+        assert 2 <= len(q["rels"]) <= 5
+        for cols, at in q["rels"]:
+            assert 1000 // 2 <= len(cols[0]) <= 20000 and all(c.dtype == np.int32 for c in cols)
+        if q["theta"]:
+            assert 0.5 <= q["theta"] <= 1.5
+        if q["shape"] == "star":
+            fact, dims = q["rels"][0], q["rels"][1:]
+            for j, (cols, at) in enumerate(dims):
+                assert np.array_equal(np.sort(cols[0]), np.arange(len(cols[0])))   # unique dimension keys
+                assert fact[0][j].max() < len(cols[0])
+            assert O.mhj(q["rels"])[0] == len(fact[0][0])                         # every foreign key matches
+
+
+def test_query_mix_chains_keep_skew_on_the_build_side():
+    qs = [q for q in data.query_mix(40, seed=11, min_rows=2000, max_rows=20000) if q["shape"] == "chain" and q["theta"]]
+    assert qs
+    for q in qs:
+        for i, (cols, at) in enumerate(q["rels"]):
+            assert at == [i, i + 1]
+            if i:
+                # the probe side (column 1 of the relation before) is uniform, the
+                # build side (column 0 here) Zipf: its most frequent key is far above the mean
+                c0 = cols[0]
+                top = np.bincount(c0 - c0.min()).max()
+                assert top > 4 * len(c0) / max(1, len(np.unique(c0)))
+
+
+def test_bench_percentiles():
+    import bench
+    xs = [5.0, 1.0, 3.0, 2.0, 4.0]
+    assert bench.pct(xs, 50) == 3.0 and bench.pct(xs, 99) == 5.0 and bench.pct(xs, 0) == 1.0
