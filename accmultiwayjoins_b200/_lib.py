@@ -122,6 +122,9 @@ class amj_serve_opts(C.Structure):
         ("ooc_lane", C.c_int),
         ("ooc_mem", C.c_uint64),
         ("ooc_slice_rows", C.c_uint64),
+        ("index_cache_bytes", C.c_uint64),
+        ("no_index_cache", C.c_int),
+        ("pad", C.c_int),
     ]
 
 
@@ -152,6 +155,9 @@ class amj_serve_stats(C.Structure):
         ("budget_bytes", C.c_uint64),
         ("peak_reserved_bytes", C.c_uint64),
         ("launches", C.c_uint64),
+        ("index_hits", C.c_uint64),
+        ("index_builds", C.c_uint64),
+        ("index_bytes", C.c_uint64),
         ("max_inflight_batches", C.c_uint32),
         ("lanes", C.c_uint32),
     ]

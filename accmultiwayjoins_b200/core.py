@@ -244,11 +244,13 @@ class Server:
     here until its result has been waited for."""
 
     def __init__(self, ctx: "Context", lanes: int = 2, max_batch: int = 256, mem_budget: int = 0,
-                 ooc_lane: bool = True, ooc_mem: int = 0, ooc_slice_rows: int = 0, **batch_kw):
+                 ooc_lane: bool = True, ooc_mem: int = 0, ooc_slice_rows: int = 0, index_cache: bool = True,
+                 index_cache_bytes: int = 0, **batch_kw):
         o = L.amj_serve_opts()
         o.lanes, o.max_batch, o.mem_budget = lanes, max_batch, mem_budget
         o.batch = Batch._opts(**batch_kw)
         o.ooc_lane, o.ooc_mem, o.ooc_slice_rows = int(bool(ooc_lane)), ooc_mem, ooc_slice_rows
+        o.index_cache_bytes, o.no_index_cache = index_cache_bytes, 0 if index_cache else 1
         h = C.c_void_p()
         self.handle = None
         L.check(L.load().amj_server_create(ctx.handle, C.byref(o), C.byref(h)), "server_create")

@@ -641,10 +641,12 @@ void fill_level_desc(const LevelSpec &ls, int layout, int key_mode, uint32_t mas
     for (int c = 0; c < 4; c++) d->attr[c] = (int8_t)(c < ls.ncols ? ls.attr[c] : 0);
 }
 
-static void fill_level(const LevelSpec &ls, const HashIndex &ix, LevelDesc *d) {
+void fill_level_from_index(const LevelSpec &ls, const HashIndex &ix, LevelDesc *d) {
     const int32_t *cols[4] = {ix.cols[0].p, ix.cols[1].p, ix.cols[2].p, ix.cols[3].p};
     fill_level_desc(ls, ix.layout, ix.key_mode, ix.mask, ix.buc_ptrs.p, cols, ix.slots.p, d);
 }
+
+static void fill_level(const LevelSpec &ls, const HashIndex &ix, LevelDesc *d) { fill_level_from_index(ls, ix, d); }
 
 void plan_common(const HostPlan &hp, const amj_opts &o, ProbePlan *P) {
     P->L = (int8_t)hp.L;
@@ -821,6 +823,14 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
         const LevelSpec &ls = hp.lv[l];
         IndexKey key{ls.rel, {-1, -1, -1, -1}, ls.ncols, ls.key_mode, layout};
         for (int c = 0; c < ls.ncols; c++) key.src[c] = ls.src_col[c];
+        key.uid = ls.rel->uid;
+        key.load_factor = ctx->opts.load_factor;
+        if (ctx->iprov) {
+            if (const HashIndex *kept = ctx->iprov->get(ctx, key, ls)) {
+                lvix[l] = kept;
+                continue;
+            }
+        }
         auto it = X.indexes.find(key);
         if (it == X.indexes.end()) {
             HashIndex ix;

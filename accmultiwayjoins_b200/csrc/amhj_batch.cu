@@ -327,6 +327,7 @@ static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
     // ---- jobs: one per distinct index; bucket-layout jobs first
     std::map<IndexKey, int> job_of;
     std::vector<std::vector<int>> level_job(nq);
+    std::vector<std::vector<const HashIndex *>> level_kept(nq);   // indexes kept by the context's provider
     struct Pending {
         IndexKey key;
         const LevelSpec *ls;
@@ -341,6 +342,14 @@ static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
             if (ls.ncols > 2) layout = AMJ_LAYOUT_BUCKET;   // open addressing holds two columns
             IndexKey key{ls.rel, {-1, -1, -1, -1}, ls.ncols, ls.key_mode, layout};
             for (int c = 0; c < ls.ncols; c++) key.src[c] = ls.src_col[c];
+            key.uid = ls.rel->uid;
+            key.load_factor = o.load_factor;
+            const HashIndex *kept = ctx->iprov ? ctx->iprov->get(ctx, key, ls) : nullptr;
+            level_kept[q].push_back(kept);
+            if (kept) {
+                level_job[q].push_back(-1);
+                continue;
+            }
             auto it = job_of.find(key);
             if (it == job_of.end()) {
                 it = job_of.emplace(key, (int)pend.size()).first;
@@ -445,6 +454,10 @@ static int batch_prepare(amj_batch *b, const amj_batch_opts &o) {
         P.l0_start = b->l0.p + qrow[q];
         P.lbs = 1;
         for (int l = 0; l < hp.L; l++) {
+            if (level_kept[q][l]) {
+                fill_level_from_index(hp.lv[l], *level_kept[q][l], &P.lv[l]);
+                continue;
+            }
             const BatchJob &J = b->jobs[where[level_job[q][l]]];
             if (J.layout == AMJ_LAYOUT_BUCKET)
                 fill_level_desc(hp.lv[l], J.layout, J.key_mode, J.mask, b->gptrs.p + J.base, gc, nullptr, &P.lv[l]);

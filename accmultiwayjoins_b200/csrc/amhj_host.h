@@ -28,11 +28,25 @@ struct IndexKey {
     const amj_rel *rel;
     int src[4];
     int ncols, key_mode, layout;
+    uint64_t uid = 0;   // the relation's serial number: a reused address is another relation
+    float load_factor = 0.f;
     bool operator<(const IndexKey &o) const {
-        return std::tie(rel, src[0], src[1], src[2], src[3], ncols, key_mode, layout) <
-               std::tie(o.rel, o.src[0], o.src[1], o.src[2], o.src[3], o.ncols, o.key_mode, o.layout);
+        return std::tie(uid, rel, src[0], src[1], src[2], src[3], ncols, key_mode, layout, load_factor) <
+               std::tie(o.uid, o.rel, o.src[0], o.src[1], o.src[2], o.src[3], o.ncols, o.key_mode, o.layout,
+                        o.load_factor);
     }
 };
+
+// Indexes kept across calls.  get() returns a complete index of the level's
+// relation columns (built on ctx's stream and synchronised on a miss), or
+// null when the provider keeps no index for it (the caller builds its own).
+struct IndexProvider {
+    virtual ~IndexProvider() = default;
+    virtual const HashIndex *get(amj_ctx *ctx, const IndexKey &key, const LevelSpec &ls) = 0;
+};
+
+// Level descriptor of a complete index.
+void fill_level_from_index(const LevelSpec &ls, const HashIndex &ix, LevelDesc *d);
 
 // Compile a query (reference exec_AMHJ.cu:70-89, TRI/FOUR :32-69) into the
 // probe relation and the ordered build levels.

@@ -23,6 +23,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -46,6 +47,58 @@ struct ServeReq {
     int state = 0;                   // 0 waiting, 1 running, 2 done
     uint32_t batch_id = 0, batch_size = 0;
     bool spilled = false;
+};
+
+// Indexes of the resident relations, kept for the server's lifetime and
+// shared by its lanes and its out-of-core lane: a request whose build
+// relations were indexed before only probes.  An index is built on the first
+// miss, on the calling lane's stream, and synchronised before anyone uses it;
+// keys carry the relation's serial number, so a released relation's address
+// reused by a new one never hits.  Indexes that would exceed the capacity
+// are not kept (the batch builds them as usual).
+struct ServerIndexCache : IndexProvider {
+    std::mutex mu;
+    std::map<IndexKey, std::unique_ptr<HashIndex>> kept;
+    std::map<IndexKey, int> refused;
+    uint64_t bytes = 0, cap = 0, hits = 0, builds = 0;
+
+    static uint64_t index_bytes(const HashIndex &ix) {
+        uint64_t b = ix.buc_ptrs.n * sizeof(uint32_t) + ix.slots.n * sizeof(int2);
+        for (const auto &c : ix.cols) b += c.n * sizeof(int32_t);
+        return b;
+    }
+
+    const HashIndex *get(amj_ctx *ctx, const IndexKey &key, const LevelSpec &ls) override {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = kept.find(key);
+        if (it != kept.end()) {
+            hits++;
+            return it->second.get();
+        }
+        if (refused.count(key)) return nullptr;
+        const uint64_t n = ls.rel->n;
+        const double lf = key.load_factor > 0.f ? key.load_factor : 0.5;
+        const uint64_t est = n * 4ull * ls.ncols + (uint64_t)((double)n / lf) * 8 + 4096;
+        if (bytes + est > cap) {
+            refused[key] = 1;
+            return nullptr;
+        }
+        auto ix = std::make_unique<HashIndex>();
+        const int32_t *cols[4] = {nullptr, nullptr, nullptr, nullptr};
+        for (int c = 0; c < ls.ncols; c++) cols[c] = ls.rel->d_cols[ls.src_col[c]];
+        int rc = build_hash_index(ctx, cols, ls.ncols, n, key.layout, ls.key_mode, key.load_factor, ix.get());
+        if (rc == AMJ_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = AMJ_ECUDA;
+        if (rc != AMJ_OK) {
+            (void)cudaGetLastError();
+            refused[key] = 1;
+            return nullptr;
+        }
+        builds++;
+        bytes += index_bytes(*ix);
+        const HashIndex *p = ix.get();
+        kept.emplace(key, std::move(ix));
+        return p;
+    }
 };
 
 struct Lane {
@@ -76,6 +129,7 @@ struct amj_server {
     std::chrono::steady_clock::time_point t0;
     amj_serve_stats st{};
     uint32_t inflight = 0;
+    std::unique_ptr<ServerIndexCache> cache;
 
     double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
@@ -251,7 +305,15 @@ extern "C" int amj_server_create(amj_ctx *ctx, const amj_serve_opts *opts, amj_s
     AMJ_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
     uint64_t ooc_reserve = 0;
     if (s->opts.ooc_lane) ooc_reserve = s->opts.ooc_mem ? s->opts.ooc_mem : (uint64_t)(fr / 8);
-    s->budget = s->opts.mem_budget ? s->opts.mem_budget : (uint64_t)(fr * 0.8) - ooc_reserve;
+    uint64_t cache_cap = 0;
+    if (!s->opts.no_index_cache) cache_cap = s->opts.index_cache_bytes ? s->opts.index_cache_bytes : (uint64_t)(fr * 0.35);
+    const uint64_t reserved0 = ooc_reserve + cache_cap;
+    s->budget = s->opts.mem_budget ? s->opts.mem_budget
+                                   : ((uint64_t)(fr * 0.8) > reserved0 ? (uint64_t)(fr * 0.8) - reserved0 : fr / 16);
+    if (cache_cap) {
+        s->cache = std::make_unique<ServerIndexCache>();
+        s->cache->cap = cache_cap;
+    }
     // The persistent kernels of the lanes and of the ooc lane run at the same
     // time; their idle warps wait for their own unstarted blocks, so all of
     // them must be resident together.  Each gets an equal share of four probe
@@ -268,6 +330,7 @@ extern "C" int amj_server_create(amj_ctx *ctx, const amj_serve_opts *opts, amj_s
         Lane ln;
         int rc = amj_ctx_create(ctx->device, &lo, &ln.ctx);
         if (rc == AMJ_OK) rc = amj_batch_create(ln.ctx, &ln.b);
+        if (rc == AMJ_OK) ln.ctx->iprov = s->cache.get();
         if (rc != AMJ_OK) {
             if (ln.ctx) amj_ctx_destroy(ln.ctx);
             for (Lane &l : s->lanes) {
@@ -284,6 +347,7 @@ extern "C" int amj_server_create(amj_ctx *ctx, const amj_serve_opts *opts, amj_s
         if (kernels > 1 && oo.max_blocks == 0) oo.max_blocks = (uint32_t)share;
         if (s->opts.ooc_slice_rows) oo.ooc_slice_rows = s->opts.ooc_slice_rows;
         int rc = amj_ctx_create(ctx->device, &oo, &s->ooc_ctx);
+        if (rc == AMJ_OK) s->ooc_ctx->iprov = s->cache.get();
         if (rc != AMJ_OK) {
             for (Lane &l : s->lanes) {
                 amj_batch_destroy(l.b);
@@ -372,6 +436,12 @@ extern "C" int amj_server_stats(amj_server *s, amj_serve_stats *out) {
     out->launches = 0;
     for (const Lane &ln : s->lanes) out->launches += ln.ctx->launches;
     if (s->ooc_ctx) out->launches += s->ooc_ctx->launches;
+    if (s->cache) {
+        std::lock_guard<std::mutex> ck(s->cache->mu);
+        out->index_hits = s->cache->hits;
+        out->index_builds = s->cache->builds;
+        out->index_bytes = s->cache->bytes;
+    }
     out->lanes = (uint32_t)s->lanes.size();
     return AMJ_OK;
 }
@@ -386,10 +456,15 @@ extern "C" int amj_server_destroy(amj_server *s) {
     s->cv_ooc.notify_all();
     if (s->loop.joinable()) s->loop.join();
     if (s->ooc_loop.joinable()) s->ooc_loop.join();
-    for (Lane &ln : s->lanes) {
+    for (Lane &ln : s->lanes)
         if (ln.b) amj_batch_destroy(ln.b);
-        amj_ctx_destroy(ln.ctx);
+    // the kept indexes were allocated on the lanes' contexts: free them first
+    if (s->cache) {
+        for (Lane &ln : s->lanes) cudaStreamSynchronize(ln.ctx->stream);
+        if (s->ooc_ctx) cudaStreamSynchronize(s->ooc_ctx->stream);
+        s->cache.reset();
     }
+    for (Lane &ln : s->lanes) amj_ctx_destroy(ln.ctx);
     if (s->ooc_ctx) amj_ctx_destroy(s->ooc_ctx);
     delete s;
     return AMJ_OK;

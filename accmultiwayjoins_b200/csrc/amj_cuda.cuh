@@ -114,6 +114,10 @@ __host__ __device__ __forceinline__ uint32_t hash_key(int32_t k) {
 // ---------------------------------------------------------------------------
 // Context
 // ---------------------------------------------------------------------------
+namespace amj {
+struct IndexProvider;
+}
+
 struct amj_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -128,10 +132,12 @@ struct amj_ctx {
     cudaStream_t side_stream[2] = {nullptr, nullptr};   // ooc copy / prefetch streams
     unsigned long long launches = 0;                     // kernels launched through this context
     cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};   // per-kernel timing
+    amj::IndexProvider *iprov = nullptr;   // indexes kept across calls (set by the request server)
 };
 
 struct amj_rel {
     amj_ctx *ctx = nullptr;
+    uint64_t uid = 0;                          // serial number, unique for the process's lifetime
     uint64_t n = 0;
     int ncols = 0;
     uint32_t attrs[AMJ_MAX_COLS] = {};

@@ -7,6 +7,8 @@
 // device's memory pool), every relation / result has an owner, and errors
 // come back as status codes with a per-thread message.
 #include "amj_cuda.cuh"
+
+#include <atomic>
 #include "amj_ops.cuh"
 
 #include <cstdio>
@@ -225,8 +227,10 @@ extern "C" int amj_rel_create(amj_ctx *ctx, uint64_t n, int ncols, const uint32_
         for (int d = 0; d < c; d++)
             if (attrs[d] == attrs[c]) return fail(AMJ_EINVAL, "rel_create: repeated attribute in one relation");
     }
+    static std::atomic<uint64_t> next_uid{1};
     auto *r = new amj_rel();
     r->ctx = ctx;
+    r->uid = next_uid.fetch_add(1);
     r->n = n;
     r->ncols = ncols;
     r->where = where;

@@ -224,8 +224,10 @@ int  amj_batch_destroy(amj_batch *b);
  * (AMJ_MEM_HOST_STREAMED), requests submitted with ooc = 1, and requests too
  * large for the whole budget run through the out-of-core operator on their
  * own lane (context, stream and host thread), streaming probe slices from
- * pinned host memory.  Results are the same as one amj_amhj_execute call per
- * query (count and checksum). */
+ * pinned host memory.  The hash indexes of resident relations are kept
+ * across requests (the relations must not change while the server runs).
+ * Results are the same as one amj_amhj_execute call per query (count and
+ * checksum). */
 typedef struct amj_server amj_server;
 
 typedef struct amj_serve_opts {
@@ -238,6 +240,10 @@ typedef struct amj_serve_opts {
     int      ooc_lane;        /* 1: run out-of-core and spilled requests on their own lane */
     uint64_t ooc_mem;         /* device bytes of the ooc lane's slices (0: free / 8)       */
     uint64_t ooc_slice_rows;  /* ooc probe slice rows (0: derived from ooc_mem)            */
+    uint64_t index_cache_bytes; /* device bytes of hash indexes kept across requests (0: 35%
+                                   of the free memory at creation)                          */
+    int      no_index_cache;  /* 1: build every request's indexes anew                      */
+    int      pad;
 } amj_serve_opts;
 
 typedef struct amj_serve_result {
@@ -256,6 +262,7 @@ typedef struct amj_serve_stats {
     uint64_t submitted, completed, rejected, spilled, batches, ooc_runs;
     uint64_t budget_bytes, peak_reserved_bytes;
     uint64_t launches;        /* kernels launched by the lanes and the ooc lane   */
+    uint64_t index_hits, index_builds, index_bytes;   /* kept-index cache          */
     uint32_t max_inflight_batches, lanes;
 } amj_serve_stats;
 

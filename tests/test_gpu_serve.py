@@ -128,6 +128,37 @@ def test_host_resident_relations_go_through_the_ooc_lane_beside_batches(mix):
         srv.close()
 
 
+def test_index_cache_keeps_indexes_across_requests(mix):
+    qs, want = mix
+    with Context(0) as ctx:
+        rels = [[ctx.relation(c, a) for c, a in q["rels"]] for q in qs[:10]]
+        srv = ctx.server(lanes=2, max_batch=4)
+        for _ in range(3):
+            ts = [srv.submit(q["qt"], r) for q, r in zip(qs[:10], rels)]
+            assert [(g.count, g.checksum) for g in (srv.wait(t) for t in ts)] == want[:10]
+        st = srv.stats()
+        assert st["index_builds"] > 0 and st["index_hits"] >= 2 * st["index_builds"] and st["index_bytes"] > 0
+        srv.close()
+        # a relation created after another was released (possibly at its address) is indexed anew
+        srv = ctx.server(lanes=1)
+        q1 = data.chain_relations(5000, 1 << 10, 3, seed=1)
+        r1 = [ctx.relation(c, a) for c, a in q1]
+        g1 = srv.wait(srv.submit("NORMAL", r1))
+        for r in r1:
+            r.release()
+        q2 = data.chain_relations(5000, 1 << 10, 3, seed=2)
+        r2 = [ctx.relation(c, a) for c, a in q2]
+        g2 = srv.wait(srv.submit("NORMAL", r2))
+        assert (g1.count, g1.checksum) == O.mhj(q1) and (g2.count, g2.checksum) == O.mhj(q2)
+        srv.close()
+        # without the cache every request builds its own indexes: same results
+        srv = ctx.server(lanes=2, max_batch=4, index_cache=False)
+        ts = [srv.submit(q["qt"], r) for q, r in zip(qs[:10], rels)]
+        assert [(g.count, g.checksum) for g in (srv.wait(t) for t in ts)] == want[:10]
+        assert srv.stats()["index_builds"] == 0
+        srv.close()
+
+
 def test_server_rejects_bad_requests():
     with Context(0) as ctx:
         srv = ctx.server(lanes=1, ooc_lane=False)
