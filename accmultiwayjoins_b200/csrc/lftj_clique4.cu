@@ -216,14 +216,6 @@ __global__ __launch_bounds__(256) void lftj_clique4_kernel(const __grid_constant
     }
 }
 
-__global__ void max_children_kernel(const uint64_t *__restrict__ off, uint64_t n, unsigned long long *out) {
-    unsigned long long m = 0;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        m = umax(m, off[i + 1] - off[i]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = umax(m, __shfl_xor_sync(AMJ_FULL_MASK, m, o));
-    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
-}
 
 struct C4Counters {
     unsigned long long cursor, count, checksum, out_cursor, max_deg;

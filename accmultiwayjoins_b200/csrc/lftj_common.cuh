@@ -158,4 +158,17 @@ __device__ __forceinline__ void warp_intersect(const int32_t *X, uint64_t nx, co
     });
 }
 
+// *out = max(*out, the longest child list among off[0..n])
+static __global__ void max_children_kernel(const uint64_t *__restrict__ off, uint64_t n, unsigned long long *out) {
+    unsigned long long m = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        m = (off[i + 1] - off[i] > m ? off[i + 1] - off[i] : m);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(AMJ_FULL_MASK, m, o);
+        m = v > m ? v : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 }  // namespace amj
