@@ -351,13 +351,17 @@ class Context:
         return out
 
     def amhj(self, query_type, relations: Sequence[Relation], ooc: int = 0, ws: int = 0, dro: int = 0,
-             fib: int = 0, materialize: bool = False, reorder: bool = True) -> Result:
+             fib: int = 0, materialize: bool = False, reorder: bool = True, degree_order: bool = True) -> Result:
+        """degree_order=False joins a TRI / FOUR edge relation as given, never its
+        degree-ordered copy (the results are the same)."""
         lib = L.load()
         qt = _QUERY[query_type] if isinstance(query_type, str) else int(query_type)
         arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
         flags = (L.AMJ_F_MATERIALIZE | L.AMJ_F_HOST_RESULT) if materialize else 0
         if not reorder:
             flags |= L.AMJ_F_NO_REORDER
+        if not degree_order:
+            flags |= L.AMJ_F_KEEP_ORDER
         res = L.amj_result()
         L.check(lib.amj_amhj_execute(self.handle, qt, arr, len(relations), int(ooc), int(ws), int(dro), int(fib),
                                      flags, C.byref(res)), "amhj_execute")

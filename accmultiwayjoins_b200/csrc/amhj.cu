@@ -800,6 +800,25 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
     for (int i = 0; i < nrels; i++)
         if (!rels[i]) return fail(AMJ_EINVAL, "amhj_execute: null relation");
     AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
+    // TRI / FOUR over an oriented edge relation: join its degree-ordered copy
+    // and report every tuple sorted (the same bag; shorter hub lists)
+    amj_rel ordered;
+    amj_rel *ordered_rels[1] = {&ordered};
+    DBuf<int32_t> ord0, ord1;
+    bool sort_out = false;
+    if ((query_type == AMJ_QUERY_TRI || query_type == AMJ_QUERY_FOUR) && nrels == 1 && rels[0]->ncols == 2 &&
+        rels[0]->where != AMJ_MEM_HOST_STREAMED && !(flags & AMJ_F_KEEP_ORDER)) {
+        AMJ_TRY(degree_ordered_copy(ctx, rels[0]->d_cols[0], rels[0]->d_cols[1], rels[0]->n, &ord0, &ord1,
+                                    &sort_out));
+        if (sort_out) {
+            ordered = *rels[0];
+            ordered.uid = 0;   // a temporary relation: never kept by an index provider
+            ordered.owned = false;
+            ordered.d_cols[0] = ord0.p;
+            ordered.d_cols[1] = ord1.p;
+            rels = ordered_rels;
+        }
+    }
     HostPlan hp;
     AMJ_TRY(compile_plan(query_type, rels, nrels, flags, &hp));
     result_init(out, hp.k);
@@ -825,7 +844,7 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
         for (int c = 0; c < ls.ncols; c++) key.src[c] = ls.src_col[c];
         key.uid = ls.rel->uid;
         key.load_factor = ctx->opts.load_factor;
-        if (ctx->iprov) {
+        if (ctx->iprov && ls.rel->uid) {
             if (const HashIndex *kept = ctx->iprov->get(ctx, key, ls)) {
                 lvix[l] = kept;
                 continue;
@@ -858,6 +877,7 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
     plan_common(hp, ctx->opts, &P);
     for (int l = 0; l < hp.L; l++) fill_level(hp.lv[l], *lvix[l], &P.lv[l]);
     plan_inline(P);
+    P.sort_out = sort_out ? 1 : 0;
     AMJ_TRY(X.st.alloc(ctx, 1));
     PL.st = X.st.p;
     PL.status = ctx->d_status;

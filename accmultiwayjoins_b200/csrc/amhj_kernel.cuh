@@ -433,13 +433,12 @@ __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q,
             if (cached) {
                 cw = WT ? F.w[o] : 1u;
 #pragma unroll
-                for (int a = 0; a < AMJ_MAX_ATTRS; a++) {
-                    if (a < P.k) {
-                        const int32_t v = ((P.fib_suffix_attrs >> a) & 1u) ? P.fib_cols[a][cslot] : F.vals[a * 32 + o];
-                        tv[a] = v;
-                        h = amj_hash_step(h, v);
-                    }
-                }
+                for (int a = 0; a < AMJ_MAX_ATTRS; a++)
+                    if (a < P.k) tv[a] = ((P.fib_suffix_attrs >> a) & 1u) ? P.fib_cols[a][cslot] : F.vals[a * 32 + o];
+                if (P.sort_out) sort_tuple(tv, P.k);
+#pragma unroll
+                for (int a = 0; a < AMJ_MAX_ATTRS; a++)
+                    if (a < P.k) h = amj_hash_step(h, tv[a]);
                 acc.fib += cw;
             }
             emit_weighted<MODE>(P, Q, lane, tv, h, cw, acc, u);
@@ -465,12 +464,12 @@ __device__ __forceinline__ void probe_step(const ProbePlan &P, const WsQueue &Q,
         uint64_t h = AMJ_CHECKSUM_SEED;
         if (live) {
 #pragma unroll
-            for (int a = 0; a < AMJ_MAX_ATTRS; a++) {
-                if (a < P.k) {
-                    tv[a] = val(a);
-                    h = amj_hash_step(h, tv[a]);
-                }
-            }
+            for (int a = 0; a < AMJ_MAX_ATTRS; a++)
+                if (a < P.k) tv[a] = val(a);
+            if (P.sort_out) sort_tuple(tv, P.k);
+#pragma unroll
+            for (int a = 0; a < AMJ_MAX_ATTRS; a++)
+                if (a < P.k) h = amj_hash_step(h, tv[a]);
         }
         emit_weighted<MODE, WT>(P, Q, lane, tv, h, wt, acc, u);
         return;

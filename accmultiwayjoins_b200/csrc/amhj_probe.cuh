@@ -56,6 +56,8 @@ struct alignas(16) ProbePlan {
     int8_t next_lv[AMJ_MAX_BUILD_TABLES];
     int8_t prev_lv[AMJ_MAX_BUILD_TABLES];
     uint8_t has_inl;                    // any level inlined: run the weighted kernels
+    uint8_t sort_out;                   // TRI / FOUR over the degree-ordered copy of an oriented
+                                        // relation: every tuple is reported with its values sorted
     // bind_col[d][a]: the column of level d that binds attribute a, or -1
     // (the value then comes from the frontier)
     int8_t bind_col[AMJ_MAX_BUILD_TABLES][AMJ_MAX_ATTRS];
@@ -147,6 +149,28 @@ __device__ __forceinline__ Frontier frontier_at(char *wbase, const ProbePlan &P,
 }
 
 constexpr uint8_t FIB_FLAG = 0x80;   // frontier entry served from the frequent-item cache
+
+// sort the tuple of a TRI (k = 3) or FOUR (k = 4) query: a sorting network
+__device__ __forceinline__ void sort_tuple(int32_t *tv, int k) {
+    auto cs = [&](int i, int j) {
+        if (tv[i] > tv[j]) {
+            const int32_t t = tv[i];
+            tv[i] = tv[j];
+            tv[j] = t;
+        }
+    };
+    if (k == 3) {
+        cs(0, 1);
+        cs(1, 2);
+        cs(0, 1);
+    } else if (k == 4) {
+        cs(0, 1);
+        cs(2, 3);
+        cs(0, 2);
+        cs(1, 3);
+        cs(1, 2);
+    }
+}
 
 // cache index of a frequent key, or -1
 __device__ __forceinline__ int fib_find(const ProbePlan &P, int32_t key) {

@@ -58,6 +58,11 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
 // time between two events recorded on the context stream (ms)
 double event_ms(cudaEvent_t a, cudaEvent_t b);
 
+// Degree-ordered copy (ns, nd) of the edge relation (c0, c1) when every edge
+// has 0 <= c0 < c1 (*oriented); otherwise nothing is allocated.
+int degree_ordered_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *ns,
+                        DBuf<int32_t> *nd, bool *oriented);
+
 // copy materialised device result columns to pinned host memory (when asked)
 int finish_result_columns(amj_ctx *ctx, amj_result *res, int flags);
 

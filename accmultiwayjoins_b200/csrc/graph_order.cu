@@ -1,0 +1,86 @@
+// Degree ordering of an oriented edge relation.
+//
+// When every edge (u, v) of a self-joined relation has 0 <= u < v, the
+// triangles (and 4-cliques) of the join in attribute order are exactly the
+// increasing triples (quadruples) of the undirected graph, each once.  Any
+// acyclic orientation lists each of them once too, so an operator may join
+// the copy oriented from the lower to the higher (degree, id) and report
+// every tuple in increasing order: the same bag, the same checksum.  Hub
+// vertices then keep short child lists.  Used by ALFTJ (triangle, 4-clique)
+// and by AMHJ TRI / FOUR.
+#include "amj_ops.cuh"
+
+#include <algorithm>
+
+namespace amj {
+
+__global__ void orient_check_kernel(const int32_t *__restrict__ s, const int32_t *__restrict__ d, uint64_t n,
+                                    unsigned int *bad, int *maxv) {
+    unsigned int b = 0;
+    int m = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const int32_t u = s[i], v = d[i];
+        b |= (u < 0 || u >= v) ? 1u : 0u;
+        m = v > m ? v : m;
+    }
+    b = __reduce_or_sync(AMJ_FULL_MASK, b);
+    m = __reduce_max_sync(AMJ_FULL_MASK, m);
+    if ((threadIdx.x & 31) == 0) {
+        if (b) atomicOr(bad, 1u);
+        atomicMax(maxv, m);
+    }
+}
+
+__global__ void degree_kernel(const int32_t *__restrict__ s, const int32_t *__restrict__ d, uint64_t n,
+                              unsigned int *deg) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        atomicAdd(&deg[s[i]], 1u);
+        atomicAdd(&deg[d[i]], 1u);
+    }
+}
+
+__global__ void reorient_kernel(const int32_t *__restrict__ s, const int32_t *__restrict__ d, uint64_t n,
+                                const unsigned int *__restrict__ deg, int32_t *__restrict__ ns,
+                                int32_t *__restrict__ nd) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const int32_t u = s[i], v = d[i];
+        const uint64_t ku = ((uint64_t)deg[u] << 32) | (uint32_t)u, kv = ((uint64_t)deg[v] << 32) | (uint32_t)v;
+        ns[i] = ku < kv ? u : v;
+        nd[i] = ku < kv ? v : u;
+    }
+}
+
+int degree_ordered_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *ns,
+                        DBuf<int32_t> *nd, bool *oriented) {
+    *oriented = false;
+    if (n == 0) return AMJ_OK;
+    struct Probe {
+        unsigned int bad;
+        int maxv;
+    };
+    DBuf<Probe> pr;
+    AMJ_TRY(pr.alloc(ctx, 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(pr.p, 0, sizeof(Probe), ctx->stream));
+    const unsigned g = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 16);
+    note_launch(ctx);
+    orient_check_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, &pr.p->bad, &pr.p->maxv);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    Probe h;
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&h, pr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (h.bad) return AMJ_OK;
+    DBuf<unsigned int> deg;
+    AMJ_TRY(deg.alloc(ctx, (uint64_t)h.maxv + 1));
+    AMJ_TRY(ns->alloc(ctx, n));
+    AMJ_TRY(nd->alloc(ctx, n));
+    AMJ_CUDA_TRY(cudaMemsetAsync(deg.p, 0, ((uint64_t)h.maxv + 1) * sizeof(unsigned int), ctx->stream));
+    note_launch(ctx);
+    degree_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, deg.p);
+    note_launch(ctx);
+    reorient_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, deg.p, ns->p, nd->p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    *oriented = true;
+    return AMJ_OK;
+}
+
+}  // namespace amj

@@ -21,89 +21,21 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
                   uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out);
 
-// ---- degree ordering of an oriented edge relation ----
-// When every edge (u, v) of the self-joined relation has 0 <= u < v, the
-// triangles (and 4-cliques) of the join in attribute order are exactly the
-// increasing triples (quadruples) of the undirected graph, each once.  Any
-// acyclic orientation lists each of them once too, so the join runs on the
-// copy oriented from the lower to the higher (degree, id) and the kernels
-// report every tuple in increasing order: the same bag, the same checksum.
-// Hub vertices then keep short child lists, which shortens the intersections.
-
-__global__ void orient_check_kernel(const int32_t *__restrict__ s, const int32_t *__restrict__ d, uint64_t n,
-                                    unsigned int *bad, int *maxv) {
-    unsigned int b = 0;
-    int m = 0;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const int32_t u = s[i], v = d[i];
-        b |= (u < 0 || u >= v) ? 1u : 0u;
-        m = v > m ? v : m;
-    }
-    b = __reduce_or_sync(AMJ_FULL_MASK, b);
-    m = __reduce_max_sync(AMJ_FULL_MASK, m);
-    if ((threadIdx.x & 31) == 0) {
-        if (b) atomicOr(bad, 1u);
-        atomicMax(maxv, m);
-    }
-}
-
-__global__ void degree_kernel(const int32_t *__restrict__ s, const int32_t *__restrict__ d, uint64_t n,
-                              unsigned int *deg) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        atomicAdd(&deg[s[i]], 1u);
-        atomicAdd(&deg[d[i]], 1u);
-    }
-}
-
-__global__ void reorient_kernel(const int32_t *__restrict__ s, const int32_t *__restrict__ d, uint64_t n,
-                                const unsigned int *__restrict__ deg, int32_t *__restrict__ ns,
-                                int32_t *__restrict__ nd) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const int32_t u = s[i], v = d[i];
-        const uint64_t ku = ((uint64_t)deg[u] << 32) | (uint32_t)u, kv = ((uint64_t)deg[v] << 32) | (uint32_t)v;
-        ns[i] = ku < kv ? u : v;
-        nd[i] = ku < kv ? v : u;
-    }
-}
-
 // Trie of the self-joined edge relation: the degree-ordered copy when the
-// relation is oriented (*sorted = 1), else the relation itself.
+// relation is oriented and `allow` (*sorted = 1), else the relation itself.
 static int build_self_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, int *sorted, bool allow) {
     *sorted = 0;
     if (r->ncols != 2) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must have two columns");
     if (r->where == AMJ_MEM_HOST_STREAMED) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must be on the device");
     const bool swap = r->attrs[0] > r->attrs[1];
     const int32_t *c0 = r->d_cols[swap ? 1 : 0], *c1 = r->d_cols[swap ? 0 : 1];
-    const uint64_t n = r->n;
-    if (n == 0 || !allow) return build_trie2(ctx, c0, c1, n, t);
-    struct Probe {
-        unsigned int bad;
-        int maxv;
-    };
-    DBuf<Probe> pr;
-    AMJ_TRY(pr.alloc(ctx, 1));
-    AMJ_CUDA_TRY(cudaMemsetAsync(pr.p, 0, sizeof(Probe), ctx->stream));
-    const unsigned g = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 16);
-    note_launch(ctx);
-    orient_check_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, &pr.p->bad, &pr.p->maxv);
-    AMJ_CUDA_TRY(cudaGetLastError());
-    Probe h;
-    AMJ_CUDA_TRY(cudaMemcpyAsync(&h, pr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    if (h.bad) return build_trie2(ctx, c0, c1, n, t);
-    DBuf<unsigned int> deg;
+    if (!allow) return build_trie2(ctx, c0, c1, r->n, t);
     DBuf<int32_t> ns, nd;
-    AMJ_TRY(deg.alloc(ctx, (uint64_t)h.maxv + 1));
-    AMJ_TRY(ns.alloc(ctx, n));
-    AMJ_TRY(nd.alloc(ctx, n));
-    AMJ_CUDA_TRY(cudaMemsetAsync(deg.p, 0, ((uint64_t)h.maxv + 1) * sizeof(unsigned int), ctx->stream));
-    note_launch(ctx);
-    degree_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, deg.p);
-    note_launch(ctx);
-    reorient_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, deg.p, ns.p, nd.p);
-    AMJ_CUDA_TRY(cudaGetLastError());
+    bool oriented = false;
+    AMJ_TRY(degree_ordered_copy(ctx, c0, c1, r->n, &ns, &nd, &oriented));
+    if (!oriented) return build_trie2(ctx, c0, c1, r->n, t);
     *sorted = 1;
-    return build_trie2(ctx, ns.p, nd.p, n, t);
+    return build_trie2(ctx, ns.p, nd.p, r->n, t);
 }
 }
 

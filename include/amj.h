@@ -72,8 +72,9 @@ extern "C" {
 #define AMJ_F_NO_REORDER   0x4  /* keep fully-bound tables at their query position */
 #define AMJ_F_CLIQUE4      0x8  /* amj_lftj_execute, one relation: the 4-clique (the
                                    FOUR pattern) instead of the triangle, DFS only */
-#define AMJ_F_KEEP_ORDER   0x10 /* amj_lftj_execute, one relation: join the relation as
-                                   given, never its degree-ordered copy             */
+#define AMJ_F_KEEP_ORDER   0x10 /* amj_lftj_execute, one relation, and amj_amhj_execute
+                                   TRI / FOUR: join the relation as given, never its
+                                   degree-ordered copy                              */
 #define AMJ_F_DEGREE_ORDER 0x20 /* amj_lftj_execute, one oriented relation: join its
                                    degree-ordered copy (the default for BFS and the
                                    4-clique; DFS triangles keep the relation's order) */

@@ -146,15 +146,21 @@ def test_amhj_star(layout):
 
 @pytest.mark.parametrize("qt", ["TRI", "FOUR"])
 @pytest.mark.parametrize("reorder", [True, False])
-def test_amhj_tri_four(ctx, qt, reorder):
+@pytest.mark.parametrize("degree_order", [True, False])
+def test_amhj_tri_four(ctx, qt, reorder, degree_order):
+    """Every switch, on the relation as given and on its degree-ordered copy
+    (the default for an oriented relation); tuples come out in increasing
+    order either way."""
     s, d = data.rmat(10, 6000, 0.57, 0.19, 0.19, seed=21)
     e = ctx.relation([s, d], [0, 1])
     want = O.triangle(s, d) if qt == "TRI" else O.four_clique(s, d)
     for sw in SWITCHES:
-        got = ctx.amhj(qt, [e], reorder=reorder, **sw)
+        got = ctx.amhj(qt, [e], reorder=reorder, degree_order=degree_order, **sw)
         assert (got.count, got.checksum) == want, sw
-    got = ctx.amhj(qt, [e], materialize=True, reorder=reorder)
+    got = ctx.amhj(qt, [e], materialize=True, reorder=reorder, degree_order=degree_order)
     assert data.checksum(got.columns) == want[1]
+    t = got.tuples()
+    assert np.all(t[:, :-1] < t[:, 1:])
 
 
 def test_amhj_dro_residual_resume():
