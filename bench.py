@@ -422,6 +422,15 @@ def run_batch(args, rank, world, local_rank):
     clocks = sampler.stop()
     ms = sum(dev_ms) / len(dev_ms)
     e2e = sum(e2e_ms) / len(e2e_ms)
+    n_queries = len(wl.queries)
+    if world > 1:
+        # whole job: tuples summed over the ranks, times the slowest rank's
+        t = torch.tensor([float(total), float(plain_tuples), float(n_queries)], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t)
+        m = torch.tensor([ms, e2e, plain_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(m, op=torch.distributed.ReduceOp.MAX)
+        total, plain_tuples, n_queries = int(t[0].item()), int(t[1].item()), int(t[2].item())
+        ms, e2e, plain_s = m.tolist()
     if rank != 0:
         b.close()
         ctx.close()
@@ -430,15 +439,15 @@ def run_batch(args, rank, world, local_rank):
         "metric": METRIC, "value": total / (ms * 1e-3), "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic (seeded)",
-        "config": {"workload": wl.describe(""), "queries": len(wl.queries), "output_tuples": total,
+        "config": {"workload": wl.describe("+rank" if world > 1 else ""), "queries": n_queries, "output_tuples": total,
                    "l2": "inputs far larger than L2 (%.1f GB of relations)" % (wl.h2d / 1e9),
                    "opts": {"layout": int(opts.layout), "load_factor": float(opts.load_factor),
                             "block_size": int(opts.block_size), "task_chunk": int(opts.task_chunk),
                             "use_graph": int(opts.use_graph)},
                    "tuned_on": "every 8th query, full grid" if args.tune else "defaults",
                    "tune_s": tune_s, "tune_best_sample_ms": tune_ms, "generation_s": wl.gen_s},
-        "e2e": {"value": total / (e2e * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": wl.h2d,
-                "d2h_bytes_per_step": 16 * len(wl.queries), "ms_per_step": e2e},
+        "e2e": {"value": total / (e2e * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": wl.h2d * world,
+                "d2h_bytes_per_step": 16 * n_queries, "ms_per_step": e2e},
         "batched_vs_plain": {
             "plain_value": plain_tuples / plain_s, "plain_ms_total": plain_s * 1e3,
             "batched_over_plain": (total / (ms * 1e-3)) / (plain_tuples / plain_s),
@@ -555,6 +564,17 @@ def run_serve(args, rank, world, local_rank):
     # the window runs from the first timed submission until every timed request has completed
     total = sum(r.count for _, r in res)
     wall = time.perf_counter() - t0
+    n_req = len(res)
+    if world > 1:
+        dev = torch.device("cuda", local_rank)
+        t = torch.tensor([float(total), float(n_req)], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t)
+        w = torch.tensor([wall], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.MAX)
+        total, n_req, wall = int(t[0].item()), int(t[1].item()), float(w.item())
+    if rank != 0:
+        ctx.close()
+        return
     lat = [r.latency_ms for i, r in res if i >= 0]
     olat = [r.latency_ms for i, r in res if i < 0]
     bsz = [r.batch_size for i, r in res if i >= 0]
@@ -562,8 +582,8 @@ def run_serve(args, rank, world, local_rank):
         "metric": METRIC, "value": total / wall, "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
-        "config": {"workload": wl.describe(""), "step": "one second of the request stream",
-                   "requests": len(res), "ooc_requests": len(olat), "output_tuples": total,
+        "config": {"workload": wl.describe("+rank" if world > 1 else ""), "step": "one second of the request stream",
+                   "requests": n_req, "ooc_requests": len(olat), "output_tuples": total,
                    "l2": "resident relations and ooc inputs larger than L2"},
         "e2e": {"value": total / wall, "unit": "tuples/s",
                 "h2d_bytes_per_step": int(len(olat) * 8 * args.ooc_rows / args.steps),
