@@ -113,12 +113,6 @@ int compile_plan(int query_type, amj_rel *const *rels, int nrels, int flags, Hos
         L++;
     }
     hp->L = L;
-    for (int a = 0; a < AMJ_MAX_ATTRS; a++) hp->last_src[a] = -1;
-    if (L > 0) {
-        const LevelSpec &last = hp->lv[L - 1];
-        for (int c = 0; c < last.ncols; c++)
-            if ((last.bind_mask >> c) & 1) hp->last_src[last.attr[c]] = c;
-    }
     return AMJ_OK;
 }
 
@@ -656,7 +650,6 @@ void plan_common(const HostPlan &hp, const amj_opts &o, ProbePlan *P) {
         P->probe_col[c] = hp.probe->d_cols[c];
         P->probe_attr[c] = (int8_t)hp.probe_attr[c];
     }
-    for (int a = 0; a < AMJ_MAX_ATTRS; a++) P->last_src[a] = (int8_t)hp.last_src[a];
     P->task_chunk = (uint32_t)o.task_chunk;
     P->task_cap = (uint32_t)std::min<uint64_t>(o.task_capacity, 0x7fffffffull);
     P->spin_limit_ns = (uint64_t)o.spin_limit_ms * 1000000ull;

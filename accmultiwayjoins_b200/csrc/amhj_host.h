@@ -21,7 +21,6 @@ struct HostPlan {
     int probe_attr[AMJ_MAX_COLS] = {};
     int L = 0, k = 0;
     LevelSpec lv[AMJ_MAX_BUILD_TABLES];
-    int last_src[AMJ_MAX_ATTRS] = {};
 };
 
 struct IndexKey {

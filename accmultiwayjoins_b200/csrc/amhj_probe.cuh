@@ -44,7 +44,6 @@ struct alignas(16) ProbePlan {
     const int32_t *probe_col[AMJ_MAX_COLS];
     int8_t probe_attr[AMJ_MAX_COLS];
     int8_t probe_ncols, L, k, pad0;
-    int8_t last_src[AMJ_MAX_ATTRS];     // output attr a: -1 from the tuple, c >= 0 from last level column c
     LevelDesc lv[AMJ_MAX_BUILD_TABLES];
     // Inline filters: a level that binds nothing and is looked up by the
     // pair of its columns (C(0,2) of the triangle, D/E/F of the 4-clique) is

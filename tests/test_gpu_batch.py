@@ -109,6 +109,35 @@ def test_batch_work_sharing_across_queries():
         assert r.tasks_pushed > 0 and r.tasks_popped == r.tasks_pushed
 
 
+@pytest.mark.parametrize("layout", ["bucket", "oa"])
+def test_batch_limits_and_empty_relations(layout):
+    """A 7-relation chain (6 build tables, 8 attributes), a 5-relation star,
+    an empty build relation, an empty probe relation and a one-row query, in
+    one batch: equal to one call per query and to the oracle."""
+    long_chain = data.chain_relations(3000, 3000, 7, seed=31)
+    fact, dims = data.star_relations(5000, [300, 200, 100, 50], theta=1.2, seed=32)
+    star = [fact] + dims
+    empty_build = data.chain_relations(2000, 256, 3, seed=33)
+    empty_build[1] = ([np.zeros(0, np.int32), np.zeros(0, np.int32)], [1, 2])
+    empty_probe = data.chain_relations(2000, 256, 3, seed=34)
+    empty_probe[0] = ([np.zeros(0, np.int32), np.zeros(0, np.int32)], [0, 1])
+    one = [([np.array([5], np.int32), np.array([7], np.int32)], [0, 1]),
+           ([np.array([7, 7], np.int32), np.array([1, 2], np.int32)], [1, 2])]
+    queries = [long_chain, star, empty_build, empty_probe, one]
+    with Context(0) as ctx:
+        b = ctx.batch()
+        rels = []
+        for q in queries:
+            r = [ctx.relation(c, a) for c, a in q]
+            rels.append(r)
+            b.submit("NORMAL", r)
+        got = b.run(layout=layout, block_size=256)
+        for q, r, c, k in zip(queries, rels, got.counts, got.checksums):
+            alone = ctx.amhj("NORMAL", r)
+            assert (alone.count, alone.checksum) == (c, k) == O.mhj(q)
+        assert got.counts[2] == 0 and got.counts[3] == 0 and got.counts[4] == 2
+
+
 def test_batch_tuner_picks_a_grid_point(mix):
     qs, want = mix
     with Context(0) as ctx:
