@@ -21,6 +21,9 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
                   uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out);
 
+// the generic join (lftj_generic.cu)
+int lftj_generic_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int ooc, int flags, amj_result *out);
+
 // Trie of the self-joined edge relation: the degree-ordered copy when the
 // relation is oriented and `allow` (*sorted = 1), else the relation itself.
 static int build_self_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, int *sorted, bool allow) {
@@ -107,9 +110,27 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     if (nrels == 2) return fail(AMJ_EINVAL, "lftj_execute: wrong number of datasets: 2");
     for (int i = 0; i < nrels; i++)
         if (!rels[i]) return fail(AMJ_EINVAL, "lftj_execute: null relation");
-    if (nrels > 3) return fail(AMJ_EUNSUPPORTED, "lftj_execute: at most 3 relations (MAX_NUM_TABLES)");
+    if (nrels > 16) return fail(AMJ_EUNSUPPORTED, "lftj_execute: at most 16 relations");
     AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
     if (flags & AMJ_F_CLIQUE4) return lftj_clique4_execute(ctx, rels, nrels, algo, ooc, flags, out);
+    if (nrels >= 3) {
+        // the triangle pattern (0,1), (1,2), (0,2) keeps its own kernels; any
+        // other query goes to the generic join (the reference stops at 3 tables)
+        bool tri = nrels == 3;
+        uint32_t pairs = 0;
+        for (int i = 0; i < nrels && tri; i++) {
+            if (rels[i]->ncols != 2) {
+                tri = false;
+                break;
+            }
+            const uint32_t lo = std::min(rels[i]->attrs[0], rels[i]->attrs[1]);
+            const uint32_t hi = std::max(rels[i]->attrs[0], rels[i]->attrs[1]);
+            const uint32_t bit = (lo == 0 && hi == 1) ? 1u : (lo == 1 && hi == 2) ? 2u : (lo == 0 && hi == 2) ? 4u : 0u;
+            if (!bit || (pairs & bit)) tri = false;
+            pairs |= bit;
+        }
+        if (!tri) return lftj_generic_execute(ctx, rels, nrels, ooc, flags, out);
+    }
     result_init(out, 3);
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));

@@ -153,8 +153,12 @@ int  amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *rels, int nr
                       int ooc, int ws, int dro, int fib, int flags, amj_result *out);
 
 /* ---- ALFTJ: exec-LFTJ <path> <0=BFS|1=DFS> <ooc> <ws> ----
- * nrels == 1: triangle self-join R(a,b) S(b,c) T(a,c) over one edge relation.
- * nrels >= 3: multi-way join of 2-column relations (attributes from rels).
+ * nrels == 1: triangle self-join R(a,b) S(b,c) T(a,c) over one edge relation
+ *             (AMJ_F_CLIQUE4: the 4-clique).
+ * nrels == 3 carrying (0,1), (1,2), (0,2): the triangle over three relations.
+ * any other nrels >= 3 (up to 16): the connected join of 2-column relations
+ *             over attributes 0..k-1, k <= 8, in identity attribute order (the
+ *             reference's LFTJ stops at 3 attributes and 3 tables); ooc = 0.
  * nrels == 2 is rejected, as in the reference (LFTJ-GPU/exec_LFTJ.cu:92-95). */
 int  amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels,
                       int algo, int ooc, int ws, int flags, amj_result *out);

@@ -430,6 +430,58 @@ def test_lftj_three_relations_and_cross_operator(ctx):
     assert (amhj.count, amhj.checksum) == (dfs.count, dfs.checksum) == (bfs.count, bfs.checksum) == want
 
 
+def distinct_rel(n, dom, seed, attrs):
+    """A 2-column relation of distinct tuples (the LFTJ set semantics)."""
+    a = data.uniform(n, 0, dom, seed, 0)
+    b = data.uniform(n, 0, dom, seed, 1)
+    pairs = np.unique(np.stack([a, b], 1), axis=0)
+    return ([np.ascontiguousarray(pairs[:, 0]), np.ascontiguousarray(pairs[:, 1])], attrs)
+
+
+GENERIC_QUERIES = {
+    "4-cycle": [(0, 1), (1, 2), (2, 3), (0, 3)],
+    "path4": [(0, 1), (1, 2), (2, 3)],
+    "4-clique": [(0, 1), (1, 2), (2, 3), (0, 3), (0, 2), (1, 3)],
+    "5-cycle+chord": [(0, 1), (1, 2), (2, 3), (3, 4), (0, 4), (1, 3)],
+    "swapped columns": [(1, 0), (2, 1), (0, 2), (3, 2)],
+}
+
+
+@pytest.mark.parametrize("name", list(GENERIC_QUERIES))
+@pytest.mark.parametrize("algo", ["DFS", "BFS"])
+def test_lftj_generic_queries_match_amhj_and_oracle(ctx, name, algo):
+    """Queries beyond the triangle (the reference's LFTJ stops at 3
+    attributes and 3 tables) run through the generic leapfrog join: equal to
+    AMHJ on the same relations and to the oracle."""
+    pats = GENERIC_QUERIES[name]
+    dom = 300 if len(pats) <= 4 else 120
+    rels = [distinct_rel(4000, dom, 40 + i, list(p)) for i, p in enumerate(pats)]
+    hs = [ctx.relation(c, a) for c, a in rels]
+    want = O.mhj(rels)
+    got = ctx.lftj(hs, algo=algo)
+    assert (got.count, got.checksum) == want
+    assert got.num_attrs == 1 + max(max(p) for p in pats)
+    amhj = ctx.amhj("NORMAL", hs)
+    assert (amhj.count, amhj.checksum) == want
+
+
+def test_lftj_generic_materialized_and_rejections(ctx):
+    rels = [distinct_rel(3000, 200, 60 + i, list(p)) for i, p in enumerate(GENERIC_QUERIES["4-cycle"])]
+    hs = [ctx.relation(c, a) for c, a in rels]
+    got = ctx.lftj(hs, materialize=True)
+    cnt, chk, cols = O.mhj(rels, tuples=True)
+    assert got.count == cnt and data.checksum(got.columns) == chk
+    assert np.array_equal(sorted_rows(got.columns), sorted_rows(cols))
+    # attribute 2 shares no relation with an earlier attribute: a cross product
+    bad = [ctx.relation(c, a) for c, a in [distinct_rel(100, 50, 1, [0, 1]), distinct_rel(100, 50, 2, [2, 3]),
+                                            distinct_rel(100, 50, 3, [1, 3])]]
+    with pytest.raises(AmjError) as e:
+        ctx.lftj(bad)
+    assert e.value.status == L.AMJ_EUNSUPPORTED
+    with pytest.raises(AmjError):
+        ctx.lftj(hs, ooc=1)
+
+
 def test_lftj_out_of_core_slices():
     with Context(0, ooc_slice_rows=5000) as ctx:
         s, d = data.rmat(11, 30000, 0.57, 0.19, 0.19, 7)
