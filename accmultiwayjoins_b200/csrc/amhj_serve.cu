@@ -26,6 +26,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -47,6 +48,7 @@ struct ServeReq {
     int state = 0;                   // 0 waiting, 1 running, 2 done
     uint32_t batch_id = 0, batch_size = 0;
     bool spilled = false;
+    std::string error;               // message of a failed request
 };
 
 // Indexes of the resident relations, kept for the server's lifetime and
@@ -149,6 +151,10 @@ uint64_t request_bytes(const HostPlan &hp, const amj_batch_opts &o) {
 
 void finish(amj_server *s, ServeReq *r, int status) {
     r->status = status;
+    if (status != AMJ_OK && r->error.empty()) {
+        const char *m = amj_last_error();   // the failing call ran on this thread
+        r->error = m ? m : "";
+    }
     r->t_done = s->now();
     r->state = 2;
     s->st.completed++;
@@ -203,6 +209,8 @@ void server_loop(amj_server *s) {
                     s->pending.pop_front();
                     if (!s->opts.ooc_lane) {
                         s->st.rejected++;
+                        r->error = "the request needs more device memory than the whole budget, and the server "
+                                   "has no out-of-core lane";
                         finish(s, r, AMJ_EREJECT);
                         s->cv_done.notify_all();
                         continue;
@@ -422,8 +430,9 @@ extern "C" int amj_server_wait(amj_server *s, uint64_t ticket, uint32_t timeout_
     out->batch_id = r->batch_id;
     out->batch_size = r->batch_size;
     const int status = r->status;
+    const std::string err = r->error;
     s->reqs.erase(it);
-    if (status != AMJ_OK) return fail(status, "server_wait: the request failed");
+    if (status != AMJ_OK) return fail(status, "server_wait: the request failed: " + err);
     return AMJ_OK;
 }
 

@@ -105,7 +105,7 @@ def test_admission_waits_for_memory_and_spills_what_never_fits():
         t = srv.submit("NORMAL", brels)
         with pytest.raises(AmjError) as e:
             srv.wait(t)
-        assert e.value.status == L.AMJ_EREJECT
+        assert e.value.status == L.AMJ_EREJECT and "budget" in str(e.value)
         assert srv.stats()["rejected"] == 1
         srv.close()
 
