@@ -214,6 +214,11 @@ SIGNATURES = {
     "amj_trie_save": (C.c_int, [_P, C.c_char_p, C.c_uint32, C.c_uint32]),
     "amj_trie_load": (C.c_int, [_P, C.c_char_p, C.POINTER(_P), _U32P, _U32P]),
     "amj_trie_release": (None, [_P]),
+    "amj_trie_build_n": (C.c_int, [_P, C.POINTER(_P), C.c_int, C.c_uint64, C.POINTER(_P)]),
+    "amj_trie_info": (C.c_int, [_P, C.POINTER(C.c_int), _U64P]),
+    "amj_trie_download_level": (C.c_int, [_P, C.c_int, _I32P, _U64P]),
+    "amj_trie_save_n": (C.c_int, [_P, C.c_char_p, _U32P]),
+    "amj_trie_load_n": (C.c_int, [_P, C.c_char_p, C.POINTER(_P), _U32P, C.POINTER(C.c_int)]),
     "amj_selftest_bounded_wait": (C.c_int, [_P, C.c_uint32]),
     "amj_gen_uniform_i32": (C.c_int, [_I32P, C.c_uint64, C.c_int64, C.c_int64, C.c_uint64, C.c_uint64]),
     "amj_gen_permutation_i32": (C.c_int, [_I32P, C.c_uint64, C.c_uint64, C.c_uint64]),

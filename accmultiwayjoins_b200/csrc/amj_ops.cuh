@@ -68,7 +68,29 @@ int finish_result_columns(amj_ctx *ctx, amj_result *res, int flags);
 
 }  // namespace amj
 
+namespace amj {
+constexpr int TRIE_MAX_LEVELS = 8;
+
+// N-level trie: level l holds the last values of the distinct (l+1)-prefixes
+// of the sorted rows, off[l] the offsets of their children in level l+1; the
+// last level is the sorted last column, duplicates kept.
+struct TrieN {
+    int levels = 0;
+    uint64_t len[TRIE_MAX_LEVELS] = {};
+    DBuf<int32_t> data[TRIE_MAX_LEVELS];
+    DBuf<uint64_t> off[TRIE_MAX_LEVELS - 1];
+};
+
+int build_trieN(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, uint64_t n, TrieN *out);
+}  // namespace amj
+
+// A trie handle: a 2-level trie (t, levels = 0 in tn) or an N-level one (tn).
 struct amj_trie {
     amj_ctx *ctx = nullptr;
     amj::Trie2 t;
+    amj::TrieN tn;
+    int levels() const { return tn.levels ? tn.levels : 2; }
+    uint64_t len(int l) const { return tn.levels ? tn.len[l] : (l == 0 ? t.len0 : t.len1); }
+    const int32_t *data(int l) const { return tn.levels ? tn.data[l].p : (l == 0 ? t.data0.p : t.data1.p); }
+    const uint64_t *off(int l) const { return tn.levels ? tn.off[l].p : t.off0.p; }
 };

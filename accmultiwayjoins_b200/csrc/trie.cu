@@ -14,6 +14,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 namespace amj {
 
@@ -165,9 +166,178 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
     return AMJ_OK;
 }
 
+// ---- N-level tries ----
+// Rows are ordered by a stable LSD radix sort of the row permutation, one
+// column at a time from the last: items (column value - min) << 32 | row,
+// sorted on the value bits only.  Then per level a head flag marks the rows
+// whose (l+1)-prefix differs from the previous row's, a scan numbers the
+// heads, and a scatter writes the level's values and child offsets.
+
+__global__ void minmax_col_kernel(const int32_t *__restrict__ c, uint64_t n, uint32_t *mm) {
+    uint32_t mn = 0xffffffffu, mx = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = (uint32_t)c[i] ^ 0x80000000u;
+        mn = min(mn, a);
+        mx = max(mx, a);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        mn = min(mn, __shfl_xor_sync(AMJ_FULL_MASK, mn, d));
+        mx = max(mx, __shfl_xor_sync(AMJ_FULL_MASK, mx, d));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&mm[0], mn);
+        atomicMax(&mm[1], mx);
+    }
+}
+
+__global__ void pack_col_kernel(const int32_t *__restrict__ c, const uint32_t *__restrict__ perm, uint64_t n,
+                                uint32_t mn, uint64_t *__restrict__ items) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = perm ? perm[i] : (uint32_t)i;
+        items[i] = ((uint64_t)(((uint32_t)c[r] ^ 0x80000000u) - mn) << 32) | r;
+    }
+}
+
+__global__ void perm_from_items_kernel(const uint64_t *__restrict__ items, uint64_t n, uint32_t *__restrict__ perm) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        perm[i] = (uint32_t)items[i];
+}
+
+__global__ void gather_perm_kernel(const int32_t *__restrict__ c, const uint32_t *__restrict__ perm, uint64_t n,
+                                   int32_t *__restrict__ out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = c[perm ? perm[i] : i];
+}
+
+// head[i] = 1 when row i's (l+1)-prefix differs from row i-1's
+__global__ void prefix_heads_kernel(int32_t *const *__restrict__ S, int l, uint64_t n, uint32_t *__restrict__ head) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        bool h = i == 0;
+        for (int c = 0; c <= l && !h; c++) h = S[c][i] != S[c][i - 1];
+        head[i] = h ? 1u : 0u;
+    }
+}
+
+// level l: values and child offsets at the heads' ranks
+__global__ void scatter_level_kernel(const int32_t *__restrict__ Sl, const uint32_t *__restrict__ head,
+                                     const uint32_t *__restrict__ rank, const uint32_t *__restrict__ next_rank,
+                                     uint64_t n, int32_t *__restrict__ data, uint64_t *__restrict__ off) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (!head[i]) continue;
+        const uint32_t r = rank[i];
+        data[r] = Sl[i];
+        off[r] = next_rank ? next_rank[i] : i;
+    }
+}
+
+int build_trieN(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, uint64_t n, TrieN *out) {
+    if (ncols < 1 || ncols > TRIE_MAX_LEVELS) return fail(AMJ_EINVAL, "trie_build_n: 1..8 columns");
+    if (n >= (1ull << 32)) return fail(AMJ_EUNSUPPORTED, "trie_build_n: 2^32 or more rows");
+    out->levels = ncols;
+    // sorted columns
+    std::vector<DBuf<int32_t>> S(ncols);
+    DBuf<uint32_t> perm;
+    if (n > 1) {
+        DBuf<uint64_t> a, b;
+        DBuf<uint32_t> mm;
+        AMJ_TRY(a.alloc(ctx, n));
+        AMJ_TRY(b.alloc(ctx, n));
+        AMJ_TRY(perm.alloc(ctx, n));
+        AMJ_TRY(mm.alloc(ctx, 2 * ncols));
+        std::vector<uint32_t> init(2 * ncols);
+        for (int c = 0; c < ncols; c++) {
+            init[2 * c] = 0xffffffffu;
+            init[2 * c + 1] = 0;
+        }
+        AMJ_CUDA_TRY(cudaMemcpyAsync(mm.p, init.data(), 8 * ncols, cudaMemcpyHostToDevice, ctx->stream));
+        for (int c = 0; c < ncols; c++) {
+            note_launch(ctx);
+            minmax_col_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_cols[c], n, mm.p + 2 * c);
+        }
+        AMJ_CUDA_TRY(cudaGetLastError());
+        std::vector<uint32_t> h(2 * ncols);
+        AMJ_CUDA_TRY(cudaMemcpyAsync(h.data(), mm.p, 8 * ncols, cudaMemcpyDeviceToHost, ctx->stream));
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        bool have_perm = false;
+        for (int c = ncols - 1; c >= 0; c--) {
+            const uint32_t range = h[2 * c + 1] - h[2 * c];
+            int bits = 0;
+            while (bits < 32 && (uint64_t)range >> bits) bits++;
+            if (bits == 0) continue;   // constant column: the order stays
+            note_launch(ctx);
+            pack_col_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_cols[c], have_perm ? perm.p : nullptr, n,
+                                                                      h[2 * c], a.p);
+            AMJ_CUDA_TRY(cudaGetLastError());
+            uint64_t *sorted = nullptr;
+            AMJ_TRY(radix_sort_u64(ctx, a.p, b.p, n, SK_IDENT, 32, 32 + bits, &sorted));
+            note_launch(ctx);
+            perm_from_items_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, perm.p);
+            AMJ_CUDA_TRY(cudaGetLastError());
+            have_perm = true;
+        }
+        if (!have_perm) perm.release();
+    }
+    for (int c = 0; c < ncols; c++) {
+        AMJ_TRY(S[c].alloc(ctx, n ? n : 1));
+        if (n) {
+            note_launch(ctx);
+            gather_perm_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_cols[c], perm.p, n, S[c].p);
+        }
+    }
+    AMJ_CUDA_TRY(cudaGetLastError());
+    // heads and ranks of every level but the last
+    const int L = ncols - 1;
+    std::vector<DBuf<uint32_t>> head(L), rank(L);
+    std::vector<uint32_t> cnt(L, 0);
+    DBuf<int32_t *> sp;
+    AMJ_TRY(sp.alloc(ctx, ncols));
+    std::vector<int32_t *> hp(ncols);
+    for (int c = 0; c < ncols; c++) hp[c] = S[c].p;
+    AMJ_CUDA_TRY(cudaMemcpyAsync(sp.p, hp.data(), ncols * sizeof(int32_t *), cudaMemcpyHostToDevice, ctx->stream));
+    DBuf<uint32_t> totals;
+    AMJ_TRY(totals.alloc(ctx, L ? L : 1));
+    for (int l = 0; l < L; l++) {
+        AMJ_TRY(head[l].alloc(ctx, n ? n : 1));
+        AMJ_TRY(rank[l].alloc(ctx, n ? n : 1));
+        if (n) {
+            note_launch(ctx);
+            prefix_heads_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sp.p, l, n, head[l].p);
+            AMJ_CUDA_TRY(cudaGetLastError());
+            AMJ_TRY(scan_exclusive_u32(ctx, head[l].p, rank[l].p, n, totals.p + l));
+        } else {
+            AMJ_CUDA_TRY(cudaMemsetAsync(totals.p + l, 0, 4, ctx->stream));
+        }
+    }
+    if (L) {
+        AMJ_CUDA_TRY(cudaMemcpyAsync(cnt.data(), totals.p, 4 * L, cudaMemcpyDeviceToHost, ctx->stream));
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    }
+    for (int l = 0; l < L; l++) {
+        out->len[l] = cnt[l];
+        AMJ_TRY(out->data[l].alloc(ctx, cnt[l] ? cnt[l] : 1));
+        AMJ_TRY(out->off[l].alloc(ctx, (uint64_t)cnt[l] + 1));
+        if (n) {
+            note_launch(ctx);
+            scatter_level_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(
+                S[l].p, head[l].p, rank[l].p, l + 1 < L ? rank[l + 1].p : nullptr, n, out->data[l].p, out->off[l].p);
+            AMJ_CUDA_TRY(cudaGetLastError());
+        }
+        const uint64_t end = l + 1 < L ? (uint64_t)cnt[l + 1] : n;
+        AMJ_CUDA_TRY(cudaMemcpyAsync(out->off[l].p + cnt[l], &end, 8, cudaMemcpyHostToDevice, ctx->stream));
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    }
+    out->len[L] = n;
+    out->data[L] = std::move(S[L]);
+    return AMJ_OK;
+}
+
 }  // namespace amj
 
 using namespace amj;
+
+extern "C" int amj_trie_download_level(const amj_trie *t, int level, int32_t *data, uint64_t *offsets);
+extern "C" int amj_trie_save_n(const amj_trie *t, const char *path, const uint32_t *attrs);
 
 extern "C" int amj_trie_build(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, amj_trie **out) {
     if (!ctx || !out || (n && (!d_c0 || !d_c1))) return fail(AMJ_EINVAL, "trie_build: null argument");
@@ -190,24 +360,20 @@ extern "C" int amj_trie_build(amj_ctx *ctx, const int32_t *d_c0, const int32_t *
 extern "C" int amj_trie_view(const amj_trie *t, uint64_t *len0, uint64_t *len1, const int32_t **d_data0,
                              const uint64_t **d_offsets0, const int32_t **d_data1) {
     if (!t) return fail(AMJ_EINVAL, "trie_view: null trie");
-    if (len0) *len0 = t->t.len0;
-    if (len1) *len1 = t->t.len1;
-    if (d_data0) *d_data0 = t->t.data0.p;
-    if (d_offsets0) *d_offsets0 = t->t.off0.p;
-    if (d_data1) *d_data1 = t->t.data1.p;
+    if (t->levels() != 2) return fail(AMJ_EINVAL, "trie_view: not a 2-level trie");
+    if (len0) *len0 = t->len(0);
+    if (len1) *len1 = t->len(1);
+    if (d_data0) *d_data0 = t->data(0);
+    if (d_offsets0) *d_offsets0 = t->off(0);
+    if (d_data1) *d_data1 = t->data(1);
     return AMJ_OK;
 }
 
 extern "C" int amj_trie_download(const amj_trie *t, int32_t *data0, uint64_t *offsets0, int32_t *data1) {
     if (!t || !data0 || !offsets0 || !data1) return fail(AMJ_EINVAL, "trie_download: null argument");
-    amj_ctx *ctx = t->ctx;
-    if (t->t.len0)
-        AMJ_CUDA_TRY(cudaMemcpyAsync(data0, t->t.data0.p, t->t.len0 * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    if (t->t.len1)
-        AMJ_CUDA_TRY(cudaMemcpyAsync(data1, t->t.data1.p, t->t.len1 * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaMemcpyAsync(offsets0, t->t.off0.p, (t->t.len0 + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return AMJ_OK;
+    if (t->levels() != 2) return fail(AMJ_EINVAL, "trie_download: not a 2-level trie");
+    AMJ_TRY(amj_trie_download_level(t, 0, data0, offsets0));
+    return amj_trie_download_level(t, 1, data1, nullptr);
 }
 
 extern "C" void amj_trie_release(amj_trie *t) {
@@ -222,24 +388,9 @@ extern "C" void amj_trie_release(amj_trie *t) {
 // (data_len[l]+1 entries each).
 extern "C" int amj_trie_save(const amj_trie *t, const char *path, uint32_t a0, uint32_t a1) {
     if (!t || !path) return fail(AMJ_EINVAL, "trie_save: null argument");
-    amj_ctx *ctx = t->ctx;
-    const uint64_t l0 = t->t.len0, l1 = t->t.len1;
-    std::vector<int32_t> d0(l0), d1(l1);
-    std::vector<uint64_t> o0(l0 + 1);
-    if (l0) AMJ_CUDA_TRY(cudaMemcpyAsync(d0.data(), t->t.data0.p, l0 * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    if (l1) AMJ_CUDA_TRY(cudaMemcpyAsync(d1.data(), t->t.data1.p, l1 * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaMemcpyAsync(o0.data(), t->t.off0.p, (l0 + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    FILE *f = std::fopen(path, "wb");
-    if (!f) return fail(AMJ_EIO, std::string("trie_save: cannot open ") + path);
-    const uint32_t na = 2;
-    const uint64_t lens[2] = {l0, l1};
+    if (t->levels() != 2) return fail(AMJ_EINVAL, "trie_save: not a 2-level trie");
     const uint32_t attrs[2] = {a0, a1};
-    bool ok = std::fwrite(&na, 4, 1, f) == 1 && std::fwrite(lens, 8, 2, f) == 2 && std::fwrite(attrs, 4, 2, f) == 2 &&
-              (l0 == 0 || std::fwrite(d0.data(), 4, l0, f) == l0) && (l1 == 0 || std::fwrite(d1.data(), 4, l1, f) == l1) &&
-              std::fwrite(o0.data(), 8, l0 + 1, f) == l0 + 1;
-    if (std::fclose(f) != 0) ok = false;
-    return ok ? AMJ_OK : fail(AMJ_EIO, std::string("trie_save: write failed for ") + path);
+    return amj_trie_save_n(t, path, attrs);
 }
 
 extern "C" int amj_trie_load(amj_ctx *ctx, const char *path, amj_trie **out, uint32_t *a0, uint32_t *a1) {
@@ -279,6 +430,125 @@ extern "C" int amj_trie_load(amj_ctx *ctx, const char *path, amj_trie **out, uin
     }
     if (a0) *a0 = attrs[0];
     if (a1) *a1 = attrs[1];
+    *out = t;
+    return AMJ_OK;
+}
+
+extern "C" int amj_trie_build_n(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, uint64_t n, amj_trie **out) {
+    if (!ctx || !out || !d_cols) return fail(AMJ_EINVAL, "trie_build_n: null argument");
+    if (ncols < 1 || ncols > TRIE_MAX_LEVELS) return fail(AMJ_EINVAL, "trie_build_n: 1..8 columns");
+    for (int c = 0; c < ncols && n; c++)
+        if (!d_cols[c]) return fail(AMJ_EINVAL, "trie_build_n: null column");
+    *out = nullptr;
+    auto *t = new amj_trie();
+    t->ctx = ctx;
+    int rc = build_trieN(ctx, d_cols, ncols, n, &t->tn);
+    if (rc == AMJ_OK) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "trie_build_n");
+    }
+    if (rc != AMJ_OK) {
+        delete t;
+        return rc;
+    }
+    *out = t;
+    return AMJ_OK;
+}
+
+extern "C" int amj_trie_info(const amj_trie *t, int *levels, uint64_t *lens) {
+    if (!t) return fail(AMJ_EINVAL, "trie_info: null trie");
+    if (levels) *levels = t->levels();
+    if (lens)
+        for (int l = 0; l < t->levels(); l++) lens[l] = t->len(l);
+    return AMJ_OK;
+}
+
+extern "C" int amj_trie_download_level(const amj_trie *t, int level, int32_t *data, uint64_t *offsets) {
+    if (!t || !data) return fail(AMJ_EINVAL, "trie_download_level: null argument");
+    if (level < 0 || level >= t->levels()) return fail(AMJ_EINVAL, "trie_download_level: no such level");
+    amj_ctx *ctx = t->ctx;
+    const uint64_t n = t->len(level);
+    if (n) AMJ_CUDA_TRY(cudaMemcpyAsync(data, t->data(level), n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (offsets && level + 1 < t->levels())
+        AMJ_CUDA_TRY(cudaMemcpyAsync(offsets, t->off(level), (n + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return AMJ_OK;
+}
+
+// .tr with any number of levels (same layout as amj_trie_save)
+extern "C" int amj_trie_save_n(const amj_trie *t, const char *path, const uint32_t *attrs) {
+    if (!t || !path || !attrs) return fail(AMJ_EINVAL, "trie_save_n: null argument");
+    const int L = t->levels();
+    std::vector<std::vector<int32_t>> d(L);
+    std::vector<std::vector<uint64_t>> o(L > 1 ? L - 1 : 0);
+    for (int l = 0; l < L; l++) {
+        d[l].resize(t->len(l));
+        if (l + 1 < L) o[l].resize(t->len(l) + 1);
+        AMJ_TRY(amj_trie_download_level(t, l, d[l].data(), l + 1 < L ? o[l].data() : nullptr));
+    }
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(AMJ_EIO, std::string("trie_save_n: cannot open ") + path);
+    const uint32_t na = (uint32_t)L;
+    bool ok = std::fwrite(&na, 4, 1, f) == 1;
+    for (int l = 0; l < L && ok; l++) {
+        const uint64_t len = t->len(l);
+        ok = std::fwrite(&len, 8, 1, f) == 1;
+    }
+    ok = ok && std::fwrite(attrs, 4, L, f) == (size_t)L;
+    for (int l = 0; l < L && ok; l++) ok = d[l].empty() || std::fwrite(d[l].data(), 4, d[l].size(), f) == d[l].size();
+    for (int l = 0; l + 1 < L && ok; l++) ok = std::fwrite(o[l].data(), 8, o[l].size(), f) == o[l].size();
+    if (std::fclose(f) != 0) ok = false;
+    return ok ? AMJ_OK : fail(AMJ_EIO, std::string("trie_save_n: write failed for ") + path);
+}
+
+extern "C" int amj_trie_load_n(amj_ctx *ctx, const char *path, amj_trie **out, uint32_t *attrs, int *levels) {
+    if (!ctx || !path || !out) return fail(AMJ_EINVAL, "trie_load_n: null argument");
+    *out = nullptr;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(AMJ_EIO, std::string("trie_load_n: cannot open ") + path);
+    uint32_t na = 0;
+    uint64_t lens[TRIE_MAX_LEVELS] = {};
+    uint32_t at[TRIE_MAX_LEVELS] = {};
+    bool ok = std::fread(&na, 4, 1, f) == 1 && na >= 1 && na <= (uint32_t)TRIE_MAX_LEVELS &&
+              std::fread(lens, 8, na, f) == na && std::fread(at, 4, na, f) == na;
+    std::vector<std::vector<int32_t>> d(ok ? na : 0);
+    std::vector<std::vector<uint64_t>> o(ok && na > 1 ? na - 1 : 0);
+    for (uint32_t l = 0; ok && l < na; l++) {
+        d[l].resize(lens[l]);
+        ok = lens[l] == 0 || std::fread(d[l].data(), 4, lens[l], f) == lens[l];
+    }
+    for (uint32_t l = 0; ok && l + 1 < na; l++) {
+        o[l].resize(lens[l] + 1);
+        ok = std::fread(o[l].data(), 8, lens[l] + 1, f) == lens[l] + 1 && o[l][lens[l]] == lens[l + 1];
+    }
+    std::fclose(f);
+    if (!ok) return fail(AMJ_EIO, "trie_load_n: bad, truncated or inconsistent file");
+    auto *t = new amj_trie();
+    t->ctx = ctx;
+    t->tn.levels = (int)na;
+    int rc = AMJ_OK;
+    for (uint32_t l = 0; rc == AMJ_OK && l < na; l++) {
+        t->tn.len[l] = lens[l];
+        rc = t->tn.data[l].alloc(ctx, lens[l] ? lens[l] : 1);
+        if (rc == AMJ_OK && lens[l] &&
+            cudaMemcpyAsync(t->tn.data[l].p, d[l].data(), lens[l] * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+            rc = AMJ_ECUDA;
+        if (rc == AMJ_OK && l + 1 < na) {
+            rc = t->tn.off[l].alloc(ctx, lens[l] + 1);
+            if (rc == AMJ_OK && cudaMemcpyAsync(t->tn.off[l].p, o[l].data(), (lens[l] + 1) * 8, cudaMemcpyHostToDevice,
+                                                ctx->stream) != cudaSuccess)
+                rc = AMJ_ECUDA;
+        }
+    }
+    if (rc == AMJ_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = AMJ_ECUDA;
+    if (rc != AMJ_OK) {
+        (void)cudaGetLastError();
+        delete t;
+        return rc == AMJ_ECUDA ? fail(rc, "trie_load_n: device copy failed") : rc;
+    }
+    if (attrs)
+        for (uint32_t l = 0; l < na; l++) attrs[l] = at[l];
+    if (levels) *levels = (int)na;
     *out = t;
     return AMJ_OK;
 }

@@ -327,6 +327,23 @@ int  amj_trie_save(const amj_trie *t, const char *path, uint32_t a0, uint32_t a1
 int  amj_trie_load(amj_ctx *ctx, const char *path, amj_trie **out, uint32_t *a0, uint32_t *a1);
 void amj_trie_release(amj_trie *t);
 
+/* N-level tries (1..8 columns), the general IndexedTrie of the reference
+ * (LFTJ-GPU/IndexedTrie.cuh:21-209, built by constructSortedTrie for any
+ * number of attributes, multi_partitioning.cuh:129-293): level l holds the
+ * last values of the distinct (l+1)-prefixes of the lexicographically sorted
+ * rows and, except for the last level, the u64 offsets of their children in
+ * level l+1 (len[l] + 1 entries); the last level is the sorted last column,
+ * duplicates kept.  amj_trie_info / download_level / save_n also accept the
+ * 2-level tries of amj_trie_build and amj_trie_load; the .tr layout is the
+ * one of amj_trie_save with num_attrs levels. */
+int  amj_trie_build_n(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, uint64_t n,
+                      amj_trie **out);
+int  amj_trie_info(const amj_trie *t, int *levels, uint64_t *lens /* [8] */);
+int  amj_trie_download_level(const amj_trie *t, int level, int32_t *data, uint64_t *offsets);
+int  amj_trie_save_n(const amj_trie *t, const char *path, const uint32_t *attrs /* [levels] */);
+int  amj_trie_load_n(amj_ctx *ctx, const char *path, amj_trie **out, uint32_t *attrs /* [8] */,
+                     int *levels);
+
 /* ---- failure detection self-test ----
  * Launches a kernel that waits on a device flag nothing sets.  The wait is
  * bounded by limit_ms (%globaltimer); the call must return AMJ_ETIMEOUT and

@@ -17,6 +17,10 @@
  *                    order (what RadixPartitioner::splitKI produces up to the
  *                    order inside a bucket, MHJ-GPU/Indexing/radix_partitioning.cuh:508-578)
  *  orc_trie_build    2-level IndexedTrie (LFTJ-GPU/multi_partitioning.cuh:129-293)
+ *  orc_trie_build_n  the same for 1..8 columns: rows sorted lexicographically;
+ *                    level l holds the distinct (l+1)-prefixes' last values and
+ *                    the offsets of their children in level l+1; the last level
+ *                    is the sorted last column, duplicates kept
  *  orc_mhj           multi-way hash join, depth-first with backtracking per
  *                    probe row (MHJ-CPU/MHJ.cpp:176-279) comparing every bound
  *                    attribute (the multi-key compare of
@@ -78,6 +82,56 @@ static int64_t pack_pair(int32_t a, int32_t b) {
 }
 static int32_t pair_c0(int64_t p) { return (int32_t)(uint32_t)((uint64_t)p >> 32); }
 static int32_t pair_c1(int64_t p) { return (int32_t)((uint32_t)(uint64_t)p ^ 0x80000000u); }
+
+/* lexicographic order of rows over ncols columns (qsort context through a static) */
+static const int32_t *const *g_tn_cols;
+static int g_tn_ncols;
+static int cmp_rows(const void *a, const void *b) {
+    const uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+    for (int c = 0; c < g_tn_ncols; c++) {
+        const int32_t u = g_tn_cols[c][x], v = g_tn_cols[c][y];
+        if (u != v) return u < v ? -1 : 1;
+    }
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* data[l] must hold n values and off[l] n + 1 (l < ncols - 1); len[l] gets
+   the number of values of level l.  Not reentrant (qsort context). */
+int orc_trie_build_n(const int32_t *const *cols, int ncols, uint64_t n, int32_t *const *data, uint64_t *const *off,
+                     uint64_t *len) {
+    if (ncols < 1 || ncols > ORC_MAX_ATTRS) return -1;
+    uint64_t *perm = (uint64_t *)malloc((n ? n : 1) * sizeof(uint64_t));
+    if (!perm) return -2;
+    for (uint64_t i = 0; i < n; i++) perm[i] = i;
+    g_tn_cols = cols;
+    g_tn_ncols = ncols;
+    qsort(perm, n, sizeof(uint64_t), cmp_rows);
+    /* cnt[l]: nodes of level l so far */
+    uint64_t cnt[ORC_MAX_ATTRS] = {0};
+    for (uint64_t i = 0; i < n; i++) {
+        int changed = i == 0;
+        for (int l = 0; l < ncols; l++) {
+            if (!changed && cols[l][perm[i]] != cols[l][perm[i - 1]]) changed = 1;
+            if (l == ncols - 1) {
+                data[l][i] = cols[l][perm[i]];
+                continue;
+            }
+            if (changed) {
+                /* a new node at level l; its first child is the next node of level l+1 */
+                data[l][cnt[l]] = cols[l][perm[i]];
+                off[l][cnt[l]] = (l + 1 == ncols - 1) ? i : cnt[l + 1];
+                cnt[l]++;
+            }
+        }
+    }
+    for (int l = 0; l + 1 < ncols; l++) {
+        off[l][cnt[l]] = (l + 1 == ncols - 1) ? n : cnt[l + 1];
+        len[l] = cnt[l];
+    }
+    len[ncols - 1] = n;
+    free(perm);
+    return 0;
+}
 
 int orc_trie_build(const int32_t *c0, const int32_t *c1, uint64_t n, int32_t *data0, uint64_t *off0, int32_t *data1,
                    uint64_t *len0) {

@@ -140,6 +140,24 @@ def four_clique(src, dst, nthreads=0):
     return cnt.value, chk.value
 
 
+def trie_build_n(cols):
+    """N-level trie of the columns: (data per level, offsets per level but the last)."""
+    lib = orc()
+    cols = [np.ascontiguousarray(c, np.int32) for c in cols]
+    k, n = len(cols), cols[0].shape[0]
+    data = [np.empty(max(n, 1), np.int32) for _ in range(k)]
+    off = [np.empty(n + 1, np.uint64) for _ in range(k - 1)] or [np.empty(1, np.uint64)]
+    lens = (C.c_uint64 * k)()
+    cp = (C.POINTER(C.c_int32) * k)(*[_i32p(c) for c in cols])
+    dp = (C.POINTER(C.c_int32) * k)(*[_i32p(d) for d in data])
+    op = (C.POINTER(C.c_uint64) * max(1, k - 1))(*[o.ctypes.data_as(C.POINTER(C.c_uint64)) for o in off])
+    rc = lib.orc_trie_build_n(cp, k, n, dp, op, lens)
+    if rc != 0:
+        raise ValueError(f"orc_trie_build_n failed ({rc})")
+    lens = [int(lens[i]) for i in range(k)]
+    return [data[l][:lens[l]].copy() for l in range(k)], [off[l][:lens[l] + 1].copy() for l in range(k - 1)]
+
+
 def trie_build(c0, c1):
     lib = orc()
     c0 = np.ascontiguousarray(c0, np.int32)

@@ -141,6 +141,54 @@ def test_trie_build_oracle_is_a_csr(built):
     assert np.array_equal(np.diff(o0.astype(np.int64)), counts)
 
 
+def trie_levels_by_definition(cols):
+    """Level l = last values of the distinct (l+1)-prefixes of the sorted rows;
+    offsets of level l = first row-rank of each prefix's children in level l+1."""
+    a = np.stack([np.asarray(c, np.int64) for c in cols], 1)
+    a = a[np.lexsort(a.T[::-1])] if len(a) else a
+    k = a.shape[1]
+    data, off = [], []
+    prefixes = []
+    for l in range(k - 1):
+        heads = np.ones(len(a), bool)
+        if len(a):
+            heads[1:] = np.any(a[1:, :l + 1] != a[:-1, :l + 1], axis=1)
+        prefixes.append(heads)
+        data.append(a[heads, l].astype(np.int32))
+    data.append(a[:, k - 1].astype(np.int32))
+    for l in range(k - 1):
+        nxt = np.cumsum(prefixes[l + 1]) - 1 if l + 1 < k - 1 else np.arange(len(a))
+        starts = nxt[prefixes[l]].astype(np.uint64)
+        end = prefixes[l + 1].sum() if l + 1 < k - 1 else len(a)
+        off.append(np.append(starts, np.uint64(end)))
+    return data, off
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5])
+def test_trie_build_n_oracle_by_definition(built, k):
+    rng = np.random.Generator(np.random.PCG64(k))
+    n = 3000
+    cols = [rng.integers(-4, 4, n).astype(np.int32) for _ in range(k)]
+    cols[0][::7] = -(1 << 31)
+    data, off = O.trie_build_n(cols)
+    wd, wo = trie_levels_by_definition(cols)
+    assert len(data) == k and len(off) == k - 1
+    for a, b in zip(data, wd):
+        assert np.array_equal(a, b)
+    for a, b in zip(off, wo):
+        assert np.array_equal(a, b)
+    if k == 2:
+        d0, o0, d1 = O.trie_build(cols[0], cols[1])
+        assert np.array_equal(d0, data[0]) and np.array_equal(o0, off[0]) and np.array_equal(d1, data[1])
+
+
+def test_trie_build_n_oracle_small_example(built):
+    c = [np.array(x, np.int32) for x in ([3, 1, 2, 3, 2, 3], [5, 2, 4, 5, 9, 1], [1, 8, 8, 0, 7, 2])]
+    data, off = O.trie_build_n(c)
+    assert [list(d) for d in data] == [[1, 2, 3], [2, 4, 9, 1, 5], [8, 8, 7, 2, 0, 1]]
+    assert [list(o) for o in off] == [[0, 1, 3, 5], [0, 1, 2, 3, 4, 6]]
+
+
 def test_bucket_build_oracle(built):
     keys = data.uniform(5000, -1000, 1000, seed=3)
     hk, idx, bp = O.bucket_build(keys, 1024)

@@ -101,6 +101,99 @@ def test_trie_tr_file_round_trip(ctx, tmp_path):
     lib.amj_trie_release(h2)
 
 
+def trie_n_levels(h):
+    lib = L.load()
+    lv = C.c_int()
+    lens = (C.c_uint64 * 8)()
+    L.check(lib.amj_trie_info(h, C.byref(lv), lens))
+    data, off = [], []
+    for l in range(lv.value):
+        d = np.empty(max(lens[l], 1), np.int32)
+        o = np.empty(lens[l] + 1, np.uint64)
+        last = l + 1 == lv.value
+        L.check(lib.amj_trie_download_level(h, l, d.ctypes.data_as(C.POINTER(C.c_int32)),
+                                            None if last else o.ctypes.data_as(C.POINTER(C.c_uint64))))
+        data.append(d[:lens[l]])
+        if not last:
+            off.append(o)
+    return data, off
+
+
+def trie_n_build(ctx, cols):
+    import torch
+    dc = [torch.from_numpy(np.ascontiguousarray(c, np.int32)).cuda() for c in cols]
+    n = len(cols[0])
+    ptrs = (C.c_void_p * len(cols))(*[c.data_ptr() if n else None for c in dc])
+    h = C.c_void_p()
+    L.check(L.load().amj_trie_build_n(ctx.handle, ptrs, len(cols), n, C.byref(h)))
+    return h
+
+
+@pytest.mark.parametrize("k,n,case", [(1, 1000, "narrow"), (2, 1 << 20, "rmat"), (3, 200000, "narrow"),
+                                      (3, 2_000_000, "wide"), (4, 100000, "const"), (5, 300000, "narrow"),
+                                      (3, 0, "empty"), (4, 1, "one"), (8, 5000, "narrow")])
+def test_trie_build_n_matches_oracle(ctx, k, n, case):
+    rng = np.random.Generator(np.random.PCG64(k * 7 + n))
+    if case == "rmat":
+        cols = list(data.rmat(16, n, 0.57, 0.19, 0.19, 3))
+    elif case == "wide":
+        cols = [rng.integers(-(1 << 31), 1 << 31, n, dtype=np.int64).astype(np.int32) for _ in range(k)]
+        cols[1][::2] = cols[1][0]
+    else:
+        cols = [rng.integers(-3, 6, n).astype(np.int32) for _ in range(k)]
+        if case == "const":
+            cols[2][:] = 77
+            cols[0][:] = -(1 << 31)
+    h = trie_n_build(ctx, cols)
+    got_d, got_o = trie_n_levels(h)
+    L.load().amj_trie_release(h)
+    want_d, want_o = O.trie_build_n(cols)
+    assert len(got_d) == k and len(got_o) == k - 1
+    for a, b in zip(got_d, want_d):
+        assert np.array_equal(a, b)
+    for a, b in zip(got_o, want_o):
+        assert np.array_equal(a, b)
+
+
+def test_trie_n_tr_file_round_trip_and_2_level_compatibility(ctx, tmp_path):
+    lib = L.load()
+    rng = np.random.Generator(np.random.PCG64(9))
+    cols = [rng.integers(0, 50, 40000).astype(np.int32) for _ in range(4)]
+    h = trie_n_build(ctx, cols)
+    p = str(tmp_path / "t4.tr").encode()
+    attrs = (C.c_uint32 * 4)(3, 0, 2, 1)
+    L.check(lib.amj_trie_save_n(h, p, attrs))
+    h2, got_attrs, lv = C.c_void_p(), (C.c_uint32 * 8)(), C.c_int()
+    L.check(lib.amj_trie_load_n(ctx.handle, p, C.byref(h2), got_attrs, C.byref(lv)))
+    assert lv.value == 4 and list(got_attrs)[:4] == [3, 0, 2, 1]
+    a, b = trie_n_levels(h), trie_n_levels(h2)
+    assert all(np.array_equal(x, y) for x, y in zip(a[0] + a[1], b[0] + b[1]))
+    # 2-level calls refuse a 4-level trie
+    with pytest.raises(AmjError):
+        L.check(lib.amj_trie_save(h, p, 0, 1))
+    lib.amj_trie_release(h)
+    lib.amj_trie_release(h2)
+    # a 2-level trie written by either writer is the same file, and both readers read it
+    s, d = data.rmat(10, 8000, 0.57, 0.19, 0.19, 4)
+    h2l, _, _, _ = trie_arrays(ctx, s, d)
+    hn = trie_n_build(ctx, [s, d])
+    p1, p2 = str(tmp_path / "a.tr").encode(), str(tmp_path / "b.tr").encode()
+    L.check(lib.amj_trie_save(h2l, p1, 5, 6))
+    L.check(lib.amj_trie_save_n(hn, p2, (C.c_uint32 * 2)(5, 6)))
+    assert open(p1, "rb").read() == open(p2, "rb").read()
+    h3 = C.c_void_p()
+    L.check(lib.amj_trie_load_n(ctx.handle, p1, C.byref(h3), None, None))
+    a, b = trie_n_levels(h2l), trie_n_levels(h3)
+    assert all(np.array_equal(x, y) for x, y in zip(a[0] + a[1], b[0] + b[1]))
+    # the 2-level download of an N-level trie with two levels
+    l0, l1 = C.c_uint64(), C.c_uint64()
+    L.check(lib.amj_trie_view(hn, C.byref(l0), C.byref(l1), None, None, None))
+    o0, oo, o1 = O.trie_build(s, d)
+    assert (l0.value, l1.value) == (len(o0), len(o1))
+    for x in (h2l, hn, h3):
+        lib.amj_trie_release(x)
+
+
 # ------------------------------------------------------------------- AMHJ
 
 SWITCHES = [dict(ws=0, dro=0, fib=0), dict(ws=1, dro=0, fib=0), dict(ws=0, dro=1, fib=0), dict(ws=1, dro=1, fib=0),
