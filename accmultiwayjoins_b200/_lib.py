@@ -54,6 +54,7 @@ class amj_opts(C.Structure):
         ("lftj_heavy_degree", C.c_uint32),
         ("dro_headroom", C.c_float),
         ("max_blocks", C.c_uint32),
+        ("lftj_rank_bits", C.c_uint32),
     ]
 
 

@@ -308,7 +308,8 @@ class Context:
 
     def __init__(self, device: int = 0, layout: str = "bucket", load_factor: float = 0.5, task_chunk: int = 1024,
                  spin_limit_ms: int = 5000, task_capacity: int = 1 << 22, ooc_slice_rows: int = 0,
-                 mem_budget: int = 0, lftj_heavy_degree: int = 0, dro_headroom: float = 0.0, max_blocks: int = 0):
+                 mem_budget: int = 0, lftj_heavy_degree: int = 0, dro_headroom: float = 0.0, max_blocks: int = 0,
+                 lftj_rank_bits: int = 0):
         lib = L.load()
         o = L.amj_opts()
         o.block_size = 256
@@ -322,6 +323,7 @@ class Context:
         o.lftj_heavy_degree = lftj_heavy_degree
         o.dro_headroom = dro_headroom
         o.max_blocks = max_blocks
+        o.lftj_rank_bits = lftj_rank_bits
         h = C.c_void_p()
         self.handle = None
         self._relations = weakref.WeakSet()

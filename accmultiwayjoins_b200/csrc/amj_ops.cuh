@@ -63,6 +63,11 @@ double event_ms(cudaEvent_t a, cudaEvent_t b);
 int degree_ordered_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *ns,
                         DBuf<int32_t> *nd, bool *oriented);
 
+// The same copy with every vertex renamed to its rank in (degree, id) order:
+// edges (rank lo, rank hi), *inv[rank] = the vertex id, *nv ranks.
+int degree_ranked_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *ns,
+                       DBuf<int32_t> *nd, DBuf<int32_t> *inv, uint64_t *nv, bool *oriented);
+
 // copy materialised device result columns to pinned host memory (when asked)
 int finish_result_columns(amj_ctx *ctx, amj_result *res, int flags);
 

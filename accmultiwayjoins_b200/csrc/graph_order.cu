@@ -83,4 +83,87 @@ int degree_ordered_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint
     return AMJ_OK;
 }
 
+// key (degree << idbits | id) of every vertex id in [0, nv)
+__global__ void rank_keys_kernel(const unsigned int *__restrict__ deg, uint64_t nv, int idbits,
+                                 uint64_t *__restrict__ keys) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nv; i += (uint64_t)gridDim.x * blockDim.x)
+        keys[i] = ((uint64_t)deg[i] << idbits) | i;
+}
+
+// rank[id] and inv[rank] from the sorted keys
+__global__ void rank_scatter_kernel(const uint64_t *__restrict__ sorted, uint64_t nv, int idbits,
+                                    int32_t *__restrict__ rank, int32_t *__restrict__ inv) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nv; i += (uint64_t)gridDim.x * blockDim.x) {
+        const int32_t id = (int32_t)(sorted[i] & ((1ull << idbits) - 1));
+        inv[i] = id;
+        rank[id] = (int32_t)i;
+    }
+}
+
+__global__ void rank_edges_kernel(const int32_t *__restrict__ s, const int32_t *__restrict__ d, uint64_t n,
+                                  const int32_t *__restrict__ rank, int32_t *__restrict__ ns, int32_t *__restrict__ nd) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const int32_t ru = rank[s[i]], rv = rank[d[i]];
+        ns[i] = ru < rv ? ru : rv;
+        nd[i] = ru < rv ? rv : ru;
+    }
+}
+
+int degree_ranked_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *ns,
+                       DBuf<int32_t> *nd, DBuf<int32_t> *inv, uint64_t *nv, bool *oriented) {
+    *oriented = false;
+    *nv = 0;
+    if (n == 0) return AMJ_OK;
+    struct Probe {
+        unsigned int bad;
+        int maxv;
+    };
+    DBuf<Probe> pr;
+    AMJ_TRY(pr.alloc(ctx, 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(pr.p, 0, sizeof(Probe), ctx->stream));
+    const unsigned g = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 16);
+    note_launch(ctx);
+    orient_check_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, &pr.p->bad, &pr.p->maxv);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    Probe h;
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&h, pr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (h.bad) return AMJ_OK;
+    const uint64_t V = (uint64_t)h.maxv + 1;
+    DBuf<unsigned int> deg;
+    AMJ_TRY(deg.alloc(ctx, V));
+    AMJ_CUDA_TRY(cudaMemsetAsync(deg.p, 0, V * sizeof(unsigned int), ctx->stream));
+    note_launch(ctx);
+    degree_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, deg.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    DBuf<uint64_t> ka, kb;
+    AMJ_TRY(ka.alloc(ctx, V));
+    AMJ_TRY(kb.alloc(ctx, V));
+    const unsigned gv = (unsigned)std::min<uint64_t>((V + 255) / 256, (uint64_t)ctx->num_sms * 16);
+    // a vertex has degree at most 2n: keys of idbits + degbits bits
+    int idbits = 1, degbits = 1;
+    while (idbits < 31 && (V - 1) >> idbits) idbits++;
+    while ((2 * n) >> degbits) degbits++;
+    if (idbits + degbits > 64) return fail(AMJ_EUNSUPPORTED, "degree ranks: relation too large");
+    note_launch(ctx);
+    rank_keys_kernel<<<gv, 256, 0, ctx->stream>>>(deg.p, V, idbits, ka.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    uint64_t *sorted = nullptr;
+    AMJ_TRY(radix_sort_u64(ctx, ka.p, kb.p, V, SK_IDENT, 0, idbits + degbits, &sorted));
+    DBuf<int32_t> rank;
+    AMJ_TRY(rank.alloc(ctx, V));
+    AMJ_TRY(inv->alloc(ctx, V));
+    note_launch(ctx);
+    rank_scatter_kernel<<<gv, 256, 0, ctx->stream>>>(sorted, V, idbits, rank.p, inv->p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_TRY(ns->alloc(ctx, n));
+    AMJ_TRY(nd->alloc(ctx, n));
+    note_launch(ctx);
+    rank_edges_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, rank.p, ns->p, nd->p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    *nv = V;
+    *oriented = true;
+    return AMJ_OK;
+}
+
 }  // namespace amj

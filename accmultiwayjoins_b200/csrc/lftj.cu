@@ -48,11 +48,19 @@ struct TriArgs {
     // heavy_deg children whose T-children span at most bitmap_bits values
     TrieRef R;
     uint64_t r_lo, r_hi;          // R level-1 slice handled by this launch
-    unsigned long long *cursor0;  // level-0 claim cursor of the bitmap kernel
+    unsigned long long *cursor0;  // claim cursor of the bitmap kernel over heavy_list
+    const uint32_t *heavy_list;   // R's level-0 indexes of the heavy vertices
+    const unsigned long long *heavy_n;
     uint32_t heavy_deg;           // 0: no bitmap kernel
     uint32_t bitmap_bits;
     int sorted_out;               // the tries hold a degree-ordered copy of an oriented relation:
                                   // every triangle is listed with its values in increasing order
+    // rank kernel: the tries hold the degree-ranked copy (vertex = rank in
+    // (degree, id) order); inv[rank] is the vertex id
+    const int32_t *inv;
+    uint32_t rank_base;           // first rank of the per-warp bitmap
+    uint32_t rank_bits;           // ranks the bitmap covers
+    unsigned long long *cursor_r; // claim cursor of the rank kernel
 };
 
 // A triangle found as (a, b, c) in the tuple the query lists: attribute order,
@@ -69,6 +77,12 @@ __device__ __forceinline__ void tri_order(const TriArgs &A, int32_t &a, int32_t 
 // checksum term of the triangle (a, b, c); hab is the hash of (a, b)
 __device__ __forceinline__ uint64_t tri_chk(const TriArgs &A, uint64_t hab, int32_t a, int32_t b, int32_t c) {
     if (!A.sorted_out) return amj_hash_step(hab, c);
+    tri_order(A, a, b, c);
+    return amj_hash_step(amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a), b), c);
+}
+
+// checksum term of the triangle (a, b, c) from scratch
+__device__ __forceinline__ uint64_t tri_chk3(const TriArgs &A, int32_t a, int32_t b, int32_t c) {
     tri_order(A, a, b, c);
     return amj_hash_step(amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a), b), c);
 }
@@ -90,6 +104,20 @@ __device__ __forceinline__ bool heavy_vertex(const TriArgs &A, uint64_t r_deg, u
     const int64_t sp = (int64_t)A.T.data1[ea - 1] - (int64_t)lo + 1;
     span = (uint32_t)sp;
     return sp > 0 && sp <= (int64_t)A.bitmap_bits;
+}
+
+// R's level-0 indexes of the vertices the bitmap kernel owns, in any order
+__global__ void heavy_list_kernel(const __grid_constant__ TriArgs A, uint32_t *list, unsigned long long *n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < A.R.len0;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t rs = A.R.off0[i], re = A.R.off0[i + 1];
+        if ((rs > A.r_lo ? rs : A.r_lo) >= (re < A.r_hi ? re : A.r_hi)) continue;
+        uint64_t ta, ea;
+        child_range(A.T, A.R.data0[i], ta, ea);
+        int32_t lo;
+        uint32_t span;
+        if (heavy_vertex(A, re - rs, ta, ea, lo, span)) list[atomicAdd(n, 1ull)] = (uint32_t)i;
+    }
 }
 
 constexpr int BM_THREADS = 1024;
@@ -123,7 +151,10 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
     unsigned long long cnt = 0, chk = 0;
     __syncthreads();
     while (true) {
-        if (tid == 0) s_i = atomicAdd(A.cursor0, 1ull);
+        if (tid == 0) {
+            const unsigned long long x = atomicAdd(A.cursor0, 1ull);
+            s_i = x < *A.heavy_n ? A.heavy_list[x] : ~0ull;
+        }
         __syncthreads();
         const unsigned long long i = s_i;
         __syncthreads();
@@ -253,6 +284,187 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
             bits[r >> 5] = 0u;
         }
         __syncthreads();
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if (lane == 0 && cnt) {
+        atomicAdd(A.count, cnt);
+        atomicAdd(A.checksum, chk);
+    }
+}
+
+// ---- rank kernel ----
+// The degree-ranked copy of an oriented edge relation: every vertex renamed
+// to its rank in (degree, id) order, edges from the lower to the higher
+// rank.  Out-neighbours then concentrate on the highest ranks (on R-MAT
+// scale 20, 99.8% of the values the lookups see lie in the top 32K ranks), so
+// each warp keeps a bitmap of the top rank_bits ranks (4 KB) and a lookup is
+// one shared-memory load and a bit test.  Persistent warps claim 32 level-1
+// entries (a, b) of R at a time.  For each run of one a among them, the
+// children T(a) set their bits (those below the bitmap, a sorted prefix of
+// T(a), are copied to shared memory); then the children S(b) of each b of
+// the run stream through the warp, TR_UNROLL x 32 values per step with all
+// loads issued before the tests.  A value below the bitmap is looked up by
+// binary search in T(a)'s low prefix.  Hits go to a per-warp queue of
+// (c, entry) pairs; the id mapping, the checksum and the writes run on 32
+// queued triangles at a time, so lanes without a hit do not wait on them.
+constexpr int TR_THREADS = 256;
+constexpr int TR_WARPS = TR_THREADS / 32;
+constexpr uint32_t TR_BITS = 32768;            // bitmap ranks per warp (the most)
+constexpr int TR_LOWCAP = 256;                 // low prefix entries kept in shared memory
+constexpr int TR_UNROLL = 8;
+constexpr int TR_QCAP = 512;                   // queued hits per warp (ring)
+
+struct TrWarp {
+    uint32_t bm[TR_BITS / 32];
+    int32_t low[TR_LOWCAP];
+    int2 q[TR_QCAP];   // (c, lane of the entry)
+};
+constexpr size_t TR_SMEM = TR_WARPS * sizeof(TrWarp);
+static_assert(sizeof(TrWarp) % 16 == 0, "TrWarp keeps 16-byte alignment");
+
+__device__ __forceinline__ bool tr_sorted_find(const int32_t *v, uint64_t n, int32_t c) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (v[mid] < c) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && v[lo] == c;
+}
+
+template <bool WRITE>
+__global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_rank_kernel(const __grid_constant__ TriArgs A) {
+    extern __shared__ __align__(16) unsigned char tr_smem[];
+    const int lane = threadIdx.x & 31;
+    TrWarp &W = ((TrWarp *)tr_smem)[threadIdx.x >> 5];
+    const uint32_t base = A.rank_base, nbits = A.rank_bits;
+    for (uint32_t k = lane; k < TR_BITS / 32; k += 32) W.bm[k] = 0u;
+    __syncwarp();
+    unsigned long long cnt = 0, chk = 0;
+    uint32_t qh = 0, qn = 0;   // queue head and length
+    int32_t ja = 0, jb = 0;    // this lane's entry of the current chunk (ranks)
+    int32_t ida = 0, idb = 0;  // and its vertex ids
+    // the first n queued hits, one per lane
+    auto flush = [&](uint32_t n) {
+        __syncwarp();
+        const bool mine = (uint32_t)lane < n;
+        const int2 e = mine ? W.q[(qh + lane) & (TR_QCAP - 1)] : make_int2(0, 0);
+        const int32_t a = __shfl_sync(AMJ_FULL_MASK, ida, e.y);
+        const int32_t b = __shfl_sync(AMJ_FULL_MASK, idb, e.y);
+        __syncwarp();
+        const int32_t c = mine ? A.inv[e.x] : 0;
+        if (WRITE) {
+            unsigned long long at = 0;
+            if (lane == 0) at = atomicAdd(A.out_cursor, (unsigned long long)n);
+            at = __shfl_sync(AMJ_FULL_MASK, at, 0);
+            if (mine && at + lane < A.out_cap) tri_store(A, at + lane, a, b, c);
+        }
+        if (mine) {
+            cnt++;
+            chk += tri_chk3(A, a, b, c);
+        }
+        qh = (qh + n) & (TR_QCAP - 1);
+        qn -= n;
+    };
+    while (true) {
+        unsigned long long at = 0;
+        if (lane == 0) at = atomicAdd(A.cursor_r, 32ull);
+        at = __shfl_sync(AMJ_FULL_MASK, at, 0);
+        if (at >= A.r_n) break;
+        const uint64_t j = at + lane;
+        const bool valid = j < A.r_n;
+        ja = valid ? A.r_src[j] : 0;
+        jb = valid ? A.r_dst[j] : 0;
+        ida = valid ? A.inv[ja] : 0;
+        idb = valid ? A.inv[jb] : 0;
+        uint64_t sb = 0, se = 0;
+        if (valid) child_range(A.S, jb, sb, se);
+        unsigned pending = __ballot_sync(AMJ_FULL_MASK, valid && se > sb);
+        // R's entries are sorted by a: each a of the chunk is one run of lanes
+        while (pending) {
+            const int32_t a = __shfl_sync(AMJ_FULL_MASK, ja, __ffs(pending) - 1);
+            const unsigned run = pending & __ballot_sync(AMJ_FULL_MASK, ja == a);
+            pending &= ~run;
+            uint64_t ta, te;
+            child_range(A.T, a, ta, te);
+            const uint64_t da = te - ta;
+            if (da == 0) continue;
+            const int32_t *tl = A.T.data1 + ta;
+            // set the bits of T(a); its values below the bitmap are a sorted prefix
+            uint32_t nl = 0;
+            for (uint64_t k0 = 0; k0 < da; k0 += 32) {
+                const uint64_t k = k0 + lane;
+                const bool in = k < da;
+                const int32_t v = in ? tl[k] : 0;
+                const uint32_t r = (uint32_t)v - base;
+                if (in && r < nbits) atomicOr(&W.bm[r >> 5], 1u << (r & 31));
+                else if (in && k < TR_LOWCAP) W.low[k] = v;
+                nl += __popc(__ballot_sync(AMJ_FULL_MASK, in && r >= nbits));
+            }
+            __syncwarp();
+            const bool low_smem = nl <= TR_LOWCAP;
+            unsigned rb = run;
+            while (rb) {
+                const int l = __ffs(rb) - 1;
+                rb &= rb - 1;
+                const uint64_t wsb = __shfl_sync(AMJ_FULL_MASK, sb, l);
+                const uint32_t len = (uint32_t)(__shfl_sync(AMJ_FULL_MASK, se, l) - wsb);
+                const int32_t *lst = A.S.data1 + wsb;
+                for (uint32_t k0 = 0; k0 < len; k0 += 32 * TR_UNROLL) {
+                    const uint32_t rem = len - k0;
+                    int32_t cv[TR_UNROLL];
+#pragma unroll
+                    for (int u = 0; u < TR_UNROLL; u++)
+                        if ((uint32_t)u * 32 < rem) {
+                            const uint32_t k = u * 32 + lane;
+                            cv[u] = lst[k0 + (k < rem ? k : 0)];
+                        }
+                    uint32_t bits = 0, lowbits = 0;
+#pragma unroll
+                    for (int u = 0; u < TR_UNROLL; u++)
+                        if ((uint32_t)u * 32 < rem) {
+                            const bool in = (uint32_t)(u * 32 + lane) < rem;
+                            const uint32_t r = (uint32_t)cv[u] - base;
+                            const bool top = r < nbits;
+                            const uint32_t w = W.bm[top ? (r >> 5) : 0u];
+                            bits |= (uint32_t)(in && top && ((w >> (r & 31)) & 1u)) << u;
+                            lowbits |= (uint32_t)(in && !top) << u;
+                        }
+                    if (__any_sync(AMJ_FULL_MASK, lowbits != 0)) {
+#pragma unroll
+                        for (int u = 0; u < TR_UNROLL; u++)
+                            if ((lowbits >> u) & 1u) {
+                                const bool hit = low_smem ? tr_sorted_find(W.low, nl, cv[u])
+                                                          : tr_sorted_find(tl, nl, cv[u]);
+                                bits |= (uint32_t)hit << u;
+                            }
+                    }
+                    const uint32_t nh = __popc(bits);
+                    const uint32_t incl = warp_inclusive_scan(nh, lane);
+                    const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, incl, 31);
+                    if (tot) {
+                        uint32_t pos = qh + qn + incl - nh;
+#pragma unroll
+                        for (int u = 0; u < TR_UNROLL; u++)
+                            if ((bits >> u) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u], l);
+                        qn += tot;
+                        while (qn >= 32) flush(32);
+                    }
+                }
+            }
+            // clear the words of T(a)'s bits
+            __syncwarp();
+            for (uint64_t k0 = 0; k0 < da; k0 += 32) {
+                const uint64_t k = k0 + lane;
+                if (k < da) {
+                    const uint32_t r = (uint32_t)tl[k] - base;
+                    if (r < nbits) W.bm[r >> 5] = 0u;
+                }
+            }
+            __syncwarp();
+        }
+        if (qn) flush(qn);
     }
     cnt = warp_sum(cnt);
     chk = warp_sum(chk);
@@ -475,7 +687,7 @@ __global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const 
 // ---- host side ----
 
 struct LftjCounters {
-    unsigned long long cursor, count, checksum, out_cursor, cursor0;
+    unsigned long long cursor, count, checksum, out_cursor, cursor0, cursor_r, heavy_n;
 };
 
 
@@ -484,7 +696,8 @@ struct LftjCounters {
 // written too (out_cap rows available).
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
-                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out) {
+                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out,
+                  const int32_t *inv, uint64_t nv, uint32_t rank_bits) {
     bool timed[2] = {false, false};
     TriArgs A{};
     A.sorted_out = sorted_out;
@@ -507,6 +720,8 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
     A.checksum = &ctr.p->checksum;
     A.out_cursor = &ctr.p->out_cursor;
     A.cursor0 = &ctr.p->cursor0;
+    DBuf<uint32_t> heavy;
+    A.cursor_r = &ctr.p->cursor_r;
     const bool write = out != nullptr;
     if (write) {
         for (int i = 0; i < 3; i++) A.out[i] = out[i];
@@ -514,35 +729,64 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
     }
     if (A.r_n) {
         if (algo == AMJ_LFTJ_DFS) {
-            if (heavy_deg) {
+            // a degree-ranked trie goes to the rank kernel alone
+            const bool rest = inv == nullptr;
+            AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
+            if (inv) {
+                uint32_t bits = TR_BITS;
+                if (rank_bits && rank_bits < bits) bits = rank_bits < 32 ? 32u : rank_bits;
+                if (nv < bits) bits = (uint32_t)((nv + 31) / 32 * 32);
+                if (bits == 0) bits = 32;
+                A.inv = inv;
+                A.rank_bits = bits;
+                A.rank_base = (uint32_t)(nv > bits ? nv - bits : 0);
+                auto kr = write ? lftj_tri_rank_kernel<true> : lftj_tri_rank_kernel<false>;
+                AMJ_CUDA_TRY(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM));
+                int per_sm = 0;
+                AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, TR_THREADS, TR_SMEM));
+                if (per_sm < 1) per_sm = 1;
+                note_launch(ctx);
+                kr<<<(unsigned)(ctx->num_sms * per_sm), TR_THREADS, TR_SMEM, ctx->stream>>>(A);
+                AMJ_CUDA_TRY(cudaGetLastError());
+                timed[0] = true;
+            }
+            if (rest && heavy_deg) {
                 // the bitmap kernel takes the heavy vertices; its shared memory: bitmap + 1024 x 24 B
                 const uint32_t bits_max = 1u << 20;
                 const size_t smem = (size_t)bits_max / 8 + (size_t)BM_THREADS * (8 + 8 + 4 + 4 + 4);
-                if (smem <= (size_t)ctx->max_smem_optin) {
+                if (smem <= (size_t)ctx->max_smem_optin && R.len0) {
                     A.heavy_deg = heavy_deg;
                     A.bitmap_bits = bits_max;
+                    AMJ_TRY(heavy.alloc(ctx, R.len0));
+                    A.heavy_list = heavy.p;
+                    A.heavy_n = &ctr.p->heavy_n;
+                    note_launch(ctx);
+                    heavy_list_kernel<<<(unsigned)std::min<uint64_t>((R.len0 + 255) / 256, (uint64_t)ctx->num_sms * 8), 256, 0,
+                                        ctx->stream>>>(A, heavy.p, &ctr.p->heavy_n);
+                    AMJ_CUDA_TRY(cudaGetLastError());
                     auto kb = write ? lftj_tri_bitmap_kernel<true> : lftj_tri_bitmap_kernel<false>;
                     AMJ_CUDA_TRY(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                     note_launch(ctx);
-                    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
                     kb<<<(unsigned)ctx->num_sms, BM_THREADS, smem, ctx->stream>>>(A);
                     AMJ_CUDA_TRY(cudaGetLastError());
-                    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
                     timed[0] = true;
                 }
             }
-            int per_sm = 0;
-            AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per_sm, write ? lftj_tri_dfs_kernel<true> : lftj_tri_dfs_kernel<false>, 256, 0));
-            if (per_sm < 1) per_sm = 1;
-            const unsigned grid = (unsigned)(ctx->num_sms * per_sm);
-            note_launch(ctx);
-            AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[2], ctx->stream));
-            if (write) lftj_tri_dfs_kernel<true><<<grid, 256, 0, ctx->stream>>>(A);
-            else lftj_tri_dfs_kernel<false><<<grid, 256, 0, ctx->stream>>>(A);
-            AMJ_CUDA_TRY(cudaGetLastError());
-            AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[3], ctx->stream));
-            timed[1] = true;
+            AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
+            if (rest) {
+                int per_sm = 0;
+                AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &per_sm, write ? lftj_tri_dfs_kernel<true> : lftj_tri_dfs_kernel<false>, 256, 0));
+                if (per_sm < 1) per_sm = 1;
+                const unsigned grid = (unsigned)(ctx->num_sms * per_sm);
+                note_launch(ctx);
+                AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[2], ctx->stream));
+                if (write) lftj_tri_dfs_kernel<true><<<grid, 256, 0, ctx->stream>>>(A);
+                else lftj_tri_dfs_kernel<false><<<grid, 256, 0, ctx->stream>>>(A);
+                AMJ_CUDA_TRY(cudaGetLastError());
+                AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[3], ctx->stream));
+                timed[1] = true;
+            }
         } else {
             DBuf<unsigned long long> cand;
             AMJ_TRY(cand.alloc(ctx, A.r_n + 1));

@@ -19,7 +19,8 @@ int lftj_clique4(amj_ctx *ctx, const Trie2 &T, int32_t *const *out, uint64_t out
                  uint64_t *checksum, uint64_t *written, double *kernel_ms, int sorted_out);
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
-                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out);
+                  uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out,
+                  const int32_t *inv, uint64_t nv, uint32_t rank_bits);
 
 // the generic join (lftj_generic.cu)
 int lftj_generic_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int ooc, int flags, amj_result *out);
@@ -38,6 +39,21 @@ static int build_self_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, int *sorted
     AMJ_TRY(degree_ordered_copy(ctx, c0, c1, r->n, &ns, &nd, &oriented));
     if (!oriented) return build_trie2(ctx, c0, c1, r->n, t);
     *sorted = 1;
+    return build_trie2(ctx, ns.p, nd.p, r->n, t);
+}
+
+// Trie of the degree-ranked copy (*inv maps ranks to vertex ids) when the
+// relation is oriented; otherwise the trie of the relation itself, *nv = 0.
+static int build_ranked_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, DBuf<int32_t> *inv, uint64_t *nv) {
+    *nv = 0;
+    if (r->ncols != 2) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must have two columns");
+    if (r->where == AMJ_MEM_HOST_STREAMED) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must be on the device");
+    const bool swap = r->attrs[0] > r->attrs[1];
+    const int32_t *c0 = r->d_cols[swap ? 1 : 0], *c1 = r->d_cols[swap ? 0 : 1];
+    DBuf<int32_t> ns, nd;
+    bool oriented = false;
+    AMJ_TRY(degree_ranked_copy(ctx, c0, c1, r->n, &ns, &nd, inv, nv, &oriented));
+    if (!oriented) return build_trie2(ctx, c0, c1, r->n, t);
     return build_trie2(ctx, ns.p, nd.p, r->n, t);
 }
 }
@@ -138,13 +154,20 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     Trie2 tries[3];
     const Trie2 *R = nullptr, *S = nullptr, *T = nullptr;
     int sorted_out = 0;
+    DBuf<int32_t> inv;   // ranks to vertex ids, for a degree-ranked trie
+    uint64_t nv = 0;
     if (nrels == 1) {
-        // the bitmap DFS kernel is fastest on the relation's own orientation
-        // (hubs keep long child lists); BFS gains from the degree order
-        bool deg_order = algo == AMJ_LFTJ_BFS;
+        // BFS and the DFS rank kernel (ws=1) join the degree-ordered copy:
+        // hubs keep short child lists
+        bool deg_order = algo == AMJ_LFTJ_BFS || ws;
         if (flags & AMJ_F_DEGREE_ORDER) deg_order = true;
         if (flags & AMJ_F_KEEP_ORDER) deg_order = false;
-        AMJ_TRY(build_self_trie(ctx, rels[0], &tries[0], &sorted_out, deg_order));
+        if (deg_order && algo == AMJ_LFTJ_DFS && ws) {
+            AMJ_TRY(build_ranked_trie(ctx, rels[0], &tries[0], &inv, &nv));
+            sorted_out = nv ? 1 : 0;
+        } else {
+            AMJ_TRY(build_self_trie(ctx, rels[0], &tries[0], &sorted_out, deg_order));
+        }
         R = S = T = &tries[0];
     } else {
         for (int i = 0; i < 3; i++) {
@@ -165,6 +188,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     const int small_sum = ws ? 48 : 0x7fffffff;
     // ws=1 also hands vertices with many children to the block-wide bitmap kernel
     const uint32_t heavy_deg = ws ? (ctx->opts.lftj_heavy_degree ? ctx->opts.lftj_heavy_degree : 32u) : 0u;
+    const int32_t *rank_inv = nv ? inv.p : nullptr;
     const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
     const uint64_t nr = R->len1;
     uint64_t slice = nr;
@@ -180,7 +204,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         const uint64_t hi = std::min(nr, lo + slice);
         uint64_t c = 0, h = 0, w = 0;
         rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, lo, hi, heavy_deg,
-                           out->kernel_ms, sorted_out);
+                           out->kernel_ms, sorted_out, rank_inv, nv, ctx->opts.lftj_rank_bits);
         if (rc != AMJ_OK) break;
         if (materialize) {
             int32_t *cols[3] = {nullptr, nullptr, nullptr};
@@ -188,7 +212,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
             uint64_t c2 = 0, h2 = 0;
             if (rc == AMJ_OK)
                 rc = lftj_triangle(ctx, *R, *S, *T, algo, cols, c, &c2, &h2, &w, small_sum, lo, hi, heavy_deg,
-                                   out->kernel_ms + 2, sorted_out);
+                                   out->kernel_ms + 2, sorted_out, rank_inv, nv, ctx->opts.lftj_rank_bits);
             if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
                 rc = fail(AMJ_ECUDA, "LFTJ: write pass disagrees with count pass");
             if (rc == AMJ_OK && ooc) {

@@ -105,6 +105,10 @@ typedef struct amj_opts {
                                   (0: every block that fits on the device); kernels
                                   of several contexts running at once must fit
                                   together, since idle warps wait for the others  */
+    uint32_t lftj_rank_bits;   /* ALFTJ DFS ws=1 over the degree-ranked copy: ranks
+                                  each warp's bitmap covers, the highest ones
+                                  (0: 32768, the most; rounded up to 32); lower
+                                  ranks are found by binary search               */
 } amj_opts;
 
 typedef struct amj_result {
@@ -119,7 +123,7 @@ typedef struct amj_result {
     double   total_ms;                /* whole call, device time               */
     uint64_t stats[12];               /* operator counters, see amj_stat_name  */
     double   kernel_ms[4];            /* device time of the main kernels: ALFTJ DFS
-                                         [0] bitmap [1] warp intersection, BFS
+                                         [0] rank or bitmap [1] warp intersection, BFS
                                          [0] candidate count [1] expand ([2], [3]
                                          the same in a write pass); AMHJ [0] count
                                          passes [1] write passes                  */

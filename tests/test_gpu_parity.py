@@ -432,13 +432,22 @@ def test_amhj_rejects_bad_queries(ctx):
 @pytest.mark.parametrize("algo", ["DFS", "BFS"])
 @pytest.mark.parametrize("ws", [0, 1])
 @pytest.mark.parametrize("heavy", [0, 1, 8])
-def test_lftj_triangle_small(algo, ws, heavy):
-    with Context(0, lftj_heavy_degree=heavy) as ctx:
+@pytest.mark.parametrize("rankbits", [0, 32])
+def test_lftj_triangle_small(algo, ws, heavy, rankbits):
+    """DFS ws=1 is the rank kernel over the degree-ranked copy; rankbits 32
+    sends nearly every lookup below the bitmap, to the binary search."""
+    if rankbits and (algo == "BFS" or not ws):
+        pytest.skip("the rank kernel is the DFS ws=1 path")
+    with Context(0, lftj_heavy_degree=heavy, lftj_rank_bits=rankbits) as ctx:
         for seed, scale, ne in [(1, 8, 1500), (2, 12, 50000)]:
             s, d = data.rmat(scale, ne, 0.57, 0.19, 0.19, seed)
             e = ctx.relation([s, d], [0, 1])
             got = ctx.lftj([e], algo=algo, ws=ws)
             assert (got.count, got.checksum) == O.triangle(s, d)
+            if algo == "DFS" and ws:
+                m = ctx.lftj([e], algo=algo, ws=ws, materialize=True)
+                assert (m.count, m.checksum) == (got.count, got.checksum)
+                assert data.checksum(m.columns) == got.checksum
 
 
 @pytest.mark.parametrize("scale,ne,seed", [(8, 1500, 1), (12, 60000, 2), (14, 1 << 18, 22)])
@@ -573,6 +582,29 @@ def test_lftj_generic_materialized_and_rejections(ctx):
     assert e.value.status == L.AMJ_EUNSUPPORTED
     with pytest.raises(AmjError):
         ctx.lftj(hs, ooc=1)
+
+
+@pytest.mark.parametrize("rankbits", [0, 32, 1000])
+def test_lftj_rank_kernel_bitmap_and_low_prefix(rankbits):
+    """R-MAT scale 17: with the default bitmap nearly every value is a bit
+    test; with 32 ranks, vertices with more than 256 children below the
+    bitmap search T(a) in device memory instead of shared memory."""
+    s, d = data.rmat(17, 1 << 21, 0.57, 0.19, 0.19, 3)
+    want = O.triangle(s, d)
+    with Context(0, lftj_rank_bits=rankbits) as ctx:
+        e = ctx.relation([s, d], [0, 1])
+        got = ctx.lftj([e], algo="DFS", ws=1)
+        assert (got.count, got.checksum) == want
+        keep = ctx.lftj([e], algo="DFS", ws=1, degree_order=False)
+        assert (keep.count, keep.checksum) == want
+    s, d = data.rmat(10, 9000, 0.57, 0.19, 0.19, 4)
+    cnt, chk, cols = O.triangle(s, d, tuples=True)
+    with Context(0, lftj_rank_bits=rankbits, ooc_slice_rows=2000) as ctx:
+        e = ctx.relation([s, d], [0, 1])
+        for ooc in (0, 1):
+            m = ctx.lftj([e], algo="DFS", ws=1, ooc=ooc, materialize=True)
+            assert (m.count, m.checksum) == (cnt, chk)
+            assert np.array_equal(sorted_rows(m.columns), sorted_rows(cols))
 
 
 def test_lftj_out_of_core_slices():
