@@ -53,6 +53,9 @@ struct Trie2 {
     uint64_t rp_count = 0;     // 0 when no dense array was built
 };
 
+// Level 1 of a built 2-level trie has TRIE_LEVEL1_PAD spare values after its
+// last one, so kernels may read it in aligned 16-byte quads.
+constexpr uint64_t TRIE_LEVEL1_PAD = 4;
 int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out);
 
 // time between two events recorded on the context stream (ms)

@@ -58,6 +58,8 @@ struct TriArgs {
     // rank kernel: the tries hold the degree-ranked copy (vertex = rank in
     // (degree, id) order); inv[rank] is the vertex id
     const int32_t *inv;
+    const uint64_t *wedge;        // (b << 32 | entry) of this slice's entries, sorted by b
+    const int32_t *src1;          // level-0 value of every level-1 entry of R
     uint32_t rank_base;           // first rank of the per-warp bitmap
     uint32_t rank_bits;           // ranks the bitmap covers
     unsigned long long *cursor_r; // claim cursor of the rank kernel
@@ -293,35 +295,39 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
     }
 }
 
-// ---- rank kernel ----
+// ---- wedge kernel ----
 // The degree-ranked copy of an oriented edge relation: every vertex renamed
 // to its rank in (degree, id) order, edges from the lower to the higher
-// rank.  Out-neighbours then concentrate on the highest ranks (on R-MAT
-// scale 20, 99.8% of the values the lookups see lie in the top 32K ranks), so
-// each warp keeps a bitmap of the top rank_bits ranks (4 KB) and a lookup is
-// one shared-memory load and a bit test.  Persistent warps claim 32 level-1
-// entries (a, b) of R at a time.  For each run of one a among them, the
-// children T(a) set their bits (those below the bitmap, a sorted prefix of
-// T(a), are copied to shared memory); then the children S(b) of each b of
-// the run stream through the warp, TR_UNROLL x 32 values per step with all
-// loads issued before the tests.  A value below the bitmap is looked up by
-// binary search in T(a)'s low prefix.  Hits go to a per-warp queue of
-// (c, entry) pairs; the id mapping, the checksum and the writes run on 32
+// rank.  A triangle is then a wedge a -> b, a -> c with b < c closed by the
+// edge b -> c: for every edge (a, b), the children of a ranked above b (the
+// suffix of T(a) after b) are tested against the children of b.  That is
+// sum over a of C(d+(a), 2) tests (1.23 G on R-MAT scale 20, against 4.42 G
+// for streaming S(b) per edge).  The edges come grouped by b (a stable sort
+// of (b, entry)), so each warp keeps the children of one b as a bitmap in
+// shared memory.  Out-neighbours concentrate on the highest ranks (on R-MAT
+// scale 20, 99.8% of the tested values lie in the top 32K ranks), so the
+// bitmap covers the top rank_bits ranks (4 KB) and a test is one
+// shared-memory load; the rare values below it are binary-searched in
+// S(b)'s low prefix (a sorted prefix, kept in shared memory up to 256).
+// Persistent warps claim 32 edges at a time; each edge's suffix streams
+// through the warp in aligned 16-byte quads.  Hits go to a per-warp queue
+// of (c, edge) pairs; the id mapping, the checksum and the writes run on 32
 // queued triangles at a time, so lanes without a hit do not wait on them.
 constexpr int TR_THREADS = 256;
 constexpr int TR_WARPS = TR_THREADS / 32;
 constexpr uint32_t TR_BITS = 32768;            // bitmap ranks per warp (the most)
 constexpr int TR_LOWCAP = 256;                 // low prefix entries kept in shared memory
-constexpr int TR_UNROLL = 8;
+constexpr int TR_UNROLL = 2;                   // quads per lane per step
 constexpr int TR_QCAP = 512;                   // queued hits per warp (ring)
 
 struct TrWarp {
     uint32_t bm[TR_BITS / 32];
     int32_t low[TR_LOWCAP];
-    int2 q[TR_QCAP];   // (c, lane of the entry)
+    int2 q[TR_QCAP];   // (c, lane of the edge)
 };
 constexpr size_t TR_SMEM = TR_WARPS * sizeof(TrWarp);
 static_assert(sizeof(TrWarp) % 16 == 0, "TrWarp keeps 16-byte alignment");
+static_assert(TR_QCAP >= 32 + 32 * 4 * TR_UNROLL, "the queue takes one step's hits");
 
 __device__ __forceinline__ bool tr_sorted_find(const int32_t *v, uint64_t n, int32_t c) {
     uint64_t lo = 0, hi = n;
@@ -333,18 +339,26 @@ __device__ __forceinline__ bool tr_sorted_find(const int32_t *v, uint64_t n, int
     return lo < n && v[lo] == c;
 }
 
+// bit of rank value c in the warp's bitmap (the index stays in bounds for
+// values outside it, which the caller masks off)
+__device__ __forceinline__ uint32_t tr_bit(const uint32_t *bm, int32_t c, uint32_t base) {
+    const uint32_t r = ((uint32_t)c - base) & (TR_BITS - 1);
+    return __funnelshift_r(bm[r >> 5], 0u, r) & 1u;
+}
+
 template <bool WRITE>
-__global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_rank_kernel(const __grid_constant__ TriArgs A) {
+__global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __grid_constant__ TriArgs A) {
     extern __shared__ __align__(16) unsigned char tr_smem[];
     const int lane = threadIdx.x & 31;
     TrWarp &W = ((TrWarp *)tr_smem)[threadIdx.x >> 5];
     const uint32_t base = A.rank_base, nbits = A.rank_bits;
+    const int32_t *d1 = A.T.data1;
+    const int4 *dq = reinterpret_cast<const int4 *>(d1);
     for (uint32_t k = lane; k < TR_BITS / 32; k += 32) W.bm[k] = 0u;
     __syncwarp();
     unsigned long long cnt = 0, chk = 0;
     uint32_t qh = 0, qn = 0;   // queue head and length
-    int32_t ja = 0, jb = 0;    // this lane's entry of the current chunk (ranks)
-    int32_t ida = 0, idb = 0;  // and its vertex ids
+    int32_t ida = 0, idb = 0;  // vertex ids of this lane's edge (a, b)
     // the first n queued hits, one per lane
     auto flush = [&](uint32_t n) {
         __syncwarp();
@@ -367,6 +381,54 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_rank_kernel(const __gr
         qh = (qh + n) & (TR_QCAP - 1);
         qn -= n;
     };
+    // the current b: its children S(b) = sl_[0, db) have their bits set
+    bool have_b = false;
+    int32_t cur_b = 0;
+    uint64_t db = 0;
+    const int32_t *bl = nullptr;
+    uint32_t nl = 0;   // children of b below the bitmap (a sorted prefix)
+    auto set_bits = [&](int32_t b) {
+        uint64_t sb, se;
+        child_range(A.S, b, sb, se);
+        db = se - sb;
+        bl = d1 + sb;
+        nl = 0;
+        for (uint64_t k0 = 0; k0 < db; k0 += 128) {
+            int32_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint64_t k = k0 + u * 32 + lane;
+                v[u] = k < db ? bl[k] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint64_t k = k0 + u * 32 + lane;
+                const bool in = k < db;
+                const uint32_t r = (uint32_t)v[u] - base;
+                if (in && r < nbits) atomicOr(&W.bm[r >> 5], 1u << (r & 31));
+                else if (in && k < TR_LOWCAP) W.low[k] = v[u];
+                nl += __popc(__ballot_sync(AMJ_FULL_MASK, in && r >= nbits));
+            }
+        }
+        __syncwarp();
+    };
+    auto clear_bits = [&]() {
+        __syncwarp();
+        for (uint64_t k0 = 0; k0 < db; k0 += 128) {
+            int32_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint64_t k = k0 + u * 32 + lane;
+                v[u] = k < db ? bl[k] : (int32_t)(base - 1);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t r = (uint32_t)v[u] - base;
+                if (r < nbits) W.bm[r >> 5] = 0u;
+            }
+        }
+        __syncwarp();
+    };
     while (true) {
         unsigned long long at = 0;
         if (lane == 0) at = atomicAdd(A.cursor_r, 32ull);
@@ -374,104 +436,148 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_rank_kernel(const __gr
         if (at >= A.r_n) break;
         const uint64_t j = at + lane;
         const bool valid = j < A.r_n;
-        ja = valid ? A.r_src[j] : 0;
-        jb = valid ? A.r_dst[j] : 0;
-        ida = valid ? A.inv[ja] : 0;
-        idb = valid ? A.inv[jb] : 0;
-        uint64_t sb = 0, se = 0;
-        if (valid) child_range(A.S, jb, sb, se);
-        unsigned pending = __ballot_sync(AMJ_FULL_MASK, valid && se > sb);
-        // R's entries are sorted by a: each a of the chunk is one run of lanes
-        while (pending) {
-            const int32_t a = __shfl_sync(AMJ_FULL_MASK, ja, __ffs(pending) - 1);
-            const unsigned run = pending & __ballot_sync(AMJ_FULL_MASK, ja == a);
-            pending &= ~run;
-            uint64_t ta, te;
+        int32_t b = 0;
+        uint64_t ts = 0, te = 0;   // suffix of T(a) after b
+        if (valid) {
+            const uint64_t w = A.wedge[j];
+            const uint32_t idx = (uint32_t)w;
+            b = (int32_t)(w >> 32);
+            const int32_t a = A.src1[idx];
+            uint64_t ta;
             child_range(A.T, a, ta, te);
-            const uint64_t da = te - ta;
-            if (da == 0) continue;
-            const int32_t *tl = A.T.data1 + ta;
-            // set the bits of T(a); its values below the bitmap are a sorted prefix
-            uint32_t nl = 0;
-            for (uint64_t k0 = 0; k0 < da; k0 += 32) {
-                const uint64_t k = k0 + lane;
-                const bool in = k < da;
-                const int32_t v = in ? tl[k] : 0;
-                const uint32_t r = (uint32_t)v - base;
-                if (in && r < nbits) atomicOr(&W.bm[r >> 5], 1u << (r & 31));
-                else if (in && k < TR_LOWCAP) W.low[k] = v;
-                nl += __popc(__ballot_sync(AMJ_FULL_MASK, in && r >= nbits));
+            ts = (uint64_t)idx + 1;
+            ida = A.inv[a];
+            idb = A.inv[b];
+        }
+        // tl: first value of the suffix in the bitmap's ranks (the values
+        // below form a short sorted prefix: gallop, then bisect)
+        uint64_t tl = ts;
+        if (te > ts && d1[ts] < (int32_t)base) {
+            uint64_t lo = ts + 1, hi = te, step = 1;
+            while (lo + step < te && d1[lo + step - 1] < (int32_t)base) {
+                lo += step;
+                step <<= 1;
             }
-            __syncwarp();
+            if (lo + step < hi) hi = lo + step;
+            while (lo < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if (d1[mid] < (int32_t)base) lo = mid + 1;
+                else hi = mid;
+            }
+            tl = lo;
+        }
+        unsigned todo = __ballot_sync(AMJ_FULL_MASK, valid && te > ts);
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int32_t wb = __shfl_sync(AMJ_FULL_MASK, b, l);
+            if (!have_b || wb != cur_b) {
+                if (have_b) clear_bits();
+                set_bits(wb);
+                cur_b = wb;
+                have_b = true;
+            }
+            if (db == 0) continue;
             const bool low_smem = nl <= TR_LOWCAP;
-            unsigned rb = run;
-            while (rb) {
-                const int l = __ffs(rb) - 1;
-                rb &= rb - 1;
-                const uint64_t wsb = __shfl_sync(AMJ_FULL_MASK, sb, l);
-                const uint32_t len = (uint32_t)(__shfl_sync(AMJ_FULL_MASK, se, l) - wsb);
-                const int32_t *lst = A.S.data1 + wsb;
-                for (uint32_t k0 = 0; k0 < len; k0 += 32 * TR_UNROLL) {
-                    const uint32_t rem = len - k0;
-                    int32_t cv[TR_UNROLL];
-#pragma unroll
-                    for (int u = 0; u < TR_UNROLL; u++)
-                        if ((uint32_t)u * 32 < rem) {
-                            const uint32_t k = u * 32 + lane;
-                            cv[u] = lst[k0 + (k < rem ? k : 0)];
-                        }
-                    uint32_t bits = 0, lowbits = 0;
-#pragma unroll
-                    for (int u = 0; u < TR_UNROLL; u++)
-                        if ((uint32_t)u * 32 < rem) {
-                            const bool in = (uint32_t)(u * 32 + lane) < rem;
-                            const uint32_t r = (uint32_t)cv[u] - base;
-                            const bool top = r < nbits;
-                            const uint32_t w = W.bm[top ? (r >> 5) : 0u];
-                            bits |= (uint32_t)(in && top && ((w >> (r & 31)) & 1u)) << u;
-                            lowbits |= (uint32_t)(in && !top) << u;
-                        }
-                    if (__any_sync(AMJ_FULL_MASK, lowbits != 0)) {
-#pragma unroll
-                        for (int u = 0; u < TR_UNROLL; u++)
-                            if ((lowbits >> u) & 1u) {
-                                const bool hit = low_smem ? tr_sorted_find(W.low, nl, cv[u])
-                                                          : tr_sorted_find(tl, nl, cv[u]);
-                                bits |= (uint32_t)hit << u;
-                            }
-                    }
-                    const uint32_t nh = __popc(bits);
-                    const uint32_t incl = warp_inclusive_scan(nh, lane);
-                    const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, incl, 31);
-                    if (tot) {
-                        uint32_t pos = qh + qn + incl - nh;
-#pragma unroll
-                        for (int u = 0; u < TR_UNROLL; u++)
-                            if ((bits >> u) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u], l);
-                        qn += tot;
-                        while (qn >= 32) flush(32);
-                    }
-                }
-            }
-            // clear the words of T(a)'s bits
-            __syncwarp();
-            for (uint64_t k0 = 0; k0 < da; k0 += 32) {
+            const uint64_t wts = __shfl_sync(AMJ_FULL_MASK, ts, l);
+            const uint64_t wtl = __shfl_sync(AMJ_FULL_MASK, tl, l);
+            const uint64_t wte = __shfl_sync(AMJ_FULL_MASK, te, l);
+            // values below the bitmap: binary search in S(b)'s low prefix
+            for (uint64_t k0 = wts; k0 < wtl; k0 += 32) {
                 const uint64_t k = k0 + lane;
-                if (k < da) {
-                    const uint32_t r = (uint32_t)tl[k] - base;
-                    if (r < nbits) W.bm[r >> 5] = 0u;
+                bool hit = false;
+                int32_t c = 0;
+                if (k < wtl) {
+                    c = d1[k];
+                    hit = nl && (low_smem ? tr_sorted_find(W.low, nl, c) : tr_sorted_find(bl, nl, c));
+                }
+                const unsigned m = __ballot_sync(AMJ_FULL_MASK, hit);
+                if (hit) W.q[(qh + qn + __popc(m & lanemask_lt())) & (TR_QCAP - 1)] = make_int2(c, l);
+                qn += __popc(m);
+                while (qn >= 32) flush(32);
+            }
+            // values in the bitmap, as aligned quads of level 1
+            const uint64_t qlo = wtl >> 2, qhi = (wte + 3) >> 2;
+            const uint32_t h = (uint32_t)(wtl & 3);
+            const uint32_t hl = h + (uint32_t)(wte - wtl);   // suffix end, from the first quad's start
+            for (uint64_t q0 = qlo; q0 < qhi; q0 += 32 * TR_UNROLL) {
+                const uint32_t remq = (uint32_t)(qhi - q0 < 32 * TR_UNROLL ? qhi - q0 : 32 * TR_UNROLL);
+                const uint32_t qoff = (uint32_t)(q0 - qlo);
+                int4 cv[TR_UNROLL];
+#pragma unroll
+                for (int u = 0; u < TR_UNROLL; u++)
+                    if ((uint32_t)u * 32 < remq) {
+                        const uint32_t kq = u * 32 + lane;
+                        cv[u] = dq[q0 + (kq < remq ? kq : 0)];
+                    }
+                uint32_t bits = 0;
+#pragma unroll
+                for (int u = 0; u < TR_UNROLL; u++)
+                    if ((uint32_t)u * 32 < remq) {
+                        const uint32_t kq = u * 32 + lane;
+                        // values t of this quad inside the suffix: lo <= t < hi
+                        const uint32_t e0 = 4 * (qoff + kq);
+                        const uint32_t lo = e0 == 0 ? h : 0u;
+                        const uint32_t hi = hl > e0 ? (hl - e0 < 4 ? hl - e0 : 4u) : 0u;
+                        const uint32_t m4 = kq < remq && hi > lo ? ((0xFu >> (4 - hi)) & (0xFu << lo)) : 0u;
+                        const uint32_t t4 = tr_bit(W.bm, cv[u].x, base) | (tr_bit(W.bm, cv[u].y, base) << 1) |
+                                            (tr_bit(W.bm, cv[u].z, base) << 2) | (tr_bit(W.bm, cv[u].w, base) << 3);
+                        bits |= (t4 & m4) << (4 * u);
+                    }
+                const uint32_t nh = __popc(bits);
+                const uint32_t incl = warp_inclusive_scan(nh, lane);
+                const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, incl, 31);
+                if (tot) {
+                    uint32_t pos = qh + qn + incl - nh;
+#pragma unroll
+                    for (int u = 0; u < TR_UNROLL; u++) {
+                        if ((bits >> (4 * u)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].x, l);
+                        if ((bits >> (4 * u + 1)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].y, l);
+                        if ((bits >> (4 * u + 2)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].z, l);
+                        if ((bits >> (4 * u + 3)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].w, l);
+                    }
+                    qn += tot;
+                    while (qn >= 32) flush(32);
                 }
             }
-            __syncwarp();
         }
         if (qn) flush(qn);
     }
+    if (have_b) clear_bits();
     cnt = warp_sum(cnt);
     chk = warp_sum(chk);
     if (lane == 0 && cnt) {
         atomicAdd(A.count, cnt);
         atomicAdd(A.checksum, chk);
     }
+}
+
+// (b << 32 | entry) for every level-1 entry (a, b) of R
+__global__ void wedge_keys_kernel(const int32_t *__restrict__ data1, uint64_t n, uint64_t *__restrict__ keys) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        keys[i] = ((uint64_t)(uint32_t)data1[i] << 32) | i;
+}
+
+// The level-1 entries of a degree-ranked trie grouped by b: a stable sort
+// of (b << 32 | entry) on the rank bits of b.
+int build_wedges(amj_ctx *ctx, const Trie2 &R, uint64_t nv, DBuf<uint64_t> *out) {
+    const uint64_t n = R.len1;
+    if (n >= (1ull << 32)) return fail(AMJ_EUNSUPPORTED, "LFTJ: 2^32 or more edges");
+    DBuf<uint64_t> other;
+    AMJ_TRY(out->alloc(ctx, n ? n : 1));
+    if (n == 0) return AMJ_OK;
+    AMJ_TRY(other.alloc(ctx, n));
+    note_launch(ctx);
+    wedge_keys_kernel<<<(unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 16), 256, 0,
+                        ctx->stream>>>(R.data1.p, n, out->p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    int bits = 1;
+    while (bits < 32 && (nv - 1) >> bits) bits++;
+    uint64_t *sorted = nullptr;
+    AMJ_TRY(radix_sort_u64(ctx, out->p, other.p, n, SK_IDENT, 32, 32 + bits, &sorted));
+    if (sorted != out->p)
+        AMJ_CUDA_TRY(cudaMemcpyAsync(out->p, sorted, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    return AMJ_OK;
 }
 
 template <bool WRITE>
@@ -697,7 +803,7 @@ struct LftjCounters {
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
                   uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out,
-                  const int32_t *inv, uint64_t nv, uint32_t rank_bits) {
+                  const int32_t *inv, const uint64_t *wedge, uint64_t nv, uint32_t rank_bits) {
     bool timed[2] = {false, false};
     TriArgs A{};
     A.sorted_out = sorted_out;
@@ -729,18 +835,22 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
     }
     if (A.r_n) {
         if (algo == AMJ_LFTJ_DFS) {
-            // a degree-ranked trie goes to the rank kernel alone
+            // a degree-ranked trie goes to the wedge kernel alone
             const bool rest = inv == nullptr;
             AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
             if (inv) {
+                if (reinterpret_cast<uintptr_t>(S.data1.p) & 15)
+                    return fail(AMJ_ECUDA, "LFTJ: trie level 1 is not 16-byte aligned");
                 uint32_t bits = TR_BITS;
                 if (rank_bits && rank_bits < bits) bits = rank_bits < 32 ? 32u : rank_bits;
                 if (nv < bits) bits = (uint32_t)((nv + 31) / 32 * 32);
                 if (bits == 0) bits = 32;
                 A.inv = inv;
+                A.wedge = wedge + r_lo;
+                A.src1 = R.src1.p;
                 A.rank_bits = bits;
                 A.rank_base = (uint32_t)(nv > bits ? nv - bits : 0);
-                auto kr = write ? lftj_tri_rank_kernel<true> : lftj_tri_rank_kernel<false>;
+                auto kr = write ? lftj_tri_wedge_kernel<true> : lftj_tri_wedge_kernel<false>;
                 AMJ_CUDA_TRY(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM));
                 int per_sm = 0;
                 AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, TR_THREADS, TR_SMEM));

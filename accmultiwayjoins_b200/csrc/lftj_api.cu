@@ -20,7 +20,8 @@ int lftj_clique4(amj_ctx *ctx, const Trie2 &T, int32_t *const *out, uint64_t out
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
                   uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out,
-                  const int32_t *inv, uint64_t nv, uint32_t rank_bits);
+                  const int32_t *inv, const uint64_t *wedge, uint64_t nv, uint32_t rank_bits);
+int build_wedges(amj_ctx *ctx, const Trie2 &R, uint64_t nv, DBuf<uint64_t> *out);
 
 // the generic join (lftj_generic.cu)
 int lftj_generic_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int ooc, int flags, amj_result *out);
@@ -155,6 +156,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     const Trie2 *R = nullptr, *S = nullptr, *T = nullptr;
     int sorted_out = 0;
     DBuf<int32_t> inv;   // ranks to vertex ids, for a degree-ranked trie
+    DBuf<uint64_t> wedges;   // its level-1 entries grouped by b
     uint64_t nv = 0;
     if (nrels == 1) {
         // BFS and the DFS rank kernel (ws=1) join the degree-ordered copy:
@@ -165,6 +167,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         if (deg_order && algo == AMJ_LFTJ_DFS && ws) {
             AMJ_TRY(build_ranked_trie(ctx, rels[0], &tries[0], &inv, &nv));
             sorted_out = nv ? 1 : 0;
+            if (nv) AMJ_TRY(build_wedges(ctx, tries[0], nv, &wedges));
         } else {
             AMJ_TRY(build_self_trie(ctx, rels[0], &tries[0], &sorted_out, deg_order));
         }
@@ -204,7 +207,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         const uint64_t hi = std::min(nr, lo + slice);
         uint64_t c = 0, h = 0, w = 0;
         rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, lo, hi, heavy_deg,
-                           out->kernel_ms, sorted_out, rank_inv, nv, ctx->opts.lftj_rank_bits);
+                           out->kernel_ms, sorted_out, rank_inv, wedges.p, nv, ctx->opts.lftj_rank_bits);
         if (rc != AMJ_OK) break;
         if (materialize) {
             int32_t *cols[3] = {nullptr, nullptr, nullptr};
@@ -212,7 +215,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
             uint64_t c2 = 0, h2 = 0;
             if (rc == AMJ_OK)
                 rc = lftj_triangle(ctx, *R, *S, *T, algo, cols, c, &c2, &h2, &w, small_sum, lo, hi, heavy_deg,
-                                   out->kernel_ms + 2, sorted_out, rank_inv, nv, ctx->opts.lftj_rank_bits);
+                                   out->kernel_ms + 2, sorted_out, rank_inv, wedges.p, nv, ctx->opts.lftj_rank_bits);
             if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
                 rc = fail(AMJ_ECUDA, "LFTJ: write pass disagrees with count pass");
             if (rc == AMJ_OK && ooc) {

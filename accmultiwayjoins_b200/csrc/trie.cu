@@ -106,7 +106,7 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
         AMJ_TRY(out->off0.alloc(ctx, 1));
         AMJ_CUDA_TRY(cudaMemsetAsync(out->off0.p, 0, sizeof(uint64_t), ctx->stream));
         AMJ_TRY(out->data0.alloc(ctx, 1));
-        AMJ_TRY(out->data1.alloc(ctx, 1));
+        AMJ_TRY(out->data1.alloc(ctx, TRIE_LEVEL1_PAD));
         return AMJ_OK;
     }
     DBuf<uint32_t> mm;
@@ -131,7 +131,7 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
     uint64_t *sorted = nullptr;
     AMJ_TRY(radix_sort_u64(ctx, a.p, b.p, n, SK_IDENT, 0, bits0 + bits1, &sorted));
 
-    AMJ_TRY(out->data1.alloc(ctx, n));
+    AMJ_TRY(out->data1.alloc(ctx, n + TRIE_LEVEL1_PAD));
     AMJ_TRY(out->src1.alloc(ctx, n));
     DBuf<uint32_t> head;
     AMJ_TRY(head.alloc(ctx, n + 1));

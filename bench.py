@@ -159,7 +159,7 @@ class Triangle:
         return self.E * (8 + 32) + 4 * int(shorter.sum())
 
     def kernel_name(self):
-        return "lftj_tri_bitmap_kernel + lftj_tri_dfs_kernel (intersection)"
+        return "lftj_tri_wedge_kernel (intersection)" if self.algo == "DFS" else "lftj_tri_bfs kernels (intersection)"
 
     def cpu_baseline(self):
         from oracle import oracle as O

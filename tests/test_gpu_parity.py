@@ -434,10 +434,10 @@ def test_amhj_rejects_bad_queries(ctx):
 @pytest.mark.parametrize("heavy", [0, 1, 8])
 @pytest.mark.parametrize("rankbits", [0, 32])
 def test_lftj_triangle_small(algo, ws, heavy, rankbits):
-    """DFS ws=1 is the rank kernel over the degree-ranked copy; rankbits 32
+    """DFS ws=1 is the wedge kernel over the degree-ranked copy; rankbits 32
     sends nearly every lookup below the bitmap, to the binary search."""
     if rankbits and (algo == "BFS" or not ws):
-        pytest.skip("the rank kernel is the DFS ws=1 path")
+        pytest.skip("the wedge kernel is the DFS ws=1 path")
     with Context(0, lftj_heavy_degree=heavy, lftj_rank_bits=rankbits) as ctx:
         for seed, scale, ne in [(1, 8, 1500), (2, 12, 50000)]:
             s, d = data.rmat(scale, ne, 0.57, 0.19, 0.19, seed)
@@ -585,10 +585,10 @@ def test_lftj_generic_materialized_and_rejections(ctx):
 
 
 @pytest.mark.parametrize("rankbits", [0, 32, 1000])
-def test_lftj_rank_kernel_bitmap_and_low_prefix(rankbits):
+def test_lftj_wedge_kernel_bitmap_and_low_prefix(rankbits):
     """R-MAT scale 17: with the default bitmap nearly every value is a bit
-    test; with 32 ranks, vertices with more than 256 children below the
-    bitmap search T(a) in device memory instead of shared memory."""
+    test; with 32 ranks, vertices b with more than 256 children below the
+    bitmap search S(b) in device memory instead of shared memory."""
     s, d = data.rmat(17, 1 << 21, 0.57, 0.19, 0.19, 3)
     want = O.triangle(s, d)
     with Context(0, lftj_rank_bits=rankbits) as ctx:
