@@ -317,17 +317,18 @@ constexpr int TR_THREADS = 256;
 constexpr int TR_WARPS = TR_THREADS / 32;
 constexpr uint32_t TR_BITS = 32768;            // bitmap ranks per warp (the most)
 constexpr int TR_LOWCAP = 256;                 // low prefix entries kept in shared memory
-constexpr int TR_UNROLL = 2;                   // quads per lane per step
+constexpr int TR_UNROLL = 4;                   // quads per lane per step
 constexpr int TR_QCAP = 512;                   // queued hits per warp (ring)
 
 struct TrWarp {
     uint32_t bm[TR_BITS / 32];
     int32_t low[TR_LOWCAP];
     int2 q[TR_QCAP];   // (c, lane of the edge)
+    uint8_t pos[TR_UNROLL][32];   // lane of the edge whose quads start at each window position
 };
 constexpr size_t TR_SMEM = TR_WARPS * sizeof(TrWarp);
 static_assert(sizeof(TrWarp) % 16 == 0, "TrWarp keeps 16-byte alignment");
-static_assert(TR_QCAP >= 32 + 32 * 4 * TR_UNROLL, "the queue takes one step's hits");
+static_assert(TR_QCAP >= 32 * 4 * TR_UNROLL, "the queue takes one step's hits");
 
 __device__ __forceinline__ bool tr_sorted_find(const int32_t *v, uint64_t n, int32_t c) {
     uint64_t lo = 0, hi = n;
@@ -466,11 +467,15 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
             }
             tl = lo;
         }
+        // quads of this edge's suffix part in the bitmap's ranks
+        const uint32_t nq = te > tl ? (uint32_t)(((te + 3) >> 2) - (tl >> 2)) : 0u;
+        const uint32_t qs = (uint32_t)(tl >> 2), h = (uint32_t)(tl & 3), len = (uint32_t)(te - tl);
         unsigned todo = __ballot_sync(AMJ_FULL_MASK, valid && te > ts);
+        // the edges of one b form a run of lanes (the edges are sorted by b)
         while (todo) {
-            const int l = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int32_t wb = __shfl_sync(AMJ_FULL_MASK, b, l);
+            const int32_t wb = __shfl_sync(AMJ_FULL_MASK, b, __ffs(todo) - 1);
+            const unsigned run = todo & __ballot_sync(AMJ_FULL_MASK, b == wb);
+            todo &= ~run;
             if (!have_b || wb != cur_b) {
                 if (have_b) clear_bits();
                 set_bits(wb);
@@ -478,63 +483,88 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
                 have_b = true;
             }
             if (db == 0) continue;
+            const bool in_run = (run >> lane) & 1u;
+            // suffix values below the bitmap (rare): binary search in S(b)'s low prefix
             const bool low_smem = nl <= TR_LOWCAP;
-            const uint64_t wts = __shfl_sync(AMJ_FULL_MASK, ts, l);
-            const uint64_t wtl = __shfl_sync(AMJ_FULL_MASK, tl, l);
-            const uint64_t wte = __shfl_sync(AMJ_FULL_MASK, te, l);
-            // values below the bitmap: binary search in S(b)'s low prefix
-            for (uint64_t k0 = wts; k0 < wtl; k0 += 32) {
-                const uint64_t k = k0 + lane;
-                bool hit = false;
-                int32_t c = 0;
-                if (k < wtl) {
-                    c = d1[k];
-                    hit = nl && (low_smem ? tr_sorted_find(W.low, nl, c) : tr_sorted_find(bl, nl, c));
+            unsigned lows = run & __ballot_sync(AMJ_FULL_MASK, tl > ts);
+            while (lows) {
+                const int l = __ffs(lows) - 1;
+                lows &= lows - 1;
+                const uint64_t wts = __shfl_sync(AMJ_FULL_MASK, ts, l);
+                const uint64_t wtl = __shfl_sync(AMJ_FULL_MASK, tl, l);
+                for (uint64_t k0 = wts; k0 < wtl; k0 += 32) {
+                    const uint64_t k = k0 + lane;
+                    bool hit = false;
+                    int32_t c = 0;
+                    if (k < wtl) {
+                        c = d1[k];
+                        hit = nl && (low_smem ? tr_sorted_find(W.low, nl, c) : tr_sorted_find(bl, nl, c));
+                    }
+                    const unsigned m = __ballot_sync(AMJ_FULL_MASK, hit);
+                    if (hit) W.q[(qh + qn + __popc(m & lanemask_lt())) & (TR_QCAP - 1)] = make_int2(c, l);
+                    qn += __popc(m);
+                    while (qn >= 32) flush(32);
                 }
-                const unsigned m = __ballot_sync(AMJ_FULL_MASK, hit);
-                if (hit) W.q[(qh + qn + __popc(m & lanemask_lt())) & (TR_QCAP - 1)] = make_int2(c, l);
-                qn += __popc(m);
-                while (qn >= 32) flush(32);
             }
-            // values in the bitmap, as aligned quads of level 1
-            const uint64_t qlo = wtl >> 2, qhi = (wte + 3) >> 2;
-            const uint32_t h = (uint32_t)(wtl & 3);
-            const uint32_t hl = h + (uint32_t)(wte - wtl);   // suffix end, from the first quad's start
-            for (uint64_t q0 = qlo; q0 < qhi; q0 += 32 * TR_UNROLL) {
-                const uint32_t remq = (uint32_t)(qhi - q0 < 32 * TR_UNROLL ? qhi - q0 : 32 * TR_UNROLL);
-                const uint32_t qoff = (uint32_t)(q0 - qlo);
+            // the run's suffixes as one stream of quads: P = this edge's first
+            // quad in the stream, Q = the stream's length
+            const uint32_t x = in_run ? nq : 0u;
+            const uint32_t incl = warp_inclusive_scan(x, lane);
+            const uint32_t P = incl - x;
+            const uint32_t Q = __shfl_sync(AMJ_FULL_MASK, incl, 31);
+            const bool has = x > 0;
+            for (uint32_t f0 = 0; f0 < Q; f0 += 32 * TR_UNROLL) {
                 int4 cv[TR_UNROLL];
+                uint32_t m4[TR_UNROLL];
+                int own[TR_UNROLL];
 #pragma unroll
                 for (int u = 0; u < TR_UNROLL; u++)
-                    if ((uint32_t)u * 32 < remq) {
-                        const uint32_t kq = u * 32 + lane;
-                        cv[u] = dq[q0 + (kq < remq ? kq : 0)];
+                    if (f0 + (uint32_t)u * 32 < Q) {
+                        // owner of quad w0 + lane: the last edge starting at or before it
+                        const uint32_t w0 = f0 + u * 32;
+                        const uint32_t d = P - w0;
+                        const bool st = has && P > w0 && d < 32;
+                        const uint32_t M = __reduce_or_sync(AMJ_FULL_MASK, st ? (1u << d) : 0u);
+                        if (st) W.pos[u][d] = (uint8_t)lane;
+                        const unsigned before = __ballot_sync(AMJ_FULL_MASK, has && P <= w0);
+                        __syncwarp();
+                        const uint32_t mle = M & (0xFFFFFFFFu >> (31 - lane));
+                        const int o = mle ? (int)W.pos[u][31 - __clz(mle)] : 31 - __clz(before);
+                        own[u] = o;
+                        const uint32_t oqs = __shfl_sync(AMJ_FULL_MASK, qs, o);
+                        const uint32_t oP = __shfl_sync(AMJ_FULL_MASK, P, o);
+                        const uint32_t oh = __shfl_sync(AMJ_FULL_MASK, h, o);
+                        const uint32_t ohl = oh + __shfl_sync(AMJ_FULL_MASK, len, o);
+                        const uint32_t f = w0 + lane;
+                        const bool vq = f < Q;
+                        const uint32_t rel = f - oP;
+                        // values t of this quad inside the suffix: lo <= t < hi
+                        const uint32_t e0 = 4 * rel;
+                        const uint32_t lo = e0 == 0 ? oh : 0u;
+                        const uint32_t hi = ohl > e0 ? (ohl - e0 < 4 ? ohl - e0 : 4u) : 0u;
+                        m4[u] = vq && hi > lo ? ((0xFu >> (4 - hi)) & (0xFu << lo)) : 0u;
+                        cv[u] = dq[vq ? (uint64_t)oqs + rel : (uint64_t)oqs];
                     }
                 uint32_t bits = 0;
 #pragma unroll
                 for (int u = 0; u < TR_UNROLL; u++)
-                    if ((uint32_t)u * 32 < remq) {
-                        const uint32_t kq = u * 32 + lane;
-                        // values t of this quad inside the suffix: lo <= t < hi
-                        const uint32_t e0 = 4 * (qoff + kq);
-                        const uint32_t lo = e0 == 0 ? h : 0u;
-                        const uint32_t hi = hl > e0 ? (hl - e0 < 4 ? hl - e0 : 4u) : 0u;
-                        const uint32_t m4 = kq < remq && hi > lo ? ((0xFu >> (4 - hi)) & (0xFu << lo)) : 0u;
+                    if (f0 + (uint32_t)u * 32 < Q) {
                         const uint32_t t4 = tr_bit(W.bm, cv[u].x, base) | (tr_bit(W.bm, cv[u].y, base) << 1) |
                                             (tr_bit(W.bm, cv[u].z, base) << 2) | (tr_bit(W.bm, cv[u].w, base) << 3);
-                        bits |= (t4 & m4) << (4 * u);
+                        bits |= (t4 & m4[u]) << (4 * u);
                     }
                 const uint32_t nh = __popc(bits);
-                const uint32_t incl = warp_inclusive_scan(nh, lane);
-                const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, incl, 31);
+                const uint32_t hincl = warp_inclusive_scan(nh, lane);
+                const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, hincl, 31);
                 if (tot) {
-                    uint32_t pos = qh + qn + incl - nh;
+                    if (qn + tot > TR_QCAP) flush(qn);   // (nearly every value a hit) make room
+                    uint32_t pos = qh + qn + hincl - nh;
 #pragma unroll
                     for (int u = 0; u < TR_UNROLL; u++) {
-                        if ((bits >> (4 * u)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].x, l);
-                        if ((bits >> (4 * u + 1)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].y, l);
-                        if ((bits >> (4 * u + 2)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].z, l);
-                        if ((bits >> (4 * u + 3)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].w, l);
+                        if ((bits >> (4 * u)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].x, own[u]);
+                        if ((bits >> (4 * u + 1)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].y, own[u]);
+                        if ((bits >> (4 * u + 2)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].z, own[u]);
+                        if ((bits >> (4 * u + 3)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].w, own[u]);
                     }
                     qn += tot;
                     while (qn >= 32) flush(32);
