@@ -152,12 +152,9 @@ __global__ __launch_bounds__(RS_THREADS) void rs_downsweep_kernel(const uint64_t
         const bool valid = idx < n;
         it[r] = valid ? in[idx] : 0ull;
         const uint32_t d = valid ? ((uint32_t)(sort_key<KK>(it[r]) >> shift) & dmask) : 0u;
-        unsigned peers = __ballot_sync(AMJ_FULL_MASK, valid);
-        for (int b = 0; b < bits; b++) {
-            const bool bit = (d >> b) & 1u;
-            const unsigned bb = __ballot_sync(AMJ_FULL_MASK, bit);
-            peers &= bit ? bb : ~bb;
-        }
+        // lanes holding the same digit (invalid lanes match only each other)
+        const unsigned peers = __match_any_sync(AMJ_FULL_MASK, valid ? d : 0xffffffffu) &
+                               __ballot_sync(AMJ_FULL_MASK, valid);
         const uint32_t rank = __popc(peers & lt);
         const uint32_t before = valid ? wcnt[warp][d] : 0u;
         __syncwarp();

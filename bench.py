@@ -152,10 +152,22 @@ class Triangle:
         return ctx.lftj(rels, algo=self.algo, ws=1)
 
     def algorithmic_bytes(self):
-        """Per intersection: every edge once (8 B), two row-pointer pairs
-        (32 B) and the shorter child list of the edge once (4 B each)."""
-        deg = np.bincount(self.src, minlength=1 << self.scale).astype(np.int64)
-        shorter = np.minimum(deg[self.src], deg[self.dst])
+        """DFS (the wedge kernel over the degree-ranked copy): per edge its
+        (b, entry) item (8 B), the level-0 value a (4 B) and the end of a's
+        child range (8 B); per tested value 4 B, sum over a of C(d+(a), 2)
+        values with d+ the out-degree in (degree, id) order.  BFS / AMHJ:
+        every edge once (8 B), two row-pointer pairs (32 B) and the shorter
+        child list of the edge once (4 B each), in the relation's order."""
+        V = 1 << self.scale
+        src, dst = self.src.astype(np.int64), self.dst.astype(np.int64)
+        if self.algo == "DFS":
+            deg = np.bincount(src, minlength=V) + np.bincount(dst, minlength=V)
+            key_s, key_d = deg[src] * V + src, deg[dst] * V + dst
+            lo = np.where(key_s < key_d, src, dst)
+            dplus = np.bincount(lo, minlength=V).astype(np.int64)
+            return self.E * (8 + 4 + 8) + 4 * int((dplus * (dplus - 1) // 2).sum())
+        deg = np.bincount(src, minlength=V).astype(np.int64)
+        shorter = np.minimum(deg[src], deg[dst])
         return self.E * (8 + 32) + 4 * int(shorter.sum())
 
     def kernel_name(self):
@@ -616,10 +628,10 @@ def profiled_traffic(args):
     full-size triangle workload, or None."""
     if args.workload != "triangle" or args.scale != SCALE or args.algo != "DFS":
         return None
-    p = os.path.join(ROOT, "profiles", "lftj_intersect_c2_traffic.md")
+    p = os.path.join(ROOT, "profiles", "lftj_tri_wedge_kernel_c2.md")
     if not os.path.exists(p):
         return None
-    m = re.search(r"traffic_bytes_per_intersection:\s*([0-9]+)", open(p).read())
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", open(p).read())
     return int(m.group(1)) if m else None
 
 
