@@ -126,7 +126,7 @@ __global__ __launch_bounds__(RS_THREADS) void rs_upsweep_kernel(const uint64_t *
 }
 
 template <int KK>
-__global__ __launch_bounds__(RS_THREADS) void rs_downsweep_kernel(const uint64_t *__restrict__ in,
+__global__ __launch_bounds__(RS_THREADS, 3) void rs_downsweep_kernel(const uint64_t *__restrict__ in,
                                                                    uint64_t *__restrict__ out, uint32_t n,
                                                                    int shift, int bits,
                                                                    const uint32_t *__restrict__ offs,
@@ -146,11 +146,16 @@ __global__ __launch_bounds__(RS_THREADS) void rs_downsweep_kernel(const uint64_t
     const unsigned lt = lanemask_lt();
     uint64_t it[RS_IPT];
     uint32_t rk[RS_IPT];
+    // all of the thread's loads in flight before the ranking
+#pragma unroll
+    for (int r = 0; r < RS_IPT; r++) {
+        const uint64_t idx = base + (uint64_t)r * 32 + lane;
+        it[r] = idx < n ? in[idx] : 0ull;
+    }
 #pragma unroll
     for (int r = 0; r < RS_IPT; r++) {
         const uint64_t idx = base + (uint64_t)r * 32 + lane;
         const bool valid = idx < n;
-        it[r] = valid ? in[idx] : 0ull;
         const uint32_t d = valid ? ((uint32_t)(sort_key<KK>(it[r]) >> shift) & dmask) : 0u;
         // lanes holding the same digit (invalid lanes match only each other)
         const unsigned peers = __match_any_sync(AMJ_FULL_MASK, valid ? d : 0xffffffffu) &
