@@ -324,7 +324,6 @@ struct TrWarp {
     uint32_t bm[TR_BITS / 32];
     int32_t low[TR_LOWCAP];
     int2 q[TR_QCAP];   // (c, lane of the edge)
-    uint8_t pos[TR_UNROLL][32];   // lane of the edge whose quads start at each window position
 };
 constexpr size_t TR_SMEM = TR_WARPS * sizeof(TrWarp);
 static_assert(sizeof(TrWarp) % 16 == 0, "TrWarp keeps 16-byte alignment");
@@ -513,46 +512,53 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
             const uint32_t P = incl - x;
             const uint32_t Q = __shfl_sync(AMJ_FULL_MASK, incl, 31);
             const bool has = x > 0;
+            const uint32_t qsh = qs | (h << 30);   // first quad (< 2^30) and head offset
+            const uint32_t hl = h + len;           // suffix end, from the first quad's start
+            const uint32_t pend = P + x;           // end of this edge's quads in the stream
+            const unsigned hm = __ballot_sync(AMJ_FULL_MASK, has);
             for (uint32_t f0 = 0; f0 < Q; f0 += 32 * TR_UNROLL) {
+                // this lane's quads f0 + TR_UNROLL * lane + t; the owner of the
+                // first is the last lane whose quads start at or before it (the
+                // starts P never decrease over the lanes)
+                const uint32_t fl = f0 + TR_UNROLL * lane;
+                int o = 0;
+#pragma unroll
+                for (int sft = 16; sft >= 1; sft >>= 1)
+                    if (__shfl_sync(AMJ_FULL_MASK, P, o + sft) <= fl) o += sft;
                 int4 cv[TR_UNROLL];
                 uint32_t m4[TR_UNROLL];
                 int own[TR_UNROLL];
+                uint32_t oqsh = 0, oP = 0, ohl = 0, oe = 0;
 #pragma unroll
-                for (int u = 0; u < TR_UNROLL; u++)
-                    if (f0 + (uint32_t)u * 32 < Q) {
-                        // owner of quad w0 + lane: the last edge starting at or before it
-                        const uint32_t w0 = f0 + u * 32;
-                        const uint32_t d = P - w0;
-                        const bool st = has && P > w0 && d < 32;
-                        const uint32_t M = __reduce_or_sync(AMJ_FULL_MASK, st ? (1u << d) : 0u);
-                        if (st) W.pos[u][d] = (uint8_t)lane;
-                        const unsigned before = __ballot_sync(AMJ_FULL_MASK, has && P <= w0);
-                        __syncwarp();
-                        const uint32_t mle = M & (0xFFFFFFFFu >> (31 - lane));
-                        const int o = mle ? (int)W.pos[u][31 - __clz(mle)] : 31 - __clz(before);
-                        own[u] = o;
-                        const uint32_t oqs = __shfl_sync(AMJ_FULL_MASK, qs, o);
-                        const uint32_t oP = __shfl_sync(AMJ_FULL_MASK, P, o);
-                        const uint32_t oh = __shfl_sync(AMJ_FULL_MASK, h, o);
-                        const uint32_t ohl = oh + __shfl_sync(AMJ_FULL_MASK, len, o);
-                        const uint32_t f = w0 + lane;
-                        const bool vq = f < Q;
-                        const uint32_t rel = f - oP;
-                        // values t of this quad inside the suffix: lo <= t < hi
-                        const uint32_t e0 = 4 * rel;
-                        const uint32_t lo = e0 == 0 ? oh : 0u;
-                        const uint32_t hi = ohl > e0 ? (ohl - e0 < 4 ? ohl - e0 : 4u) : 0u;
-                        m4[u] = vq && hi > lo ? ((0xFu >> (4 - hi)) & (0xFu << lo)) : 0u;
-                        cv[u] = dq[vq ? (uint64_t)oqs + rel : (uint64_t)oqs];
+                for (int u = 0; u < TR_UNROLL; u++) {
+                    const uint32_t f = fl + u;
+                    // quads of consecutive f cross at most one edge boundary
+                    if (u > 0 && f >= oe) {
+                        const unsigned rest = hm & ~(0xFFFFFFFFu >> (31 - o));
+                        if (rest) o = __ffs(rest) - 1;
                     }
+                    oqsh = __shfl_sync(AMJ_FULL_MASK, qsh, o);
+                    oP = __shfl_sync(AMJ_FULL_MASK, P, o);
+                    ohl = __shfl_sync(AMJ_FULL_MASK, hl, o);
+                    oe = __shfl_sync(AMJ_FULL_MASK, pend, o);
+                    own[u] = o;
+                    const bool vq = f < Q;
+                    const uint32_t rel = f - oP;
+                    // values t of this quad inside the suffix: lo <= t < hi
+                    const uint32_t e0 = 4 * rel;
+                    const uint32_t lo = e0 == 0 ? (oqsh >> 30) : 0u;
+                    const uint32_t hi = ohl > e0 ? (ohl - e0 < 4 ? ohl - e0 : 4u) : 0u;
+                    m4[u] = vq && hi > lo ? ((0xFu >> (4 - hi)) & (0xFu << lo)) : 0u;
+                    const uint64_t q = (uint64_t)(oqsh & 0x3FFFFFFFu) + (vq ? rel : 0u);
+                    cv[u] = dq[q];
+                }
                 uint32_t bits = 0;
 #pragma unroll
-                for (int u = 0; u < TR_UNROLL; u++)
-                    if (f0 + (uint32_t)u * 32 < Q) {
-                        const uint32_t t4 = tr_bit(W.bm, cv[u].x, base) | (tr_bit(W.bm, cv[u].y, base) << 1) |
-                                            (tr_bit(W.bm, cv[u].z, base) << 2) | (tr_bit(W.bm, cv[u].w, base) << 3);
-                        bits |= (t4 & m4[u]) << (4 * u);
-                    }
+                for (int u = 0; u < TR_UNROLL; u++) {
+                    const uint32_t t4 = tr_bit(W.bm, cv[u].x, base) | (tr_bit(W.bm, cv[u].y, base) << 1) |
+                                        (tr_bit(W.bm, cv[u].z, base) << 2) | (tr_bit(W.bm, cv[u].w, base) << 3);
+                    bits |= (t4 & m4[u]) << (4 * u);
+                }
                 const uint32_t nh = __popc(bits);
                 const uint32_t hincl = warp_inclusive_scan(nh, lane);
                 const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, hincl, 31);
