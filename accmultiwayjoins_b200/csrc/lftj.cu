@@ -62,7 +62,9 @@ struct TriArgs {
     const int32_t *src1;          // level-0 value of every level-1 entry of R
     uint32_t rank_base;           // first rank of the per-warp bitmap
     uint32_t rank_bits;           // ranks the bitmap covers
-    unsigned long long *cursor_r; // claim cursor of the rank kernel
+    unsigned long long *cursor_r; // claim cursor of the wedge kernel
+    int bfs_wedge;                // BFS over one degree-ordered relation (R = S = T): the
+                                  // candidates of entry (a, b) are T(a)'s values after b
 };
 
 // A triangle found as (a, b, c) in the tuple the query lists: attribute order,
@@ -731,13 +733,19 @@ __global__ __launch_bounds__(256) void lftj_tri_dfs_kernel(const __grid_constant
 // ---- BFS ----
 
 // candidates of entry j: the shorter child list of (S(b), T(a)); 0 when either is empty
+// (wedge form: T(a)'s values after b, when S(b) is not empty)
 __global__ void lftj_tri_bfs_count_kernel(const __grid_constant__ TriArgs A, unsigned long long *cand) {
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < A.r_n; j += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t sb, eb, ta = 0, ea = 0;
         child_range(A.S, A.r_dst[j], sb, eb);
         if (eb > sb) child_range(A.T, A.r_src[j], ta, ea);
         const uint64_t lb = eb - sb, la = ea - ta;
-        cand[j] = (lb && la) ? (lb < la ? lb : la) : 0ull;
+        if (A.bfs_wedge) {
+            const uint64_t g = A.r_lo + j;   // the entry's position in T(a)
+            cand[j] = (lb && ea > g + 1) ? ea - g - 1 : 0ull;
+        } else {
+            cand[j] = (lb && la) ? (lb < la ? lb : la) : 0ull;
+        }
     }
 }
 
@@ -796,9 +804,11 @@ __global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const 
             uint64_t sb, eb, ta, ea;
             child_range(A.S, b, sb, eb);
             child_range(A.T, a, ta, ea);
-            // expand the shorter list, search the longer
-            const bool s_short = (eb - sb) <= (ea - ta);
-            const int32_t c = s_short ? A.S.data1[sb + k] : A.T.data1[ta + k];
+            // expand the shorter list, search the longer (wedge form: expand
+            // T(a) after b, search S(b))
+            const bool s_short = !A.bfs_wedge && (eb - sb) <= (ea - ta);
+            const int32_t c = s_short ? A.S.data1[sb + k]
+                                      : A.T.data1[(A.bfs_wedge ? A.r_lo + e + 1 : ta) + k];
             const int32_t *hay = s_short ? A.T.data1 : A.S.data1;
             uint64_t lo = s_short ? ta : sb, hi = s_short ? ea : eb;
             while (lo < hi) {
@@ -808,11 +818,12 @@ __global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const 
             }
             const bool found = lo < (s_short ? ea : eb) && hay[lo] == c;
             if (found) {
+                const int32_t xa = A.inv ? A.inv[a] : a, xb = A.inv ? A.inv[b] : b, xc = A.inv ? A.inv[c] : c;
                 cnt++;
-                chk += tri_chk(A, amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a), b), a, b, c);
+                chk += tri_chk(A, amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, xa), xb), xa, xb, xc);
                 if (WRITE) {
                     const unsigned long long p = atomicAdd(A.out_cursor, 1ull);
-                    if (p < A.out_cap) tri_store(A, p, a, b, c);
+                    if (p < A.out_cap) tri_store(A, p, xa, xb, xc);
                 }
             }
         }
@@ -934,6 +945,9 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
                 timed[1] = true;
             }
         } else {
+            // a degree-ranked trie (ranks as vertex ids): wedge candidates, ids mapped back
+            A.bfs_wedge = inv != nullptr && &R == &S && &S == &T;
+            A.inv = inv;
             DBuf<unsigned long long> cand;
             AMJ_TRY(cand.alloc(ctx, A.r_n + 1));
             const unsigned g1 = (unsigned)std::min<uint64_t>((A.r_n + 255) / 256, (uint64_t)ctx->num_sms * 16);

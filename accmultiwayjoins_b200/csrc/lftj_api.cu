@@ -164,10 +164,11 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         bool deg_order = algo == AMJ_LFTJ_BFS || ws;
         if (flags & AMJ_F_DEGREE_ORDER) deg_order = true;
         if (flags & AMJ_F_KEEP_ORDER) deg_order = false;
-        if (deg_order && algo == AMJ_LFTJ_DFS && ws) {
+        if (deg_order && (algo == AMJ_LFTJ_BFS || ws)) {
+            // the degree-ranked copy: the wedge kernel (DFS) or wedge candidates (BFS)
             AMJ_TRY(build_ranked_trie(ctx, rels[0], &tries[0], &inv, &nv));
             sorted_out = nv ? 1 : 0;
-            if (nv) AMJ_TRY(build_wedges(ctx, tries[0], nv, &wedges));
+            if (nv && algo == AMJ_LFTJ_DFS) AMJ_TRY(build_wedges(ctx, tries[0], nv, &wedges));
         } else {
             AMJ_TRY(build_self_trie(ctx, rels[0], &tries[0], &sorted_out, deg_order));
         }
