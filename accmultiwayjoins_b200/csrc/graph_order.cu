@@ -69,6 +69,9 @@ int degree_ordered_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint
     AMJ_CUDA_TRY(cudaMemcpyAsync(&h, pr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
     AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (h.bad) return AMJ_OK;
+    // per-vertex arrays are sized by the largest id: sparse ids keep the
+    // relation's own order instead
+    if ((uint64_t)h.maxv + 1 > 4 * n + (1ull << 20)) return AMJ_OK;
     DBuf<unsigned int> deg;
     AMJ_TRY(deg.alloc(ctx, (uint64_t)h.maxv + 1));
     AMJ_TRY(ns->alloc(ctx, n));
@@ -142,6 +145,9 @@ int degree_ranked_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint6
     AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (h.bad) return AMJ_OK;
     const uint64_t V = (uint64_t)h.maxv + 1;
+    // per-vertex arrays are sized by the largest id: sparse ids keep the
+    // relation's own order instead
+    if (V > 4 * n + (1ull << 20)) return AMJ_OK;
     DBuf<unsigned int> deg;
     AMJ_TRY(deg.alloc(ctx, V));
     AMJ_CUDA_TRY(cudaMemsetAsync(deg.p, 0, V * sizeof(unsigned int), ctx->stream));

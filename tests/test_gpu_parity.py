@@ -607,6 +607,32 @@ def test_lftj_wedge_kernel_bitmap_and_low_prefix(rankbits):
             assert np.array_equal(sorted_rows(m.columns), sorted_rows(cols))
 
 
+def tiny_graphs():
+    k5 = [(u, v) for u in range(5) for v in range(u + 1, 5)]
+    big = [(5, 1 << 30), (5, (1 << 31) - 2), (1 << 30, (1 << 31) - 2), (7, 9)]
+    return {"K5": k5, "one triangle": [(0, 1), (0, 2), (1, 2)], "star": [(0, 1), (0, 2), (0, 3)],
+            "one edge": [(3, 4)], "sparse huge ids": big,
+            "two triangles on an edge": [(0, 1), (0, 2), (1, 2), (0, 3), (1, 3)]}
+
+
+@pytest.mark.parametrize("name", list(tiny_graphs()))
+def test_lftj_triangle_tiny_and_sparse_graphs(ctx, name):
+    """Small graphs through every triangle path; ids up to 2^31 - 2 make the
+    degree order step aside (its arrays are sized by the largest id), and the
+    relation is joined in its own order."""
+    edges = tiny_graphs()[name]
+    s = np.array([u for u, _ in edges], np.int32)
+    d = np.array([v for _, v in edges], np.int32)
+    want = O.triangle(s, d)
+    e = ctx.relation([s, d], [0, 1])
+    for algo in ("DFS", "BFS"):
+        for ws in (0, 1):
+            got = ctx.lftj([e], algo=algo, ws=ws, materialize=True)
+            assert (got.count, got.checksum) == want, (algo, ws)
+            assert data.checksum(got.columns) == want[1]
+    assert (lambda r: (r.count, r.checksum))(ctx.amhj("TRI", [e], ws=1)) == want
+
+
 def test_lftj_out_of_core_slices():
     with Context(0, ooc_slice_rows=5000) as ctx:
         s, d = data.rmat(11, 30000, 0.57, 0.19, 0.19, 7)
