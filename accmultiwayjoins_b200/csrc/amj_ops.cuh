@@ -56,7 +56,9 @@ struct Trie2 {
 // Level 1 of a built 2-level trie has TRIE_LEVEL1_PAD spare values after its
 // last one, so kernels may read it in aligned 16-byte quads.
 constexpr uint64_t TRIE_LEVEL1_PAD = 4;
-int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out);
+// distinct: drop repeated rows (the set semantics of the leapfrog triejoin)
+int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out,
+                bool distinct = false);
 
 // time between two events recorded on the context stream (ms)
 double event_ms(cudaEvent_t a, cudaEvent_t b);

@@ -8,6 +8,9 @@
 // (exec_LFTJ.cu:92-95); three relations must carry the attribute pairs
 // (0,1), (1,2), (0,2).  Each trie is built with its columns in attribute
 // order, as the reference orders them through a std::map (exec_LFTJ.cu:148-156).
+// The relations are joined as sets, the semantics of the leapfrog triejoin:
+// a repeated row counts once (the trie builds drop repeats; the reference's
+// inputs are deduplicated edge lists).
 #include "amj_ops.cuh"
 
 #include <algorithm>
@@ -34,13 +37,13 @@ static int build_self_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, int *sorted
     if (r->where == AMJ_MEM_HOST_STREAMED) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must be on the device");
     const bool swap = r->attrs[0] > r->attrs[1];
     const int32_t *c0 = r->d_cols[swap ? 1 : 0], *c1 = r->d_cols[swap ? 0 : 1];
-    if (!allow) return build_trie2(ctx, c0, c1, r->n, t);
+    if (!allow) return build_trie2(ctx, c0, c1, r->n, t, true);
     DBuf<int32_t> ns, nd;
     bool oriented = false;
     AMJ_TRY(degree_ordered_copy(ctx, c0, c1, r->n, &ns, &nd, &oriented));
-    if (!oriented) return build_trie2(ctx, c0, c1, r->n, t);
+    if (!oriented) return build_trie2(ctx, c0, c1, r->n, t, true);
     *sorted = 1;
-    return build_trie2(ctx, ns.p, nd.p, r->n, t);
+    return build_trie2(ctx, ns.p, nd.p, r->n, t, true);
 }
 
 // Trie of the degree-ranked copy (*inv maps ranks to vertex ids) when the
@@ -54,8 +57,8 @@ static int build_ranked_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, DBuf<int3
     DBuf<int32_t> ns, nd;
     bool oriented = false;
     AMJ_TRY(degree_ranked_copy(ctx, c0, c1, r->n, &ns, &nd, inv, nv, &oriented));
-    if (!oriented) return build_trie2(ctx, c0, c1, r->n, t);
-    return build_trie2(ctx, ns.p, nd.p, r->n, t);
+    if (!oriented) return build_trie2(ctx, c0, c1, r->n, t, true);
+    return build_trie2(ctx, ns.p, nd.p, r->n, t, true);
 }
 }
 
@@ -65,7 +68,7 @@ static int build_rel_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t) {
     if (r->ncols != 2) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must have two columns");
     if (r->where == AMJ_MEM_HOST_STREAMED) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must be on the device");
     const bool swap = r->attrs[0] > r->attrs[1];
-    return build_trie2(ctx, r->d_cols[swap ? 1 : 0], r->d_cols[swap ? 0 : 1], r->n, t);
+    return build_trie2(ctx, r->d_cols[swap ? 1 : 0], r->d_cols[swap ? 0 : 1], r->n, t, true);
 }
 
 // The 4-clique over one edge relation (AMJ_F_CLIQUE4): a count pass, then

@@ -313,7 +313,7 @@ int lftj_generic_compile(amj_ctx *ctx, amj_rel *const *rels, int nrels, GenQuery
         const int x = (int)(swap ? rels[i]->attrs[1] : rels[i]->attrs[0]);
         const int y = (int)(swap ? rels[i]->attrs[0] : rels[i]->attrs[1]);
         AMJ_TRY(build_trie2(ctx, rels[i]->d_cols[swap ? 1 : 0], rels[i]->d_cols[swap ? 0 : 1], rels[i]->n,
-                            &Q->tries[i]));
+                            &Q->tries[i], true));
         const TrieRef tr = trie_ref(Q->tries[i]);
         if (Q->lv[y].n >= GEN_MAX_LISTS) return fail(AMJ_EUNSUPPORTED, "LFTJ: more than 8 relations close one attribute");
         Q->lv[y].t[Q->lv[y].n] = tr;

@@ -80,6 +80,26 @@ __global__ void scatter_level0_kernel(const uint64_t *__restrict__ items, const 
     (void)head;
 }
 
+// adjacent equal items of a sorted array (duplicate rows), counted per block
+__global__ void count_dups_kernel(const uint64_t *__restrict__ items, uint64_t n, unsigned long long *dups) {
+    unsigned long long c = 0;
+    for (uint64_t i = 1 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        c += items[i] == items[i - 1];
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(dups, c);
+}
+
+__global__ void first_of_run_kernel(const uint64_t *__restrict__ items, uint64_t n, uint32_t *__restrict__ flag) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        flag[i] = (i == 0 || items[i] != items[i - 1]) ? 1u : 0u;
+}
+
+__global__ void compact_runs_kernel(const uint64_t *__restrict__ items, const uint32_t *__restrict__ pos, uint64_t n,
+                                    uint64_t *__restrict__ out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (i == 0 || items[i] != items[i - 1]) out[pos[i]] = items[i];
+}
+
 // child counts of every level-0 value, indexed densely by value - min
 __global__ void dense_counts_kernel(const int32_t *__restrict__ data0, const uint64_t *__restrict__ off0,
                                     uint64_t len0, int32_t vmin, uint64_t *__restrict__ counts) {
@@ -98,7 +118,7 @@ static int bits_for(uint32_t range) {
     return b;
 }
 
-int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out) {
+int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out, bool distinct) {
     if (n >= (1ull << 32) - 4096) return fail(AMJ_EUNSUPPORTED, "trie build: 2^32 or more rows");
     out->len1 = n;
     if (n == 0) {
@@ -130,6 +150,33 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
     AMJ_CUDA_TRY(cudaGetLastError());
     uint64_t *sorted = nullptr;
     AMJ_TRY(radix_sort_u64(ctx, a.p, b.p, n, SK_IDENT, 0, bits0 + bits1, &sorted));
+    if (distinct && n > 1) {
+        // set semantics: drop repeated rows (adjacent after the sort)
+        DBuf<unsigned long long> dups;
+        AMJ_TRY(dups.alloc(ctx, 1));
+        AMJ_CUDA_TRY(cudaMemsetAsync(dups.p, 0, sizeof(unsigned long long), ctx->stream));
+        note_launch(ctx);
+        count_dups_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, dups.p);
+        AMJ_CUDA_TRY(cudaGetLastError());
+        unsigned long long h_dups = 0;
+        AMJ_CUDA_TRY(cudaMemcpyAsync(&h_dups, dups.p, sizeof(h_dups), cudaMemcpyDeviceToHost, ctx->stream));
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (h_dups) {
+            DBuf<uint32_t> pos;
+            AMJ_TRY(pos.alloc(ctx, n));
+            note_launch(ctx);
+            first_of_run_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, pos.p);
+            AMJ_CUDA_TRY(cudaGetLastError());
+            AMJ_TRY(scan_exclusive_u32(ctx, pos.p, pos.p, n, nullptr));
+            uint64_t *other = sorted == a.p ? b.p : a.p;
+            note_launch(ctx);
+            compact_runs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, pos.p, n, other);
+            AMJ_CUDA_TRY(cudaGetLastError());
+            sorted = other;
+            n -= h_dups;
+            out->len1 = n;
+        }
+    }
 
     AMJ_TRY(out->data1.alloc(ctx, n + TRIE_LEVEL1_PAD));
     AMJ_TRY(out->src1.alloc(ctx, n));

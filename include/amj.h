@@ -163,7 +163,9 @@ int  amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *rels, int nr
  * any other nrels >= 3 (up to 16): the connected join of 2-column relations
  *             over attributes 0..k-1, k <= 8, in identity attribute order (the
  *             reference's LFTJ stops at 3 attributes and 3 tables); ooc = 0.
- * nrels == 2 is rejected, as in the reference (LFTJ-GPU/exec_LFTJ.cu:92-95). */
+ * nrels == 2 is rejected, as in the reference (LFTJ-GPU/exec_LFTJ.cu:92-95).
+ * Relations are joined as sets (leapfrog triejoin semantics): a repeated row
+ * counts once. */
 int  amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels,
                       int algo, int ooc, int ws, int flags, amj_result *out);
 

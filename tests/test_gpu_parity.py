@@ -633,6 +633,33 @@ def test_lftj_triangle_tiny_and_sparse_graphs(ctx, name):
     assert (lambda r: (r.count, r.checksum))(ctx.amhj("TRI", [e], ws=1)) == want
 
 
+def test_lftj_joins_relations_as_sets(ctx):
+    """A repeated row counts once in every ALFTJ path (the leapfrog triejoin
+    is defined over sets; the reference joins deduplicated edge lists)."""
+    s, d = data.rmat(12, 40000, 0.57, 0.19, 0.19, 8)
+    rng = np.random.Generator(np.random.PCG64(8))
+    rep = rng.integers(0, len(s), len(s) // 5)
+    perm = rng.permutation(len(s) + len(rep))
+    sd, dd = np.concatenate([s, s[rep]])[perm], np.concatenate([d, d[rep]])[perm]
+    want = O.triangle(s, d)
+    e = ctx.relation([sd, dd], [0, 1])
+    for algo in ("DFS", "BFS"):
+        for ws in (0, 1):
+            got = ctx.lftj([e], algo=algo, ws=ws)
+            assert (got.count, got.checksum) == want, (algo, ws)
+    R = ctx.relation([sd, dd], [0, 1])
+    S = ctx.relation([dd, sd], [2, 1])
+    T = ctx.relation([s, d], [0, 2])
+    got = ctx.lftj([R, S, T], algo="DFS")
+    assert (got.count, got.checksum) == want
+    c4 = ctx.lftj([e], clique4=True)
+    assert (c4.count, c4.checksum) == O.four_clique(s, d)
+    cyc = [(0, 1), (1, 2), (2, 3), (0, 3)]
+    plain = ctx.lftj([ctx.relation([s, d], list(p)) for p in cyc])
+    dup = ctx.lftj([ctx.relation([sd, dd], list(p)) for p in cyc])
+    assert (dup.count, dup.checksum) == (plain.count, plain.checksum) and plain.count > 0
+
+
 def test_lftj_out_of_core_slices():
     with Context(0, ooc_slice_rows=5000) as ctx:
         s, d = data.rmat(11, 30000, 0.57, 0.19, 0.19, 7)
