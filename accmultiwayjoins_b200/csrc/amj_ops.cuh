@@ -56,9 +56,10 @@ struct Trie2 {
 // Level 1 of a built 2-level trie has TRIE_LEVEL1_PAD spare values after its
 // last one, so kernels may read it in aligned 16-byte quads.
 constexpr uint64_t TRIE_LEVEL1_PAD = 4;
-// distinct: drop repeated rows (the set semantics of the leapfrog triejoin)
+// distinct: drop repeated rows (the set semantics of the leapfrog triejoin);
+// vmax >= 0: every value of both columns lies in [0, vmax] (no min/max pass)
 int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out,
-                bool distinct = false);
+                bool distinct = false, int32_t vmax = -1);
 
 // time between two events recorded on the context stream (ms)
 double event_ms(cudaEvent_t a, cudaEvent_t b);

@@ -118,7 +118,8 @@ static int bits_for(uint32_t range) {
     return b;
 }
 
-int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out, bool distinct) {
+int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out, bool distinct,
+                int32_t vmax) {
     if (n >= (1ull << 32) - 4096) return fail(AMJ_EUNSUPPORTED, "trie build: 2^32 or more rows");
     out->len1 = n;
     if (n == 0) {
@@ -129,16 +130,22 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
         AMJ_TRY(out->data1.alloc(ctx, TRIE_LEVEL1_PAD));
         return AMJ_OK;
     }
-    DBuf<uint32_t> mm;
-    AMJ_TRY(mm.alloc(ctx, 8));
-    const uint32_t init[4] = {0xffffffffu, 0u, 0xffffffffu, 0u};
-    AMJ_CUDA_TRY(cudaMemcpyAsync(mm.p, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
-    note_launch(ctx);
-    minmax_pairs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_c0, d_c1, n, mm.p);
-    AMJ_CUDA_TRY(cudaGetLastError());
-    uint32_t h_mm[4];
-    AMJ_CUDA_TRY(cudaMemcpyAsync(h_mm, mm.p, sizeof(h_mm), cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    uint32_t h_mm[4];   // flipped min / max of both columns
+    if (vmax >= 0) {
+        // the caller knows every value lies in [0, vmax]
+        h_mm[0] = h_mm[2] = 0x80000000u;
+        h_mm[1] = h_mm[3] = (uint32_t)vmax ^ 0x80000000u;
+    } else {
+        DBuf<uint32_t> mm;
+        AMJ_TRY(mm.alloc(ctx, 8));
+        const uint32_t init[4] = {0xffffffffu, 0u, 0xffffffffu, 0u};
+        AMJ_CUDA_TRY(cudaMemcpyAsync(mm.p, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+        note_launch(ctx);
+        minmax_pairs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_c0, d_c1, n, mm.p);
+        AMJ_CUDA_TRY(cudaGetLastError());
+        AMJ_CUDA_TRY(cudaMemcpyAsync(h_mm, mm.p, sizeof(h_mm), cudaMemcpyDeviceToHost, ctx->stream));
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    }
     const uint32_t min0 = h_mm[0], min1 = h_mm[2];
     const int bits0 = bits_for(h_mm[1] - min0), bits1 = bits_for(h_mm[3] - min1);
 
@@ -150,46 +157,48 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
     AMJ_CUDA_TRY(cudaGetLastError());
     uint64_t *sorted = nullptr;
     AMJ_TRY(radix_sort_u64(ctx, a.p, b.p, n, SK_IDENT, 0, bits0 + bits1, &sorted));
+    // set semantics (distinct): repeated rows are adjacent after the sort;
+    // they are counted beside the level-1 unpack and, when there are some,
+    // dropped and the unpack redone
+    DBuf<unsigned long long> dups;
     if (distinct && n > 1) {
-        // set semantics: drop repeated rows (adjacent after the sort)
-        DBuf<unsigned long long> dups;
         AMJ_TRY(dups.alloc(ctx, 1));
         AMJ_CUDA_TRY(cudaMemsetAsync(dups.p, 0, sizeof(unsigned long long), ctx->stream));
         note_launch(ctx);
         count_dups_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, dups.p);
         AMJ_CUDA_TRY(cudaGetLastError());
-        unsigned long long h_dups = 0;
-        AMJ_CUDA_TRY(cudaMemcpyAsync(&h_dups, dups.p, sizeof(h_dups), cudaMemcpyDeviceToHost, ctx->stream));
-        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-        if (h_dups) {
-            DBuf<uint32_t> pos;
-            AMJ_TRY(pos.alloc(ctx, n));
-            note_launch(ctx);
-            first_of_run_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, pos.p);
-            AMJ_CUDA_TRY(cudaGetLastError());
-            AMJ_TRY(scan_exclusive_u32(ctx, pos.p, pos.p, n, nullptr));
-            uint64_t *other = sorted == a.p ? b.p : a.p;
-            note_launch(ctx);
-            compact_runs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, pos.p, n, other);
-            AMJ_CUDA_TRY(cudaGetLastError());
-            sorted = other;
-            n -= h_dups;
-            out->len1 = n;
-        }
     }
-
     AMJ_TRY(out->data1.alloc(ctx, n + TRIE_LEVEL1_PAD));
     AMJ_TRY(out->src1.alloc(ctx, n));
     DBuf<uint32_t> head;
     AMJ_TRY(head.alloc(ctx, n + 1));
-    note_launch(ctx);
-    unpack_trie_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, min0, min1, bits1, out->data1.p,
-                                                                   out->src1.p, head.p);
-    AMJ_CUDA_TRY(cudaGetLastError());
-    AMJ_TRY(scan_exclusive_u32(ctx, head.p, head.p, n, head.p + n));
     uint32_t len0 = 0;
-    AMJ_CUDA_TRY(cudaMemcpyAsync(&len0, head.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    unsigned long long h_dups = 0;
+    for (int round = 0; round < 2; round++) {
+        note_launch(ctx);
+        unpack_trie_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, min0, min1, bits1, out->data1.p,
+                                                                       out->src1.p, head.p);
+        AMJ_CUDA_TRY(cudaGetLastError());
+        AMJ_TRY(scan_exclusive_u32(ctx, head.p, head.p, n, head.p + n));
+        AMJ_CUDA_TRY(cudaMemcpyAsync(&len0, head.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        if (round == 0 && dups.p)
+            AMJ_CUDA_TRY(cudaMemcpyAsync(&h_dups, dups.p, sizeof(h_dups), cudaMemcpyDeviceToHost, ctx->stream));
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (round > 0 || h_dups == 0) break;
+        DBuf<uint32_t> pos;
+        AMJ_TRY(pos.alloc(ctx, n));
+        note_launch(ctx);
+        first_of_run_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, n, pos.p);
+        AMJ_CUDA_TRY(cudaGetLastError());
+        AMJ_TRY(scan_exclusive_u32(ctx, pos.p, pos.p, n, nullptr));
+        uint64_t *other = sorted == a.p ? b.p : a.p;
+        note_launch(ctx);
+        compact_runs_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(sorted, pos.p, n, other);
+        AMJ_CUDA_TRY(cudaGetLastError());
+        sorted = other;
+        n -= h_dups;
+        out->len1 = n;
+    }
     out->len0 = len0;
     AMJ_TRY(out->data0.alloc(ctx, len0));
     AMJ_TRY(out->off0.alloc(ctx, (uint64_t)len0 + 1));
