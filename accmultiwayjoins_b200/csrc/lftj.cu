@@ -16,6 +16,9 @@
 // and ballot-driven galloping (exponential then 32-ary search) over runs that
 // cannot match.  Counting and the tuple checksum happen in registers; in
 // write mode each warp reserves output rows with one atomic per round.
+// Over one oriented edge relation with ws=1 the degree-ranked copy is joined
+// instead, by the wedge kernel below: for every edge (a, b), the values of
+// T(a) after b are tested against a per-warp bitmap of S(b).
 //
 // BFS (reference LFTJ_BFS np_join_np / p_join_np / p_join_p,
 // LFTJ-GPU/LFTJ_BFS.cuh:143-500): level-synchronous.  One kernel counts the
@@ -25,7 +28,9 @@
 // shared-memory binary search over the tile's offsets, then c is looked up in
 // the other child list.  Everything runs on the device, including the load
 // balancing the reference does on the CPU (LFTJ_BFS.cuh:396-397), and the
-// count it computes is returned (the reference returns 0, :496).
+// count it computes is returned (the reference returns 0, :496).  Over the
+// degree-ranked copy of one relation the candidates of (a,b) are T(a)'s
+// values after b, searched in S(b).
 #include "lftj_common.cuh"
 
 #include <algorithm>
@@ -55,7 +60,7 @@ struct TriArgs {
     uint32_t bitmap_bits;
     int sorted_out;               // the tries hold a degree-ordered copy of an oriented relation:
                                   // every triangle is listed with its values in increasing order
-    // rank kernel: the tries hold the degree-ranked copy (vertex = rank in
+    // wedge kernel: the tries hold the degree-ranked copy (vertex = rank in
     // (degree, id) order); inv[rank] is the vertex id
     const int32_t *inv;
     const uint64_t *wedge;        // (b << 32 | entry) of this slice's entries, sorted by b

@@ -162,7 +162,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     DBuf<uint64_t> wedges;   // its level-1 entries grouped by b
     uint64_t nv = 0;
     if (nrels == 1) {
-        // BFS and the DFS rank kernel (ws=1) join the degree-ordered copy:
+        // BFS and the DFS wedge kernel (ws=1) join the degree-ranked copy:
         // hubs keep short child lists
         bool deg_order = algo == AMJ_LFTJ_BFS || ws;
         if (flags & AMJ_F_DEGREE_ORDER) deg_order = true;
