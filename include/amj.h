@@ -76,8 +76,9 @@ extern "C" {
                                    TRI / FOUR: join the relation as given, never its
                                    degree-ordered copy                              */
 #define AMJ_F_DEGREE_ORDER 0x20 /* amj_lftj_execute, one oriented relation: join its
-                                   degree-ordered copy (the default for BFS and the
-                                   4-clique; DFS triangles keep the relation's order) */
+                                   degree-ordered copy (the default for BFS, for DFS
+                                   with ws=1 and for the 4-clique; the triangle paths
+                                   join it with vertices renamed to their ranks) */
 
 /* ---- relation residency ---- */
 #define AMJ_MEM_DEVICE 0   /* columns are device pointers, borrowed            */
