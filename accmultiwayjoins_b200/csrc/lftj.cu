@@ -64,6 +64,8 @@ struct TriArgs {
     // (degree, id) order); inv[rank] is the vertex id
     const int32_t *inv;
     const uint64_t *wedge;        // (b << 32 | entry) of this slice's entries, sorted by b
+    const uint64_t *moff;         // matrix mode: first word of every vertex a's matrix
+    uint32_t *mtx;                // matrix mode: row x of a's matrix has bit y when (a, x, y) is a triangle
     const int32_t *src1;          // level-0 value of every level-1 entry of R
     uint32_t rank_base;           // first rank of the per-warp bitmap
     uint32_t rank_bits;           // ranks the bitmap covers
@@ -353,8 +355,13 @@ __device__ __forceinline__ uint32_t tr_bit(const uint32_t *bm, int32_t c, uint32
     return __funnelshift_r(bm[r >> 5], 0u, r) & 1u;
 }
 
-template <bool WRITE>
+// MODE 0: count and checksum; 1: also write the tuples; 2 (matrix mode):
+// record every triangle (a, x, y) as bit y - ta of row x - ta of a's matrix
+// (ta = the start of T(a) in level 1; rows have ceil(d+(a) / 32) words).
+template <int MODE>
 __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __grid_constant__ TriArgs A) {
+    constexpr bool WRITE = MODE == 1;
+    constexpr bool MATRIX = MODE == 2;
     extern __shared__ __align__(16) unsigned char tr_smem[];
     const int lane = threadIdx.x & 31;
     TrWarp &W = ((TrWarp *)tr_smem)[threadIdx.x >> 5];
@@ -366,6 +373,8 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
     unsigned long long cnt = 0, chk = 0;
     uint32_t qh = 0, qn = 0;   // queue head and length
     int32_t ida = 0, idb = 0;  // vertex ids of this lane's edge (a, b)
+    uint64_t rowbase = 0;      // matrix mode: first word of this edge's row
+    uint32_t ta32 = 0;         // matrix mode: start of T(a) in level 1
     // the first n queued hits, one per lane
     auto flush = [&](uint32_t n) {
         __syncwarp();
@@ -453,8 +462,13 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
             uint64_t ta;
             child_range(A.T, a, ta, te);
             ts = (uint64_t)idx + 1;
-            ida = A.inv[a];
-            idb = A.inv[b];
+            if (MATRIX) {
+                rowbase = A.moff[a] + ((uint64_t)idx - ta) * ((te - ta + 31) / 32);
+                ta32 = (uint32_t)ta;
+            } else {
+                ida = A.inv[a];
+                idb = A.inv[b];
+            }
         }
         // tl: first value of the suffix in the bitmap's ranks (the values
         // below form a short sorted prefix: gallop, then bisect)
@@ -498,6 +512,8 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
                 lows &= lows - 1;
                 const uint64_t wts = __shfl_sync(AMJ_FULL_MASK, ts, l);
                 const uint64_t wtl = __shfl_sync(AMJ_FULL_MASK, tl, l);
+                const uint64_t lrb = __shfl_sync(AMJ_FULL_MASK, rowbase, l);
+                const uint32_t lta = __shfl_sync(AMJ_FULL_MASK, ta32, l);
                 for (uint64_t k0 = wts; k0 < wtl; k0 += 32) {
                     const uint64_t k = k0 + lane;
                     bool hit = false;
@@ -505,6 +521,13 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
                     if (k < wtl) {
                         c = d1[k];
                         hit = nl && (low_smem ? tr_sorted_find(W.low, nl, c) : tr_sorted_find(bl, nl, c));
+                    }
+                    if (MATRIX) {
+                        if (hit) {
+                            const uint32_t col = (uint32_t)k - lta;
+                            atomicOr(&A.mtx[lrb + (col >> 5)], 1u << (col & 31));
+                        }
+                        continue;
                     }
                     const unsigned m = __ballot_sync(AMJ_FULL_MASK, hit);
                     if (hit) W.q[(qh + qn + __popc(m & lanemask_lt())) & (TR_QCAP - 1)] = make_int2(c, l);
@@ -533,7 +556,7 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
                 for (int sft = 16; sft >= 1; sft >>= 1)
                     if (__shfl_sync(AMJ_FULL_MASK, P, o + sft) <= fl) o += sft;
                 int4 cv[TR_UNROLL];
-                uint32_t m4[TR_UNROLL];
+                uint32_t m4[TR_UNROLL], qi[TR_UNROLL];
                 int own[TR_UNROLL];
                 uint32_t oqsh = 0, oP = 0, ohl = 0, oe = 0;
 #pragma unroll
@@ -556,8 +579,8 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
                     const uint32_t lo = e0 == 0 ? (oqsh >> 30) : 0u;
                     const uint32_t hi = ohl > e0 ? (ohl - e0 < 4 ? ohl - e0 : 4u) : 0u;
                     m4[u] = vq && hi > lo ? ((0xFu >> (4 - hi)) & (0xFu << lo)) : 0u;
-                    const uint64_t q = (uint64_t)(oqsh & 0x3FFFFFFFu) + (vq ? rel : 0u);
-                    cv[u] = dq[q];
+                    qi[u] = (oqsh & 0x3FFFFFFFu) + (vq ? rel : 0u);
+                    cv[u] = dq[qi[u]];
                 }
                 uint32_t bits = 0;
 #pragma unroll
@@ -565,6 +588,21 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
                     const uint32_t t4 = tr_bit(W.bm, cv[u].x, base) | (tr_bit(W.bm, cv[u].y, base) << 1) |
                                         (tr_bit(W.bm, cv[u].z, base) << 2) | (tr_bit(W.bm, cv[u].w, base) << 3);
                     bits |= (t4 & m4[u]) << (4 * u);
+                }
+                if (MATRIX) {
+                    // value t of quad qi sits at level-1 position 4 qi + t
+#pragma unroll
+                    for (int u = 0; u < TR_UNROLL; u++) {
+                        const uint64_t orb = __shfl_sync(AMJ_FULL_MASK, rowbase, own[u]);
+                        const uint32_t ota = __shfl_sync(AMJ_FULL_MASK, ta32, own[u]);
+#pragma unroll
+                        for (int t = 0; t < 4; t++)
+                            if ((bits >> (4 * u + t)) & 1u) {
+                                const uint32_t col = 4 * qi[u] + t - ota;
+                                atomicOr(&A.mtx[orb + (col >> 5)], 1u << (col & 31));
+                            }
+                    }
+                    continue;
                 }
                 const uint32_t nh = __popc(bits);
                 const uint32_t hincl = warp_inclusive_scan(nh, lane);
@@ -593,6 +631,70 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
         atomicAdd(A.count, cnt);
         atomicAdd(A.checksum, chk);
     }
+}
+
+// words of every vertex a's matrix (d+(a) rows of ceil(d+(a) / 32) words),
+// indexed by a's rank; the scan turns them into first words
+__global__ void matrix_words_kernel(const int32_t *__restrict__ data0, const uint64_t *__restrict__ off0,
+                                    uint64_t len0, uint64_t *__restrict__ words) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len0; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = off0[i + 1] - off0[i];
+        words[(uint32_t)data0[i]] = k * ((k + 31) / 32);
+    }
+}
+
+// The triangle matrices of a degree-ranked trie R (ranks 0..nv-1): row x of
+// vertex a's matrix has bit y for every triangle (a, x, y), x and y counted
+// from the start of T(a).  *moff gets the first word of each matrix; the
+// matrices need *words 32-bit words.  Fails with AMJ_ENOMEM beyond max_words.
+int lftj_tri_matrices(amj_ctx *ctx, const Trie2 &R, const uint64_t *wedge, uint64_t nv, uint32_t rank_bits,
+                      uint64_t max_words, DBuf<uint64_t> *moff, DBuf<uint32_t> *mtx, uint64_t *words) {
+    AMJ_TRY(moff->alloc(ctx, nv + 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(moff->p, 0, (nv + 1) * sizeof(uint64_t), ctx->stream));
+    if (R.len0) {
+        note_launch(ctx);
+        matrix_words_kernel<<<(unsigned)std::min<uint64_t>((R.len0 + 255) / 256, (uint64_t)ctx->num_sms * 16), 256,
+                              0, ctx->stream>>>(R.data0.p, R.off0.p, R.len0, moff->p);
+        AMJ_CUDA_TRY(cudaGetLastError());
+    }
+    AMJ_TRY(scan_exclusive_u64(ctx, moff->p, moff->p, nv + 1, nullptr));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(words, moff->p + nv, sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (*words > max_words) return fail(AMJ_ENOMEM, "LFTJ 4-clique: the triangle matrices do not fit");
+    AMJ_TRY(mtx->alloc(ctx, *words ? *words : 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(mtx->p, 0, (*words ? *words : 1) * sizeof(uint32_t), ctx->stream));
+    if (R.len1 == 0) return AMJ_OK;
+    if (reinterpret_cast<uintptr_t>(R.data1.p) & 15) return fail(AMJ_ECUDA, "LFTJ: trie level 1 is not 16-byte aligned");
+    DBuf<unsigned long long> cursor;
+    AMJ_TRY(cursor.alloc(ctx, 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(cursor.p, 0, sizeof(unsigned long long), ctx->stream));
+    TriArgs A{};
+    A.r_src = R.src1.p;
+    A.r_dst = R.data1.p;
+    A.r_n = R.len1;
+    A.S = A.T = A.R = trie_ref(R);
+    A.r_lo = 0;
+    A.r_hi = R.len1;
+    A.sorted_out = 1;
+    A.wedge = wedge;
+    A.src1 = R.src1.p;
+    A.moff = moff->p;
+    A.mtx = mtx->p;
+    A.cursor_r = cursor.p;
+    uint32_t bits = TR_BITS;
+    if (rank_bits && rank_bits < bits) bits = rank_bits < 32 ? 32u : rank_bits;
+    if (nv < bits) bits = (uint32_t)((nv + 31) / 32 * 32);
+    A.rank_bits = bits;
+    A.rank_base = (uint32_t)(nv > bits ? nv - bits : 0);
+    auto kr = lftj_tri_wedge_kernel<2>;
+    AMJ_CUDA_TRY(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM));
+    int per_sm = 0;
+    AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, TR_THREADS, TR_SMEM));
+    if (per_sm < 1) per_sm = 1;
+    note_launch(ctx);
+    kr<<<(unsigned)(ctx->num_sms * per_sm), TR_THREADS, TR_SMEM, ctx->stream>>>(A);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    return AMJ_OK;
 }
 
 // (b << 32 | entry) for every level-1 entry (a, b) of R
@@ -902,7 +1004,7 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
                 A.src1 = R.src1.p;
                 A.rank_bits = bits;
                 A.rank_base = (uint32_t)(nv > bits ? nv - bits : 0);
-                auto kr = write ? lftj_tri_wedge_kernel<true> : lftj_tri_wedge_kernel<false>;
+                auto kr = write ? lftj_tri_wedge_kernel<1> : lftj_tri_wedge_kernel<0>;
                 AMJ_CUDA_TRY(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM));
                 int per_sm = 0;
                 AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, TR_THREADS, TR_SMEM));

@@ -20,6 +20,12 @@
 namespace amj {
 int lftj_clique4(amj_ctx *ctx, const Trie2 &T, int32_t *const *out, uint64_t out_cap, uint64_t *count,
                  uint64_t *checksum, uint64_t *written, double *kernel_ms, int sorted_out);
+struct C4Matrix;
+int lftj_clique4_matrix_prepare(amj_ctx *ctx, const Trie2 &T, const int32_t *inv, const uint64_t *wedge, uint64_t nv,
+                                uint32_t rank_bits, C4Matrix **out);
+void lftj_clique4_matrix_release(C4Matrix *m);
+int lftj_clique4_matrix(amj_ctx *ctx, const Trie2 &T, const int32_t *inv, const C4Matrix *m, int32_t *const *out,
+                        uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, double *kernel_ms);
 int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, int algo, int32_t *const *out,
                   uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, int small_sum,
                   uint64_t r_lo, uint64_t r_hi, uint32_t heavy_deg, double *kernel_ms, int sorted_out,
@@ -83,10 +89,36 @@ static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
     Trie2 t;
     int sorted_out = 0;
-    AMJ_TRY(build_self_trie(ctx, rels[0], &t, &sorted_out, (flags & AMJ_F_KEEP_ORDER) == 0));
+    // an oriented relation with out-degrees up to 1024 in degree order: the
+    // triangle matrices of its degree-ranked copy; otherwise the 4-clique
+    // kernel over the degree-ordered copy (or the relation as given)
+    DBuf<int32_t> inv;
+    uint64_t nv = 0;
+    struct MatGuard {
+        C4Matrix *m = nullptr;
+        ~MatGuard() { lftj_clique4_matrix_release(m); }
+    } mat;
+    if ((flags & AMJ_F_KEEP_ORDER) == 0) {
+        AMJ_TRY(build_ranked_trie(ctx, rels[0], &t, &inv, &nv));
+        if (nv) {
+            DBuf<uint64_t> wedges;
+            AMJ_TRY(build_wedges(ctx, t, nv, &wedges));
+            AMJ_TRY(lftj_clique4_matrix_prepare(ctx, t, inv.p, wedges.p, nv, ctx->opts.lftj_rank_bits, &mat.m));
+            if (!mat.m) {
+                t = Trie2();
+                inv.release();
+                AMJ_TRY(build_self_trie(ctx, rels[0], &t, &sorted_out, true));
+            }
+        }
+    } else {
+        AMJ_TRY(build_self_trie(ctx, rels[0], &t, &sorted_out, false));
+    }
     AMJ_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
     uint64_t c = 0, h = 0;
-    AMJ_TRY(lftj_clique4(ctx, t, nullptr, 0, &c, &h, nullptr, &out->kernel_ms[0], sorted_out));
+    if (mat.m)
+        AMJ_TRY(lftj_clique4_matrix(ctx, t, inv.p, mat.m, nullptr, 0, &c, &h, nullptr, &out->kernel_ms[0]));
+    else
+        AMJ_TRY(lftj_clique4(ctx, t, nullptr, 0, &c, &h, nullptr, &out->kernel_ms[0], sorted_out));
     out->count = c;
     out->checksum = h;
     const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
@@ -95,7 +127,9 @@ static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         int rc = AMJ_OK;
         for (int a = 0; a < 4 && rc == AMJ_OK; a++) rc = dev_alloc(ctx, (void **)&cols[a], (c ? c : 1) * 4);
         uint64_t c2 = 0, h2 = 0, w = 0;
-        if (rc == AMJ_OK) rc = lftj_clique4(ctx, t, cols, c, &c2, &h2, &w, &out->kernel_ms[1], sorted_out);
+        if (rc == AMJ_OK)
+            rc = mat.m ? lftj_clique4_matrix(ctx, t, inv.p, mat.m, cols, c, &c2, &h2, &w, &out->kernel_ms[1])
+                       : lftj_clique4(ctx, t, cols, c, &c2, &h2, &w, &out->kernel_ms[1], sorted_out);
         if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
             rc = fail(AMJ_ECUDA, "LFTJ 4-clique: write pass disagrees with count pass");
         if (rc != AMJ_OK) {

@@ -223,6 +223,265 @@ struct C4Counters {
 
 // One 4-clique pass over the trie T of the edge relation: count and checksum,
 // and the tuples when `out` is given (out_cap rows).
+// ---- 4-cliques from triangle matrices (degree-ranked copy) ----
+// Over the degree-ranked copy every 4-clique a < x < y < z (ranks) is a
+// triangle (x, y, z) inside N+(a).  The wedge kernel in matrix mode records
+// the triangles (a, x, y) as bits: row x - ta of a's matrix holds bit y - ta
+// (ta = the start of T(a), so rows and columns are positions in N+(a)).
+// Then the 4-cliques through (a, x, y) are the set bits of row x AND row y:
+// persistent warps claim 32 level-1 entries (a, x) at a time, and for each
+// one walk the bits y of row x; each AND is one word per lane (rows have at
+// most 32 words: this path takes out-degrees up to 1024).  Found 4-cliques
+// go to a per-warp queue of (entry lane, y, z) and are mapped to ids, sorted,
+// hashed and written 32 at a time.
+constexpr int C4M_THREADS = 256;
+constexpr int C4M_WARPS = C4M_THREADS / 32;
+constexpr int C4M_QCAP = 2048;   // queued 4-cliques per warp (ring; one AND adds at most 1024)
+constexpr uint32_t C4M_MAX_DEG = 1024;
+constexpr size_t C4M_SMEM = (size_t)C4M_WARPS * C4M_QCAP * 4;
+
+struct C4MArgs {
+    const int32_t *src1;     // rank a of every level-1 entry
+    const int32_t *id1;      // vertex id of every level-1 value
+    const int32_t *inv;      // rank -> vertex id
+    TrieRef T;
+    const uint64_t *moff;    // first matrix word of every rank
+    const uint32_t *mtx;
+    uint64_t n;
+    unsigned long long *cursor, *count, *checksum, *out_cursor;
+    int32_t *out[4];
+    uint64_t out_cap;
+};
+
+template <bool WRITE>
+__global__ __launch_bounds__(C4M_THREADS) void lftj_clique4_matrix_kernel(const __grid_constant__ C4MArgs A) {
+    extern __shared__ uint32_t c4m_smem[];
+    const int lane = threadIdx.x & 31;
+    uint32_t *q = c4m_smem + (threadIdx.x >> 5) * C4M_QCAP;
+    unsigned long long cnt = 0, chk = 0;
+    uint32_t qh = 0, qn = 0;
+    int32_t ida = 0, idx_ = 0;   // ids of this lane's entry (a, x)
+    uint32_t ta32 = 0;           // start of T(a)
+    // the first n queued 4-cliques, one per lane: (z << 15) | (y << 5) | lane of (a, x)
+    auto flush = [&](uint32_t n) {
+        __syncwarp();
+        const bool mine = (uint32_t)lane < n;
+        const uint32_t e = mine ? q[(qh + lane) & (C4M_QCAP - 1)] : 0u;
+        const int l = (int)(e & 31u);
+        const int32_t a = __shfl_sync(AMJ_FULL_MASK, ida, l);
+        const int32_t x = __shfl_sync(AMJ_FULL_MASK, idx_, l);
+        const uint32_t t0 = __shfl_sync(AMJ_FULL_MASK, ta32, l);
+        __syncwarp();
+        int32_t v[4] = {a, x, 0, 0};
+        if (mine) {
+            v[2] = A.id1[t0 + ((e >> 5) & 1023u)];
+            v[3] = A.id1[t0 + (e >> 15)];
+        }
+        // the tuple in increasing order (sorting network of four)
+        int32_t t;
+        if (v[0] > v[1]) { t = v[0]; v[0] = v[1]; v[1] = t; }
+        if (v[2] > v[3]) { t = v[2]; v[2] = v[3]; v[3] = t; }
+        if (v[0] > v[2]) { t = v[0]; v[0] = v[2]; v[2] = t; }
+        if (v[1] > v[3]) { t = v[1]; v[1] = v[3]; v[3] = t; }
+        if (v[1] > v[2]) { t = v[1]; v[1] = v[2]; v[2] = t; }
+        if (WRITE) {
+            unsigned long long at = 0;
+            if (lane == 0) at = atomicAdd(A.out_cursor, (unsigned long long)n);
+            at = __shfl_sync(AMJ_FULL_MASK, at, 0);
+            if (mine && at + lane < A.out_cap)
+                for (int i = 0; i < 4; i++) A.out[i][at + lane] = v[i];
+        }
+        if (mine) {
+            cnt++;
+            chk += amj_hash_step(amj_hash_step(amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, v[0]), v[1]), v[2]),
+                                 v[3]);
+        }
+        qh = (qh + n) & (C4M_QCAP - 1);
+        qn -= n;
+    };
+    while (true) {
+        unsigned long long at = 0;
+        if (lane == 0) at = atomicAdd(A.cursor, 32ull);
+        at = __shfl_sync(AMJ_FULL_MASK, at, 0);
+        if (at >= A.n) break;
+        const uint64_t j = at + lane;
+        const bool valid = j < A.n;
+        uint32_t w = 0;
+        uint64_t rowbase = 0, mbase = 0;
+        if (valid) {
+            const int32_t a = A.src1[j];
+            uint64_t ta, te;
+            child_range(A.T, a, ta, te);
+            w = (uint32_t)((te - ta + 31) / 32);
+            mbase = A.moff[a];
+            rowbase = mbase + (j - ta) * w;
+            ida = A.inv[a];
+            idx_ = A.id1[j];
+            ta32 = (uint32_t)ta;
+        }
+        unsigned todo = __ballot_sync(AMJ_FULL_MASK, valid && w > 0);
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t wl = __shfl_sync(AMJ_FULL_MASK, w, l);
+            const uint64_t rb = __shfl_sync(AMJ_FULL_MASK, rowbase, l);
+            const uint64_t mb = __shfl_sync(AMJ_FULL_MASK, mbase, l);
+            // row x, one word per lane; its bits y are the triangles (a, x, y)
+            const uint32_t rx = (uint32_t)lane < wl ? A.mtx[rb + lane] : 0u;
+            unsigned wm = __ballot_sync(AMJ_FULL_MASK, rx != 0);
+            while (wm) {
+                const int wy = __ffs(wm) - 1;
+                wm &= wm - 1;
+                uint32_t word = __shfl_sync(AMJ_FULL_MASK, rx, wy);
+                while (word) {
+                    const int by = __ffs(word) - 1;
+                    word &= word - 1;
+                    const uint32_t y = (uint32_t)wy * 32 + by;
+                    // z: bits of row x AND row y (row y holds bits above y only)
+                    uint32_t c = 0;
+                    if (lane >= wy && (uint32_t)lane < wl) c = rx & A.mtx[mb + (uint64_t)y * wl + lane];
+                    const uint32_t nh = __popc(c);
+                    const uint32_t incl = warp_inclusive_scan(nh, lane);
+                    const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, incl, 31);
+                    if (tot) {
+                        uint32_t pos = qh + qn + incl - nh;
+                        while (c) {
+                            const uint32_t bz = __ffs(c) - 1;
+                            c &= c - 1;
+                            q[pos++ & (C4M_QCAP - 1)] = (((uint32_t)lane * 32 + bz) << 15) | (y << 5) | (uint32_t)l;
+                        }
+                        qn += tot;
+                        while (qn >= 32) flush(32);
+                    }
+                }
+            }
+        }
+        if (qn) flush(qn);
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if ((threadIdx.x & 31) == 0 && cnt) {
+        atomicAdd(A.count, cnt);
+        atomicAdd(A.checksum, chk);
+    }
+}
+
+__global__ void level1_ids_kernel(const int32_t *__restrict__ data1, uint64_t n, const int32_t *__restrict__ inv,
+                                  int32_t *__restrict__ id1) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        id1[i] = inv[data1[i]];
+}
+
+int lftj_tri_matrices(amj_ctx *ctx, const Trie2 &R, const uint64_t *wedge, uint64_t nv, uint32_t rank_bits,
+                      uint64_t max_words, DBuf<uint64_t> *moff, DBuf<uint32_t> *mtx, uint64_t *words);
+
+// Largest child list of the trie (its longest out-neighbour list).
+static int trie_max_children(amj_ctx *ctx, const Trie2 &T, uint64_t *maxc) {
+    *maxc = 0;
+    if (T.len0 == 0) return AMJ_OK;
+    DBuf<unsigned long long> m;
+    AMJ_TRY(m.alloc(ctx, 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(m.p, 0, sizeof(unsigned long long), ctx->stream));
+    note_launch(ctx);
+    max_children_kernel<<<(unsigned)std::min<uint64_t>((T.len0 + 255) / 256, (uint64_t)ctx->num_sms * 8), 256, 0,
+                          ctx->stream>>>(T.off0.p, T.len0, m.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    unsigned long long h = 0;
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&h, m.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    *maxc = h;
+    return AMJ_OK;
+}
+
+// Prepared state of the matrix path over one degree-ranked trie.
+struct C4Matrix {
+    DBuf<uint64_t> moff;
+    DBuf<uint32_t> mtx;
+    DBuf<int32_t> id1;
+};
+
+// Whether the matrix path takes the degree-ranked trie T (every out-degree at
+// most 1024, the matrices within half the free device memory), and if so the
+// triangle matrices and the ids of level 1.
+int lftj_clique4_matrix_prepare(amj_ctx *ctx, const Trie2 &T, const int32_t *inv, const uint64_t *wedge, uint64_t nv,
+                                uint32_t rank_bits, C4Matrix **out) {
+    *out = nullptr;
+    uint64_t maxc = 0;
+    AMJ_TRY(trie_max_children(ctx, T, &maxc));
+    if (maxc > C4M_MAX_DEG) return AMJ_OK;
+    size_t fr = 0, tot = 0;
+    AMJ_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    auto *m = new C4Matrix();
+    uint64_t words = 0;
+    int rc = lftj_tri_matrices(ctx, T, wedge, nv, rank_bits, fr / 2 / 4, &m->moff, &m->mtx, &words);
+    if (rc == AMJ_ENOMEM) {   // the matrices do not fit: not this path
+        delete m;
+        return AMJ_OK;
+    }
+    if (rc == AMJ_OK) rc = m->id1.alloc(ctx, T.len1 ? T.len1 : 1);
+    if (rc == AMJ_OK && T.len1) {
+        note_launch(ctx);
+        level1_ids_kernel<<<(unsigned)std::min<uint64_t>((T.len1 + 255) / 256, (uint64_t)ctx->num_sms * 16), 256, 0,
+                            ctx->stream>>>(T.data1.p, T.len1, inv, m->id1.p);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(AMJ_ECUDA, "LFTJ 4-clique: level-1 ids");
+    }
+    if (rc != AMJ_OK) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return AMJ_OK;
+}
+
+void lftj_clique4_matrix_release(C4Matrix *m) { delete m; }
+
+// 4-cliques of the degree-ranked trie T from its prepared matrices: count and
+// checksum, and with out the sorted tuples (out_cap rows available).
+int lftj_clique4_matrix(amj_ctx *ctx, const Trie2 &T, const int32_t *inv, const C4Matrix *m, int32_t *const *out,
+                        uint64_t out_cap, uint64_t *count, uint64_t *checksum, uint64_t *written, double *kernel_ms) {
+    DBuf<C4Counters> ctr;
+    AMJ_TRY(ctr.alloc(ctx, 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(ctr.p, 0, sizeof(C4Counters), ctx->stream));
+    *count = *checksum = 0;
+    if (written) *written = 0;
+    if (T.len1 == 0) return AMJ_OK;
+    const bool write = out != nullptr;
+    C4MArgs A{};
+    A.src1 = T.src1.p;
+    A.id1 = m->id1.p;
+    A.inv = inv;
+    A.T = trie_ref(T);
+    A.moff = m->moff.p;
+    A.mtx = m->mtx.p;
+    A.n = T.len1;
+    A.cursor = &ctr.p->cursor;
+    A.count = &ctr.p->count;
+    A.checksum = &ctr.p->checksum;
+    A.out_cursor = &ctr.p->out_cursor;
+    if (write) {
+        for (int i = 0; i < 4; i++) A.out[i] = out[i];
+        A.out_cap = out_cap;
+    }
+    auto kern = write ? lftj_clique4_matrix_kernel<true> : lftj_clique4_matrix_kernel<false>;
+    AMJ_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C4M_SMEM));
+    int per_sm = 0;
+    AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C4M_THREADS, C4M_SMEM));
+    if (per_sm < 1) per_sm = 1;
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
+    note_launch(ctx);
+    kern<<<(unsigned)(ctx->num_sms * per_sm), C4M_THREADS, C4M_SMEM, ctx->stream>>>(A);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
+    C4Counters h;
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&h, ctr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (kernel_ms) *kernel_ms += event_ms(ctx->kev[0], ctx->kev[1]);
+    *count = h.count;
+    *checksum = h.checksum;
+    if (written) *written = std::min<unsigned long long>(h.out_cursor, out_cap);
+    return AMJ_OK;
+}
+
 int lftj_clique4(amj_ctx *ctx, const Trie2 &T, int32_t *const *out, uint64_t out_cap, uint64_t *count,
                  uint64_t *checksum, uint64_t *written, double *kernel_ms, int sorted_out) {
     DBuf<C4Counters> ctr;
