@@ -119,3 +119,33 @@ def test_cli_drivers_exist_and_print_usage(built):
         assert os.access(exe, os.X_OK), exe
         r = subprocess.run([exe], capture_output=True, text=True)
         assert r.returncode == 2 and "usage" in r.stderr
+
+
+MIRRORED_STRUCTS = ["amj_opts", "amj_result", "amj_batch_opts", "amj_batch_stats", "amj_batch_tune_grid",
+                    "amj_serve_opts", "amj_serve_result", "amj_serve_stats"]
+
+
+def test_ctypes_mirrors_match_the_header(tmp_path):
+    """Every ctypes structure has the size and field offsets the C compiler
+    gives the struct of the same name in include/amj.h (a mismatch would pass
+    options and read results at the wrong bytes)."""
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "amj.h"', "int main(void) {"]
+    for name in MIRRORED_STRUCTS:
+        ct = getattr(L, name)
+        lines.append(f'printf("{name} sizeof %zu\\n", sizeof({name}));')
+        for f in ct._fields_:
+            lines.append(f'printf("{name} {f[0]} %zu\\n", offsetof({name}, {f[0]}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = {}
+    for line in subprocess.check_output([str(exe)], text=True).splitlines():
+        s, f, v = line.split()
+        got[(s, f)] = int(v)
+    for name in MIRRORED_STRUCTS:
+        ct = getattr(L, name)
+        assert got[(name, "sizeof")] == C.sizeof(ct), name
+        for f in ct._fields_:
+            assert got[(name, f[0])] == getattr(ct, f[0]).offset, (name, f[0])
