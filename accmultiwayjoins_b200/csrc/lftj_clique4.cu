@@ -236,9 +236,11 @@ struct C4Counters {
 // hashed and written 32 at a time.
 constexpr int C4M_THREADS = 256;
 constexpr int C4M_WARPS = C4M_THREADS / 32;
-constexpr int C4M_QCAP = 2048;   // queued 4-cliques per warp (ring; one AND adds at most 1024)
+constexpr int C4M_QCAP = 1024;   // queued 4-cliques per warp (ring; one step adds at most 1024)
 constexpr uint32_t C4M_MAX_DEG = 1024;
-constexpr size_t C4M_SMEM = (size_t)C4M_WARPS * C4M_QCAP * 4;
+// per warp: the queue, then the bits y of the current row x
+constexpr size_t C4M_WARP_WORDS = C4M_QCAP + C4M_MAX_DEG / 2;
+constexpr size_t C4M_SMEM = (size_t)C4M_WARPS * C4M_WARP_WORDS * 4;
 
 struct C4MArgs {
     const int32_t *src1;     // rank a of every level-1 entry
@@ -257,7 +259,8 @@ template <bool WRITE>
 __global__ __launch_bounds__(C4M_THREADS) void lftj_clique4_matrix_kernel(const __grid_constant__ C4MArgs A) {
     extern __shared__ uint32_t c4m_smem[];
     const int lane = threadIdx.x & 31;
-    uint32_t *q = c4m_smem + (threadIdx.x >> 5) * C4M_QCAP;
+    uint32_t *q = c4m_smem + (threadIdx.x >> 5) * C4M_WARP_WORDS;
+    uint16_t *ylist = reinterpret_cast<uint16_t *>(q + C4M_QCAP);
     unsigned long long cnt = 0, chk = 0;
     uint32_t qh = 0, qn = 0;
     int32_t ida = 0, idx_ = 0;   // ids of this lane's entry (a, x)
@@ -328,33 +331,48 @@ __global__ __launch_bounds__(C4M_THREADS) void lftj_clique4_matrix_kernel(const 
             const uint64_t mb = __shfl_sync(AMJ_FULL_MASK, mbase, l);
             // row x, one word per lane; its bits y are the triangles (a, x, y)
             const uint32_t rx = (uint32_t)lane < wl ? A.mtx[rb + lane] : 0u;
-            unsigned wm = __ballot_sync(AMJ_FULL_MASK, rx != 0);
-            while (wm) {
-                const int wy = __ffs(wm) - 1;
-                wm &= wm - 1;
-                uint32_t word = __shfl_sync(AMJ_FULL_MASK, rx, wy);
-                while (word) {
-                    const int by = __ffs(word) - 1;
-                    word &= word - 1;
-                    const uint32_t y = (uint32_t)wy * 32 + by;
-                    // z: bits of row x AND row y (row y holds bits above y only)
-                    uint32_t c = 0;
-                    if (lane >= wy && (uint32_t)lane < wl) c = rx & A.mtx[mb + (uint64_t)y * wl + lane];
-                    const uint32_t nh = __popc(c);
-                    const uint32_t incl = warp_inclusive_scan(nh, lane);
-                    const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, incl, 31);
-                    if (tot) {
-                        uint32_t pos = qh + qn + incl - nh;
-                        while (c) {
-                            const uint32_t bz = __ffs(c) - 1;
-                            c &= c - 1;
-                            q[pos++ & (C4M_QCAP - 1)] = (((uint32_t)lane * 32 + bz) << 15) | (y << 5) | (uint32_t)l;
-                        }
-                        qn += tot;
-                        while (qn >= 32) flush(32);
-                    }
+            const uint32_t nyl = __popc(rx);
+            const uint32_t yincl = warp_inclusive_scan(nyl, lane);
+            const uint32_t ny = __shfl_sync(AMJ_FULL_MASK, yincl, 31);
+            if (ny == 0) continue;
+            {
+                uint32_t p = yincl - nyl, m = rx;
+                while (m) {
+                    const uint32_t b = __ffs(m) - 1;
+                    m &= m - 1;
+                    ylist[p++] = (uint16_t)(lane * 32 + b);
                 }
             }
+            __syncwarp();
+            // 32 / wp bits y per step, wp lanes (one per word of row y) each
+            uint32_t wp = 1;
+            while (wp < wl) wp <<= 1;
+            const uint32_t G = 32 / wp, slot = (uint32_t)lane / wp, wd = (uint32_t)lane & (wp - 1);
+            const uint32_t rxw = __shfl_sync(AMJ_FULL_MASK, rx, (int)wd);
+            for (uint32_t b0 = 0; b0 < ny; b0 += G) {
+                const uint32_t yi = b0 + slot;
+                uint32_t c = 0, y = 0;
+                if (yi < ny) {
+                    y = ylist[yi];
+                    // z: bits of row x AND row y (row y holds bits above y only)
+                    if (wd < wl && wd >= y / 32) c = rxw & A.mtx[mb + (uint64_t)y * wl + wd];
+                }
+                const uint32_t nh = __popc(c);
+                const uint32_t incl = warp_inclusive_scan(nh, lane);
+                const uint32_t tot = __shfl_sync(AMJ_FULL_MASK, incl, 31);
+                if (tot) {
+                    if (qn + tot > C4M_QCAP) flush(qn);   // make room (tot is at most 1024)
+                    uint32_t pos = qh + qn + incl - nh;
+                    while (c) {
+                        const uint32_t bz = __ffs(c) - 1;
+                        c &= c - 1;
+                        q[pos++ & (C4M_QCAP - 1)] = ((wd * 32 + bz) << 15) | (y << 5) | (uint32_t)l;
+                    }
+                    qn += tot;
+                    while (qn >= 32) flush(32);
+                }
+            }
+            __syncwarp();
         }
         if (qn) flush(qn);
     }
