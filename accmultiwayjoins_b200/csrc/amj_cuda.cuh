@@ -133,6 +133,8 @@ struct amj_ctx {
     unsigned long long launches = 0;                     // kernels launched through this context
     cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};   // per-kernel timing
     amj::IndexProvider *iprov = nullptr;   // indexes kept across calls (set by the request server)
+    void *c4_mtx = nullptr;                // 4-clique triangle matrices, kept across calls (grow-only)
+    uint64_t c4_mtx_words = 0;
 };
 
 struct amj_rel {

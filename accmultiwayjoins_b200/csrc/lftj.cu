@@ -648,7 +648,7 @@ __global__ void matrix_words_kernel(const int32_t *__restrict__ data0, const uin
 // from the start of T(a).  *moff gets the first word of each matrix; the
 // matrices need *words 32-bit words.  Fails with AMJ_ENOMEM beyond max_words.
 int lftj_tri_matrices(amj_ctx *ctx, const Trie2 &R, const uint64_t *wedge, uint64_t nv, uint32_t rank_bits,
-                      uint64_t max_words, DBuf<uint64_t> *moff, DBuf<uint32_t> *mtx, uint64_t *words) {
+                      uint64_t max_words, DBuf<uint64_t> *moff, uint32_t **mtx, uint64_t *words) {
     AMJ_TRY(moff->alloc(ctx, nv + 1));
     AMJ_CUDA_TRY(cudaMemsetAsync(moff->p, 0, (nv + 1) * sizeof(uint64_t), ctx->stream));
     if (R.len0) {
@@ -661,8 +661,24 @@ int lftj_tri_matrices(amj_ctx *ctx, const Trie2 &R, const uint64_t *wedge, uint6
     AMJ_CUDA_TRY(cudaMemcpyAsync(words, moff->p + nv, sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream));
     AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (*words > max_words) return fail(AMJ_ENOMEM, "LFTJ 4-clique: the triangle matrices do not fit");
-    AMJ_TRY(mtx->alloc(ctx, *words ? *words : 1));
-    AMJ_CUDA_TRY(cudaMemsetAsync(mtx->p, 0, (*words ? *words : 1) * sizeof(uint32_t), ctx->stream));
+    // the matrices live in one buffer the context keeps between calls (they
+    // are the largest allocation of the query; allocating them anew every
+    // call stalled the host while the device memory pool grew)
+    const uint64_t need = *words ? *words : 1;
+    if (ctx->c4_mtx_words < need) {
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (ctx->c4_mtx) (void)cudaFree(ctx->c4_mtx);
+        ctx->c4_mtx = nullptr;
+        ctx->c4_mtx_words = 0;
+        if (cudaMalloc(&ctx->c4_mtx, need * sizeof(uint32_t)) != cudaSuccess) {
+            (void)cudaGetLastError();
+            ctx->c4_mtx = nullptr;
+            return fail(AMJ_ENOMEM, "LFTJ 4-clique: the triangle matrices do not fit");
+        }
+        ctx->c4_mtx_words = need;
+    }
+    *mtx = static_cast<uint32_t *>(ctx->c4_mtx);
+    AMJ_CUDA_TRY(cudaMemsetAsync(*mtx, 0, need * sizeof(uint32_t), ctx->stream));
     if (R.len1 == 0) return AMJ_OK;
     if (reinterpret_cast<uintptr_t>(R.data1.p) & 15) return fail(AMJ_ECUDA, "LFTJ: trie level 1 is not 16-byte aligned");
     DBuf<unsigned long long> cursor;
@@ -679,7 +695,7 @@ int lftj_tri_matrices(amj_ctx *ctx, const Trie2 &R, const uint64_t *wedge, uint6
     A.wedge = wedge;
     A.src1 = R.src1.p;
     A.moff = moff->p;
-    A.mtx = mtx->p;
+    A.mtx = *mtx;
     A.cursor_r = cursor.p;
     uint32_t bits = TR_BITS;
     if (rank_bits && rank_bits < bits) bits = rank_bits < 32 ? 32u : rank_bits;

@@ -391,7 +391,7 @@ __global__ void level1_ids_kernel(const int32_t *__restrict__ data1, uint64_t n,
 }
 
 int lftj_tri_matrices(amj_ctx *ctx, const Trie2 &R, const uint64_t *wedge, uint64_t nv, uint32_t rank_bits,
-                      uint64_t max_words, DBuf<uint64_t> *moff, DBuf<uint32_t> *mtx, uint64_t *words);
+                      uint64_t max_words, DBuf<uint64_t> *moff, uint32_t **mtx, uint64_t *words);
 
 // Largest child list of the trie (its longest out-neighbour list).
 static int trie_max_children(amj_ctx *ctx, const Trie2 &T, uint64_t *maxc) {
@@ -414,7 +414,7 @@ static int trie_max_children(amj_ctx *ctx, const Trie2 &T, uint64_t *maxc) {
 // Prepared state of the matrix path over one degree-ranked trie.
 struct C4Matrix {
     DBuf<uint64_t> moff;
-    DBuf<uint32_t> mtx;
+    uint32_t *mtx = nullptr;   // the context's matrix buffer
     DBuf<int32_t> id1;
 };
 
@@ -431,7 +431,9 @@ int lftj_clique4_matrix_prepare(amj_ctx *ctx, const Trie2 &T, const int32_t *inv
     AMJ_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
     auto *m = new C4Matrix();
     uint64_t words = 0;
-    int rc = lftj_tri_matrices(ctx, T, wedge, nv, rank_bits, fr / 2 / 4, &m->moff, &m->mtx, &words);
+    // at most half the free memory, or the buffer the context already holds
+    const uint64_t max_words = std::max<uint64_t>(fr / 2 / 4, ctx->c4_mtx_words);
+    int rc = lftj_tri_matrices(ctx, T, wedge, nv, rank_bits, max_words, &m->moff, &m->mtx, &words);
     if (rc == AMJ_ENOMEM) {   // the matrices do not fit: not this path
         delete m;
         return AMJ_OK;
@@ -470,7 +472,7 @@ int lftj_clique4_matrix(amj_ctx *ctx, const Trie2 &T, const int32_t *inv, const 
     A.inv = inv;
     A.T = trie_ref(T);
     A.moff = m->moff.p;
-    A.mtx = m->mtx.p;
+    A.mtx = m->mtx;
     A.n = T.len1;
     A.cursor = &ctr.p->cursor;
     A.count = &ctr.p->count;

@@ -182,6 +182,7 @@ extern "C" void amj_ctx_destroy(amj_ctx *c) {
         if (c->side_stream[i]) (void)cudaStreamDestroy(c->side_stream[i]);
     if (c->d_status) (void)cudaFree(c->d_status);
     if (c->h_status) (void)cudaFreeHost(c->h_status);
+    if (c->c4_mtx) (void)cudaFree(c->c4_mtx);
     if (c->own_stream && c->stream) (void)cudaStreamDestroy(c->stream);
     (void)cudaGetLastError();
     delete c;

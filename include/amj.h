@@ -166,7 +166,9 @@ int  amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *rels, int nr
  *             reference's LFTJ stops at 3 attributes and 3 tables); ooc = 0.
  * nrels == 2 is rejected, as in the reference (LFTJ-GPU/exec_LFTJ.cu:92-95).
  * Relations are joined as sets (leapfrog triejoin semantics): a repeated row
- * counts once. */
+ * counts once.  The 4-clique over an oriented relation keeps its triangle
+ * matrices (at most half the free device memory) with the context between
+ * calls; amj_ctx_destroy releases them. */
 int  amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels,
                       int algo, int ooc, int ws, int flags, amj_result *out);
 
