@@ -1,10 +1,10 @@
 // amj_bucket_build_static: the bucket-CSR build of amj_bucket_build for
 // callers that cannot allocate device memory.
 //
-// Some hosts of this library may not call cudaMalloc at all: code running
-// inside a CUDA stream capture that must stay free of allocation nodes, a
-// plugin living in an engine that owns every device byte through its own
-// pool, or a real-time loop that may not block on the driver's allocator.
+// Some hosts of this library may not call cudaMalloc at all: a plugin living
+// in a query engine that owns every device byte through its own pool and
+// accounts for it, or a real-time loop that may not block on the driver's
+// allocator (cudaMalloc can synchronise the device and take milliseconds).
 // For them this entry point works entirely in a fixed scratch area compiled
 // into the library (a file-scope __device__ array), plus the input and
 // output buffers the caller passes in.  It calls no cudaMalloc, cudaFree,
@@ -20,7 +20,8 @@
 //    results; serialise them;
 //  - the first call on a device looks up the area's device address (a
 //    driver query, no allocation); make that first call before any stream
-//    capture begins.
+//    capture begins;
+//  - the call synchronises `stream` before it returns.
 #include "hash_build_kernels.cuh"
 #include "primitives_kernels.cuh"
 

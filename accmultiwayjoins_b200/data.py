@@ -5,6 +5,12 @@ The workloads follow the reference's data shapes: uniform int32 key columns
 (MHJ-GPU/data_generator.cuh:110-187), and graph edge relations.  The
 reference reads external graph files; here an R-MAT generator stands in for
 them (self-loops dropped, edges oriented u<v, duplicates removed, shuffled).
+
+The workload builders (chain_relations, star_relations, query_mix) take an
+optional `gen`: any object with the four primitive generators uniform,
+permutation, zipf and rmat of this module's signatures.  By default they are
+this module's own (libamj); a caller that must not load the library passes
+another implementation of the same definitions.
 """
 from __future__ import annotations
 
@@ -55,28 +61,50 @@ def rmat(scale: int, nedges: int, a: float, b: float, c: float, seed: int):
     return src[:m].copy(), dst[:m].copy()
 
 
-def chain_relations(n: int, key_range: int, nrels: int = 3, seed: int = 1):
+class _Libamj:
+    """The primitive generators of this module (libamj)."""
+
+    @staticmethod
+    def uniform(*a, **k):
+        return uniform(*a, **k)
+
+    @staticmethod
+    def permutation(*a, **k):
+        return permutation(*a, **k)
+
+    @staticmethod
+    def zipf(*a, **k):
+        return zipf(*a, **k)
+
+    @staticmethod
+    def rmat(*a, **k):
+        return rmat(*a, **k)
+
+
+def chain_relations(n: int, key_range: int, nrels: int = 3, seed: int = 1, gen=None):
     """The chain workload R1(0,1) R2(1,2) .. : nrels relations of n rows, two
     uniform int32 columns in [0, key_range), relation i seeded seed+i."""
+    g = gen or _Libamj
     rels = []
     for i in range(nrels):
         s = seed + i
-        rels.append(([uniform(n, 0, key_range, s, 0), uniform(n, 0, key_range, s, 1)], [i, i + 1]))
+        rels.append(([g.uniform(n, 0, key_range, s, 0), g.uniform(n, 0, key_range, s, 1)], [i, i + 1]))
     return rels
 
 
-def star_relations(fact_rows: int, dim_rows, theta: float = 1.1, seed: int = 3):
+def star_relations(fact_rows: int, dim_rows, theta: float = 1.1, seed: int = 3, gen=None):
     """The star workload: fact F(0..d-1) of Zipf foreign keys and dimensions
     Dj(j, d+j) of (unique key, uniform payload)."""
+    g = gen or _Libamj
     d = len(dim_rows)
     dims = []
     fact_cols = []
     for j, m in enumerate(dim_rows):
-        keys = permutation(m, seed, 100 + j)
-        payload = uniform(m, -(1 << 31), (1 << 31), seed, 200 + j)
+        keys = g.permutation(m, seed, 100 + j)
+        payload = g.uniform(m, -(1 << 31), (1 << 31), seed, 200 + j)
         dims.append(([keys, payload], [j, d + j]))
-        rank_to_key = permutation(m, seed, 300 + j)
-        fact_cols.append(zipf(fact_rows, m, theta, seed, 400 + j, rank_to_key=rank_to_key))
+        rank_to_key = g.permutation(m, seed, 300 + j)
+        fact_cols.append(g.zipf(fact_rows, m, theta, seed, 400 + j, rank_to_key=rank_to_key))
     return (fact_cols, list(range(d))), dims
 
 
@@ -85,7 +113,7 @@ def _log_uniform(rng, lo: float, hi: float) -> float:
 
 
 def query_mix(count: int, seed: int = 4, min_rows: int = 10_000, max_rows: int = 4_000_000, min_dom_bits: int = 12,
-              max_dom_bits: int = 24, theta_range=(0.5, 1.5), out_cap: int = 1 << 24):
+              max_dom_bits: int = 24, theta_range=(0.5, 1.5), out_cap: int = 1 << 24, gen=None):
     """The heterogeneous query mix of the batched workload, one query at a time.
 
     Each query is a chain or a star of 2-5 relations, or a triangle, drawn
@@ -105,6 +133,7 @@ def query_mix(count: int, seed: int = 4, min_rows: int = 10_000, max_rows: int =
       (0.57, 0.19, 0.19) with E generated edges and scale log2(E / 8).
 
     Yields dicts with shape, qt, rels (list of (columns, attrs)) and theta."""
+    g = gen or _Libamj
     rng = np.random.Generator(np.random.PCG64(seed))
     for q in range(count):
         shape = ("chain", "star", "triangle")[int(rng.integers(0, 3))]
@@ -114,7 +143,7 @@ def query_mix(count: int, seed: int = 4, min_rows: int = 10_000, max_rows: int =
         if shape == "triangle":
             e = int(_log_uniform(rng, min_rows, max_rows))
             scale = max(8, int(round(np.log2(max(e, 256) / 8))))
-            s, d = rmat(scale, e, 0.57, 0.19, 0.19, qseed)
+            s, d = g.rmat(scale, e, 0.57, 0.19, 0.19, qseed)
             yield dict(shape=shape, qt="TRI", rels=[([s, d], [0, 1])], theta=0.0)
             continue
         r = int(rng.integers(2, 6))
@@ -124,14 +153,14 @@ def query_mix(count: int, seed: int = 4, min_rows: int = 10_000, max_rows: int =
             fact_cols, dims = [], []
             for j in range(d):
                 m = sizes[j + 1]
-                keys = permutation(m, qseed, 100 + j)
-                payload = uniform(m, 0, 1 << 30, qseed, 200 + j)
+                keys = g.permutation(m, qseed, 100 + j)
+                payload = g.uniform(m, 0, 1 << 30, qseed, 200 + j)
                 dims.append(([keys, payload], [j, d + j]))
                 if zipfian:
-                    fact_cols.append(zipf(sizes[0], m, theta, qseed, 400 + j,
-                                          rank_to_key=permutation(m, qseed, 300 + j)))
+                    fact_cols.append(g.zipf(sizes[0], m, theta, qseed, 400 + j,
+                                          rank_to_key=g.permutation(m, qseed, 300 + j)))
                 else:
-                    fact_cols.append(uniform(sizes[0], 0, m, qseed, 400 + j))
+                    fact_cols.append(g.uniform(sizes[0], 0, m, qseed, 400 + j))
             yield dict(shape=shape, qt="NORMAL", rels=[(fact_cols, list(range(d)))] + dims, theta=theta)
             continue
         doms = [int(_log_uniform(rng, 1 << min_dom_bits, 1 << max_dom_bits)) for _ in range(r - 1)]
@@ -155,14 +184,14 @@ def query_mix(count: int, seed: int = 4, min_rows: int = 10_000, max_rows: int =
         rels = []
         for i in range(r):
             if i == 0:
-                c0 = uniform(sizes[i], 0, 1 << max_dom_bits, qseed, 10 * i)
+                c0 = g.uniform(sizes[i], 0, 1 << max_dom_bits, qseed, 10 * i)
             elif zipfian:
-                c0 = zipf(sizes[i], doms[i - 1], theta, qseed, 10 * i,
-                          rank_to_key=permutation(doms[i - 1], qseed, 10 * i + 2))
+                c0 = g.zipf(sizes[i], doms[i - 1], theta, qseed, 10 * i,
+                          rank_to_key=g.permutation(doms[i - 1], qseed, 10 * i + 2))
             else:
-                c0 = uniform(sizes[i], 0, doms[i - 1], qseed, 10 * i)
+                c0 = g.uniform(sizes[i], 0, doms[i - 1], qseed, 10 * i)
             hi = doms[i] if i < r - 1 else (1 << max_dom_bits)
-            c1 = uniform(sizes[i], 0, hi, qseed, 10 * i + 1)
+            c1 = g.uniform(sizes[i], 0, hi, qseed, 10 * i + 1)
             rels.append(([c0, c1], [i, i + 1]))
         yield dict(shape=shape, qt="NORMAL", rels=rels, theta=theta)
 

@@ -300,10 +300,9 @@ int  amj_bucket_build(amj_ctx *ctx, const int32_t *d_keys, uint64_t n, uint64_t 
                       int32_t *d_hash_keys, uint32_t *d_idx_in_origin, uint32_t *d_buc_ptrs);
 
 /* amj_bucket_build_static: the same bucket-CSR build, for callers that may
- * not allocate device memory (inside a stream capture that must stay free of
- * allocation nodes, under an engine that owns all device memory through its
- * own pool, or on a latency-critical path that cannot wait on the driver's
- * allocator).  No counterpart in the reference.  It allocates nothing: its
+ * not allocate device memory (a plugin under an engine that owns all device
+ * memory through its own pool, or a latency-critical loop that cannot wait on
+ * the driver's allocator).  No counterpart in the reference.  It allocates nothing: its
  * scratch is a fixed area inside the library (about 16.3 MB, resident on
  * every device that loads the library until exit), so n is limited to
  * AMJ_BUCKET_STATIC_MAX_KEYS and buckets to AMJ_BUCKET_STATIC_MAX_BUCKETS

@@ -1,5 +1,6 @@
 """ctypes bindings of the CPU oracle (liborc.so) and of the reference's
-MHJ-CPU harness (_ref/libmhjref.so).
+MHJ-CPU harness (_ref/libmhjref.so as shipped, _ref/libmhjref_mk.so with the
+reference's multi-key probe branch, MHJ-CPU/MHJ.cpp:64-90 and :205-245).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py as the checker.  The product (libamj.so and the
@@ -17,9 +18,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_PATH = os.path.join(HERE, "liborc.so")
 REF_PATH = os.path.join(HERE, "_ref", "libmhjref.so")
+REF_MK_PATH = os.path.join(HERE, "_ref", "libmhjref_mk.so")
 
 _orc = None
 _ref = None
+_ref_mk = None
 
 
 class orc_rel(C.Structure):
@@ -52,24 +55,46 @@ def orc():
                                      P(P(C.c_int32)), C.c_uint64]
         lib.orc_four_clique.argtypes = [P(C.c_int32), P(C.c_int32), C.c_uint64, C.c_int, P(C.c_uint64),
                                         P(C.c_uint64)]
+        lib.orc_gen_uniform_i32.argtypes = [P(C.c_int32), C.c_uint64, C.c_int64, C.c_int64, C.c_uint64,
+                                            C.c_uint64]
+        lib.orc_gen_permutation_i32.argtypes = [P(C.c_int32), C.c_uint64, C.c_uint64, C.c_uint64]
+        lib.orc_gen_zipf_i32.argtypes = [P(C.c_int32), C.c_uint64, C.c_uint64, C.c_double, P(C.c_int32),
+                                         C.c_uint64, C.c_uint64]
+        lib.orc_gen_rmat.argtypes = [C.c_int, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                     P(C.c_int32), P(C.c_int32), P(C.c_uint64)]
         _orc = lib
     return _orc
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_PATH)
+def ref_available(multi_key: bool = False) -> bool:
+    return os.path.exists(REF_MK_PATH if multi_key else REF_PATH)
 
 
-def ref():
-    global _ref
+def _ref_argtypes():
+    P = C.POINTER
+    return [C.c_int, P(C.c_uint64), P(C.c_int), P(C.c_uint32), P(P(C.c_int32)), C.c_int, P(C.c_uint64),
+            P(C.c_uint64), P(P(C.c_int32)), C.c_uint64, P(C.c_int), P(C.c_double)]
+
+
+def ref(multi_key: bool = False, relabel: bool = False):
+    """The MHJ-CPU harness's entry point: mhjref_run (single-key, as shipped)
+    or mhjref_run_mk (the reference's multi-key probe); with relabel, the
+    variant that renames result values through a map and sorts each tuple."""
+    global _ref, _ref_mk
+    relabel_args = [C.POINTER(C.c_int32), C.c_uint64]
+    if multi_key:
+        if _ref_mk is None:
+            lib = C.CDLL(REF_MK_PATH)
+            lib.mhjref_run_mk.argtypes = _ref_argtypes()
+            lib.mhjref_run_mk_relabel.argtypes = _ref_argtypes() + relabel_args
+            _ref_mk = lib
+        return _ref_mk.mhjref_run_mk_relabel if relabel else _ref_mk.mhjref_run_mk
     if _ref is None:
         lib = C.CDLL(REF_PATH)
-        P = C.POINTER
-        lib.mhjref_run.argtypes = [C.c_int, P(C.c_uint64), P(C.c_int), P(C.c_uint32), P(P(C.c_int32)), C.c_int,
-                                   P(C.c_uint64), P(C.c_uint64), P(P(C.c_int32)), C.c_uint64, P(C.c_int),
-                                   P(C.c_double)]
+        lib.mhjref_run.argtypes = _ref_argtypes()
+        lib.mhjref_run_relabel.argtypes = _ref_argtypes() + relabel_args
         _ref = lib
-    return _ref
+    return _ref.mhjref_run_relabel if relabel else _ref.mhjref_run
 
 
 def _tuple_buffers(k, cap):
@@ -187,10 +212,21 @@ def bucket_build(keys, buckets):
     return hk[:n], idx[:n], bp
 
 
-def mhj_reference(relations, nthreads=0, tuples=False):
+def mhj_reference(relations, nthreads=0, tuples=False, multi_key=False, relabel=None):
     """Run the reference's MHJ-CPU (TBJ) on relations in query order.
-    Returns (count, checksum, seconds[, columns])."""
-    lib = ref()
+    multi_key=True runs its multi-key probe, which compares every bound
+    attribute (the semantics of TRI and FOUR; equal to the single-key probe
+    on chains and stars).  relabel (int32 array): result values are renamed
+    through it and every tuple sorted before hashing (see
+    degree_ordered_copy).  Returns (count, checksum, seconds[, columns])."""
+    base = ref(multi_key, relabel is not None)
+    if relabel is not None:
+        lab = np.ascontiguousarray(relabel, np.int32)
+
+        def run(*a):
+            return base(*a, _i32p(lab), lab.shape[0])
+    else:
+        run = base
     nt = len(relations)
     if nt < 3:
         # a two-relation join (one build table) crashes TBJ as compiled here
@@ -216,18 +252,96 @@ def mhj_reference(relations, nthreads=0, tuples=False):
     cnt, chk, kk, secs = C.c_uint64(), C.c_uint64(), C.c_int(), C.c_double()
     tcols, tarr, cap = None, None, 0
     if tuples:
-        rc = lib.mhjref_run(nt, lens, ncols, attrs, data, nthreads, C.byref(cnt), C.byref(chk), None, 0,
-                            C.byref(kk), C.byref(secs))
-        assert rc == 0, rc
+        rc = run(nt, lens, ncols, attrs, data, nthreads, C.byref(cnt), C.byref(chk), None, 0, C.byref(kk),
+                 C.byref(secs))
+        if rc != 0:
+            raise ValueError(f"the MHJ-CPU harness failed ({rc})")
         cap = cnt.value
         tcols, tarr = _tuple_buffers(k, cap)
-    rc = lib.mhjref_run(nt, lens, ncols, attrs, data, nthreads, C.byref(cnt), C.byref(chk), tarr, cap,
-                        C.byref(kk), C.byref(secs))
+    rc = run(nt, lens, ncols, attrs, data, nthreads, C.byref(cnt), C.byref(chk), tarr, cap, C.byref(kk),
+             C.byref(secs))
     if rc != 0:
-        raise ValueError(f"mhjref_run failed ({rc})")
+        raise ValueError(f"the MHJ-CPU harness failed ({rc})")
     if tuples:
         return cnt.value, chk.value, secs.value, [c[:cap] for c in tcols]
     return cnt.value, chk.value, secs.value
+
+
+# ---- seeded inputs, generated without the product library (orc_gen.cpp) ----
+
+def gen_uniform(n, lo, hi, seed, stream=0):
+    out = np.empty(n, np.int32)
+    if orc().orc_gen_uniform_i32(_i32p(out), n, lo, hi, seed, stream) != 0:
+        raise ValueError("orc_gen_uniform_i32: bad arguments")
+    return out
+
+
+def gen_permutation(n, seed, stream=0):
+    out = np.empty(n, np.int32)
+    if orc().orc_gen_permutation_i32(_i32p(out), n, seed, stream) != 0:
+        raise ValueError("orc_gen_permutation_i32: bad arguments")
+    return out
+
+
+def gen_zipf(n, domain, theta, seed, stream=0, rank_to_key=None):
+    out = np.empty(n, np.int32)
+    rk = None if rank_to_key is None else np.ascontiguousarray(rank_to_key, np.int32)
+    if orc().orc_gen_zipf_i32(_i32p(out), n, domain, theta, _i32p(rk), seed, stream) != 0:
+        raise ValueError("orc_gen_zipf_i32: bad arguments")
+    return out
+
+
+def gen_rmat(scale, nedges, a, b, c, seed):
+    """Cleaned R-MAT edge relation (src < dst, no duplicates, shuffled)."""
+    src = np.empty(nedges, np.int32)
+    dst = np.empty(nedges, np.int32)
+    m = C.c_uint64()
+    if orc().orc_gen_rmat(scale, nedges, a, b, c, seed, _i32p(src), _i32p(dst), C.byref(m)) != 0:
+        raise ValueError("orc_gen_rmat: bad arguments")
+    return src[:m.value].copy(), dst[:m.value].copy()
+
+
+class GENERATORS:
+    """The primitive generators in the form accmultiwayjoins_b200.data's
+    workload builders take (their `gen` argument): chain_relations,
+    star_relations and query_mix then run without loading libamj."""
+    uniform = staticmethod(gen_uniform)
+    permutation = staticmethod(gen_permutation)
+    zipf = staticmethod(gen_zipf)
+    rmat = staticmethod(gen_rmat)
+
+
+def degree_ordered_copy(src, dst):
+    """Rename the vertices of an edge relation by their rank in (degree, id)
+    order and orient every edge from the lower to the higher rank.  Returns
+    (src', dst', rank_to_id).  Triangles and 4-cliques are the same vertex
+    sets in both graphs, and each is listed once under either orientation, so
+    the cyclic queries over the copy, renamed back through rank_to_id with
+    every tuple sorted, give the tuples of the queries over the relation
+    oriented u < v."""
+    src = np.asarray(src, np.int64)
+    dst = np.asarray(dst, np.int64)
+    n_v = int(max(src.max(initial=-1), dst.max(initial=-1))) + 1
+    deg = np.bincount(src, minlength=n_v) + np.bincount(dst, minlength=n_v)
+    order = np.lexsort((np.arange(n_v), deg))          # rank -> id, by (degree, id)
+    rank = np.empty(n_v, np.int64)
+    rank[order] = np.arange(n_v)
+    rs, rd = rank[src], rank[dst]
+    lo, hi = np.minimum(rs, rd), np.maximum(rs, rd)
+    return lo.astype(np.int32), hi.astype(np.int32), order.astype(np.int32)
+
+
+def tri_relations(src, dst):
+    """The TRI attribute pattern over one edge relation, A(0,1) B(1,2) C(0,2)
+    (MHJ-GPU/exec_AMHJ.cu:32-49)."""
+    return [([src, dst], [0, 1]), ([src, dst], [1, 2]), ([src, dst], [0, 2])]
+
+
+def four_relations(src, dst):
+    """The FOUR attribute pattern over one edge relation, A(0,1) B(1,2) C(2,3)
+    D(0,3) E(0,2) F(1,3) (MHJ-GPU/exec_AMHJ.cu:50-69)."""
+    pats = [(0, 1), (1, 2), (2, 3), (0, 3), (0, 2), (1, 3)]
+    return [([src, dst], list(p)) for p in pats]
 
 
 def timed(fn, *args, **kw):

@@ -66,12 +66,83 @@ def make_case(case):
     raise ValueError(kind)
 
 
-@pytest.mark.parametrize("case", load_golden()["cases"], ids=lambda c: c["name"])
+# the CPU suite stays within minutes: cases whose oracle run takes longer
+# (the full-size star and triangle) are checked by the GPU tests only
+CPU_CASES = [c for c in load_golden()["cases"]
+             if c.get("fact_rows", 0) <= 1_000_000 and c.get("edges", 0) <= 1_000_000]
+
+
+@pytest.mark.parametrize("case", [c for c in CPU_CASES if c["kind"] in ("chain", "star")], ids=lambda c: c["name"])
 def test_oracle_matches_golden(built, case):
     rels = make_case(case)
     cnt, chk = O.mhj(rels)
     assert cnt == case["count"]
     assert f"{chk:016x}" == case["checksum"]
+
+
+@pytest.mark.parametrize("case", [c for c in CPU_CASES if c["kind"] in ("tri", "four")], ids=lambda c: c["name"])
+def test_cyclic_restatements_match_reference_golden(built, case):
+    """The triangle and 4-clique restatements against the reference's own
+    multi-key probe (fixtures written by tests/golden/make_golden.py)."""
+    s, d = O.gen_rmat(case["scale"], case["nedges"], *case["abc"], seed=case["seed"])
+    assert s.shape[0] == case["edges"]
+    got = O.triangle(s, d) if case["kind"] == "tri" else O.four_clique(s, d)
+    assert got == (case["count"], int(case["checksum"], 16))
+
+
+@pytest.mark.skipif(not O.ref_available(multi_key=True), reason="reference MHJ-CPU harness not built")
+@pytest.mark.parametrize("abc", [(0.57, 0.19, 0.19), (0.6, 0.15, 0.15)])
+def test_reference_multi_key_probe_answers_tri_and_four(built, abc):
+    """The reference's multi-key probe on the TRI / FOUR patterns equals the
+    restatements, on the relation as given and through the degree-ordered
+    copy renamed back; the shipped single-key probe does not (it never
+    compares the second attribute of C(0,2))."""
+    s, d = O.gen_rmat(9, 6000, *abc, seed=31)
+    tri, four = O.triangle(s, d), O.four_clique(s, d)
+    assert O.mhj_reference(O.tri_relations(s, d), nthreads=4, multi_key=True)[:2] == tri
+    assert O.mhj_reference(O.four_relations(s, d), nthreads=4, multi_key=True)[:2] == four
+    s2, d2, rank_to_id = O.degree_ordered_copy(s, d)
+    assert O.mhj_reference(O.tri_relations(s2, d2), nthreads=3, multi_key=True, relabel=rank_to_id)[:2] == tri
+    assert O.mhj_reference(O.four_relations(s2, d2), nthreads=2, multi_key=True, relabel=rank_to_id)[:2] == four
+    assert O.mhj_reference(O.tri_relations(s, d), nthreads=4)[0] > tri[0]
+    # chains: the multi-key probe compares only the join key, as the shipped one
+    rels = data.chain_relations(5000, 1 << 10, 3, seed=2, gen=O.GENERATORS)
+    assert O.mhj_reference(rels, multi_key=True)[:2] == O.mhj_reference(rels)[:2]
+
+
+@pytest.mark.skipif(not O.ref_available(multi_key=True), reason="reference MHJ-CPU harness not built")
+def test_reference_multi_key_tuples_equal_restatement_tuples(built):
+    s, d = O.gen_rmat(8, 1500, 0.57, 0.19, 0.19, seed=3)
+    cnt, chk, _, cols = O.mhj_reference(O.tri_relations(s, d), nthreads=2, tuples=True, multi_key=True)
+    ocnt, ochk, ocols = O.triangle(s, d, tuples=True)
+    assert (cnt, chk) == (ocnt, ochk)
+    a, b = np.stack(cols, 1), np.stack(ocols, 1)
+    assert np.array_equal(a[np.lexsort(a.T[::-1])], b[np.lexsort(b.T[::-1])])
+
+
+@pytest.mark.parametrize("gen", ["rmat", "chain", "star"])
+def test_oracle_generators_equal_product_generators(built, gen):
+    """The oracle's own input generators (used by the CPU arm of bench.py so
+    that it never loads the product library) are bit-identical to the
+    product's."""
+    if gen == "rmat":
+        for args in [(8, 2000, 0.57, 0.19, 0.19, 3), (14, 1 << 18, 0.6, 0.15, 0.15, 22), (1, 10, 0.3, 0.3, 0.3, 1)]:
+            for x, y in zip(O.gen_rmat(*args), data.rmat(*args)):
+                assert np.array_equal(x, y)
+    elif gen == "chain":
+        a = data.chain_relations(50000, 1 << 12, 4, seed=5, gen=O.GENERATORS)
+        b = data.chain_relations(50000, 1 << 12, 4, seed=5)
+        assert [at for _, at in a] == [at for _, at in b]
+        for (ca, _), (cb, _) in zip(a, b):
+            assert all(np.array_equal(x, y) for x, y in zip(ca, cb))
+    else:
+        (fa, ta), da = data.star_relations(40000, [1000, 200, 100, 10], theta=1.1, seed=3, gen=O.GENERATORS)
+        (fb, tb), db = data.star_relations(40000, [1000, 200, 100, 10], theta=1.1, seed=3)
+        assert ta == tb and all(np.array_equal(x, y) for x, y in zip(fa, fb))
+        for (ca, aa), (cb, ab) in zip(da, db):
+            assert aa == ab and all(np.array_equal(x, y) for x, y in zip(ca, cb))
+    assert np.array_equal(O.gen_uniform(1000, -(1 << 31), 1 << 31, 9, 4), data.uniform(1000, -(1 << 31), 1 << 31, 9, 4))
+    assert np.array_equal(O.gen_zipf(1000, 77, 0.7, 9, 2), data.zipf(1000, 77, 0.7, 9, 2))
 
 
 @pytest.mark.skipif(not O.ref_available(), reason="reference MHJ-CPU harness not built (reference sources absent)")

@@ -214,7 +214,8 @@ def test_amhj_chain_all_switches(layout, sw, materialize):
             assert data.checksum(got.columns) == chk
 
 
-@pytest.mark.parametrize("case", json.load(open(GOLDEN))["cases"], ids=lambda c: c["name"])
+@pytest.mark.parametrize("case", [c for c in json.load(open(GOLDEN))["cases"] if c["kind"] in ("chain", "star")],
+                         ids=lambda c: c["name"])
 def test_amhj_golden(ctx, case):
     if case["kind"] == "chain":
         rels = data.chain_relations(case["n"], case["key_range"], case["nrels"], seed=case["seed"])

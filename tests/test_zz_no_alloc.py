@@ -1,10 +1,11 @@
 """amj_bucket_build_static, the allocation-free bucket build, against
 amj_bucket_build through the C ABI.
 
-It exists for callers that may not allocate device memory (stream capture
-without allocation nodes, engines that own every device byte, latency-critical
-loops); its scratch is a fixed area compiled into the library.  The file name
-sorts last so a run that stops at the first failure has run everything else.
+It exists for callers that may not allocate device memory (engines that own
+every device byte through their own pool, loops that may not wait on the
+driver's allocator); its scratch is a fixed area compiled into the library and
+shared by every call.  The file name sorts last so a run that stops at the
+first failure has run everything else.
 """
 import ctypes as C
 
@@ -44,8 +45,11 @@ def run_both(ctx, keys, buckets):
 
 def test_static_scratch_bucket_build_matches_allocating_build():
     with Context(0) as ctx:
-        cases = [(300_000, 1 << 18, -(1 << 30), 1 << 30, 1), (MAX_KEYS, 1 << 20, 0, 1 << 18, 2)]
-        for n, buckets, lo, hi, seed in cases:   # two calls in a row on the shared scratch
+        # two full-size calls in a row on the shared scratch, then the edges:
+        # one bucket (no sort pass), no keys, and a small call after a large one
+        cases = [(300_000, 1 << 18, -(1 << 30), 1 << 30, 1), (MAX_KEYS, 1 << 20, 0, 1 << 18, 2),
+                 (5000, 1, -100, 100, 3), (0, 1 << 4, 0, 16, 4), (0, 1, 0, 16, 5), (777, 1 << 20, 0, 1 << 24, 6)]
+        for n, buckets, lo, hi, seed in cases:
             keys = data.uniform(n, lo, hi, seed=seed)
             (hk0, ix0, bp0), (hk1, ix1, bp1) = run_both(ctx, keys, buckets)
             assert np.array_equal(bp0, bp1)
