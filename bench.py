@@ -9,16 +9,16 @@ the radix sort, then the leapfrog intersection, returning count and
 checksum.  The unit of work is one output tuple (one triangle).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--algo DFS|BFS|AMHJ] [--scale S] [--workload triangle|chain|batch]
+                  [--algo DFS|BFS|AMHJ] [--scale S]
+                  [--workload triangle|chain|four|batch|serve] [--no-configs]
 
 --scale S runs the same workload on a smaller R-MAT graph (2^S vertices,
 2^(S+4) edges), for profiling.  --workload chain runs the 3-way chain join
 R1(a,b) R2(b,c) R3(c,d) (3 x 1M rows, keys uniform in [0, 2^18), seeds 1-3)
-through AMHJ (count + checksum, hash builds included), with the reference's
-own MHJ-CPU (compiled from its sources into oracle/_ref) as CPU baseline.
---workload batch runs 512 heterogeneous queries as one batch (autotuned,
-CUDA-graph replay) and reports, beside its tuples/s, the one-query-per-call
-tuples/s on the same queries and p50/p99 latencies of both forms.
+through AMHJ (count + checksum, hash builds included).  --workload batch
+runs 512 heterogeneous queries as one batch (autotuned, CUDA-graph replay)
+and reports, beside its tuples/s, the one-query-per-call tuples/s on the
+same queries and p50/p99 latencies of both forms.
 
 * value: tuples/s with the input resident on the device (whole job: sum of
   the ranks' tuples / max over ranks of the timed K steps).
@@ -28,9 +28,17 @@ tuples/s on the same queries and p50/p99 latencies of both forms.
 * roofline: the intersection kernels (triangle) or the probe kernel (chain),
   timed with CUDA events inside the library; algorithmic bytes per launch
   as documented below; traffic from the committed ncu capture.
-* cpu_baseline: triangle: the oracle's restatement on all host cores (the
-  reference has no CPU triangle; its MHJ-CPU hard-codes a single-key compare
-  that is wrong for cyclic queries); chain: the reference MHJ-CPU.
+* configs (default triangle run, one GPU): the chain and the batched
+  configurations measured in the same run, each with its own value, e2e and
+  CPU figure; the batched record carries batched vs one-query-per-call
+  tuples/s and p50/p99 latencies.
+* cpu_baseline and --impl reference: the reference's MHJ-CPU
+  (MHJ-CPU/MHJ.cpp) compiled from its sources into oracle/_ref, on all host
+  cores: as shipped for chains and stars; its multi-key probe branch for the
+  triangle and the 4-clique, over the degree-ordered copy of the graph,
+  renamed back (see RefTriangle), one bounded probe slice per step.  The
+  reference arm generates its inputs with the oracle's generators and never
+  loads the product library.
 
 With N > 1 (torchrun) every rank runs its own independent instance of the
 workload (seed offset by rank): per-GPU work is fixed, no data-path
@@ -132,9 +140,13 @@ class Triangle:
         self.h2d = 8 * self.E
 
     def describe(self, rank_note):
-        return (f"triangle R(a,b)S(b,c)T(a,c), R-MAT scale {self.scale}, {self.nedges} edges "
+        return self.describe_static(self.scale, self.algo, rank_note)
+
+    @staticmethod
+    def describe_static(scale, algo, rank_note=""):
+        return (f"triangle R(a,b)S(b,c)T(a,c), R-MAT scale {scale}, {1 << (scale + 4)} edges "
                 f"(0.57,0.19,0.19,0.05), seed {SEED}{rank_note}; "
-                f"{'AMHJ TRI' if self.algo == 'AMHJ' else 'ALFTJ-' + self.algo} count+checksum incl. index build")
+                f"{'AMHJ TRI' if algo == 'AMHJ' else 'ALFTJ-' + algo} count+checksum incl. index build")
 
     def device_relations(self, ctx, dev):
         import torch
@@ -174,12 +186,64 @@ class Triangle:
         return "lftj_tri_wedge_kernel (intersection)" if self.algo == "DFS" else "lftj_tri_bfs kernels (intersection)"
 
     def cpu_baseline(self):
+        """The reference's MHJ-CPU multi-key probe on a bounded sample of
+        this workload (RefTriangle), about 15 s of CPU time."""
+        ref = RefTriangle(self.scale, self.nedges, SEED)
+        return ref.sample_until(15.0)
+
+
+class RefTriangle:
+    """The reference's CPU implementation of the triangle workload: MHJ-CPU
+    (MHJ-CPU/MHJ.cpp TBJ) with its multi-key probe branch (MHJ.cpp:64-90,
+    :205-245), compiled from the reference sources into
+    oracle/_ref/libmhjref_mk.so, over the TRI attribute pattern
+    (MHJ-GPU/exec_AMHJ.cu:32-49).  It joins the graph's (degree, id)-ranked
+    copy and renames the results back (the same triangles; on the relation as
+    given its probe does about 24x more work on this graph).  One sample is
+    one probe slice: 1/SLICES of the probe relation's rows against the whole
+    build relations; TBJ's own partitioning of the build relations is part
+    of every timed call.  Inputs come from the oracle's generators, so this
+    process never loads the product library."""
+
+    SLICES = 64
+
+    def __init__(self, scale, nedges, seed):
         from oracle import oracle as O
-        cores = os.cpu_count() or 1
-        t0 = time.perf_counter()
-        cnt, chk = O.triangle(self.src, self.dst, nthreads=cores)
-        sec = time.perf_counter() - t0
-        return cnt, chk, sec, cores, "port", "the full workload once (oracle triangle restatement)"
+        self.O = O
+        s, d = O.gen_rmat(scale, nedges, *RMAT_ABC, seed=seed)
+        self.E = int(s.shape[0])
+        self.s2, self.d2, self.rank_to_id = O.degree_ordered_copy(s, d)
+        self.cores = os.cpu_count() or 1
+        self.next = 0
+        self.kind = "reference" if O.ref_available(multi_key=True) else "port"
+
+    def step(self):
+        """One slice, the next in turn: (tuples, seconds in TBJ)."""
+        i = self.next % self.SLICES
+        self.next += 1
+        lo, hi = i * self.E // self.SLICES, (i + 1) * self.E // self.SLICES
+        probe = ([self.s2[lo:hi], self.d2[lo:hi]], [0, 1])
+        rels = [probe, ([self.s2, self.d2], [1, 2]), ([self.s2, self.d2], [0, 2])]
+        if self.kind == "reference":
+            cnt, _, sec = self.O.mhj_reference(rels, nthreads=self.cores, multi_key=True, relabel=self.rank_to_id)
+        else:
+            t0 = time.perf_counter()
+            cnt, _ = self.O.mhj(rels, nthreads=self.cores)
+            sec = time.perf_counter() - t0
+        return cnt, sec
+
+    def describe(self):
+        what = ("reference MHJ-CPU multi-key probe (oracle/_ref/libmhjref_mk.so)" if self.kind == "reference"
+                else "the oracle's multi-way join restatement (reference sources absent)")
+        return (f"{what} on the TRI pattern over the degree-ordered copy, one 1/{self.SLICES} probe slice per "
+                f"sample (slices in turn), whole build relations, TBJ call timed")
+
+    def sample_until(self, budget_s):
+        tuples, secs, n = 0, 0.0, 0
+        while secs < budget_s and n < self.SLICES:
+            c, t = self.step()
+            tuples, secs, n = tuples + c, secs + t, n + 1
+        return tuples, None, secs, self.cores, self.kind, f"{n} slices: " + self.describe()
 
 
 class Clique4:
@@ -199,8 +263,12 @@ class Clique4:
         self.h2d = 8 * self.E
 
     def describe(self, rank_note):
-        op = "AMHJ FOUR (ws=1 fib=1), hash builds" if self.algo == "AMHJ" else "ALFTJ 4-clique (DFS), trie build"
-        return (f"4-clique, R-MAT scale {self.scale}, {1 << (self.scale + 4)} edges "
+        return self.describe_static(self.scale, self.algo, rank_note)
+
+    @staticmethod
+    def describe_static(scale, algo, rank_note=""):
+        op = "AMHJ FOUR (ws=1 fib=1), hash builds" if algo == "AMHJ" else "ALFTJ 4-clique (DFS), trie build"
+        return (f"4-clique, R-MAT scale {scale}, {1 << (scale + 4)} edges "
                 f"(0.6,0.15,0.15,0.1), seed 22{rank_note}; {op} included, count+checksum")
 
     def device_relations(self, ctx, dev):
@@ -225,23 +293,64 @@ class Clique4:
         return "amhj_probe_kernel (count pass)" if self.algo == "AMHJ" else "lftj_clique4_kernel"
 
     def cpu_baseline(self):
-        """The oracle's 4-clique restatement on a scale-14 graph of the same
-        generator (the full graph would take hours on the CPU)."""
-        from accmultiwayjoins_b200 import data
+        """The reference's MHJ-CPU multi-key probe on the FOUR pattern over a
+        scale-14 graph of the same generator (RefClique4)."""
+        return RefClique4().sample_until(15.0)
+
+
+class RefClique4:
+    """The reference's CPU implementation of the 4-clique: MHJ-CPU's
+    multi-key probe (oracle/_ref/libmhjref_mk.so) on the FOUR attribute
+    pattern (MHJ-GPU/exec_AMHJ.cu:50-69) over the degree-ordered copy of an
+    R-MAT scale-14 graph of the configured generator (2^18 edges,
+    0.6/0.15/0.15/0.1, seed 22; the scale-22 graph's 9.4e10 4-cliques would
+    not fit the reference's in-memory result chunks), one 1/SLICES probe
+    slice per sample."""
+
+    SLICES = 16
+
+    def __init__(self):
         from oracle import oracle as O
-        cores = os.cpu_count() or 1
-        s, d = data.rmat(14, 1 << 18, 0.6, 0.15, 0.15, seed=22)
-        t0 = time.perf_counter()
-        cnt, chk = O.four_clique(s, d, nthreads=cores)
-        return cnt, chk, time.perf_counter() - t0, cores, "port", "R-MAT scale 14 of the same generator (oracle restatement)"
+        self.O = O
+        s, d = O.gen_rmat(14, 1 << 18, 0.6, 0.15, 0.15, seed=22)
+        self.E = int(s.shape[0])
+        self.s2, self.d2, self.rank_to_id = O.degree_ordered_copy(s, d)
+        self.cores = os.cpu_count() or 1
+        self.next = 0
+        self.kind = "reference" if O.ref_available(multi_key=True) else "port"
+
+    def step(self):
+        i = self.next % self.SLICES
+        self.next += 1
+        lo, hi = i * self.E // self.SLICES, (i + 1) * self.E // self.SLICES
+        rels = self.O.four_relations(self.s2, self.d2)
+        rels[0] = ([self.s2[lo:hi], self.d2[lo:hi]], [0, 1])
+        if self.kind == "reference":
+            cnt, _, sec = self.O.mhj_reference(rels, nthreads=self.cores, multi_key=True, relabel=self.rank_to_id)
+        else:
+            t0 = time.perf_counter()
+            cnt, _ = self.O.mhj(rels, nthreads=self.cores)
+            sec = time.perf_counter() - t0
+        return cnt, sec
+
+    def describe(self):
+        return (f"reference MHJ-CPU multi-key probe, FOUR pattern, R-MAT scale 14 (2^18 edges, seed 22) "
+                f"degree-ordered copy, one 1/{self.SLICES} probe slice per sample, TBJ call timed")
+
+    def sample_until(self, budget_s):
+        tuples, secs, n = 0, 0.0, 0
+        while secs < budget_s and n < self.SLICES:
+            c, t = self.step()
+            tuples, secs, n = tuples + c, secs + t, n + 1
+        return tuples, None, secs, self.cores, self.kind, f"{n} slices: " + self.describe()
 
 
 class Chain:
     B = 1 << 19   # buckets = floorPow2(1e6)
 
-    def __init__(self, args, rank):
+    def __init__(self, args, rank, gen=None):
         from accmultiwayjoins_b200 import data
-        self.rels = data.chain_relations(1_000_000, 1 << 18, 3, seed=1 + 3 * rank)
+        self.rels = data.chain_relations(1_000_000, 1 << 18, 3, seed=1 + 3 * rank, gen=gen)
         self.h2d = sum(4 * len(c[0]) * len(c) for c, _ in self.rels)
 
     def describe(self, rank_note):
@@ -304,11 +413,11 @@ class BatchMix:
     run as one amj_batch: one build pass and one persistent probe launch,
     captured once into a CUDA graph and replayed every step."""
 
-    def __init__(self, args, rank):
+    def __init__(self, args, rank, gen=None):
         from accmultiwayjoins_b200 import data
         t0 = time.perf_counter()
         self.queries = list(data.query_mix(args.queries, seed=4 + 1000 * rank, min_rows=args.min_rows,
-                                           max_rows=args.max_rows))
+                                           max_rows=args.max_rows, gen=gen))
         self.gen_s = time.perf_counter() - t0
         self.rows = sum(len(cols[0]) for q in self.queries for cols, _ in q["rels"])
         self.h2d = sum(4 * len(c) for q in self.queries for cols, _ in q["rels"] for c in cols)
@@ -322,33 +431,40 @@ class BatchMix:
                 f"4M], key domains 2^12-2^24, uniform or Zipf theta in [0.5,1.5], seed 4{rank_note}); "
                 f"one build pass + one persistent probe launch per step, CUDA graph replay")
 
-    def cpu_sample(self, budget_s=15.0):
-        """The oracle (and the reference MHJ-CPU where it applies: acyclic
-        single-key chains and stars) on the first queries until budget_s of
-        CPU time is spent."""
+    def cpu_sample(self, budget_s=15.0, start=0):
+        """The reference MHJ-CPU on the queries from `start` on, one at a
+        time, until budget_s of CPU time is spent: chains and stars of 3+
+        relations through the shipped single-key probe, triangles through its
+        multi-key probe over the degree-ordered copy.  Two-relation joins
+        crash the reference's TBJ (one build table), so those run on the
+        oracle's restatement."""
         from oracle import oracle as O
         cores = os.cpu_count() or 1
         spent, tuples, n, kinds = 0.0, 0, 0, set()
-        for q in self.queries:
+        for j in range(len(self.queries)):
+            q = self.queries[(start + j) % len(self.queries)]
             t0 = time.perf_counter()
-            if q["qt"] == "TRI":
-                s, d = q["rels"][0][0]
-                cnt, _ = O.triangle(s, d, nthreads=cores)
-                kinds.add("port")
-            elif O.ref_available() and len(q["rels"]) >= 3:
-                cnt, _, _ = O.mhj_reference(q["rels"], nthreads=cores)
+            if q["qt"] == "TRI" and O.ref_available(multi_key=True):
+                s2, d2, lab = O.degree_ordered_copy(*q["rels"][0][0])
+                cnt, _, sec = O.mhj_reference(O.tri_relations(s2, d2), nthreads=cores, multi_key=True, relabel=lab)
+                kinds.add("reference")
+            elif q["qt"] == "NORMAL" and O.ref_available() and len(q["rels"]) >= 3:
+                cnt, _, sec = O.mhj_reference(q["rels"], nthreads=cores)
                 kinds.add("reference")
             else:
-                cnt, _ = O.mhj(q["rels"], nthreads=cores)
+                rels = O.tri_relations(*q["rels"][0][0]) if q["qt"] == "TRI" else q["rels"]
+                cnt, _ = O.mhj(rels, nthreads=cores)
+                sec = time.perf_counter() - t0
                 kinds.add("port")
-            spent += time.perf_counter() - t0
+            spent += sec
             tuples += cnt
             n += 1
             if spent >= budget_s:
                 break
-        kind = "reference" if kinds == {"reference"} else "port"
-        sample = (f"first {n} of {len(self.queries)} queries, one query at a time (reference MHJ-CPU for chains and "
-                  f"stars of 3+ relations, the oracle's restatement for triangles and two-relation joins)")
+        kind = "reference" if kinds == {"reference"} else ("port" if kinds == {"port"} else "reference+port")
+        sample = (f"{n} of {len(self.queries)} queries from query {start}, one query at a time (reference MHJ-CPU: "
+                  f"single-key probe for chains and stars of 3+ relations, multi-key probe over the degree-ordered "
+                  f"copy for triangles; two-relation joins on the oracle's restatement)")
         return tuples, spent, cores, kind, sample
 
 
@@ -358,6 +474,20 @@ def pct(xs, p):
 
 
 def run_batch(args, rank, world, local_rank):
+    line = batch_line(args, rank, world, local_rank)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+# the grid point the autotuner chose on the 512-query mix (load factor 0.5,
+# block 128, task chunk 128), used where a run skips the tuner
+TUNED_BATCH_POINT = (0.5, 128, 128)
+
+
+def batch_line(args, rank, world, local_rank, fixed_point=None, cpu_budget=15.0):
+    """The batched workload measured: returns rank 0's JSON line (None on
+    the other ranks).  fixed_point (load factor, block, task chunk) skips the
+    autotuner."""
     import ctypes as C
     import torch
     from accmultiwayjoins_b200 import Context, _lib as L
@@ -393,7 +523,10 @@ def run_batch(args, rank, world, local_rank):
 
     # autotune on every 8th query, then the batched steps (graph replay)
     t0 = time.perf_counter()
-    if args.tune:
+    if fixed_point is not None:
+        opts, tune_ms = Batch_default_opts(L), None
+        opts.load_factor, opts.block_size, opts.task_chunk = fixed_point
+    elif args.tune:
         opts, tune_ms = b.tune(sample_every=8, reps=1)
     else:
         opts, tune_ms = Batch_default_opts(L), None
@@ -446,7 +579,7 @@ def run_batch(args, rank, world, local_rank):
     if rank != 0:
         b.close()
         ctx.close()
-        return
+        return None
     line = {
         "metric": METRIC, "value": total / (ms * 1e-3), "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -456,7 +589,8 @@ def run_batch(args, rank, world, local_rank):
                    "opts": {"layout": int(opts.layout), "load_factor": float(opts.load_factor),
                             "block_size": int(opts.block_size), "task_chunk": int(opts.task_chunk),
                             "use_graph": int(opts.use_graph)},
-                   "tuned_on": "every 8th query, full grid" if args.tune else "defaults",
+                   "tuned_on": ("fixed: the point the autotuner chose on this mix" if fixed_point is not None else
+                                "every 8th query, full grid" if args.tune else "defaults"),
                    "tune_s": tune_s, "tune_best_sample_ms": tune_ms, "generation_s": wl.gen_s},
         "e2e": {"value": total / (e2e * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": wl.h2d * world,
                 "d2h_bytes_per_step": 16 * n_queries, "ms_per_step": e2e},
@@ -473,12 +607,12 @@ def run_batch(args, rank, world, local_rank):
         "clocks": clocks,
     }
     if not args.no_cpu_baseline:
-        tuples, sec, cores, kind, sample = wl.cpu_sample()
+        tuples, sec, cores, kind, sample = wl.cpu_sample(budget_s=cpu_budget)
         line["cpu_baseline"] = {"value": tuples / sec, "unit": "tuples/s", "cores": cores, "kind": kind,
                                 "sample": sample}
-    print(json.dumps(line), flush=True)
     b.close()
     ctx.close()
+    return line
 
 
 class ServeMix:
@@ -495,19 +629,20 @@ class ServeMix:
     Out-of-core: R1(a,b) R2(b,c) R3(c,d) R4(d,e) of --ooc-rows rows each, keys
     uniform in [0, rows) (about one match per probe row per join)."""
 
-    def __init__(self, args, rank):
+    def __init__(self, args, rank, gen=None, with_ooc=True):
         from accmultiwayjoins_b200 import data
+        g = gen or data._Libamj
         self.args = args
         self.templates = []
         for sc in (10, 11, 12):
-            s_, d_ = data.rmat(sc, (1 << sc) * 16, 0.6, 0.15, 0.15, seed=5 + sc + 100 * rank)
+            s_, d_ = g.rmat(sc, (1 << sc) * 16, 0.6, 0.15, 0.15, seed=5 + sc + 100 * rank)
             self.templates.append(("FOUR", f"4-clique R-MAT scale {sc}", [([s_, d_], [0, 1])]))
         for fr in (50_000, 200_000, 1_000_000):
             dims = [max(100, m * fr // 60_000_000) for m in (1_000_000, 200_000, 100_000, 10_000)]
-            fact, dd = data.star_relations(fr, dims, theta=1.1, seed=7 + fr + rank)
+            fact, dd = data.star_relations(fr, dims, theta=1.1, seed=7 + fr + rank, gen=gen)
             self.templates.append(("NORMAL", f"star fact {fr} dims {dims}", [fact] + dd))
-        n = args.ooc_rows
-        self.ooc = [([data.uniform(n, 0, n, 31 + i + 10 * rank, 0), data.uniform(n, 0, n, 31 + i + 10 * rank, 1)],
+        n = args.ooc_rows if with_ooc else 0
+        self.ooc = [([g.uniform(n, 0, n, 31 + i + 10 * rank, 0), g.uniform(n, 0, n, 31 + i + 10 * rank, 1)],
                      [i, i + 1]) for i in range(4)] if n else None
 
     def describe(self, rank_note):
@@ -637,94 +772,168 @@ def profiled_traffic(args):
 
 # ------------------------------------------------------------------ arms
 
+def reference_line(args, value, ms, wl_desc, cpu):
+    return {
+        "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": wl_desc, "l2": "n/a (CPU)"},
+        "cpu_baseline": dict(cpu, value=value),
+        "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def run_reference(args, rank, world):
-    """CPU arm: the reference's CPU implementation of the workload (MHJ-CPU
-    for the chain; the oracle's triangle restatement for the triangle) on all
-    host threads.  Rank 0 only."""
+    """CPU arm: the reference's own CPU implementation of the workload on all
+    host threads, rank 0 only.  MHJ-CPU (MHJ-CPU/MHJ.cpp) compiled from the
+    reference sources into oracle/_ref: as shipped for chains and stars, its
+    multi-key probe branch for the cyclic queries.  Each step is a bounded
+    sample of the workload (see the classes Ref*).  Inputs are generated by
+    the oracle's generators (oracle/orc_gen.cpp, bit-identical to the
+    product's), so this process never loads libamj."""
     if rank != 0:
         return
+    from oracle import oracle as O
+    gen = O.GENERATORS
+    cores = os.cpu_count() or 1
     if args.workload == "serve":
-        # the reference serves nothing: its CPU join (MHJ-CPU for the stars,
-        # the oracle's restatement for the 4-cliques) runs the resident
-        # templates one request after another, drawn as the stream draws them
-        from oracle import oracle as O
-        wl = ServeMix(args, 0)
-        cores = os.cpu_count() or 1
+        # the reference serves nothing: MHJ-CPU runs the resident templates one
+        # request after another, drawn as the stream draws them (stars through
+        # the shipped probe, 4-cliques through the multi-key probe over the
+        # degree-ordered copy)
+        wl = ServeMix(args, 0, gen=gen, with_ooc=False)
+        prepared = []
+        for qt, _, rels in wl.templates:
+            if qt == "FOUR":
+                s2, d2, lab = O.degree_ordered_copy(*rels[0][0])
+                prepared.append((O.four_relations(s2, d2), True, lab))
+            else:
+                prepared.append((rels, False, None))
         rng = np.random.Generator(np.random.PCG64(5))
         vals = []
         for i in range(args.warmup + args.steps):
             t_end = time.perf_counter() + 1.0
             tuples, sec, n = 0, 0.0, 0
             while time.perf_counter() < t_end:
-                qt, _, rels = wl.templates[int(rng.integers(0, len(wl.templates)))]
-                t0 = time.perf_counter()
-                if qt == "FOUR":
-                    cnt, _ = O.four_clique(*rels[0][0])
-                elif O.ref_available():
-                    cnt, _, _ = O.mhj_reference(rels, nthreads=cores)
-                else:
-                    cnt, _ = O.mhj(rels, nthreads=cores)
-                sec += time.perf_counter() - t0
+                rels, mk, lab = prepared[int(rng.integers(0, len(prepared)))]
+                cnt, _, t = O.mhj_reference(rels, nthreads=cores, multi_key=mk, relabel=lab)
+                sec += t
                 tuples += cnt
                 n += 1
             if i >= args.warmup:
                 vals.append((tuples, sec, n))
         tuples = sum(v[0] for v in vals)
         sec = sum(v[1] for v in vals)
-        value = tuples / sec
         sample = (f"{sum(v[2] for v in vals)} requests of the resident templates, one after another, over "
-                  f"{args.steps} s (reference MHJ-CPU for the stars, the oracle's 4-clique restatement)")
-        line = {
-            "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * sec / len(vals), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
-            "impl": "reference", "config": {"workload": wl.describe(""), "l2": "n/a (CPU)"},
-            "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": "port",
-                             "sample": sample},
-            "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }
-        print(json.dumps(line), flush=True)
+                  f"{args.steps} s (reference MHJ-CPU: shipped probe for the stars, multi-key probe over the "
+                  f"degree-ordered copy for the 4-cliques; TBJ calls timed)")
+        cpu = {"unit": "tuples/s", "cores": cores, "kind": "reference", "sample": sample}
+        print(json.dumps(reference_line(args, tuples / sec, 1e3 * sec / len(vals), wl.describe(""), cpu)),
+              flush=True)
         return
     if args.workload == "batch":
-        wl = BatchMix(args, 0)
-        vals = []
+        wl = BatchMix(args, 0, gen=gen)
+        vals, start = [], 0
+        kind = sample = None
         for i in range(args.warmup + args.steps):
-            tuples, sec, cores, kind, sample = wl.cpu_sample(budget_s=10.0)
+            tuples, sec, cores, kind, sample = wl.cpu_sample(budget_s=10.0, start=start)
+            start += 1
             if i >= args.warmup:
                 vals.append((tuples, sec))
         tuples = sum(t for t, _ in vals)
         sec = sum(t for _, t in vals)
-        value = tuples / sec
-        line = {
-            "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": sec / len(vals) * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
-            "impl": "reference", "config": {"workload": wl.describe(""), "l2": "n/a (CPU)"},
-            "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample},
-            "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }
-        print(json.dumps(line), flush=True)
+        cpu = {"unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample + "; step i starts at query i"}
+        print(json.dumps(reference_line(args, tuples / sec, sec / len(vals) * 1e3, wl.describe(""), cpu)),
+              flush=True)
         return
-    wl = make_workload(args, 0)
-    times = []
-    cnt = 0
-    kind = sample = None
-    cores = os.cpu_count() or 1
+    if args.workload == "chain":
+        wl = Chain(args, 0, gen=gen)
+        step = lambda: wl.cpu_baseline()[::2][:2]  # noqa: E731  (count, seconds)
+        desc, sample = wl.describe(""), "the full workload per step (reference MHJ-CPU as shipped, TBJ call timed)"
+        kind = "reference" if O.ref_available() else "port"
+    else:
+        ref = RefClique4() if args.workload == "four" else RefTriangle(args.scale, 1 << (args.scale + 4), SEED)
+        step, kind, sample = ref.step, ref.kind, ref.describe()
+        desc = (Clique4.describe_static(args.scale, args.algo) if args.workload == "four"
+                else Triangle.describe_static(args.scale, args.algo))
+    times, tuples = [], 0
     for i in range(args.warmup + args.steps):
-        cnt, _, sec, cores, kind, sample = wl.cpu_baseline()
+        cnt, sec = step()
         if i >= args.warmup:
             times.append(sec)
-    sec = sum(times) / len(times)
-    value = cnt / sec
-    line = {
-        "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "impl": "reference",
-        "config": {"workload": wl.describe(""), "l2": "n/a (CPU)"},
-        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample},
-        "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
+            tuples += cnt
+    sec = sum(times)
+    cpu = {"unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample}
+    print(json.dumps(reference_line(args, tuples / sec, sec / len(times) * 1e3, desc, cpu)), flush=True)
+
+
+def chain_record(args, ctx, dev, stream, steps=10, warmup=3):
+    """The 3-way chain configuration (3 x 1M rows, keys U[0,2^18)) through
+    AMHJ NORMAL: device time per query with the relations resident, the same
+    through the C ABI from pinned host buffers, and the reference's MHJ-CPU
+    on the full workload."""
+    import torch
+    wl = Chain(args, 0)
+    rels = wl.device_relations(ctx, dev)
+    for _ in range(warmup):
+        r = wl.run(ctx, rels)
+    want = (r.count, r.checksum)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    ms, probe = [], []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = wl.run(ctx, rels)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+        probe.append(r.kernel_ms[0])
+        assert (r.count, r.checksum) == want
+    pinned = [torch.from_numpy(c).pin_memory().numpy() for c in wl.host_columns()]
+    e2e = []
+    for i in range(warmup + steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hr = wl.host_relations(ctx, pinned)
+        rr = wl.run(ctx, hr)
+        for h in hr:
+            h.release()
+        if i >= warmup:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+        assert (rr.count, rr.checksum) == want
+    for h in rels:
+        h.release()
+    m, e = sum(ms) / len(ms), sum(e2e) / len(e2e)
+    hbm, _ = peaks()
+    kms = sum(probe) / len(probe)
+    alg = wl.algorithmic_bytes()
+    rec = {"workload": wl.describe(""), "value": want[0] / (m * 1e-3), "unit": "tuples/s", "ms_per_step": m,
+           "steps": steps, "output_tuples": want[0],
+           "e2e": {"value": want[0] / (e * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": wl.h2d,
+                   "d2h_bytes_per_step": 16, "ms_per_step": e},
+           "probe_kernel": {"ms": kms, "alg_bytes": alg, "frac_of_hbm": alg / (kms * 1e-3) / 1e9 / hbm}}
+    if not args.no_cpu_baseline:
+        c_cnt, c_chk, sec, cores, kind, sample = wl.cpu_baseline()
+        rec["cpu_baseline"] = {"value": c_cnt / sec, "unit": "tuples/s", "cores": cores, "kind": kind,
+                               "sample": sample, "matches_gpu": bool((c_cnt, c_chk) == want)}
+    return rec
+
+
+def other_configs(args, ctx, dev, stream, local_rank):
+    """Records of the chain (C1) and batched (C4) configurations, carried on
+    the default line beside the triangle headline."""
+    import copy
+    out = {"chain": chain_record(args, ctx, dev, stream)}
+    bargs = copy.copy(args)
+    bargs.queries, bargs.steps, bargs.warmup = 512, 5, 3
+    bl = batch_line(bargs, 0, 1, local_rank, fixed_point=TUNED_BATCH_POINT, cpu_budget=10.0)
+    out["batch"] = {k: bl[k] for k in ("value", "unit", "ms_per_step", "steps", "e2e", "batched_vs_plain",
+                                       "phase_ms", "gpu_launches", "cpu_baseline") if k in bl}
+    out["batch"]["workload"] = bl["config"]["workload"]
+    out["batch"]["opts"] = bl["config"]["opts"]
+    out["batch"]["output_tuples"] = bl["config"]["output_tuples"]
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -831,10 +1040,14 @@ def run_ours(args, rank, world, local_rank):
         line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                             "frac": achieved / hbm, "traffic": profiled_traffic(args), "peak_kind": peak_kind,
                             "kernel": wl.kernel_name(), "alg_bytes_per_launch": alg}
+    if isinstance(wl, Triangle) and world == 1 and not args.no_configs:
+        line["configs"] = other_configs(args, ctx, dev, stream, local_rank)
     if not args.no_cpu_baseline:
         c_cnt, c_chk, sec, cores, kind, sample = wl.cpu_baseline()
         line["cpu_baseline"] = {"value": c_cnt / sec, "unit": "tuples/s", "cores": cores, "kind": kind,
-                                "sample": sample, "matches_gpu": bool((c_cnt, c_chk) == (count, checksum))}
+                                "sample": sample}
+        if c_chk is not None:
+            line["cpu_baseline"]["matches_gpu"] = bool((c_cnt, c_chk) == (count, checksum))
     print(json.dumps(line), flush=True)
     ctx.close()
 
@@ -860,6 +1073,8 @@ def main():
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="batch workload: skip the autotuner")
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="triangle workload: skip the chain and batched records carried on the line")
     args = ap.parse_args()
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)
