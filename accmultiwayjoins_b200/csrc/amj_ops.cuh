@@ -73,6 +73,11 @@ int degree_ordered_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint
 // edges (rank lo, rank hi), *inv[rank] = the vertex id, *nv ranks.
 int degree_ranked_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *ns,
                        DBuf<int32_t> *nd, DBuf<int32_t> *inv, uint64_t *nv, bool *oriented);
+// The ranks alone: *rank[id] and *inv[rank] over ids 0..*nv-1 (when oriented).
+int degree_ranks(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *rank,
+                 DBuf<int32_t> *inv, uint64_t *nv, bool *oriented);
+// The level-1 entries of a degree-ranked trie grouped by b (a stable sort).
+int build_wedges(amj_ctx *ctx, const Trie2 &R, uint64_t nv, DBuf<uint64_t> *out);
 
 // copy materialised device result columns to pinned host memory (when asked)
 int finish_result_columns(amj_ctx *ctx, amj_result *res, int flags);

@@ -124,8 +124,8 @@ __global__ void rank_edges_kernel(const int32_t *__restrict__ s, const int32_t *
     }
 }
 
-int degree_ranked_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *ns,
-                       DBuf<int32_t> *nd, DBuf<int32_t> *inv, uint64_t *nv, bool *oriented) {
+int degree_ranks(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *rank,
+                 DBuf<int32_t> *inv, uint64_t *nv, bool *oriented) {
     *oriented = false;
     *nv = 0;
     if (n == 0) return AMJ_OK;
@@ -170,19 +170,27 @@ int degree_ranked_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint6
     AMJ_CUDA_TRY(cudaGetLastError());
     uint64_t *sorted = nullptr;
     AMJ_TRY(radix_sort_u64(ctx, ka.p, kb.p, V, SK_IDENT, 0, idbits + degbits, &sorted));
-    DBuf<int32_t> rank;
-    AMJ_TRY(rank.alloc(ctx, V));
+    AMJ_TRY(rank->alloc(ctx, V));
     AMJ_TRY(inv->alloc(ctx, V));
     note_launch(ctx);
-    rank_scatter_kernel<<<gv, 256, 0, ctx->stream>>>(sorted, V, idbits, rank.p, inv->p);
-    AMJ_CUDA_TRY(cudaGetLastError());
-    AMJ_TRY(ns->alloc(ctx, n));
-    AMJ_TRY(nd->alloc(ctx, n));
-    note_launch(ctx);
-    rank_edges_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, rank.p, ns->p, nd->p);
+    rank_scatter_kernel<<<gv, 256, 0, ctx->stream>>>(sorted, V, idbits, rank->p, inv->p);
     AMJ_CUDA_TRY(cudaGetLastError());
     *nv = V;
     *oriented = true;
+    return AMJ_OK;
+}
+
+int degree_ranked_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n, DBuf<int32_t> *ns,
+                       DBuf<int32_t> *nd, DBuf<int32_t> *inv, uint64_t *nv, bool *oriented) {
+    DBuf<int32_t> rank;
+    AMJ_TRY(degree_ranks(ctx, c0, c1, n, &rank, inv, nv, oriented));
+    if (!*oriented) return AMJ_OK;
+    AMJ_TRY(ns->alloc(ctx, n));
+    AMJ_TRY(nd->alloc(ctx, n));
+    const unsigned g = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 16);
+    note_launch(ctx);
+    rank_edges_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, rank.p, ns->p, nd->p);
+    AMJ_CUDA_TRY(cudaGetLastError());
     return AMJ_OK;
 }
 

@@ -72,7 +72,24 @@ struct TriArgs {
     unsigned long long *cursor_r; // claim cursor of the wedge kernel
     int bfs_wedge;                // BFS over one degree-ordered relation (R = S = T): the
                                   // candidates of entry (a, b) are T(a)'s values after b
+    const struct RankId *hid;     // wedge kernel: id and first hash step of every rank
 };
+
+// The vertex id of a rank and the first step of the tuple hash over it,
+// amj_hash_step(AMJ_CHECKSUM_SEED, id): one 16-byte load gives a hit's id
+// and, when that id is the triangle's smallest, its hash prefix.
+struct __align__(16) RankId {
+    int32_t id;
+    uint32_t pad;
+    uint64_t h1;
+};
+
+__global__ void rank_ids_kernel(const int32_t *__restrict__ inv, uint64_t nv, RankId *__restrict__ hid) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nv; i += (uint64_t)gridDim.x * blockDim.x) {
+        const int32_t id = inv[i];
+        hid[i] = RankId{id, 0u, amj_hash_step(AMJ_CHECKSUM_SEED, id)};
+    }
+}
 
 // A triangle found as (a, b, c) in the tuple the query lists: attribute order,
 // or increasing order for a degree-ordered copy of an oriented relation
@@ -322,21 +339,56 @@ __global__ __launch_bounds__(BM_THREADS, 1) void lftj_tri_bitmap_kernel(const __
 // through the warp in aligned 16-byte quads.  Hits go to a per-warp queue
 // of (c, edge) pairs; the id mapping, the checksum and the writes run on 32
 // queued triangles at a time, so lanes without a hit do not wait on them.
+// Per edge the lane keeps the ids of a and b in increasing order (lo, hi)
+// and the hash prefix of lo; per hit one 16-byte load gives c's id and its
+// own prefix, so a triangle costs two hash steps: the tuple is (min(c, lo),
+// median, max(c, hi)) and its first step is the prefix of c or of lo.
+// The queue packs a hit into 32 bits (rank << 5 | lane) when every rank is
+// below 2^27; wider ranks take 64-bit entries.  Three blocks run per SM: the
+// kernel is bound by the integer (ALU) pipe, and a fourth block, which needs
+// at most 64 registers a thread, made it slower (3.85 against 3.63 ms at
+// R-MAT scale 20).
 constexpr int TR_THREADS = 256;
 constexpr int TR_WARPS = TR_THREADS / 32;
 constexpr uint32_t TR_BITS = 32768;            // bitmap ranks per warp (the most)
-constexpr int TR_LOWCAP = 256;                 // low prefix entries kept in shared memory
+constexpr int TR_LOWCAP = 192;                 // low prefix entries kept in shared memory
 constexpr int TR_UNROLL = 4;                   // quads per lane per step
 constexpr int TR_QCAP = 512;                   // queued hits per warp (ring)
+constexpr uint64_t TR_NARROW_RANKS = 1ull << 27;
 
+template <bool WIDE>
 struct TrWarp {
     uint32_t bm[TR_BITS / 32];
     int32_t low[TR_LOWCAP];
-    int2 q[TR_QCAP];   // (c, lane of the edge)
+    uint32_t q[TR_QCAP * (WIDE ? 2 : 1)];   // narrow: rank << 5 | lane; wide: (rank, lane) pairs
 };
-constexpr size_t TR_SMEM = TR_WARPS * sizeof(TrWarp);
-static_assert(sizeof(TrWarp) % 16 == 0, "TrWarp keeps 16-byte alignment");
+template <bool WIDE>
+constexpr size_t tr_smem() { return TR_WARPS * sizeof(TrWarp<WIDE>); }
+static_assert(sizeof(TrWarp<false>) % 16 == 0 && sizeof(TrWarp<true>) % 16 == 0, "TrWarp keeps 16-byte alignment");
 static_assert(TR_QCAP >= 32 * 4 * TR_UNROLL, "the queue takes one step's hits");
+
+template <bool WIDE>
+__device__ __forceinline__ void tr_qput(TrWarp<WIDE> &W, uint32_t pos, int32_t c, int lane) {
+    pos &= TR_QCAP - 1;
+    if (WIDE) {
+        W.q[2 * pos] = (uint32_t)c;
+        W.q[2 * pos + 1] = (uint32_t)lane;
+    } else {
+        W.q[pos] = ((uint32_t)c << 5) | (uint32_t)lane;
+    }
+}
+template <bool WIDE>
+__device__ __forceinline__ void tr_qget(const TrWarp<WIDE> &W, uint32_t pos, int32_t &c, int &lane) {
+    pos &= TR_QCAP - 1;
+    if (WIDE) {
+        c = (int32_t)W.q[2 * pos];
+        lane = (int)W.q[2 * pos + 1];
+    } else {
+        const uint32_t e = W.q[pos];
+        c = (int32_t)(e >> 5);
+        lane = (int)(e & 31u);
+    }
+}
 
 __device__ __forceinline__ bool tr_sorted_find(const int32_t *v, uint64_t n, int32_t c) {
     uint64_t lo = 0, hi = n;
@@ -358,13 +410,13 @@ __device__ __forceinline__ uint32_t tr_bit(const uint32_t *bm, int32_t c, uint32
 // MODE 0: count and checksum; 1: also write the tuples; 2 (matrix mode):
 // record every triangle (a, x, y) as bit y - ta of row x - ta of a's matrix
 // (ta = the start of T(a) in level 1; rows have ceil(d+(a) / 32) words).
-template <int MODE>
+template <int MODE, bool WIDE>
 __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __grid_constant__ TriArgs A) {
     constexpr bool WRITE = MODE == 1;
     constexpr bool MATRIX = MODE == 2;
     extern __shared__ __align__(16) unsigned char tr_smem[];
     const int lane = threadIdx.x & 31;
-    TrWarp &W = ((TrWarp *)tr_smem)[threadIdx.x >> 5];
+    TrWarp<WIDE> &W = ((TrWarp<WIDE> *)tr_smem)[threadIdx.x >> 5];
     const uint32_t base = A.rank_base, nbits = A.rank_bits;
     const int32_t *d1 = A.T.data1;
     const int4 *dq = reinterpret_cast<const int4 *>(d1);
@@ -372,27 +424,41 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
     __syncwarp();
     unsigned long long cnt = 0, chk = 0;
     uint32_t qh = 0, qn = 0;   // queue head and length
-    int32_t ida = 0, idb = 0;  // vertex ids of this lane's edge (a, b)
+    int32_t elo = 0, ehi = 0;  // ids of this lane's edge (a, b) in increasing order
+    uint64_t eh = 0;           // hash prefix of elo
     uint64_t rowbase = 0;      // matrix mode: first word of this edge's row
     uint32_t ta32 = 0;         // matrix mode: start of T(a) in level 1
-    // the first n queued hits, one per lane
+    // the first n queued hits, one per lane: the triangle (c, lo, hi) in
+    // increasing id order (x, y, z), hashed from the prefix of x
     auto flush = [&](uint32_t n) {
         __syncwarp();
         const bool mine = (uint32_t)lane < n;
-        const int2 e = mine ? W.q[(qh + lane) & (TR_QCAP - 1)] : make_int2(0, 0);
-        const int32_t a = __shfl_sync(AMJ_FULL_MASK, ida, e.y);
-        const int32_t b = __shfl_sync(AMJ_FULL_MASK, idb, e.y);
+        int32_t c = 0;
+        int src = 0;
+        if (mine) tr_qget<WIDE>(W, qh + lane, c, src);
+        const int32_t lo = __shfl_sync(AMJ_FULL_MASK, elo, src);
+        const int32_t hi = __shfl_sync(AMJ_FULL_MASK, ehi, src);
+        const uint64_t hlo = __shfl_sync(AMJ_FULL_MASK, eh, src);
         __syncwarp();
-        const int32_t c = mine ? A.inv[e.x] : 0;
-        if (WRITE) {
-            unsigned long long at = 0;
-            if (lane == 0) at = atomicAdd(A.out_cursor, (unsigned long long)n);
-            at = __shfl_sync(AMJ_FULL_MASK, at, 0);
-            if (mine && at + lane < A.out_cap) tri_store(A, at + lane, a, b, c);
-        }
         if (mine) {
+            const RankId r = A.hid[c];
+            const bool first = r.id < lo;
+            const int32_t x = first ? r.id : lo;
+            const int32_t y = first ? lo : min(r.id, hi);
+            const int32_t z = max(r.id, hi);
             cnt++;
-            chk += tri_chk3(A, a, b, c);
+            chk += amj_hash_step(amj_hash_step(first ? r.h1 : hlo, y), z);
+            if (WRITE) {
+                const unsigned m = __activemask();
+                unsigned long long at = 0;
+                if (lane == 0) at = atomicAdd(A.out_cursor, (unsigned long long)n);
+                at = __shfl_sync(m, at, 0);
+                if (at + lane < A.out_cap) {
+                    A.out[0][at + lane] = x;
+                    A.out[1][at + lane] = y;
+                    A.out[2][at + lane] = z;
+                }
+            }
         }
         qh = (qh + n) & (TR_QCAP - 1);
         qn -= n;
@@ -466,8 +532,11 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
                 rowbase = A.moff[a] + ((uint64_t)idx - ta) * ((te - ta + 31) / 32);
                 ta32 = (uint32_t)ta;
             } else {
-                ida = A.inv[a];
-                idb = A.inv[b];
+                const RankId ra = A.hid[a], rb = A.hid[b];
+                const bool alo = ra.id < rb.id;
+                elo = alo ? ra.id : rb.id;
+                ehi = alo ? rb.id : ra.id;
+                eh = alo ? ra.h1 : rb.h1;
             }
         }
         // tl: first value of the suffix in the bitmap's ranks (the values
@@ -530,7 +599,7 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
                         continue;
                     }
                     const unsigned m = __ballot_sync(AMJ_FULL_MASK, hit);
-                    if (hit) W.q[(qh + qn + __popc(m & lanemask_lt())) & (TR_QCAP - 1)] = make_int2(c, l);
+                    if (hit) tr_qput<WIDE>(W, qh + qn + __popc(m & lanemask_lt()), c, l);
                     qn += __popc(m);
                     while (qn >= 32) flush(32);
                 }
@@ -612,10 +681,10 @@ __global__ __launch_bounds__(TR_THREADS, 3) void lftj_tri_wedge_kernel(const __g
                     uint32_t pos = qh + qn + hincl - nh;
 #pragma unroll
                     for (int u = 0; u < TR_UNROLL; u++) {
-                        if ((bits >> (4 * u)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].x, own[u]);
-                        if ((bits >> (4 * u + 1)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].y, own[u]);
-                        if ((bits >> (4 * u + 2)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].z, own[u]);
-                        if ((bits >> (4 * u + 3)) & 1u) W.q[pos++ & (TR_QCAP - 1)] = make_int2(cv[u].w, own[u]);
+                        if ((bits >> (4 * u)) & 1u) tr_qput<WIDE>(W, pos++, cv[u].x, own[u]);
+                        if ((bits >> (4 * u + 1)) & 1u) tr_qput<WIDE>(W, pos++, cv[u].y, own[u]);
+                        if ((bits >> (4 * u + 2)) & 1u) tr_qput<WIDE>(W, pos++, cv[u].z, own[u]);
+                        if ((bits >> (4 * u + 3)) & 1u) tr_qput<WIDE>(W, pos++, cv[u].w, own[u]);
                     }
                     qn += tot;
                     while (qn >= 32) flush(32);
@@ -702,13 +771,14 @@ int lftj_tri_matrices(amj_ctx *ctx, const Trie2 &R, const uint64_t *wedge, uint6
     if (nv < bits) bits = (uint32_t)((nv + 31) / 32 * 32);
     A.rank_bits = bits;
     A.rank_base = (uint32_t)(nv > bits ? nv - bits : 0);
-    auto kr = lftj_tri_wedge_kernel<2>;
-    AMJ_CUDA_TRY(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM));
+    auto kr = lftj_tri_wedge_kernel<2, false>;
+    constexpr size_t smem = tr_smem<false>();
+    AMJ_CUDA_TRY(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, TR_THREADS, TR_SMEM));
+    AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, TR_THREADS, smem));
     if (per_sm < 1) per_sm = 1;
     note_launch(ctx);
-    kr<<<(unsigned)(ctx->num_sms * per_sm), TR_THREADS, TR_SMEM, ctx->stream>>>(A);
+    kr<<<(unsigned)(ctx->num_sms * per_sm), TR_THREADS, smem, ctx->stream>>>(A);
     AMJ_CUDA_TRY(cudaGetLastError());
     return AMJ_OK;
 }
@@ -997,6 +1067,7 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
     A.out_cursor = &ctr.p->out_cursor;
     A.cursor0 = &ctr.p->cursor0;
     DBuf<uint32_t> heavy;
+    DBuf<RankId> hid;
     A.cursor_r = &ctr.p->cursor_r;
     const bool write = out != nullptr;
     if (write) {
@@ -1020,13 +1091,22 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
                 A.src1 = R.src1.p;
                 A.rank_bits = bits;
                 A.rank_base = (uint32_t)(nv > bits ? nv - bits : 0);
-                auto kr = write ? lftj_tri_wedge_kernel<1> : lftj_tri_wedge_kernel<0>;
-                AMJ_CUDA_TRY(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM));
+                AMJ_TRY(hid.alloc(ctx, nv));
+                note_launch(ctx);
+                rank_ids_kernel<<<(unsigned)std::min<uint64_t>((nv + 255) / 256, (uint64_t)ctx->num_sms * 16), 256,
+                                  0, ctx->stream>>>(inv, nv, hid.p);
+                AMJ_CUDA_TRY(cudaGetLastError());
+                A.hid = hid.p;
+                const bool wide = nv > TR_NARROW_RANKS;
+                auto kr = wide ? (write ? lftj_tri_wedge_kernel<1, true> : lftj_tri_wedge_kernel<0, true>)
+                               : (write ? lftj_tri_wedge_kernel<1, false> : lftj_tri_wedge_kernel<0, false>);
+                const size_t smem = wide ? tr_smem<true>() : tr_smem<false>();
+                AMJ_CUDA_TRY(cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 int per_sm = 0;
-                AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, TR_THREADS, TR_SMEM));
+                AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, TR_THREADS, smem));
                 if (per_sm < 1) per_sm = 1;
                 note_launch(ctx);
-                kr<<<(unsigned)(ctx->num_sms * per_sm), TR_THREADS, TR_SMEM, ctx->stream>>>(A);
+                kr<<<(unsigned)(ctx->num_sms * per_sm), TR_THREADS, smem, ctx->stream>>>(A);
                 AMJ_CUDA_TRY(cudaGetLastError());
                 timed[0] = true;
             }

@@ -53,8 +53,10 @@ static int build_self_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, int *sorted
 }
 
 // Trie of the degree-ranked copy (*inv maps ranks to vertex ids) when the
-// relation is oriented; otherwise the trie of the relation itself, *nv = 0.
-static int build_ranked_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, DBuf<int32_t> *inv, uint64_t *nv) {
+// relation is oriented, with its level-1 entries grouped by value when
+// wedges is given; otherwise the trie of the relation itself, *nv = 0.
+static int build_ranked_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, DBuf<int32_t> *inv, uint64_t *nv,
+                             DBuf<uint64_t> *wedges) {
     *nv = 0;
     if (r->ncols != 2) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must have two columns");
     if (r->where == AMJ_MEM_HOST_STREAMED) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must be on the device");
@@ -64,7 +66,9 @@ static int build_ranked_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, DBuf<int3
     bool oriented = false;
     AMJ_TRY(degree_ranked_copy(ctx, c0, c1, r->n, &ns, &nd, inv, nv, &oriented));
     if (!oriented) return build_trie2(ctx, c0, c1, r->n, t, true);
-    return build_trie2(ctx, ns.p, nd.p, r->n, t, true, (int32_t)(*nv - 1));
+    AMJ_TRY(build_trie2(ctx, ns.p, nd.p, r->n, t, true, (int32_t)(*nv - 1)));
+    if (wedges) AMJ_TRY(build_wedges(ctx, *t, *nv, wedges));
+    return AMJ_OK;
 }
 }
 
@@ -99,10 +103,9 @@ static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         ~MatGuard() { lftj_clique4_matrix_release(m); }
     } mat;
     if ((flags & AMJ_F_KEEP_ORDER) == 0) {
-        AMJ_TRY(build_ranked_trie(ctx, rels[0], &t, &inv, &nv));
+        DBuf<uint64_t> wedges;
+        AMJ_TRY(build_ranked_trie(ctx, rels[0], &t, &inv, &nv, &wedges));
         if (nv) {
-            DBuf<uint64_t> wedges;
-            AMJ_TRY(build_wedges(ctx, t, nv, &wedges));
             AMJ_TRY(lftj_clique4_matrix_prepare(ctx, t, inv.p, wedges.p, nv, ctx->opts.lftj_rank_bits, &mat.m));
             if (!mat.m) {
                 t = Trie2();
@@ -203,9 +206,9 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         if (flags & AMJ_F_KEEP_ORDER) deg_order = false;
         if (deg_order && (algo == AMJ_LFTJ_BFS || ws)) {
             // the degree-ranked copy: the wedge kernel (DFS) or wedge candidates (BFS)
-            AMJ_TRY(build_ranked_trie(ctx, rels[0], &tries[0], &inv, &nv));
+            AMJ_TRY(build_ranked_trie(ctx, rels[0], &tries[0], &inv, &nv,
+                                      algo == AMJ_LFTJ_DFS ? &wedges : nullptr));
             sorted_out = nv ? 1 : 0;
-            if (nv && algo == AMJ_LFTJ_DFS) AMJ_TRY(build_wedges(ctx, tries[0], nv, &wedges));
         } else {
             AMJ_TRY(build_self_trie(ctx, rels[0], &tries[0], &sorted_out, deg_order));
         }
