@@ -230,6 +230,9 @@ SIGNATURES = {
     "amj_db_read": (C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.POINTER(_I32P)]),
     "amj_db_parse_name": (C.c_int, [C.c_char_p, _U64P, C.POINTER(C.c_int), _U32P]),
     "amj_checksum_host": (C.c_int, [C.POINTER(_I32P), C.c_int, C.c_uint64, _U64P]),
+    "amj_edgelist_read": (C.c_int, [C.c_char_p, C.c_int, _I32P, _I32P, C.c_uint64, _U64P]),
+    "amj_edgelist_to_db": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, _U64P]),
+    "amj_edgelist_to_tr": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_int, _U64P]),
 }
 
 _lib = None

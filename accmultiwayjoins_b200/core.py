@@ -388,6 +388,14 @@ class Context:
                                      C.byref(res)), "lftj_execute")
         return self._result(res, materialize)
 
+    def edgelist_to_tr(self, text_path: str, tr_path: str, swap: bool = False) -> int:
+        """Convert a text edge list to a .tr trie file (built on this
+        context's device); returns the number of edges."""
+        rows = C.c_uint64()
+        L.check(L.load().amj_edgelist_to_tr(self.handle, text_path.encode(), tr_path.encode(), int(swap),
+                                            C.byref(rows)), "edgelist_to_tr")
+        return int(rows.value)
+
     def batch(self) -> Batch:
         b = Batch(self)
         self._batches.add(b)

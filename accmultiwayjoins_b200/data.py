@@ -220,6 +220,32 @@ def read_db(path: str):
     return cols, [int(attrs[i]) for i in range(nc.value)]
 
 
+def read_edgelist(path: str, swap: bool = False):
+    """The edges of a text edge list as (src, dst) int32 arrays
+    (amj_edgelist_read: two integers a line separated by ' ', '|' or tab;
+    '#' / '%' comment lines skipped)."""
+    lib = L.load()
+    n = C.c_uint64()
+    L.check(lib.amj_edgelist_read(path.encode(), int(swap), None, None, 0, C.byref(n)), "edgelist_read")
+    src = np.empty(n.value, np.int32)
+    dst = np.empty(n.value, np.int32)
+    if n.value:
+        L.check(lib.amj_edgelist_read(path.encode(), int(swap), _i32p(src), _i32p(dst), n.value, C.byref(n)),
+                "edgelist_read")
+    return src, dst
+
+
+def edgelist_to_db(text_path: str, db_path: str = None, swap: bool = False) -> int:
+    """Convert a text edge list to a 2-column .db file (default name: the
+    edge list's path + ".db", as the reference's converter names it);
+    returns the number of edges."""
+    rows = C.c_uint64()
+    db_path = db_path or text_path + ".db"
+    L.check(L.load().amj_edgelist_to_db(text_path.encode(), db_path.encode(), int(swap), C.byref(rows)),
+            "edgelist_to_db")
+    return int(rows.value)
+
+
 def checksum(cols) -> int:
     """Checksum of column-major tuples (the definition in include/amj_checksum.h)."""
     cols = [np.ascontiguousarray(c, dtype=np.int32) for c in cols]

@@ -377,6 +377,26 @@ int  amj_db_write(const char *path, uint64_t n, int ncols, const int32_t *const 
 int  amj_db_read(const char *path, uint64_t n, int ncols, int32_t *const *cols);
 int  amj_db_parse_name(const char *path, uint64_t *n, int *ncols, uint32_t *attrs);
 
+/* ---- edge-list text converters ----
+ * An edge list is a text file of one edge per line: two integers separated by
+ * any run of ' ', '|' or tab; each value is stored as int32 modulo 2^32 (the
+ * reference's stoul-then-int).  Blank lines and lines starting with '#' or '%'
+ * are skipped; any other line must hold exactly two integers (AMJ_EINVAL
+ * names the first that does not).  swap != 0 reverses the two columns
+ * (MHJ-GPU/switch_el.py).
+ * amj_edgelist_read: the edges into src/dst (cap rows available; cap = 0 only
+ *   sets *n, the number of edges).
+ * amj_edgelist_to_db: the edges as a 2-column .db file (column-major int32),
+ *   replacing edgelist_2_db (MHJ-GPU/exec_el_2_db.cu:20-87), which writes
+ *   "<edgelist>.db".
+ * amj_edgelist_to_tr: the 2-level trie of the edges (amj_trie_build, level 1
+ *   keeps repeated rows) saved as a .tr file with attributes (0, 1), replacing
+ *   edgelist_to_csr (LFTJ-GPU/edgelist_to_csr.cu:19-86), which writes
+ *   "output.tr". */
+int  amj_edgelist_read(const char *path, int swap, int32_t *src, int32_t *dst, uint64_t cap, uint64_t *n);
+int  amj_edgelist_to_db(const char *text_path, const char *db_path, int swap, uint64_t *rows);
+int  amj_edgelist_to_tr(amj_ctx *ctx, const char *text_path, const char *tr_path, int swap, uint64_t *rows);
+
 /* ---- host checksum of column-major tuples (same definition as the GPU) ---- */
 int  amj_checksum_host(const int32_t *const *cols, int k, uint64_t n, uint64_t *out);
 

@@ -101,6 +101,38 @@ def test_trie_tr_file_round_trip(ctx, tmp_path):
     lib.amj_trie_release(h2)
 
 
+def test_edgelist_to_tr_equals_trie_of_the_edges(ctx, tmp_path):
+    """amj_edgelist_to_tr (the reference's edgelist_to_csr,
+    LFTJ-GPU/edgelist_to_csr.cu) writes the .tr file of the trie the
+    oracle builds from the same edges; repeated rows stay in level 1."""
+    s, d = data.rmat(11, 20000, 0.57, 0.19, 0.19, 5)
+    s = np.concatenate([s, s[:100]])
+    d = np.concatenate([d, d[:100]])
+    txt = tmp_path / "g.txt"
+    with open(txt, "w") as f:
+        f.write("# comment\n")
+        for u, v in zip(s, d):
+            f.write(f"{u}\t{v}\n")
+    out = tmp_path / "g.tr"
+    assert ctx.edgelist_to_tr(str(txt), str(out)) == len(s)
+    d0, o0, d1 = O.trie_build(s, d)
+    raw = open(out, "rb").read()
+    na = np.frombuffer(raw[:4], np.uint32)[0]
+    lens = np.frombuffer(raw[4:20], np.uint64)
+    assert na == 2 and lens.tolist() == [len(d0), len(d1)]
+    body = raw[28:]
+    f0 = np.frombuffer(body[:4 * len(d0)], np.int32)
+    f1 = np.frombuffer(body[4 * len(d0):4 * (len(d0) + len(d1))], np.int32)
+    fo = np.frombuffer(body[4 * (len(d0) + len(d1)):], np.uint64)
+    assert np.array_equal(f0, d0) and np.array_equal(f1, d1) and np.array_equal(fo, o0)
+    # the swapped list is the reverse relation
+    out2 = tmp_path / "r.tr"
+    ctx.edgelist_to_tr(str(txt), str(out2), swap=True)
+    r0, _, r1 = O.trie_build(d, s)
+    raw2 = open(out2, "rb").read()[28:]
+    assert np.array_equal(np.frombuffer(raw2[:4 * len(r0)], np.int32), r0)
+
+
 def trie_n_levels(h):
     lib = L.load()
     lv = C.c_int()
