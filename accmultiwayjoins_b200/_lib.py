@@ -194,6 +194,8 @@ SIGNATURES = {
                                    C.c_int, C.POINTER(amj_result)]),
     "amj_lftj_execute": (C.c_int, [_P, C.POINTER(_P), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.POINTER(amj_result)]),
+    "amj_lftj_execute_ordered": (C.c_int, [_P, C.POINTER(_P), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _U32P,
+                                           C.c_int, C.POINTER(amj_result)]),
     "amj_result_release": (None, [C.POINTER(amj_result)]),
     "amj_batch_create": (C.c_int, [_P, C.POINTER(_P)]),
     "amj_batch_submit": (C.c_int, [_P, C.c_int, C.POINTER(_P), C.c_int, C.c_int, _U32P]),

@@ -370,10 +370,12 @@ class Context:
         return self._result(res, materialize)
 
     def lftj(self, relations: Sequence[Relation], algo="DFS", ooc: int = 0, ws: int = 1,
-             materialize: bool = False, clique4: bool = False, degree_order=None) -> Result:
+             materialize: bool = False, clique4: bool = False, degree_order=None, attr_order=None) -> Result:
         """clique4: one edge relation joined as the 4-clique (FOUR pattern) instead of the triangle.
         degree_order: None for the operator's choice, True / False to force joining (or not) the
-        degree-ordered copy of an oriented self-joined relation (same results either way)."""
+        degree-ordered copy of an oriented self-joined relation (same results either way).
+        attr_order: the order in which attributes are bound (a permutation of 0..k-1; the
+        results are the same for every order)."""
         lib = L.load()
         arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
         flags = (L.AMJ_F_MATERIALIZE | L.AMJ_F_HOST_RESULT) if materialize else 0
@@ -384,8 +386,13 @@ class Context:
         elif degree_order is False:
             flags |= L.AMJ_F_KEEP_ORDER
         res = L.amj_result()
-        L.check(lib.amj_lftj_execute(self.handle, arr, len(relations), _ALGO[algo], int(ooc), int(ws), flags,
-                                     C.byref(res)), "lftj_execute")
+        if attr_order is None:
+            L.check(lib.amj_lftj_execute(self.handle, arr, len(relations), _ALGO[algo], int(ooc), int(ws), flags,
+                                         C.byref(res)), "lftj_execute")
+        else:
+            order = (C.c_uint32 * len(attr_order))(*[int(a) for a in attr_order])
+            L.check(lib.amj_lftj_execute_ordered(self.handle, arr, len(relations), _ALGO[algo], int(ooc), int(ws),
+                                                 flags, order, len(attr_order), C.byref(res)), "lftj_execute_ordered")
         return self._result(res, materialize)
 
     def edgelist_to_tr(self, text_path: str, tr_path: str, swap: bool = False) -> int:

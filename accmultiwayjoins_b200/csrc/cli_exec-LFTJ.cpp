@@ -1,5 +1,7 @@
-// exec-LFTJ <path> <algo 0=BFS|1=DFS> <ooc> <ws> [--materialize]
-// Same positional switches as the reference driver (LFTJ-GPU/exec_LFTJ.cu:256-268).
+// exec-LFTJ <path> <algo 0=BFS|1=DFS> <ooc> <ws> [--materialize] [--attr-order a,b,c]
+// Same positional switches as the reference driver (LFTJ-GPU/exec_LFTJ.cu:256-268);
+// --attr-order sets the binding order the reference's driver fixes to the
+// identity (exec_LFTJ.cu:230-231).
 // <path> is a directory: one .db file is the triangle self-join, three .db
 // files a 3-relation join, two files are an error (exec_LFTJ.cu:92-95).
 #include <cstring>
@@ -7,14 +9,25 @@
 
 int main(int argc, char **argv) {
     if (argc < 5) {
-        std::fprintf(stderr, "usage: %s <dir> <0=BFS|1=DFS> <ooc> <ws> [--materialize]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s <dir> <0=BFS|1=DFS> <ooc> <ws> [--materialize] [--attr-order a,b,..]\n",
+                     argv[0]);
         return 2;
     }
     std::string path = argv[1];
     const int algo = std::atoi(argv[2]), ooc = std::atoi(argv[3]), ws = std::atoi(argv[4]);
     int flags = 0;
-    for (int i = 5; i < argc; i++)
+    std::vector<uint32_t> order;
+    for (int i = 5; i < argc; i++) {
         if (std::strcmp(argv[i], "--materialize") == 0) flags |= AMJ_F_MATERIALIZE;
+        else if (std::strcmp(argv[i], "--attr-order") == 0 && i + 1 < argc) {
+            for (const char *p = argv[++i]; *p;) {
+                char *end = nullptr;
+                order.push_back((uint32_t)std::strtoul(p, &end, 10));
+                if (end == p) return cli::die(AMJ_EINVAL, "--attr-order: expected a,b,c");
+                p = *end == ',' ? end + 1 : end;
+            }
+        }
+    }
     amj_ctx *ctx = nullptr;
     int rc = amj_ctx_create(0, nullptr, &ctx);
     if (rc) return cli::die(rc, "context");
@@ -30,7 +43,9 @@ int main(int argc, char **argv) {
         if (rc) return cli::die(rc, files[i].c_str());
     }
     amj_result res;
-    rc = amj_lftj_execute(ctx, rels.data(), (int)rels.size(), algo, ooc, ws, flags, &res);
+    rc = order.empty() ? amj_lftj_execute(ctx, rels.data(), (int)rels.size(), algo, ooc, ws, flags, &res)
+                       : amj_lftj_execute_ordered(ctx, rels.data(), (int)rels.size(), algo, ooc, ws, flags, order.data(),
+                                                  (int)order.size(), &res);
     if (rc) return cli::die(rc, "lftj_execute");
     cli::print_result(algo == AMJ_LFTJ_DFS ? "ALFTJ-DFS" : "ALFTJ-BFS", res);
     amj_result_release(&res);

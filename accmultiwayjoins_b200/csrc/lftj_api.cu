@@ -33,7 +33,8 @@ int lftj_triangle(amj_ctx *ctx, const Trie2 &R, const Trie2 &S, const Trie2 &T, 
 int build_wedges(amj_ctx *ctx, const Trie2 &R, uint64_t nv, DBuf<uint64_t> *out);
 
 // the generic join (lftj_generic.cu)
-int lftj_generic_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int ooc, int flags, amj_result *out);
+int lftj_generic_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int ooc, int flags, const uint32_t *order,
+                         amj_result *out);
 
 // Trie of the self-joined edge relation: the degree-ordered copy when the
 // relation is oriented and `allow` (*sorted = 1), else the relation itself.
@@ -160,8 +161,54 @@ static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     return AMJ_OK;
 }
 
+// The self-joined edge relation as the relations of the triangle (TRI
+// pattern) or 4-clique (FOUR pattern), for the generic join in a given
+// attribute order: views of the same device columns, none owning them.
+static int self_join_views(const amj_rel *r, bool clique4, amj_rel *views, amj_rel **ptrs, int *n) {
+    if (r->ncols != 2) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must have two columns");
+    static const uint32_t tri[3][2] = {{0, 1}, {1, 2}, {0, 2}};
+    static const uint32_t four[6][2] = {{0, 1}, {1, 2}, {2, 3}, {0, 3}, {0, 2}, {1, 3}};
+    const bool swap = r->attrs[0] > r->attrs[1];
+    *n = clique4 ? 6 : 3;
+    for (int i = 0; i < *n; i++) {
+        views[i] = amj_rel();
+        views[i].ctx = r->ctx;
+        views[i].n = r->n;
+        views[i].ncols = 2;
+        views[i].where = r->where;
+        views[i].owned = false;
+        views[i].d_cols[0] = r->d_cols[swap ? 1 : 0];
+        views[i].d_cols[1] = r->d_cols[swap ? 0 : 1];
+        views[i].attrs[0] = clique4 ? four[i][0] : tri[i][0];
+        views[i].attrs[1] = clique4 ? four[i][1] : tri[i][1];
+        ptrs[i] = &views[i];
+    }
+    return AMJ_OK;
+}
+
+static bool identity_order(const uint32_t *order, int k) {
+    if (!order) return true;
+    for (int i = 0; i < k; i++)
+        if (order[i] != (uint32_t)i) return false;
+    return true;
+}
+
+static int lftj_execute_impl(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int ws, int flags,
+                             const uint32_t *order, int norder, amj_result *out);
+
 extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int ws, int flags,
                                 amj_result *out) {
+    return lftj_execute_impl(ctx, rels, nrels, algo, ooc, ws, flags, nullptr, 0, out);
+}
+
+extern "C" int amj_lftj_execute_ordered(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int ws,
+                                        int flags, const uint32_t *attr_order, int k, amj_result *out) {
+    if (attr_order && (k <= 0 || k > AMJ_MAX_ATTRS)) return fail(AMJ_EINVAL, "lftj_execute: bad attribute order length");
+    return lftj_execute_impl(ctx, rels, nrels, algo, ooc, ws, flags, attr_order, attr_order ? k : 0, out);
+}
+
+static int lftj_execute_impl(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int ws, int flags,
+                             const uint32_t *order, int norder, amj_result *out) {
     if (!ctx || !out || !rels || nrels <= 0) return fail(AMJ_EINVAL, "lftj_execute: bad arguments");
     if (algo != AMJ_LFTJ_BFS && algo != AMJ_LFTJ_DFS) return fail(AMJ_EINVAL, "lftj_execute: algo must be 0 (BFS) or 1 (DFS)");
     if (nrels == 2) return fail(AMJ_EINVAL, "lftj_execute: wrong number of datasets: 2");
@@ -169,6 +216,20 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         if (!rels[i]) return fail(AMJ_EINVAL, "lftj_execute: null relation");
     if (nrels > 16) return fail(AMJ_EUNSUPPORTED, "lftj_execute: at most 16 relations");
     AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (!identity_order(order, norder)) {
+        // a binding order other than the identity: the generic join, which
+        // reports every tuple in attribute-id order
+        if (ooc) return fail(AMJ_EUNSUPPORTED, "LFTJ: no out-of-core form with an attribute order");
+        if (nrels == 1) {
+            amj_rel views[6];
+            amj_rel *ptrs[6];
+            int nv = 0;
+            AMJ_TRY(self_join_views(rels[0], (flags & AMJ_F_CLIQUE4) != 0, views, ptrs, &nv));
+            return lftj_generic_execute(ctx, ptrs, nv, ooc, flags, order, out);
+        }
+        if (flags & AMJ_F_CLIQUE4) return fail(AMJ_EUNSUPPORTED, "LFTJ 4-clique: one edge relation");
+        return lftj_generic_execute(ctx, rels, nrels, ooc, flags, order, out);
+    }
     if (flags & AMJ_F_CLIQUE4) return lftj_clique4_execute(ctx, rels, nrels, algo, ooc, flags, out);
     if (nrels >= 3) {
         // the triangle pattern (0,1), (1,2), (0,2) keeps its own kernels; any
@@ -186,7 +247,7 @@ extern "C" int amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
             if (!bit || (pairs & bit)) tri = false;
             pairs |= bit;
         }
-        if (!tri) return lftj_generic_execute(ctx, rels, nrels, ooc, flags, out);
+        if (!tri) return lftj_generic_execute(ctx, rels, nrels, ooc, flags, nullptr, out);
     }
     result_init(out, 3);
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];

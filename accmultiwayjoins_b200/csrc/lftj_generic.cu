@@ -1,21 +1,32 @@
-// ALFTJ for any connected query over 2-column relations, up to AMJ_MAX_ATTRS
-// attributes in identity order (the reference's attribute order,
-// LFTJ-GPU/exec_LFTJ.cu:231; its LFTJ stops at 3 attributes and 3 tables,
-// LFTJ-GPU/config.h:16-17).
+// ALFTJ for any connected query, up to AMJ_MAX_ATTRS attributes, in any
+// attribute order.  The reference's LFTJ stops at 3 attributes and 3 tables
+// (LFTJ-GPU/config.h:16-17), takes 2-column relations, and binds attributes
+// in the order attr_order (LFTJ-GPU/ALFTJ.cuh:1125-1196), which its driver
+// always sets to the identity (LFTJ-GPU/exec_LFTJ.cu:230-231).
 //
-// Every relation R(x, y), x < y, becomes a trie keyed on x.  Attribute 0
-// ranges over the intersection of the level-0 arrays of the relations keyed
-// on it; attribute l >= 1 over the intersection of the child lists
-// R(v_x) of the relations closing it (those with y = l).  The join is
-// level-synchronous (the leapfrog of LFTJ_BFS, LFTJ-GPU/LFTJ_BFS.cuh:143-500,
-// generalised): per level one count kernel takes, for every partial tuple,
-// its shortest list; the candidates of all tuples form one space, which is
-// cut into pieces of bounded size; per piece an expand kernel tests each
-// candidate against the tuple's other lists (binary search) and either
-// counts and hashes finished tuples (last attribute) or keeps survivors,
-// which a scan compacts into the next level's tuples.  Memory stays bounded
-// by the piece size whatever the intermediate results.
-// Lists are strictly increasing (relations without duplicate tuples).
+// The attributes are renamed to their positions in the order.  Every
+// relation becomes a trie whose levels follow its attributes in that order
+// (2 columns: build_trie2, with dense row pointers; 3 or more: build_trieN).
+// An attribute at level d of a relation's trie is constrained by the list of
+// values under the path of the relation's earlier attributes: level 0 is the
+// whole level-0 array; deeper lists are found by descending from the root,
+// one binary search per level (a dense row-pointer load at level 1).  The
+// first attribute ranges over the intersection of the level-0 arrays keyed
+// on it; every later one over the intersection of its lists of depth >= 1.
+// The join is level-synchronous (the leapfrog of LFTJ_BFS,
+// LFTJ-GPU/LFTJ_BFS.cuh:143-500, generalised): per level one count kernel
+// takes, for every partial tuple, its shortest list; the candidates of all
+// tuples form one space, cut into pieces of bounded size; per piece an
+// expand kernel tests each candidate against the tuple's other lists
+// (binary search) and either counts and hashes finished tuples (last
+// attribute) or keeps survivors, which a scan compacts into the next level's
+// tuples.  Memory stays bounded by the piece size whatever the intermediate
+// results.  Tuples are hashed and written in attribute-id order whatever the
+// binding order, so every order gives the same result.
+// Lists of 2-column relations are strictly increasing (their tries drop
+// repeated rows: the set semantics of the triejoin); the last level of a
+// trie of 1 or of 3 or more columns keeps repeated rows, as the reference's
+// IndexedTrie does (LFTJ-GPU/multi_partitioning.cuh:283-284).
 #include "lftj_common.cuh"
 
 #include <algorithm>
@@ -24,19 +35,37 @@
 
 namespace amj {
 
-constexpr int GEN_MAX_LISTS = 8;                 // relations closing one attribute
+constexpr int GEN_MAX_LISTS = 8;                 // relations constraining one attribute
+constexpr int GEN_MAX_TRIES = 16;
 constexpr uint64_t GEN_PIECE = 1ull << 26;       // candidates per expand launch
+
+// device view of one relation's trie (2 levels with dense row pointers, or N levels)
+struct GenTrie {
+    const int32_t *data[TRIE_MAX_LEVELS];
+    const uint64_t *off[TRIE_MAX_LEVELS - 1];
+    uint64_t len0;
+    TrieRef two;                                 // 2-level tries: the dense row pointers
+    int levels;
+};
+
+// one list constraining an attribute: the values at level `depth` of trie
+// `trie` under the path of bound attributes path[0..depth-1]
+struct GenList {
+    int16_t trie;
+    int8_t depth;
+    int8_t path[TRIE_MAX_LEVELS];
+};
 
 // the lists that constrain one attribute
 struct GenLevel {
     int n;
-    TrieRef t[GEN_MAX_LISTS];
-    int8_t parent[GEN_MAX_LISTS];                // attribute whose value keys the list; -1: level 0
+    GenList l[GEN_MAX_LISTS];
 };
 
 struct GenArgs {
     GenLevel L;
-    int level;                                   // attribute being bound
+    const GenTrie *tries;
+    int level;                                   // attribute being bound (its position in the order)
     bool last;
     const int32_t *cols[AMJ_MAX_ATTRS];          // partial tuples: values of attributes 0..level-1
     uint64_t F;                                  // partial tuples
@@ -50,18 +79,45 @@ struct GenArgs {
     int32_t *out[AMJ_MAX_ATTRS];
     uint64_t out_cap;
     int k;
+    int8_t opos[AMJ_MAX_ATTRS];                  // position in the order of attribute id j
 };
 
+// first index in [s, e) of base with value >= v
+__device__ __forceinline__ uint64_t gen_lower(const int32_t *base, uint64_t s, uint64_t e, int32_t v) {
+    while (s < e) {
+        const uint64_t m = (s + e) >> 1;
+        if (base[m] < v) s = m + 1;
+        else e = m;
+    }
+    return s;
+}
+
 // range [s, e) of list i for tuple t, in the list's value array *base
-__device__ __forceinline__ void gen_range(const GenLevel &L, int i, const int32_t *const *cols, uint64_t t,
-                                          const int32_t *&base, uint64_t &s, uint64_t &e) {
-    if (L.parent[i] < 0) {
-        base = L.t[i].data0;
+__device__ __forceinline__ void gen_range(const GenArgs &A, int i, uint64_t t, const int32_t *&base, uint64_t &s,
+                                          uint64_t &e) {
+    const GenList &g = A.L.l[i];
+    const GenTrie &T = A.tries[g.trie];
+    base = T.data[g.depth];
+    if (g.depth == 0) {
         s = 0;
-        e = L.t[i].len0;
-    } else {
-        base = L.t[i].data1;
-        child_range(L.t[i], cols[L.parent[i]][t], s, e);
+        e = T.len0;
+        return;
+    }
+    if (T.levels == 2) {
+        child_range(T.two, A.cols[g.path[0]][t], s, e);
+        return;
+    }
+    s = 0;
+    e = T.len0;
+    for (int d = 0; d < g.depth; d++) {
+        const int32_t v = A.cols[g.path[d]][t];
+        const uint64_t p = gen_lower(T.data[d], s, e, v);
+        if (p == e || T.data[d][p] != v) {
+            s = e = 0;
+            return;
+        }
+        s = T.off[d][p];
+        e = T.off[d][p + 1];
     }
 }
 
@@ -72,7 +128,7 @@ __global__ void gen_count_kernel(const __grid_constant__ GenArgs A, unsigned lon
         for (int i = 0; i < A.L.n; i++) {
             const int32_t *base;
             uint64_t s, e;
-            gen_range(A.L, i, A.cols, t, base, s, e);
+            gen_range(A, i, t, base, s, e);
             if (e - s < best) {
                 best = e - s;
                 bs = s;
@@ -83,16 +139,6 @@ __global__ void gen_count_kernel(const __grid_constant__ GenArgs A, unsigned lon
         A.sidx[t] = (uint8_t)bi;
         A.sbeg[t] = bs;
     }
-}
-
-// first index in [s, e) of base with value >= v
-__device__ __forceinline__ uint64_t gen_lower(const int32_t *base, uint64_t s, uint64_t e, int32_t v) {
-    while (s < e) {
-        const uint64_t m = (s + e) >> 1;
-        if (base[m] < v) s = m + 1;
-        else e = m;
-    }
-    return s;
 }
 
 template <bool WRITE>
@@ -111,14 +157,14 @@ __global__ void gen_expand_kernel(const __grid_constant__ GenArgs A) {
         const int si = A.sidx[t];
         const int32_t *sbase;
         uint64_t ss, se;
-        gen_range(A.L, si, A.cols, t, sbase, ss, se);
+        gen_range(A, si, t, sbase, ss, se);
         const int32_t c = sbase[A.sbeg[t] + (g - A.offs[t])];
         bool keep = true;
         for (int i = 0; i < A.L.n && keep; i++) {
             if (i == si) continue;
             const int32_t *base;
             uint64_t s, e;
-            gen_range(A.L, i, A.cols, t, base, s, e);
+            gen_range(A, i, t, base, s, e);
             const uint64_t p = gen_lower(base, s, e, c);
             keep = p < e && base[p] == c;
         }
@@ -128,17 +174,21 @@ __global__ void gen_expand_kernel(const __grid_constant__ GenArgs A) {
             continue;
         }
         if (!keep) continue;
+        // the tuple in attribute-id order: attribute j sits at position opos[j]
         uint64_t h = AMJ_CHECKSUM_SEED;
-        for (int a = 0; a < A.level; a++) h = amj_hash_step(h, A.cols[a][t]);
-        h = amj_hash_step(h, c);
+        for (int j = 0; j < A.k; j++) {
+            const int l = A.opos[j];
+            h = amj_hash_step(h, l == A.level ? c : A.cols[l][t]);
+        }
         cnt++;
         chk += h;
         if (WRITE) {
             const unsigned long long p = atomicAdd(A.out_cursor, 1ull);
-            if (p < A.out_cap) {
-                for (int a = 0; a < A.level; a++) A.out[a][p] = A.cols[a][t];
-                A.out[A.level][p] = c;
-            }
+            if (p < A.out_cap)
+                for (int j = 0; j < A.k; j++) {
+                    const int l = A.opos[j];
+                    A.out[j][p] = l == A.level ? c : A.cols[l][t];
+                }
         }
     }
     if (A.last) {
@@ -172,7 +222,10 @@ __global__ void gen_compact_kernel(const __grid_constant__ GenArgs A, const uint
 struct GenQuery {
     int k = 0;
     GenLevel lv[AMJ_MAX_ATTRS];
-    std::vector<Trie2> tries;
+    std::vector<Trie2> tries2;
+    std::vector<TrieN> triesN;
+    DBuf<GenTrie> dtries;
+    int8_t opos[AMJ_MAX_ATTRS] = {};
 };
 
 struct GenRun {
@@ -197,9 +250,11 @@ static int gen_expand(GenRun &R, int level, const int32_t *const *cols, uint64_t
     GenArgs A;
     std::memset(&A, 0, sizeof(A));
     A.L = Q.lv[level];
+    A.tries = Q.dtries.p;
     A.level = level;
     A.last = level == Q.k - 1;
     A.k = Q.k;
+    for (int j = 0; j < Q.k; j++) A.opos[j] = Q.opos[j];
     for (int a = 0; a < level; a++) A.cols[a] = cols[a];
     A.F = F;
     A.count = R.ctr.p;
@@ -290,57 +345,109 @@ static int gen_pass(amj_ctx *ctx, const GenQuery &Q, int32_t *const *out, uint64
     return AMJ_OK;
 }
 
-// Compile a query of 2-column relations: attributes 0..k-1, every attribute
-// but the first closed by at least one relation with an earlier attribute.
-int lftj_generic_compile(amj_ctx *ctx, amj_rel *const *rels, int nrels, GenQuery *Q) {
+// Compile a query: attributes 0..k-1, bound in the order `order` (null: the
+// identity); every attribute after the first in the order must share a
+// relation with an earlier one.
+int lftj_generic_compile(amj_ctx *ctx, amj_rel *const *rels, int nrels, const uint32_t *order, GenQuery *Q) {
+    if (nrels > GEN_MAX_TRIES) return fail(AMJ_EUNSUPPORTED, "LFTJ: at most 16 relations");
     uint32_t seen = 0;
     for (int i = 0; i < nrels; i++) {
-        if (rels[i]->ncols != 2) return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must have two columns");
+        if (rels[i]->ncols < 1 || rels[i]->ncols > TRIE_MAX_LEVELS)
+            return fail(AMJ_EUNSUPPORTED, "LFTJ: relations of 1 to 8 columns");
         if (rels[i]->where == AMJ_MEM_HOST_STREAMED)
             return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must be on the device");
-        if (rels[i]->attrs[0] == rels[i]->attrs[1]) return fail(AMJ_EINVAL, "LFTJ: a relation repeats an attribute");
-        seen |= (1u << rels[i]->attrs[0]) | (1u << rels[i]->attrs[1]);
+        uint32_t mine = 0;
+        for (int c = 0; c < rels[i]->ncols; c++) {
+            if (rels[i]->attrs[c] >= 32 || ((mine >> rels[i]->attrs[c]) & 1))
+                return fail(AMJ_EINVAL, "LFTJ: a relation repeats an attribute");
+            mine |= 1u << rels[i]->attrs[c];
+        }
+        seen |= mine;
     }
     int k = 0;
     while (k < 32 && ((seen >> k) & 1)) k++;
     if (seen != ((1u << k) - 1) || k > AMJ_MAX_ATTRS)
         return fail(AMJ_EINVAL, "LFTJ: the relations' attributes must be exactly 0..k-1 with k <= 8");
     Q->k = k;
-    Q->tries.resize(nrels);
+    // position of every attribute in the binding order
+    int pos[AMJ_MAX_ATTRS];
+    for (int a = 0; a < k; a++) pos[a] = -1;
+    for (int i = 0; i < k; i++) {
+        const uint32_t a = order ? order[i] : (uint32_t)i;
+        if (a >= (uint32_t)k || pos[a] >= 0)
+            return fail(AMJ_EINVAL, "LFTJ: the attribute order must be a permutation of 0..k-1");
+        pos[a] = i;
+    }
+    for (int a = 0; a < k && a < AMJ_MAX_ATTRS; a++) Q->opos[a] = (int8_t)pos[a];
     for (int l = 0; l < k; l++) Q->lv[l].n = 0;
+    std::vector<GenTrie> ht(nrels);
+    Q->tries2.resize(nrels);
+    Q->triesN.resize(nrels);
     for (int i = 0; i < nrels; i++) {
-        const bool swap = rels[i]->attrs[0] > rels[i]->attrs[1];
-        const int x = (int)(swap ? rels[i]->attrs[1] : rels[i]->attrs[0]);
-        const int y = (int)(swap ? rels[i]->attrs[0] : rels[i]->attrs[1]);
-        AMJ_TRY(build_trie2(ctx, rels[i]->d_cols[swap ? 1 : 0], rels[i]->d_cols[swap ? 0 : 1], rels[i]->n,
-                            &Q->tries[i], true));
-        const TrieRef tr = trie_ref(Q->tries[i]);
-        if (Q->lv[y].n >= GEN_MAX_LISTS) return fail(AMJ_EUNSUPPORTED, "LFTJ: more than 8 relations close one attribute");
-        Q->lv[y].t[Q->lv[y].n] = tr;
-        Q->lv[y].parent[Q->lv[y].n] = (int8_t)x;
-        Q->lv[y].n++;
-        if (x == 0) {
-            if (Q->lv[0].n >= GEN_MAX_LISTS) return fail(AMJ_EUNSUPPORTED, "LFTJ: more than 8 relations on attribute 0");
-            Q->lv[0].t[Q->lv[0].n] = tr;
-            Q->lv[0].parent[Q->lv[0].n] = -1;
-            Q->lv[0].n++;
+        // the relation's columns in binding order
+        const int nc = rels[i]->ncols;
+        int colord[TRIE_MAX_LEVELS];
+        for (int c = 0; c < nc; c++) colord[c] = c;
+        std::sort(colord, colord + nc, [&](int x, int y) { return pos[rels[i]->attrs[x]] < pos[rels[i]->attrs[y]]; });
+        GenTrie &g = ht[i];
+        std::memset(&g, 0, sizeof(g));
+        if (nc == 2) {
+            AMJ_TRY(build_trie2(ctx, rels[i]->d_cols[colord[0]], rels[i]->d_cols[colord[1]], rels[i]->n,
+                                &Q->tries2[i], true));
+            const Trie2 &t = Q->tries2[i];
+            g.levels = 2;
+            g.data[0] = t.data0.p;
+            g.data[1] = t.data1.p;
+            g.off[0] = t.off0.p;
+            g.len0 = t.len0;
+            g.two = trie_ref(t);
+        } else {
+            const int32_t *cols[TRIE_MAX_LEVELS];
+            for (int c = 0; c < nc; c++) cols[c] = rels[i]->d_cols[colord[c]];
+            AMJ_TRY(build_trieN(ctx, cols, nc, rels[i]->n, &Q->triesN[i]));
+            const TrieN &t = Q->triesN[i];
+            g.levels = nc;
+            for (int c = 0; c < nc; c++) g.data[c] = t.data[c].p;
+            for (int c = 0; c + 1 < nc; c++) g.off[c] = t.off[c].p;
+            g.len0 = t.len[0];
+        }
+        // one list per attribute at depth >= 1; a level-0 list for the first
+        // attribute, and for a 1-column relation (nothing deeper implies it)
+        for (int d = 0; d < nc; d++) {
+            const int l = pos[rels[i]->attrs[colord[d]]];
+            if (d == 0 && l != 0 && nc > 1) continue;
+            GenLevel &L = Q->lv[l];
+            if (L.n >= GEN_MAX_LISTS) return fail(AMJ_EUNSUPPORTED, "LFTJ: more than 8 relations constrain one attribute");
+            GenList &gl = L.l[L.n++];
+            std::memset(&gl, 0, sizeof(gl));
+            gl.trie = (int16_t)i;
+            gl.depth = (int8_t)d;
+            for (int e = 0; e < d; e++) gl.path[e] = (int8_t)pos[rels[i]->attrs[colord[e]]];
         }
     }
-    for (int l = 1; l < k; l++)
-        if (Q->lv[l].n == 0)
+    for (int l = 1; l < k; l++) {
+        bool linked = false;
+        for (int j = 0; j < Q->lv[l].n; j++) linked |= Q->lv[l].l[j].depth > 0;
+        if (!linked)
             return fail(AMJ_EUNSUPPORTED, "LFTJ: every attribute after the first must share a relation with an earlier one");
+    }
+    if (Q->lv[0].n == 0) return fail(AMJ_EUNSUPPORTED, "LFTJ: no relation starts with the first attribute");
+    AMJ_TRY(Q->dtries.alloc(ctx, nrels));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(Q->dtries.p, ht.data(), nrels * sizeof(GenTrie), cudaMemcpyHostToDevice, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return AMJ_OK;
 }
 
 // amj_lftj_execute for queries other than the triangle: a count pass, then
 // with AMJ_F_MATERIALIZE a write pass into exactly allocated columns.
-int lftj_generic_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int ooc, int flags, amj_result *out) {
+int lftj_generic_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int ooc, int flags, const uint32_t *order,
+                         amj_result *out) {
     if (ooc) return fail(AMJ_EUNSUPPORTED, "LFTJ: no out-of-core form beyond the triangle (the generic join is "
                                            "already memory-bounded)");
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
     GenQuery Q;
-    AMJ_TRY(lftj_generic_compile(ctx, rels, nrels, &Q));
+    AMJ_TRY(lftj_generic_compile(ctx, rels, nrels, order, &Q));
     result_init(out, Q.k);
     AMJ_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
     uint64_t c = 0, h = 0;

@@ -161,16 +161,28 @@ int  amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *rels, int nr
  * nrels == 1: triangle self-join R(a,b) S(b,c) T(a,c) over one edge relation
  *             (AMJ_F_CLIQUE4: the 4-clique).
  * nrels == 3 carrying (0,1), (1,2), (0,2): the triangle over three relations.
- * any other nrels >= 3 (up to 16): the connected join of 2-column relations
- *             over attributes 0..k-1, k <= 8, in identity attribute order (the
- *             reference's LFTJ stops at 3 attributes and 3 tables); ooc = 0.
+ * any other nrels >= 3 (up to 16): the connected join of relations of 1 to 8
+ *             columns over attributes 0..k-1, k <= 8 (the reference's LFTJ
+ *             stops at 3 attributes and 3 tables of 2 columns); ooc = 0.
  * nrels == 2 is rejected, as in the reference (LFTJ-GPU/exec_LFTJ.cu:92-95).
- * Relations are joined as sets (leapfrog triejoin semantics): a repeated row
- * counts once.  The 4-clique over an oriented relation keeps its triangle
- * matrices (at most half the free device memory) with the context between
- * calls; amj_ctx_destroy releases them. */
+ * 2-column relations are joined as sets (leapfrog triejoin semantics): a
+ * repeated row counts once; tries of 3 or more columns keep repeated rows in
+ * their last level, as the reference's IndexedTrie does.  The 4-clique over
+ * an oriented relation keeps its triangle matrices (at most half the free
+ * device memory) with the context between calls; amj_ctx_destroy releases
+ * them. */
 int  amj_lftj_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels,
                       int algo, int ooc, int ws, int flags, amj_result *out);
+/* The same with the attributes bound in attr_order (k entries, a permutation
+ * of 0..k-1; null or the identity: amj_lftj_execute), replacing the
+ * attr_order argument of OOCWrapper::execute_with_{BFS,DFS}
+ * (LFTJ-GPU/ooc_wrapper.cuh:404-427, LFTJ-GPU/ALFTJ.cuh:1125-1196), which the
+ * reference's driver always sets to the identity (LFTJ-GPU/exec_LFTJ.cu:230-231).
+ * Any order gives the same result: tuples and checksum stay in attribute-id
+ * order.  A non-identity order runs the generic join (one relation: its
+ * triangle or, with AMJ_F_CLIQUE4, 4-clique pattern); ooc must be 0. */
+int  amj_lftj_execute_ordered(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int ws,
+                              int flags, const uint32_t *attr_order, int k, amj_result *out);
 
 void amj_result_release(amj_result *res);
 

@@ -600,6 +600,87 @@ def test_lftj_generic_queries_match_amhj_and_oracle(ctx, name, algo):
     assert (amhj.count, amhj.checksum) == want
 
 
+def distinct_rows(n, dom, seed, attrs):
+    """A relation of distinct tuples with len(attrs) columns."""
+    cols = [data.uniform(n, 0, dom, seed, s) for s in range(len(attrs))]
+    rows = np.unique(np.stack(cols, 1), axis=0)
+    return ([np.ascontiguousarray(rows[:, j]) for j in range(len(attrs))], attrs)
+
+
+# binding orders in which every attribute shares a relation with an earlier one
+ORDERS = {
+    "4-cycle": [(0, 1, 2, 3), (3, 2, 1, 0), (2, 1, 0, 3), (1, 0, 3, 2)],
+    "5-cycle+chord": [(4, 3, 2, 1, 0), (1, 3, 0, 2, 4), (2, 1, 3, 4, 0)],
+    "path4": [(3, 2, 1, 0), (1, 2, 0, 3)],
+}
+
+
+@pytest.mark.parametrize("name", list(ORDERS))
+def test_lftj_attribute_orders_give_the_same_result(ctx, name):
+    """attr_order (the reference's OOCWrapper / ALFTJ argument,
+    LFTJ-GPU/ALFTJ.cuh:1125-1196, always the identity in its driver): every
+    binding order gives the same bag, hashed and written in attribute-id
+    order."""
+    pats = GENERIC_QUERIES[name]
+    rels = [distinct_rel(3000, 150 if len(pats) > 4 else 250, 70 + i, list(p)) for i, p in enumerate(pats)]
+    hs = [ctx.relation(c, a) for c, a in rels]
+    want = O.mhj(rels)
+    for order in ORDERS[name]:
+        got = ctx.lftj(hs, attr_order=order)
+        assert (got.count, got.checksum) == want, order
+    m = ctx.lftj(hs, attr_order=ORDERS[name][-1], materialize=True)
+    cnt, chk, cols = O.mhj(rels, tuples=True)
+    assert np.array_equal(sorted_rows(m.columns), sorted_rows(cols))
+    if name == "4-cycle":
+        # attributes 1 and 3 share no relation: binding 3 second is a cross product
+        with pytest.raises(AmjError) as e:
+            ctx.lftj(hs, attr_order=(1, 3, 0, 2))
+        assert e.value.status == L.AMJ_EUNSUPPORTED
+
+
+@pytest.mark.parametrize("clique4", [False, True])
+def test_lftj_self_join_in_other_orders(ctx, clique4):
+    s, d = data.rmat(10, 9000, 0.57, 0.19, 0.19, 12)
+    e = ctx.relation([s, d], [0, 1])
+    want = O.four_clique(s, d) if clique4 else O.triangle(s, d)
+    orders = [(3, 1, 0, 2), (1, 2, 3, 0)] if clique4 else [(2, 1, 0), (1, 0, 2), (0, 1, 2)]
+    for order in orders:
+        got = ctx.lftj([e], clique4=clique4, attr_order=order)
+        assert (got.count, got.checksum) == want, order
+    # three relations of the triangle pattern, a non-identity order
+    hs = [ctx.relation([s, d], [0, 1]), ctx.relation([s, d], [1, 2]), ctx.relation([s, d], [0, 2])]
+    if not clique4:
+        assert (lambda r: (r.count, r.checksum))(ctx.lftj(hs, attr_order=(2, 0, 1))) == want
+    with pytest.raises(AmjError):
+        ctx.lftj([e], attr_order=(0, 0, 1))
+    with pytest.raises(AmjError):
+        ctx.lftj([e], attr_order=(1, 0, 2), ooc=1)
+
+
+@pytest.mark.parametrize("order", [None, (2, 0, 1, 3), (3, 2, 1, 0)])
+def test_lftj_relations_of_three_columns(ctx, order):
+    """Tries of three columns (build_trieN) in the generic join: a ternary
+    relation R(0,1,2) with binary S(1,3), T(2,3), a unary U(3), equal to the
+    oracle's multi-way join (the reference's LFTJ takes 2 columns only)."""
+    R = distinct_rows(20000, 40, 81, [0, 1, 2])
+    S = distinct_rel(1500, 40, 82, [1, 3])
+    T = distinct_rel(1500, 40, 83, [2, 3])
+    U = ([np.unique(data.uniform(30, 0, 40, 84, 0))], [3])
+    rels = [R, S, T, U]
+    hs = [ctx.relation(c, a) for c, a in rels]
+    want = O.mhj(rels)
+    assert want[0] > 0
+    got = ctx.lftj(hs, attr_order=order)
+    assert (got.count, got.checksum) == want
+    m = ctx.lftj(hs, attr_order=order, materialize=True)
+    assert np.array_equal(sorted_rows(m.columns), sorted_rows(O.mhj(rels, tuples=True)[2]))
+    # a 4-column relation against two binary ones
+    Q = distinct_rows(8000, 12, 85, [0, 1, 2, 3])
+    rels2 = [Q, distinct_rel(100, 12, 86, [0, 4]), distinct_rel(100, 12, 87, [3, 4])]
+    got = ctx.lftj([ctx.relation(c, a) for c, a in rels2], attr_order=None if order is None else (4, 0, 1, 2, 3))
+    assert (got.count, got.checksum) == O.mhj(rels2)
+
+
 def test_lftj_generic_materialized_and_rejections(ctx):
     rels = [distinct_rel(3000, 200, 60 + i, list(p)) for i, p in enumerate(GENERIC_QUERIES["4-cycle"])]
     hs = [ctx.relation(c, a) for c, a in rels]
