@@ -88,7 +88,6 @@ static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
                                 amj_result *out) {
     if (nrels != 1) return fail(AMJ_EUNSUPPORTED, "LFTJ 4-clique: one edge relation");
     if (algo != AMJ_LFTJ_DFS) return fail(AMJ_EUNSUPPORTED, "LFTJ 4-clique: DFS only");
-    if (ooc) return fail(AMJ_EUNSUPPORTED, "LFTJ 4-clique: no out-of-core form");
     result_init(out, 4);
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
@@ -179,6 +178,8 @@ static int self_join_views(const amj_rel *r, bool clique4, amj_rel *views, amj_r
         views[i].owned = false;
         views[i].d_cols[0] = r->d_cols[swap ? 1 : 0];
         views[i].d_cols[1] = r->d_cols[swap ? 0 : 1];
+        views[i].h_cols[0] = r->h_cols[swap ? 1 : 0];
+        views[i].h_cols[1] = r->h_cols[swap ? 0 : 1];
         views[i].attrs[0] = clique4 ? four[i][0] : tri[i][0];
         views[i].attrs[1] = clique4 ? four[i][1] : tri[i][1];
         ptrs[i] = &views[i];
@@ -216,10 +217,10 @@ static int lftj_execute_impl(amj_ctx *ctx, amj_rel *const *rels, int nrels, int 
         if (!rels[i]) return fail(AMJ_EINVAL, "lftj_execute: null relation");
     if (nrels > 16) return fail(AMJ_EUNSUPPORTED, "lftj_execute: at most 16 relations");
     AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
-    if (!identity_order(order, norder)) {
-        // a binding order other than the identity: the generic join, which
+    if (ooc || !identity_order(order, norder)) {
+        // out-of-core (value-range trie slices under a memory budget), or a
+        // binding order other than the identity: the generic join, which
         // reports every tuple in attribute-id order
-        if (ooc) return fail(AMJ_EUNSUPPORTED, "LFTJ: no out-of-core form with an attribute order");
         if (nrels == 1) {
             amj_rel views[6];
             amj_rel *ptrs[6];
@@ -296,74 +297,33 @@ static int lftj_execute_impl(amj_ctx *ctx, amj_rel *const *rels, int nrels, int 
     const int32_t *rank_inv = nv ? inv.p : nullptr;
     const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
     const uint64_t nr = R->len1;
-    uint64_t slice = nr;
-    if (ooc) {
-        slice = ctx->opts.ooc_slice_rows ? ctx->opts.ooc_slice_rows : std::max<uint64_t>(1, nr / 8);
-        slice = std::max<uint64_t>(32, slice);
-    }
-    uint64_t count = 0, checksum = 0;
-    std::vector<std::vector<int32_t>> hcols(ooc && materialize ? 3 : 0);
-    int32_t *dcols[3] = {nullptr, nullptr, nullptr};
-    int rc = AMJ_OK;
-    for (uint64_t lo = 0; rc == AMJ_OK && (lo < nr || (lo == 0 && nr == 0)); lo += slice) {
-        const uint64_t hi = std::min(nr, lo + slice);
-        uint64_t c = 0, h = 0, w = 0;
-        rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, lo, hi, heavy_deg,
+    uint64_t c = 0, h = 0, w = 0;
+    int rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, 0, nr, heavy_deg,
                            out->kernel_ms, sorted_out, rank_inv, wedges.p, nv, ctx->opts.lftj_rank_bits);
-        if (rc != AMJ_OK) break;
-        if (materialize) {
-            int32_t *cols[3] = {nullptr, nullptr, nullptr};
-            for (int a = 0; a < 3 && rc == AMJ_OK; a++) rc = dev_alloc(ctx, (void **)&cols[a], (c ? c : 1) * 4);
-            uint64_t c2 = 0, h2 = 0;
-            if (rc == AMJ_OK)
-                rc = lftj_triangle(ctx, *R, *S, *T, algo, cols, c, &c2, &h2, &w, small_sum, lo, hi, heavy_deg,
-                                   out->kernel_ms + 2, sorted_out, rank_inv, wedges.p, nv, ctx->opts.lftj_rank_bits);
-            if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
-                rc = fail(AMJ_ECUDA, "LFTJ: write pass disagrees with count pass");
-            if (rc == AMJ_OK && ooc) {
-                for (int a = 0; a < 3; a++) {
-                    const size_t old = hcols[a].size();
-                    hcols[a].resize(old + c);
-                    if (c && cudaMemcpyAsync(hcols[a].data() + old, cols[a], c * 4, cudaMemcpyDeviceToHost,
-                                             ctx->stream) != cudaSuccess)
-                        rc = fail(AMJ_ECUDA, "LFTJ ooc: result copy failed");
-                }
-                if (rc == AMJ_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
-                    rc = fail(AMJ_ECUDA, "LFTJ ooc: sync failed");
-                for (int a = 0; a < 3; a++) dev_free(ctx, cols[a]);
-            } else {
-                for (int a = 0; a < 3; a++) dcols[a] = cols[a];
-            }
+    if (rc != AMJ_OK) return rc;
+    int32_t *dcols[3] = {nullptr, nullptr, nullptr};
+    if (materialize) {
+        for (int a = 0; a < 3 && rc == AMJ_OK; a++) rc = dev_alloc(ctx, (void **)&dcols[a], (c ? c : 1) * 4);
+        uint64_t c2 = 0, h2 = 0;
+        if (rc == AMJ_OK)
+            rc = lftj_triangle(ctx, *R, *S, *T, algo, dcols, c, &c2, &h2, &w, small_sum, 0, nr, heavy_deg,
+                               out->kernel_ms + 2, sorted_out, rank_inv, wedges.p, nv, ctx->opts.lftj_rank_bits);
+        if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
+            rc = fail(AMJ_ECUDA, "LFTJ: write pass disagrees with count pass");
+        if (rc != AMJ_OK) {
+            for (int a = 0; a < 3; a++) dev_free(ctx, dcols[a]);
+            return rc;
         }
-        count += c;
-        checksum += h;
-        out->stats[7]++;
-        if (nr == 0) break;
     }
-    if (rc != AMJ_OK) {
-        for (int a = 0; a < 3; a++) dev_free(ctx, dcols[a]);
-        return rc;
-    }
-    out->count = count;
-    out->checksum = checksum;
+    out->count = c;
+    out->checksum = h;
+    out->stats[7] = 1;
     if (materialize) {
         auto *o = new ResultOwner();
         o->ctx = ctx;
         out->priv = o;
-        out->rows = count;
-        if (ooc) {
-            out->on_host = 1;
-            for (int a = 0; a < 3; a++) {
-                if (cudaMallocHost((void **)&out->cols[a], (count ? count : 1) * 4) != cudaSuccess) {
-                    (void)cudaGetLastError();
-                    amj_result_release(out);
-                    return fail(AMJ_ENOMEM, "LFTJ: pinned result allocation failed");
-                }
-                if (count) std::memcpy(out->cols[a], hcols[a].data(), count * 4);
-            }
-        } else {
-            for (int a = 0; a < 3; a++) out->cols[a] = dcols[a];
-        }
+        out->rows = c;
+        for (int a = 0; a < 3; a++) out->cols[a] = dcols[a];
     }
     AMJ_CUDA_TRY(cudaEventRecord(e2, ctx->stream));
     AMJ_CUDA_TRY(cudaEventSynchronize(e2));

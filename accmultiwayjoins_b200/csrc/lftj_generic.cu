@@ -30,7 +30,9 @@
 #include "lftj_common.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 namespace amj {
@@ -345,17 +347,27 @@ static int gen_pass(amj_ctx *ctx, const GenQuery &Q, int32_t *const *out, uint64
     return AMJ_OK;
 }
 
-// Compile a query: attributes 0..k-1, bound in the order `order` (null: the
+// The compiled query without tries: positions in the binding order, every
+// relation's columns in that order, and the lists that constrain each
+// attribute (list i of level l refers to relation trie).
+struct GenPlan {
+    int k = 0;
+    int nrels = 0;
+    int pos[AMJ_MAX_ATTRS] = {};
+    int ncols[GEN_MAX_TRIES] = {};
+    int colord[GEN_MAX_TRIES][TRIE_MAX_LEVELS] = {};
+    GenLevel lv[AMJ_MAX_ATTRS];
+};
+
+// Plan a query: attributes 0..k-1, bound in the order `order` (null: the
 // identity); every attribute after the first in the order must share a
 // relation with an earlier one.
-int lftj_generic_compile(amj_ctx *ctx, amj_rel *const *rels, int nrels, const uint32_t *order, GenQuery *Q) {
+static int gen_plan(amj_rel *const *rels, int nrels, const uint32_t *order, GenPlan *P) {
     if (nrels > GEN_MAX_TRIES) return fail(AMJ_EUNSUPPORTED, "LFTJ: at most 16 relations");
     uint32_t seen = 0;
     for (int i = 0; i < nrels; i++) {
         if (rels[i]->ncols < 1 || rels[i]->ncols > TRIE_MAX_LEVELS)
             return fail(AMJ_EUNSUPPORTED, "LFTJ: relations of 1 to 8 columns");
-        if (rels[i]->where == AMJ_MEM_HOST_STREAMED)
-            return fail(AMJ_EUNSUPPORTED, "LFTJ: relations must be on the device");
         uint32_t mine = 0;
         for (int c = 0; c < rels[i]->ncols; c++) {
             if (rels[i]->attrs[c] >= 32 || ((mine >> rels[i]->attrs[c]) & 1))
@@ -368,9 +380,9 @@ int lftj_generic_compile(amj_ctx *ctx, amj_rel *const *rels, int nrels, const ui
     while (k < 32 && ((seen >> k) & 1)) k++;
     if (seen != ((1u << k) - 1) || k > AMJ_MAX_ATTRS)
         return fail(AMJ_EINVAL, "LFTJ: the relations' attributes must be exactly 0..k-1 with k <= 8");
-    Q->k = k;
-    // position of every attribute in the binding order
-    int pos[AMJ_MAX_ATTRS];
+    P->k = k;
+    P->nrels = nrels;
+    int *pos = P->pos;
     for (int a = 0; a < k; a++) pos[a] = -1;
     for (int i = 0; i < k; i++) {
         const uint32_t a = order ? order[i] : (uint32_t)i;
@@ -378,45 +390,20 @@ int lftj_generic_compile(amj_ctx *ctx, amj_rel *const *rels, int nrels, const ui
             return fail(AMJ_EINVAL, "LFTJ: the attribute order must be a permutation of 0..k-1");
         pos[a] = i;
     }
-    for (int a = 0; a < k && a < AMJ_MAX_ATTRS; a++) Q->opos[a] = (int8_t)pos[a];
-    for (int l = 0; l < k; l++) Q->lv[l].n = 0;
-    std::vector<GenTrie> ht(nrels);
-    Q->tries2.resize(nrels);
-    Q->triesN.resize(nrels);
+    for (int l = 0; l < k; l++) P->lv[l].n = 0;
     for (int i = 0; i < nrels; i++) {
         // the relation's columns in binding order
         const int nc = rels[i]->ncols;
-        int colord[TRIE_MAX_LEVELS];
+        P->ncols[i] = nc;
+        int *colord = P->colord[i];
         for (int c = 0; c < nc; c++) colord[c] = c;
         std::sort(colord, colord + nc, [&](int x, int y) { return pos[rels[i]->attrs[x]] < pos[rels[i]->attrs[y]]; });
-        GenTrie &g = ht[i];
-        std::memset(&g, 0, sizeof(g));
-        if (nc == 2) {
-            AMJ_TRY(build_trie2(ctx, rels[i]->d_cols[colord[0]], rels[i]->d_cols[colord[1]], rels[i]->n,
-                                &Q->tries2[i], true));
-            const Trie2 &t = Q->tries2[i];
-            g.levels = 2;
-            g.data[0] = t.data0.p;
-            g.data[1] = t.data1.p;
-            g.off[0] = t.off0.p;
-            g.len0 = t.len0;
-            g.two = trie_ref(t);
-        } else {
-            const int32_t *cols[TRIE_MAX_LEVELS];
-            for (int c = 0; c < nc; c++) cols[c] = rels[i]->d_cols[colord[c]];
-            AMJ_TRY(build_trieN(ctx, cols, nc, rels[i]->n, &Q->triesN[i]));
-            const TrieN &t = Q->triesN[i];
-            g.levels = nc;
-            for (int c = 0; c < nc; c++) g.data[c] = t.data[c].p;
-            for (int c = 0; c + 1 < nc; c++) g.off[c] = t.off[c].p;
-            g.len0 = t.len[0];
-        }
         // one list per attribute at depth >= 1; a level-0 list for the first
         // attribute, and for a 1-column relation (nothing deeper implies it)
         for (int d = 0; d < nc; d++) {
             const int l = pos[rels[i]->attrs[colord[d]]];
             if (d == 0 && l != 0 && nc > 1) continue;
-            GenLevel &L = Q->lv[l];
+            GenLevel &L = P->lv[l];
             if (L.n >= GEN_MAX_LISTS) return fail(AMJ_EUNSUPPORTED, "LFTJ: more than 8 relations constrain one attribute");
             GenList &gl = L.l[L.n++];
             std::memset(&gl, 0, sizeof(gl));
@@ -427,14 +414,503 @@ int lftj_generic_compile(amj_ctx *ctx, amj_rel *const *rels, int nrels, const ui
     }
     for (int l = 1; l < k; l++) {
         bool linked = false;
-        for (int j = 0; j < Q->lv[l].n; j++) linked |= Q->lv[l].l[j].depth > 0;
+        for (int j = 0; j < P->lv[l].n; j++) linked |= P->lv[l].l[j].depth > 0;
         if (!linked)
             return fail(AMJ_EUNSUPPORTED, "LFTJ: every attribute after the first must share a relation with an earlier one");
     }
-    if (Q->lv[0].n == 0) return fail(AMJ_EUNSUPPORTED, "LFTJ: no relation starts with the first attribute");
+    if (P->lv[0].n == 0) return fail(AMJ_EUNSUPPORTED, "LFTJ: no relation starts with the first attribute");
+    return AMJ_OK;
+}
+
+static void gen_query_from_plan(const GenPlan &P, GenQuery *Q) {
+    Q->k = P.k;
+    for (int l = 0; l < P.k; l++) Q->lv[l] = P.lv[l];
+    for (int a = 0; a < P.k && a < AMJ_MAX_ATTRS; a++) Q->opos[a] = (int8_t)P.pos[a];
+}
+
+// The trie of relation i in its binding column order, on the device.
+static int gen_build_trie(amj_ctx *ctx, const amj_rel *r, const GenPlan &P, int i, Trie2 *t2, TrieN *tn,
+                          GenTrie *g) {
+    const int nc = P.ncols[i];
+    const int *colord = P.colord[i];
+    std::memset(g, 0, sizeof(*g));
+    if (nc == 2) {
+        AMJ_TRY(build_trie2(ctx, r->d_cols[colord[0]], r->d_cols[colord[1]], r->n, t2, true));
+        g->levels = 2;
+        g->data[0] = t2->data0.p;
+        g->data[1] = t2->data1.p;
+        g->off[0] = t2->off0.p;
+        g->len0 = t2->len0;
+        g->two = trie_ref(*t2);
+        return AMJ_OK;
+    }
+    const int32_t *cols[TRIE_MAX_LEVELS];
+    for (int c = 0; c < nc; c++) cols[c] = r->d_cols[colord[c]];
+    AMJ_TRY(build_trieN(ctx, cols, nc, r->n, tn));
+    g->levels = nc;
+    for (int c = 0; c < nc; c++) g->data[c] = tn->data[c].p;
+    for (int c = 0; c + 1 < nc; c++) g->off[c] = tn->off[c].p;
+    g->len0 = tn->len[0];
+    return AMJ_OK;
+}
+
+int lftj_generic_compile(amj_ctx *ctx, amj_rel *const *rels, int nrels, const uint32_t *order, GenQuery *Q) {
+    GenPlan P;
+    AMJ_TRY(gen_plan(rels, nrels, order, &P));
+    for (int i = 0; i < nrels; i++)
+        if (rels[i]->where == AMJ_MEM_HOST_STREAMED)
+            return fail(AMJ_EUNSUPPORTED, "LFTJ: host-resident relations need ooc = 1");
+    gen_query_from_plan(P, Q);
+    std::vector<GenTrie> ht(nrels);
+    Q->tries2.resize(nrels);
+    Q->triesN.resize(nrels);
+    for (int i = 0; i < nrels; i++) AMJ_TRY(gen_build_trie(ctx, rels[i], P, i, &Q->tries2[i], &Q->triesN[i], &ht[i]));
     AMJ_TRY(Q->dtries.alloc(ctx, nrels));
     AMJ_CUDA_TRY(cudaMemcpyAsync(Q->dtries.p, ht.data(), nrels * sizeof(GenTrie), cudaMemcpyHostToDevice, ctx->stream));
     AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return AMJ_OK;
+}
+
+// ---- out-of-core ----
+// The reference's OOCWrapper (LFTJ-GPU/ooc_wrapper.cuh:14-427) splits a
+// memory budget over the attributes in proportion to the tries each one
+// heads (BudgetPlanner, :14-49), chooses for every such attribute value
+// ranges of the heading tries' level 0 whose sub-tries fit its share (probe,
+// :110-172), provisions the trie slices of each combination of ranges
+// (:68-104) and joins every combination (:263-371); the ranges of one
+// attribute partition its values, so every result tuple is found in exactly
+// one combination.  Here the tries live in pinned host memory: a relation on
+// the device has its trie built there and copied out; a host-resident
+// relation (AMJ_MEM_HOST_STREAMED) is cut into value ranges of its first
+// column (in binding order) that fit the budget, and the trie of each range
+// is built on the device and appended (the ranges come in increasing order,
+// so the appended tries are the trie of the whole relation).  Each
+// combination copies to the device only the slices that changed since the
+// previous one, rebases their offsets and runs the generic join over them.
+
+struct HostTrie {
+    int levels = 0;
+    uint64_t len[TRIE_MAX_LEVELS] = {};
+    int32_t *data[TRIE_MAX_LEVELS] = {};    // pinned
+    uint64_t *off[TRIE_MAX_LEVELS - 1] = {};
+    HostTrie() = default;
+    HostTrie(const HostTrie &) = delete;
+    HostTrie &operator=(const HostTrie &) = delete;
+    ~HostTrie() {
+        for (auto *p : data)
+            if (p) cudaFreeHost(p);
+        for (auto *p : off)
+            if (p) cudaFreeHost(p);
+    }
+    // entry ranges [s[l], e[l]) of every level for level-0 entries [i0, i1)
+    void ranges(uint64_t i0, uint64_t i1, uint64_t *s, uint64_t *e) const {
+        s[0] = i0;
+        e[0] = i1;
+        for (int l = 0; l + 1 < levels; l++) {
+            s[l + 1] = off[l][s[l]];
+            e[l + 1] = off[l][e[l]];
+        }
+    }
+    uint64_t bytes(uint64_t i0, uint64_t i1) const {
+        uint64_t s[TRIE_MAX_LEVELS], e[TRIE_MAX_LEVELS];
+        ranges(i0, i1, s, e);
+        uint64_t b = 0;
+        for (int l = 0; l < levels; l++) b += 4 * (e[l] - s[l]) + (l + 1 < levels ? 8 * (e[l] - s[l] + 1) : 0);
+        return b;
+    }
+    // level-0 entries whose values lie in [lo, hi]
+    void value_range(int64_t lo, int64_t hi, uint64_t *i0, uint64_t *i1) const {
+        const int32_t *d = data[0];
+        *i0 = (uint64_t)(std::lower_bound(d, d + len[0], (int64_t)lo, [](int32_t a, int64_t v) { return a < v; }) - d);
+        *i1 = (uint64_t)(std::upper_bound(d, d + len[0], (int64_t)hi, [](int64_t v, int32_t a) { return v < a; }) - d);
+    }
+};
+
+static int host_alloc(void **p, size_t bytes) {
+    if (cudaMallocHost(p, bytes ? bytes : 4) != cudaSuccess) {
+        (void)cudaGetLastError();
+        *p = nullptr;
+        return fail(AMJ_ENOMEM, "LFTJ ooc: pinned host allocation failed");
+    }
+    return AMJ_OK;
+}
+
+// Append the device trie g (levels nc) to the host trie H.
+static int append_trie(amj_ctx *ctx, const GenTrie &g, const uint64_t *lens, HostTrie *H, uint64_t *cap) {
+    // grow the pinned arrays when needed (doubling)
+    for (int l = 0; l < H->levels; l++) {
+        const uint64_t need = H->len[l] + lens[l];
+        if (need > cap[l]) {
+            uint64_t nc = std::max<uint64_t>(need, cap[l] * 2);
+            void *nd = nullptr, *no = nullptr;
+            AMJ_TRY(host_alloc(&nd, nc * 4));
+            if (H->data[l]) std::memcpy(nd, H->data[l], H->len[l] * 4);
+            if (H->data[l]) cudaFreeHost(H->data[l]);
+            H->data[l] = (int32_t *)nd;
+            if (l + 1 < H->levels) {
+                AMJ_TRY(host_alloc(&no, (nc + 1) * 8));
+                if (H->off[l]) std::memcpy(no, H->off[l], (H->len[l] + 1) * 8);
+                else ((uint64_t *)no)[0] = 0;
+                if (H->off[l]) cudaFreeHost(H->off[l]);
+                H->off[l] = (uint64_t *)no;
+            }
+            cap[l] = nc;
+        }
+    }
+    for (int l = 0; l < H->levels; l++) {
+        if (lens[l])
+            AMJ_CUDA_TRY(cudaMemcpyAsync(H->data[l] + H->len[l], g.data[l], lens[l] * 4, cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+        if (l + 1 < H->levels)
+            AMJ_CUDA_TRY(cudaMemcpyAsync(H->off[l] + H->len[l], g.off[l], (lens[l] + 1) * 8, cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+    }
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    // the appended offsets continue from the next level's previous end
+    for (int l = 0; l + 1 < H->levels; l++) {
+        const uint64_t base = H->len[l + 1];
+        for (uint64_t j = 0; j <= lens[l]; j++) H->off[l][H->len[l] + j] += base;
+    }
+    for (int l = 0; l < H->levels; l++) H->len[l] += lens[l];
+    return AMJ_OK;
+}
+
+// The host trie of relation i (columns in binding order), built in ranges of
+// its first column's values that keep each range's rows within `budget`
+// bytes of device memory.
+static int build_host_trie(amj_ctx *ctx, const amj_rel *r, const GenPlan &P, int i, uint64_t budget, HostTrie *H) {
+    const int nc = P.ncols[i];
+    H->levels = nc;
+    uint64_t cap[TRIE_MAX_LEVELS] = {};
+    for (int l = 0; l < nc; l++) {
+        void *d = nullptr;
+        AMJ_TRY(host_alloc(&d, 4));
+        H->data[l] = (int32_t *)d;
+        cap[l] = 1;
+        if (l + 1 < nc) {
+            void *o = nullptr;
+            AMJ_TRY(host_alloc(&o, 16));
+            H->off[l] = (uint64_t *)o;
+            H->off[l][0] = 0;
+        }
+    }
+    auto add = [&](const int32_t *const *dcols, uint64_t n) -> int {
+        amj_rel view;
+        view.ctx = ctx;
+        view.n = n;
+        view.ncols = nc;
+        for (int c = 0; c < nc; c++) {
+            view.attrs[c] = (uint32_t)c;
+            view.d_cols[c] = const_cast<int32_t *>(dcols[c]);
+        }
+        GenPlan one;
+        one.ncols[0] = nc;
+        for (int c = 0; c < nc; c++) one.colord[0][c] = c;
+        Trie2 t2;
+        TrieN tn;
+        GenTrie g;
+        AMJ_TRY(gen_build_trie(ctx, &view, one, 0, &t2, &tn, &g));
+        uint64_t lens[TRIE_MAX_LEVELS] = {};
+        if (nc == 2) {
+            lens[0] = t2.len0;
+            lens[1] = t2.len1;
+        } else {
+            for (int l = 0; l < nc; l++) lens[l] = tn.len[l];
+        }
+        return append_trie(ctx, g, lens, H, cap);
+    };
+    if (r->where != AMJ_MEM_HOST_STREAMED) {
+        const int32_t *cols[TRIE_MAX_LEVELS];
+        for (int c = 0; c < nc; c++) cols[c] = r->d_cols[P.colord[i][c]];
+        return add(cols, r->n);
+    }
+    // a host-resident relation: value ranges of its first column, each range's
+    // rows gathered on the host, copied, built and appended in increasing order
+    const int32_t *h0 = r->h_cols[P.colord[i][0]];
+    const uint64_t n = r->n;
+    if (n == 0) return AMJ_OK;
+    int64_t vmin = INT32_MAX, vmax = INT32_MIN;
+#pragma omp parallel for reduction(min : vmin) reduction(max : vmax)
+    for (int64_t j = 0; j < (int64_t)n; j++) {
+        vmin = std::min<int64_t>(vmin, h0[j]);
+        vmax = std::max<int64_t>(vmax, h0[j]);
+    }
+    // rows per range: the sort and the trie take about 40 bytes a row
+    const uint64_t per = std::max<uint64_t>(1024, budget / (uint64_t)(40 + 8 * nc));
+    const uint64_t parts = std::max<uint64_t>(1, (n + per - 1) / per);
+    // value boundaries from a histogram of 4096 buckets over [vmin, vmax]
+    const int NB = 4096;
+    const double width = ((double)vmax - (double)vmin + 1.0) / NB;
+    std::vector<uint64_t> hist(NB, 0);
+    for (uint64_t j = 0; j < n; j++) hist[std::min<int64_t>(NB - 1, (int64_t)(((double)h0[j] - (double)vmin) / width))]++;
+    std::vector<int64_t> bounds;   // exclusive upper value bounds of the ranges
+    uint64_t acc = 0;
+    const uint64_t target = (n + parts - 1) / parts;
+    for (int b = 0; b < NB; b++) {
+        acc += hist[b];
+        if (acc >= target && b + 1 < NB) {
+            bounds.push_back(vmin + (int64_t)std::ceil((b + 1) * width));
+            acc = 0;
+        }
+    }
+    bounds.push_back(vmax + 1);
+    // one pass puts every row in its range (bounds ascending)
+    const size_t R = bounds.size();
+    std::vector<std::vector<std::vector<int32_t>>> part(R, std::vector<std::vector<int32_t>>(nc));
+    for (uint64_t j = 0; j < n; j++) {
+        const size_t q = (size_t)(std::upper_bound(bounds.begin(), bounds.end(), (int64_t)h0[j]) - bounds.begin());
+        for (int c = 0; c < nc; c++) part[q][c].push_back(r->h_cols[P.colord[i][c]][j]);
+    }
+    for (size_t q = 0; q < R; q++) {
+        std::vector<std::vector<int32_t>> hc = std::move(part[q]);
+        const uint64_t m = hc[0].size();
+        if (m == 0) continue;
+        std::vector<DBuf<int32_t>> dc(nc);
+        const int32_t *cols[TRIE_MAX_LEVELS];
+        for (int c = 0; c < nc; c++) {
+            AMJ_TRY(dc[c].alloc(ctx, m));
+            AMJ_CUDA_TRY(cudaMemcpyAsync(dc[c].p, hc[c].data(), m * 4, cudaMemcpyHostToDevice, ctx->stream));
+            cols[c] = dc[c].p;
+        }
+        AMJ_TRY(add(cols, m));
+    }
+    return AMJ_OK;
+}
+
+__global__ void rebase_offsets_kernel(uint64_t *off, uint64_t n, uint64_t base) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        off[i] -= base;
+}
+
+// The device copy of one trie's slice (level-0 entries [i0, i1)).
+struct DevSlice {
+    uint64_t i0 = ~0ull, i1 = ~0ull;   // the slice the buffers hold
+    uint64_t cap[TRIE_MAX_LEVELS] = {};
+    DBuf<int32_t> data[TRIE_MAX_LEVELS];
+    DBuf<uint64_t> off[TRIE_MAX_LEVELS - 1];
+};
+
+static int provision(amj_ctx *ctx, const HostTrie &H, uint64_t i0, uint64_t i1, DevSlice *S, GenTrie *g,
+                     uint64_t *copied) {
+    uint64_t s[TRIE_MAX_LEVELS], e[TRIE_MAX_LEVELS];
+    H.ranges(i0, i1, s, e);
+    if (S->i0 != i0 || S->i1 != i1) {
+        for (int l = 0; l < H.levels; l++) {
+            const uint64_t m = e[l] - s[l];
+            if (m + TRIE_LEVEL1_PAD > S->cap[l]) {
+                S->cap[l] = std::max<uint64_t>(m + TRIE_LEVEL1_PAD, S->cap[l] * 3 / 2);
+                AMJ_TRY(S->data[l].alloc(ctx, S->cap[l]));
+                if (l + 1 < H.levels) AMJ_TRY(S->off[l].alloc(ctx, S->cap[l] + 1));
+            }
+            if (m) AMJ_CUDA_TRY(cudaMemcpyAsync(S->data[l].p, H.data[l] + s[l], m * 4, cudaMemcpyHostToDevice,
+                                                ctx->stream));
+            *copied += 4 * m;
+            if (l + 1 < H.levels) {
+                AMJ_CUDA_TRY(cudaMemcpyAsync(S->off[l].p, H.off[l] + s[l], (m + 1) * 8, cudaMemcpyHostToDevice,
+                                             ctx->stream));
+                *copied += 8 * (m + 1);
+                const uint64_t base = H.off[l][s[l]];
+                if (base) {
+                    note_launch(ctx);
+                    rebase_offsets_kernel<<<gen_grid(ctx, m + 1), 256, 0, ctx->stream>>>(S->off[l].p, m + 1, base);
+                    AMJ_CUDA_TRY(cudaGetLastError());
+                }
+            }
+        }
+        S->i0 = i0;
+        S->i1 = i1;
+    }
+    std::memset(g, 0, sizeof(*g));
+    g->levels = H.levels;
+    for (int l = 0; l < H.levels; l++) g->data[l] = S->data[l].p;
+    for (int l = 0; l + 1 < H.levels; l++) g->off[l] = S->off[l].p;
+    g->len0 = i1 - i0;
+    if (H.levels == 2) {
+        g->two.data0 = g->data[0];
+        g->two.off0 = g->off[0];
+        g->two.data1 = g->data[1];
+        g->two.len0 = g->len0;
+        g->two.rp_count = 0;   // no dense row pointers: child lists by binary search
+    }
+    return AMJ_OK;
+}
+
+int lftj_generic_ooc_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int flags, const uint32_t *order,
+                             amj_result *out) {
+    cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
+    AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
+    GenPlan P;
+    AMJ_TRY(gen_plan(rels, nrels, order, &P));
+    result_init(out, P.k);
+    uint64_t budget = ctx->opts.mem_budget;
+    if (!budget) {
+        size_t fr = 0, tot = 0;
+        AMJ_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+        budget = fr / 2;
+    }
+    // host tries, one per distinct (relation, column order)
+    std::vector<std::unique_ptr<HostTrie>> hosts;
+    std::vector<int> host_of(nrels, -1);
+    for (int i = 0; i < nrels; i++) {
+        for (int j = 0; j < i && host_of[i] < 0; j++)
+            if (rels[j] == rels[i] || (rels[j]->d_cols[0] == rels[i]->d_cols[0] && rels[j]->h_cols[0] == rels[i]->h_cols[0] &&
+                                       rels[j]->n == rels[i]->n && P.ncols[j] == P.ncols[i])) {
+                bool same = true;
+                for (int c = 0; c < P.ncols[i]; c++)
+                    same &= rels[j]->d_cols[P.colord[j][c]] == rels[i]->d_cols[P.colord[i][c]] &&
+                            rels[j]->h_cols[P.colord[j][c]] == rels[i]->h_cols[P.colord[i][c]];
+                if (same) host_of[i] = host_of[j];
+            }
+        if (host_of[i] >= 0) continue;
+        hosts.emplace_back(new HostTrie());
+        host_of[i] = (int)hosts.size() - 1;
+        AMJ_TRY(build_host_trie(ctx, rels[i], P, i, budget, hosts.back().get()));
+    }
+    AMJ_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
+    // the tries each attribute heads (level 0 in binding order), and the
+    // budget share of each attribute: in proportion to its tries
+    std::vector<std::vector<int>> heads(P.k);
+    for (int i = 0; i < nrels; i++) heads[P.pos[rels[i]->attrs[P.colord[i][0]]]].push_back(i);
+    // value ranges per heading attribute: the longest ranges whose heading
+    // slices fit the share (at least one value per range)
+    std::vector<std::vector<std::pair<int64_t, int64_t>>> ranges(P.k);
+    for (int l = 0; l < P.k; l++) {
+        if (heads[l].empty()) continue;
+        const uint64_t share = std::max<uint64_t>(1, budget / (uint64_t)nrels * heads[l].size());
+        int64_t vmin = INT64_MAX, vmax = INT64_MIN;
+        for (int i : heads[l]) {
+            const HostTrie &H = *hosts[host_of[i]];
+            if (H.len[0]) {
+                vmin = std::min<int64_t>(vmin, H.data[0][0]);
+                vmax = std::max<int64_t>(vmax, H.data[0][H.len[0] - 1]);
+            }
+        }
+        if (vmin > vmax) {   // every heading trie is empty: no result
+            ranges.assign(P.k, {});
+            break;
+        }
+        auto fits = [&](int64_t lo, int64_t hi) {
+            uint64_t b = 0;
+            for (int i : heads[l]) {
+                const HostTrie &H = *hosts[host_of[i]];
+                uint64_t i0, i1;
+                H.value_range(lo, hi, &i0, &i1);
+                b += H.bytes(i0, i1);
+            }
+            return b <= share;
+        };
+        int64_t lo = vmin;
+        while (lo <= vmax) {
+            int64_t a = lo, b = vmax;   // the largest hi in [lo, vmax] that fits (at least lo)
+            if (fits(lo, vmax)) a = vmax;
+            else
+                while (a < b) {
+                    const int64_t m = a + (b - a + 1) / 2;
+                    if (fits(lo, m)) a = m;
+                    else b = m - 1;
+                }
+            ranges[l].push_back({lo, a});
+            lo = a + 1;
+        }
+    }
+    // the combinations: one range per heading attribute (odometer order, the
+    // deepest attribute fastest, so the slices of the outer ones stay)
+    std::vector<int> lvls;
+    for (int l = 0; l < P.k; l++)
+        if (!heads[l].empty()) lvls.push_back(l);
+    bool empty = false;
+    for (int l : lvls) empty |= ranges[l].empty();
+    // relations over the same host trie and heading attribute share one
+    // device slice (the views of a self-join)
+    std::vector<int> slot(nrels);
+    for (int i = 0; i < nrels; i++) {
+        slot[i] = i;
+        const int li = P.pos[rels[i]->attrs[P.colord[i][0]]];
+        for (int j = 0; j < i; j++)
+            if (host_of[j] == host_of[i] && P.pos[rels[j]->attrs[P.colord[j][0]]] == li) {
+                slot[i] = slot[j];
+                break;
+            }
+    }
+    GenQuery Q;
+    gen_query_from_plan(P, &Q);
+    AMJ_TRY(Q.dtries.alloc(ctx, nrels));
+    std::vector<DevSlice> slices(nrels);
+    std::vector<GenTrie> ht(nrels);
+    std::vector<size_t> idx(lvls.size(), 0);
+    const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
+    std::vector<std::vector<int32_t>> hcols(materialize ? P.k : 0);
+    uint64_t count = 0, checksum = 0, combos = 0, copied = 0;
+    while (!empty) {
+        for (size_t j = 0; j < lvls.size(); j++) {
+            const auto rg = ranges[lvls[j]][idx[j]];
+            for (int i : heads[lvls[j]]) {
+                if (slot[i] != i) continue;
+                const HostTrie &H = *hosts[host_of[i]];
+                uint64_t i0, i1;
+                H.value_range(rg.first, rg.second, &i0, &i1);
+                AMJ_TRY(provision(ctx, H, i0, i1, &slices[i], &ht[i], &copied));
+            }
+        }
+        for (int i = 0; i < nrels; i++) ht[i] = ht[slot[i]];
+        AMJ_CUDA_TRY(cudaMemcpyAsync(Q.dtries.p, ht.data(), nrels * sizeof(GenTrie), cudaMemcpyHostToDevice, ctx->stream));
+        uint64_t c = 0, h = 0;
+        AMJ_TRY(gen_pass(ctx, Q, nullptr, 0, &c, &h, nullptr));
+        if (materialize && c) {
+            std::vector<DBuf<int32_t>> dc(P.k);
+            int32_t *cols[AMJ_MAX_ATTRS] = {};
+            for (int a = 0; a < P.k; a++) {
+                AMJ_TRY(dc[a].alloc(ctx, c));
+                cols[a] = dc[a].p;
+            }
+            uint64_t c2 = 0, h2 = 0, w = 0;
+            AMJ_TRY(gen_pass(ctx, Q, cols, c, &c2, &h2, &w));
+            if (c2 != c || h2 != h || w != c) return fail(AMJ_ECUDA, "LFTJ ooc: write pass disagrees with count pass");
+            for (int a = 0; a < P.k; a++) {
+                const size_t old = hcols[a].size();
+                hcols[a].resize(old + c);
+                AMJ_CUDA_TRY(cudaMemcpyAsync(hcols[a].data() + old, cols[a], c * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            }
+            AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        }
+        count += c;
+        checksum += h;
+        combos++;
+        // next combination
+        int j = (int)lvls.size() - 1;
+        while (j >= 0 && ++idx[j] == ranges[lvls[j]].size()) idx[j--] = 0;
+        if (j < 0) break;
+    }
+    out->count = count;
+    out->checksum = checksum;
+    out->stats[7] = combos;     // slice combinations joined
+    if (materialize) {
+        auto *o = new ResultOwner();
+        o->ctx = ctx;
+        out->priv = o;
+        out->rows = count;
+        out->on_host = 1;
+        for (int a = 0; a < P.k; a++) {
+            if (cudaMallocHost((void **)&out->cols[a], (count ? count : 1) * 4) != cudaSuccess) {
+                (void)cudaGetLastError();
+                amj_result_release(out);
+                return fail(AMJ_ENOMEM, "LFTJ ooc: pinned result allocation failed");
+            }
+            if (count) std::memcpy(out->cols[a], hcols[a].data(), count * 4);
+        }
+    }
+    AMJ_CUDA_TRY(cudaEventRecord(e2, ctx->stream));
+    AMJ_CUDA_TRY(cudaEventSynchronize(e2));
+    out->build_ms = event_ms(e0, e1);
+    out->probe_ms = event_ms(e1, e2);
+    out->total_ms = event_ms(e0, e2);
+    if (materialize) {
+        const int rc = finish_result_columns(ctx, out, flags);
+        if (rc != AMJ_OK) {
+            amj_result_release(out);
+            return rc;
+        }
+    }
     return AMJ_OK;
 }
 
@@ -442,8 +918,7 @@ int lftj_generic_compile(amj_ctx *ctx, amj_rel *const *rels, int nrels, const ui
 // with AMJ_F_MATERIALIZE a write pass into exactly allocated columns.
 int lftj_generic_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int ooc, int flags, const uint32_t *order,
                          amj_result *out) {
-    if (ooc) return fail(AMJ_EUNSUPPORTED, "LFTJ: no out-of-core form beyond the triangle (the generic join is "
-                                           "already memory-bounded)");
+    if (ooc) return lftj_generic_ooc_execute(ctx, rels, nrels, flags, order, out);
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
     GenQuery Q;

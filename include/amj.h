@@ -163,7 +163,16 @@ int  amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *rels, int nr
  * nrels == 3 carrying (0,1), (1,2), (0,2): the triangle over three relations.
  * any other nrels >= 3 (up to 16): the connected join of relations of 1 to 8
  *             columns over attributes 0..k-1, k <= 8 (the reference's LFTJ
- *             stops at 3 attributes and 3 tables of 2 columns); ooc = 0.
+ *             stops at 3 attributes and 3 tables of 2 columns).
+ * ooc = 1 (every shape; OOCWrapper, LFTJ-GPU/ooc_wrapper.cuh:14-427): the
+ *             tries live in pinned host memory (a relation kept on the host,
+ *             AMJ_MEM_HOST_STREAMED, has its trie built in value ranges of
+ *             its first column); opts.mem_budget (0: half the free device
+ *             memory) is split over the attributes that head tries, each
+ *             such attribute's values are cut into ranges whose trie slices
+ *             fit its share, and every combination of ranges is joined on
+ *             the device (stats "slices" counts them).  Relations kept on the
+ *             host need ooc = 1.
  * nrels == 2 is rejected, as in the reference (LFTJ-GPU/exec_LFTJ.cu:92-95).
  * 2-column relations are joined as sets (leapfrog triejoin semantics): a
  * repeated row counts once; tries of 3 or more columns keep repeated rows in

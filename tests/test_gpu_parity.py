@@ -530,8 +530,8 @@ def test_lftj_clique4_materialized_and_rejections(ctx):
     assert np.array_equal(sorted_rows(got.columns), sorted_rows(m.columns))
     with pytest.raises(AmjError):
         ctx.lftj([e], algo="BFS", clique4=True)
-    with pytest.raises(AmjError):
-        ctx.lftj([e], algo="DFS", clique4=True, ooc=1)
+    ooc = ctx.lftj([e], algo="DFS", clique4=True, ooc=1)
+    assert (ooc.count, ooc.checksum) == (cnt, chk)
     empty = ctx.relation([np.zeros(0, np.int32), np.zeros(0, np.int32)], [0, 1])
     r = ctx.lftj([empty], clique4=True)
     assert (r.count, r.checksum) == (0, 0)
@@ -653,8 +653,8 @@ def test_lftj_self_join_in_other_orders(ctx, clique4):
         assert (lambda r: (r.count, r.checksum))(ctx.lftj(hs, attr_order=(2, 0, 1))) == want
     with pytest.raises(AmjError):
         ctx.lftj([e], attr_order=(0, 0, 1))
-    with pytest.raises(AmjError):
-        ctx.lftj([e], attr_order=(1, 0, 2), ooc=1)
+    ooc = ctx.lftj([e], clique4=clique4, attr_order=(1, 0, 2, 3)[:4 if clique4 else 3], ooc=1)
+    assert (ooc.count, ooc.checksum) == want
 
 
 @pytest.mark.parametrize("order", [None, (2, 0, 1, 3), (3, 2, 1, 0)])
@@ -694,8 +694,8 @@ def test_lftj_generic_materialized_and_rejections(ctx):
     with pytest.raises(AmjError) as e:
         ctx.lftj(bad)
     assert e.value.status == L.AMJ_EUNSUPPORTED
-    with pytest.raises(AmjError):
-        ctx.lftj(hs, ooc=1)
+    ooc = ctx.lftj(hs, ooc=1)
+    assert (ooc.count, ooc.checksum) == (cnt, chk)
 
 
 @pytest.mark.parametrize("rankbits", [0, 32, 1000])
@@ -775,15 +775,49 @@ def test_lftj_joins_relations_as_sets(ctx):
 
 
 def test_lftj_out_of_core_slices():
-    with Context(0, ooc_slice_rows=5000) as ctx:
-        s, d = data.rmat(11, 30000, 0.57, 0.19, 0.19, 7)
+    """ooc=1 (the reference's OOCWrapper, LFTJ-GPU/ooc_wrapper.cuh): tries in
+    pinned host memory, a memory budget split over the heading attributes,
+    value-range slices of the tries joined combination by combination.  A
+    budget far below the tries' size forces many slices; every shape gives
+    the in-memory result and the oracle's."""
+    s, d = data.rmat(11, 30000, 0.57, 0.19, 0.19, 7)
+    want = O.triangle(s, d)
+    four = O.four_clique(s, d)
+    with Context(0, mem_budget=64 << 10) as ctx:
         e = ctx.relation([s, d], [0, 1])
-        want = O.triangle(s, d)
         for algo in ("DFS", "BFS"):
             got = ctx.lftj([e], algo=algo, ooc=1, materialize=True)
             assert (got.count, got.checksum) == want
             assert data.checksum(got.columns) == want[1]
-            assert got.stats["slices"] > 1
+            assert got.stats["slices"] >= 4
+        got = ctx.lftj([e], clique4=True, ooc=1)
+        assert (got.count, got.checksum) == four and got.stats["slices"] >= 4
+        got = ctx.lftj([e], ooc=1, attr_order=(2, 0, 1))
+        assert (got.count, got.checksum) == want
+        # three relations of the triangle, and a 4-cycle of distinct relations
+        hs = [ctx.relation([s, d], [0, 1]), ctx.relation([s, d], [1, 2]), ctx.relation([s, d], [0, 2])]
+        assert (lambda r: (r.count, r.checksum))(ctx.lftj(hs, ooc=1)) == want
+    rels = [distinct_rel(3000, 200, 90 + i, list(p)) for i, p in enumerate(GENERIC_QUERIES["4-cycle"])]
+    with Context(0, mem_budget=8 << 10) as ctx:
+        got = ctx.lftj([ctx.relation(c, a) for c, a in rels], ooc=1)
+        assert (got.count, got.checksum) == O.mhj(rels) and got.stats["slices"] >= 4
+
+
+def test_lftj_out_of_core_host_resident_relation():
+    """A relation kept in pinned host memory (streamed=True) never enters the
+    device whole: its trie is built in value ranges of its first column that
+    fit the budget, and the join runs on slices."""
+    import torch
+    s, d = data.rmat(13, 120000, 0.57, 0.19, 0.19, 8)
+    want = O.triangle(s, d)
+    with Context(0, mem_budget=256 << 10) as ctx:
+        pinned = [torch.from_numpy(s).pin_memory(), torch.from_numpy(d).pin_memory()]
+        e = ctx.relation([pinned[0].numpy(), pinned[1].numpy()], [0, 1], streamed=True)
+        got = ctx.lftj([e], ooc=1)
+        assert (got.count, got.checksum) == want
+        assert got.stats["slices"] >= 4
+        with pytest.raises(AmjError):
+            ctx.lftj([e], ooc=0)
 
 
 def test_lftj_rejects_two_relations_and_edge_cases(ctx):
