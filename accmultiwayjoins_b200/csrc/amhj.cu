@@ -19,6 +19,7 @@
 #include "amhj_host.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <tuple>
@@ -824,9 +825,34 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
 
-    for (int i = 0; i < nrels; i++)
-        if (rels[i]->where == AMJ_MEM_HOST_STREAMED && !(i == 0 && ooc))
-            return fail(AMJ_EINVAL, "amhj_execute: only the probe relation of an ooc=1 query may stay on the host");
+    bool host_builds = false;
+    for (int i = 1; i < nrels; i++) host_builds |= rels[i]->where == AMJ_MEM_HOST_STREAMED;
+    if (rels[0]->where == AMJ_MEM_HOST_STREAMED && !ooc)
+        return fail(AMJ_EINVAL, "amhj_execute: a relation kept on the host needs ooc=1");
+    if (host_builds) {
+        // build relations in host memory: the staged, partitioned form
+        if (!ooc) return fail(AMJ_EINVAL, "amhj_execute: a relation kept on the host needs ooc=1");
+        if (query_type != AMJ_QUERY_NORMAL || hp.L == 0)
+            return fail(AMJ_EUNSUPPORTED, "amhj_execute: host-resident build relations need a NORMAL query");
+        // the part joins reuse the context's events: time the stages on the host
+        const auto t0 = std::chrono::steady_clock::now();
+        int rc = amhj_partitioned_execute(ctx, hp, use_ws ? 1 : 0, dro, flags, out);
+        if (rc != AMJ_OK) {
+            amj_result_release(out);
+            return rc;
+        }
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        out->total_ms = out->probe_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (materialize) {
+            rc = finish_result_columns(ctx, out, flags);
+            if (rc != AMJ_OK) {
+                amj_result_release(out);
+                return rc;
+            }
+        }
+        return AMJ_OK;
+    }
 
     ExecScratch X;
     // ---- build phase

@@ -58,4 +58,9 @@ void fill_level_desc(const LevelSpec &ls, int layout, int key_mode, uint32_t mas
 // Plan fields that depend only on the query and the options (levels excluded).
 void plan_common(const HostPlan &hp, const amj_opts &o, ProbePlan *P);
 
+// ooc = 1 with build relations in host memory: the join in stages, each a
+// hash partition of the intermediate result and one build relation into
+// parts that fit the memory budget, joined part by part (amhj_partitioned.cu).
+int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, int flags, amj_result *out);
+
 }  // namespace amj

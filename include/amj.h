@@ -153,7 +153,15 @@ int  amj_rel_info(const amj_rel *rel, uint64_t *n, int *ncols, uint32_t *attrs);
  * query order; each build relation is hashed on its first column.  TRI and
  * FOUR take one 2-column edge relation (nrels == 1).  Results follow the
  * multi-attribute compare semantics (every attribute already bound is
- * compared, MHJ-GPU/common_kernels.cuh:41-53). */
+ * compared, MHJ-GPU/common_kernels.cuh:41-53).
+ * ooc = 1 (OOC::execute, MHJ-GPU/ooc.cuh:77-307): the probe relation is
+ * joined in slices; when it is kept in host memory (AMJ_MEM_HOST_STREAMED)
+ * the slices are staged on a side stream.  When build relations are kept in
+ * host memory too (NORMAL queries), the join runs in stages, one per build
+ * relation: the intermediate result and the build relation are
+ * hash-partitioned on the key into parts within opts.mem_budget (0: half the
+ * free device memory) and joined part by part (stats "slices" counts the
+ * part joins).  Relations kept in host memory need ooc = 1. */
 int  amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *rels, int nrels,
                       int ooc, int ws, int dro, int fib, int flags, amj_result *out);
 

@@ -419,6 +419,42 @@ def test_amhj_out_of_core_streamed_large_slices():
                 assert got.stats["slices"] == 4
 
 
+@pytest.mark.parametrize("shape", ["chain4", "star4", "cyclic"])
+def test_amhj_out_of_core_build_relations_in_host_memory(shape):
+    """Build relations kept in host memory (streamed=True) with ooc=1: the
+    join runs in stages, each intermediate and build relation hash-partitioned
+    on the key into parts within the memory budget (far below the inputs
+    here), joined part by part.  Equal to the device-resident join and to the
+    oracle, for every switch."""
+    if shape == "chain4":
+        n = 200_000
+        rels = [([data.uniform(n, 0, n, 51 + i, 0), data.uniform(n, 0, n, 51 + i, 1)], [i, i + 1]) for i in range(4)]
+    elif shape == "star4":
+        fact, dims = data.star_relations(150_000, [20000, 5000, 2000, 300], theta=1.1, seed=9)
+        rels = [fact] + dims
+    else:   # a cycle closed by the last relation: a compared attribute besides the key
+        rels = [([data.uniform(30000, 0, 3000, 61 + i, 0), data.uniform(30000, 0, 3000, 61 + i, 1)], p)
+                for i, p in enumerate([[0, 1], [1, 2], [2, 3], [3, 0]])]
+    want = O.mhj(rels)
+    with Context(0, mem_budget=512 << 10) as ctx:
+        dev = [ctx.relation(c, a) for c, a in rels]
+        assert (lambda r: (r.count, r.checksum))(ctx.amhj("NORMAL", dev)) == want
+        host = [ctx.relation(c, a, streamed=True) for c, a in rels]
+        for sw in ({}, {"ws": 1}, {"dro": 1}):
+            got = ctx.amhj("NORMAL", host, ooc=1, **sw)
+            assert (got.count, got.checksum) == want, sw
+            assert got.stats["slices"] >= 4
+        # a device probe with host builds, and the materialised tuples
+        got = ctx.amhj("NORMAL", [dev[0]] + host[1:], ooc=1, materialize=True)
+        assert (got.count, got.checksum) == want
+        assert data.checksum(got.columns) == want[1]
+        if shape == "cyclic":
+            cnt, chk, cols = O.mhj(rels, tuples=True)
+            assert np.array_equal(sorted_rows(got.columns), sorted_rows(cols))
+        with pytest.raises(AmjError):
+            ctx.amhj("NORMAL", host, ooc=0)
+
+
 def test_amhj_edge_cases(ctx):
     z = np.zeros(0, np.int32)
     one = ([np.array([3], np.int32), np.array([4], np.int32)], [0, 1])
