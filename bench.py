@@ -746,6 +746,87 @@ def run_serve(args, rank, world, local_rank):
     ctx.close()
 
 
+def run_ooc(args, rank, world, local_rank):
+    """The out-of-core chain of the serving configuration on its own:
+    R1(a,b) R2(b,c) R3(c,d) R4(d,e) of --ooc-rows rows each, keys uniform in
+    [0, rows) (about one match per probe row per join), every relation kept
+    in pinned host memory.  One step is one ooc=1 query through the staged,
+    partitioned join (amhj_partitioned.cu) under a memory budget of
+    --ooc-budget-gb; the result is checked against the probe-streaming path
+    with device-resident builds (when they fit the device) and, with
+    --ooc-verify, against the oracle or the reference's MHJ-CPU on the host."""
+    import torch
+    from accmultiwayjoins_b200 import Context, data
+    torch.cuda.set_device(local_rank)
+    n = args.ooc_rows
+    t0 = time.perf_counter()
+    # every column generated straight into pinned host memory (no second copy)
+    pinned = []
+    for i in range(4):
+        cols = []
+        for s_ in (0, 1):
+            t = torch.empty(n, dtype=torch.int32, pin_memory=True)
+            t.numpy()[:] = data.uniform(n, 0, n, 41 + i + 10 * rank, s_)
+            cols.append(t)
+        pinned.append(cols)
+    rels = [([c.numpy() for c in pc], [i, i + 1]) for i, pc in enumerate(pinned)]
+    gen_s = time.perf_counter() - t0
+    budget = int(args.ooc_budget_gb * (1 << 30))
+    ctx = Context(local_rank, mem_budget=budget, spin_limit_ms=args.spin_limit_ms)
+    host = [ctx.relation(c, a, streamed=True) for c, a in rels]
+    for _ in range(args.warmup):
+        r = ctx.amhj("NORMAL", host, ooc=1)
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    ms = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        r = ctx.amhj("NORMAL", host, ooc=1)
+        ms.append((time.perf_counter() - t1) * 1e3)
+    clocks = sampler.stop()
+    want = (r.count, r.checksum)
+    check = {}
+    try:
+        dev = [ctx.relation(c, a) for c, a in rels[1:]]
+        x = ctx.amhj("NORMAL", [host[0]] + dev, ooc=1)
+        check["device_builds_equal"] = (x.count, x.checksum) == want
+        for d in dev:
+            d.release()
+    except Exception as e:   # builds that do not fit the device
+        check["device_builds"] = f"not run: {e}"
+    if args.ooc_verify != "none":
+        # the reference's MHJ-CPU keeps every result tuple and two hash tables
+        # of 16-byte entries per build relation in host memory; the oracle's
+        # restatement counts and hashes without keeping them
+        from oracle import oracle as O
+        t1 = time.perf_counter()
+        if args.ooc_verify == "reference":
+            cnt, chk, _ = O.mhj_reference(rels, nthreads=os.cpu_count() or 1)
+        else:
+            cnt, chk = O.mhj(rels, nthreads=os.cpu_count() or 1)
+        check[f"{args.ooc_verify}_equal"] = (cnt, chk) == want
+        check[f"{args.ooc_verify}_seconds"] = time.perf_counter() - t1
+    if rank == 0:
+        m = sum(ms) / len(ms)
+        line = {
+            "metric": METRIC, "value": r.count / (m * 1e-3), "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+            "config": {"workload": f"out-of-core 4-way chain R1(a,b)R2(b,c)R3(c,d)R4(d,e), 4 x {n} rows, keys "
+                                   f"U[0,{n}), all relations in pinned host memory; staged hash-partitioned join "
+                                   f"under a {args.ooc_budget_gb:g} GB device budget",
+                       "output_tuples": r.count, "checksum": f"{r.checksum:016x}", "part_joins": r.stats["slices"],
+                       "input_bytes": 32 * n, "generation_s": gen_s},
+            "e2e": {"value": r.count / (m * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": 32 * n,
+                    "d2h_bytes_per_step": 16, "note": "inputs start in host memory every step"},
+            "check": check, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    for h in host:
+        h.release()
+    ctx.close()
+
+
 def Batch_default_opts(L):
     o = L.amj_batch_opts()
     o.block_size, o.task_chunk = 256, 1024
@@ -844,6 +925,26 @@ def run_reference(args, rank, world):
         sec = sum(t for _, t in vals)
         cpu = {"unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample + "; step i starts at query i"}
         print(json.dumps(reference_line(args, tuples / sec, sec / len(vals) * 1e3, wl.describe(""), cpu)),
+              flush=True)
+        return
+    if args.workload == "ooc":
+        # the reference has no out-of-core form for build relations (its
+        # ooc=1 keeps them on the GPU): MHJ-CPU joins the same generator's
+        # chain at 4 x min(rows, 2^24) rows on the host, one full call per step
+        m = min(args.ooc_rows, 1 << 24)
+        rels = [([gen.uniform(m, 0, m, 41 + i, 0), gen.uniform(m, 0, m, 41 + i, 1)], [i, i + 1]) for i in range(4)]
+        step = lambda: O.mhj_reference(rels, nthreads=cores)[::2]  # noqa: E731  (count, seconds)
+        kind = "reference" if O.ref_available() else "port"
+        desc = f"out-of-core 4-way chain, keys U[0,rows); sample: 4 x {m} rows"
+        sample = "the chain of the same generator at 4 x min(rows, 2^24) rows, MHJ-CPU TBJ call timed"
+        times, tuples = [], 0
+        for i in range(args.warmup + args.steps):
+            cnt, sec = step()
+            if i >= args.warmup:
+                times.append(sec)
+                tuples += cnt
+        cpu = {"unit": "tuples/s", "cores": cores, "kind": kind, "sample": sample}
+        print(json.dumps(reference_line(args, tuples / sum(times), sum(times) / len(times) * 1e3, desc, cpu)),
               flush=True)
         return
     if args.workload == "chain":
@@ -1059,7 +1160,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--algo", default="DFS", choices=["DFS", "BFS", "AMHJ"])
-    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain", "four", "batch", "serve"])
+    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain", "four", "batch", "serve", "ooc"])
     ap.add_argument("--spin-limit-ms", type=int, default=5000, help="bound on every device-side wait")
     ap.add_argument("--rate", type=float, default=200.0, help="serve workload: requests per second")
     ap.add_argument("--lanes", type=int, default=3, help="serve workload: batches in flight")
@@ -1067,6 +1168,9 @@ def main():
     ap.add_argument("--ooc-rows", type=int, default=64 << 20, help="serve workload: rows per ooc relation")
     ap.add_argument("--ooc-every", type=float, default=2.5, help="serve workload: seconds between ooc joins")
     ap.add_argument("--ooc-slice", type=int, default=8 << 20, help="serve workload: ooc probe slice rows")
+    ap.add_argument("--ooc-budget-gb", type=float, default=8.0, help="ooc workload: device memory budget")
+    ap.add_argument("--ooc-verify", default="none", choices=["none", "oracle", "reference"],
+                    help="ooc workload: also check the result on the host (the oracle, or the reference MHJ-CPU)")
     ap.add_argument("--queries", type=int, default=512, help="batch workload: queries per batch")
     ap.add_argument("--min-rows", type=int, default=10_000, help="batch workload: smallest relation")
     ap.add_argument("--max-rows", type=int, default=4_000_000, help="batch workload: largest relation")
@@ -1077,7 +1181,9 @@ def main():
                     help="triangle workload: skip the chain and batched records carried on the line")
     args = ap.parse_args()
     if args.impl == "ours":
-        args.warmup = max(args.warmup, 3)
+        # the out-of-core chain runs a minute or more per step at full size:
+        # one warm-up step there, three everywhere else
+        args.warmup = max(args.warmup, 1 if args.workload == "ooc" else 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -1093,6 +1199,8 @@ def main():
         run_batch(args, rank, world, local_rank)
     elif args.workload == "serve":
         run_serve(args, rank, world, local_rank)
+    elif args.workload == "ooc":
+        run_ooc(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
     if world > 1:
