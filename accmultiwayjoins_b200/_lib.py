@@ -37,7 +37,8 @@ AMJ_QUERY_NORMAL, AMJ_QUERY_TRI, AMJ_QUERY_FOUR = 0, 1, 2
 AMJ_LFTJ_BFS, AMJ_LFTJ_DFS = 0, 1
 AMJ_LAYOUT_BUCKET, AMJ_LAYOUT_OPEN_ADDR, AMJ_LAYOUT_CUCKOO = 0, 1, 2
 AMJ_F_MATERIALIZE, AMJ_F_HOST_RESULT, AMJ_F_NO_REORDER, AMJ_F_CLIQUE4 = 0x1, 0x2, 0x4, 0x8
-AMJ_F_KEEP_ORDER, AMJ_F_DEGREE_ORDER = 0x10, 0x20
+AMJ_F_KEEP_ORDER, AMJ_F_DEGREE_ORDER, AMJ_F_CLIQUE4_LISTS = 0x10, 0x20, 0x40
+AMJ_F_THREAD_PER_ROW, AMJ_F_PAIRWISE, AMJ_F_HASH_PLAN = 0x80, 0x100, 0x200
 AMJ_MEM_DEVICE, AMJ_MEM_HOST, AMJ_MEM_HOST_STREAMED = 0, 1, 2
 
 
@@ -235,6 +236,7 @@ SIGNATURES = {
     "amj_edgelist_read": (C.c_int, [C.c_char_p, C.c_int, _I32P, _I32P, C.c_uint64, _U64P]),
     "amj_edgelist_to_db": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, _U64P]),
     "amj_edgelist_to_tr": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_int, _U64P]),
+    "amj_tbl_to_db": (C.c_int, [C.c_char_p, _U32P, _U32P, C.c_int, C.c_char_p, C.c_char_p, C.c_uint64, _U64P]),
 }
 
 _lib = None

@@ -353,9 +353,15 @@ class Context:
         return out
 
     def amhj(self, query_type, relations: Sequence[Relation], ooc: int = 0, ws: int = 0, dro: int = 0,
-             fib: int = 0, materialize: bool = False, reorder: bool = True, degree_order: bool = True) -> Result:
+             fib: int = 0, materialize: bool = False, reorder: bool = True, degree_order: bool = True,
+             plan: str = "multiway") -> Result:
         """degree_order=False joins a TRI / FOUR edge relation as given, never its
-        degree-ordered copy (the results are the same)."""
+        degree-ordered copy (the results are the same).  plan: "multiway" (the
+        operator; FOUR over one edge relation answers its last three levels from
+        the triangle matrices where they apply), "hash" (the operator with every
+        level a hash lookup), or a baseline to compare it with: "thread_per_row"
+        (one thread per probe row, count only) or "pairwise" (2-relation joins
+        with materialised intermediates)."""
         lib = L.load()
         qt = _QUERY[query_type] if isinstance(query_type, str) else int(query_type)
         arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
@@ -364,23 +370,29 @@ class Context:
             flags |= L.AMJ_F_NO_REORDER
         if not degree_order:
             flags |= L.AMJ_F_KEEP_ORDER
+        flags |= {"multiway": 0, "thread_per_row": L.AMJ_F_THREAD_PER_ROW, "pairwise": L.AMJ_F_PAIRWISE,
+                  "hash": L.AMJ_F_HASH_PLAN}[plan]
         res = L.amj_result()
         L.check(lib.amj_amhj_execute(self.handle, qt, arr, len(relations), int(ooc), int(ws), int(dro), int(fib),
                                      flags, C.byref(res)), "amhj_execute")
         return self._result(res, materialize)
 
     def lftj(self, relations: Sequence[Relation], algo="DFS", ooc: int = 0, ws: int = 1,
-             materialize: bool = False, clique4: bool = False, degree_order=None, attr_order=None) -> Result:
+             materialize: bool = False, clique4: bool = False, degree_order=None, attr_order=None,
+             clique4_lists: bool = False) -> Result:
         """clique4: one edge relation joined as the 4-clique (FOUR pattern) instead of the triangle.
         degree_order: None for the operator's choice, True / False to force joining (or not) the
         degree-ordered copy of an oriented self-joined relation (same results either way).
         attr_order: the order in which attributes are bound (a permutation of 0..k-1; the
-        results are the same for every order)."""
+        results are the same for every order).
+        clique4_lists: the 4-clique by list intersections even where the triangle matrices fit."""
         lib = L.load()
         arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
         flags = (L.AMJ_F_MATERIALIZE | L.AMJ_F_HOST_RESULT) if materialize else 0
         if clique4:
             flags |= L.AMJ_F_CLIQUE4
+            if clique4_lists:
+                flags |= L.AMJ_F_CLIQUE4_LISTS
         if degree_order is True:
             flags |= L.AMJ_F_DEGREE_ORDER
         elif degree_order is False:

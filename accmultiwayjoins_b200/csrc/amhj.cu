@@ -17,6 +17,7 @@
 //  - such filters move to the earliest level at which their attributes are
 //    bound (AMJ_F_NO_REORDER keeps the query order).
 #include "amhj_host.h"
+#include "amhj_star.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -246,7 +247,65 @@ struct PassResult {
 };
 
 static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bool dro, bool materialize,
-                      uint64_t row_lo, uint64_t row_hi, PassResult *pr, amj_result *res) {
+                      uint64_t row_lo, uint64_t row_hi, PassResult *pr, amj_result *res, bool allow_flat = true);
+
+// Count mode of a star plan (amhj_star.cuh): the flat kernel, then the DFS
+// kernel over the rows whose match product was too large for one thread.
+static int run_star_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, uint64_t row_lo, uint64_t row_hi,
+                          PassResult *pr, amj_result *res) {
+    ProbePlan &P = PL.P;
+    P.row_lo = row_lo;
+    P.row_hi = row_hi;
+    const uint64_t rows = row_hi - row_lo;
+    struct Ctr {
+        unsigned long long count, checksum;
+        unsigned int nover, pad;
+    };
+    DBuf<Ctr> ctr;
+    DBuf<uint32_t> over;
+    AMJ_TRY(ctr.alloc(ctx, 1));
+    AMJ_TRY(over.alloc(ctx, rows ? rows : 1));
+    AMJ_CUDA_TRY(cudaMemsetAsync(ctr.p, 0, sizeof(Ctr), ctx->stream));
+    const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 8);
+    note_launch(ctx);
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
+    amhj_star_kernel<<<g ? g : 1, 256, 0, ctx->stream>>>(P, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
+    Ctr h{};
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&h, ctr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    res->kernel_ms[0] += event_ms(ctx->kev[0], ctx->kev[1]);
+    pr->count = h.count;
+    pr->checksum = h.checksum;
+    if (h.nover == 0) return AMJ_OK;
+    // the listed rows, gathered into a probe relation of their own
+    std::vector<DBuf<int32_t>> cols(P.probe_ncols);
+    int32_t *cp[AMJ_MAX_COLS] = {};
+    for (int c = 0; c < P.probe_ncols; c++) {
+        AMJ_TRY(cols[c].alloc(ctx, h.nover));
+        cp[c] = cols[c].p;
+    }
+    DBuf<int32_t *> dcp;
+    AMJ_TRY(dcp.alloc(ctx, AMJ_MAX_COLS));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(dcp.p, cp, sizeof(cp), cudaMemcpyHostToDevice, ctx->stream));
+    note_launch(ctx);
+    star_gather_kernel<<<(unsigned)std::min<uint64_t>((h.nover + 255) / 256, (uint64_t)ctx->num_sms * 8), 256, 0,
+                         ctx->stream>>>(P, over.p, h.nover, dcp.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    ProbeLaunch sub = PL;
+    for (int c = 0; c < P.probe_ncols; c++) sub.P.probe_col[c] = cp[c];
+    PassResult rest;
+    AMJ_TRY(run_passes(ctx, sub, X, ws, false, false, 0, h.nover, &rest, res, false));
+    pr->count += rest.count;
+    pr->checksum += rest.checksum;
+    return AMJ_OK;
+}
+
+static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bool dro, bool materialize,
+                      uint64_t row_lo, uint64_t row_hi, PassResult *pr, amj_result *res, bool allow_flat) {
+    if (!materialize && allow_flat && star_eligible(PL.P))
+        return run_star_count(ctx, PL, X, ws, row_lo, row_hi, pr, res);
     ProbePlan &P = PL.P;
     P.row_lo = row_lo;
     P.row_hi = row_hi;
@@ -794,6 +853,14 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
     for (int i = 0; i < nrels; i++)
         if (!rels[i]) return fail(AMJ_EINVAL, "amhj_execute: null relation");
     AMJ_CUDA_TRY(cudaSetDevice(ctx->device));
+    // FOUR over one edge relation: the pair-key levels through the triangle
+    // matrices of the degree-ranked copy, where they apply
+    if (query_type == AMJ_QUERY_FOUR && nrels == 1 && rels[0]->ncols == 2 && rels[0]->where != AMJ_MEM_HOST_STREAMED &&
+        !ooc && !(flags & (AMJ_F_KEEP_ORDER | AMJ_F_HASH_PLAN | AMJ_F_THREAD_PER_ROW | AMJ_F_PAIRWISE))) {
+        bool used = false;
+        AMJ_TRY(amhj_four_by_matrices(ctx, rels[0], flags, out, &used));
+        if (used) return AMJ_OK;
+    }
     // TRI / FOUR over an oriented edge relation: join its degree-ordered copy
     // and report every tuple sorted (the same bag; shorter hub lists)
     amj_rel ordered;
@@ -825,6 +892,30 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
 
+    if (flags & AMJ_F_PAIRWISE) {
+        if (query_type != AMJ_QUERY_NORMAL || hp.L < 1 || ooc || fib)
+            return fail(AMJ_EUNSUPPORTED, "amhj_execute: the pairwise plan takes NORMAL queries, ooc=0, fib=0");
+        for (int i = 0; i < nrels; i++)
+            if (rels[i]->where == AMJ_MEM_HOST_STREAMED) return fail(AMJ_EUNSUPPORTED, "pairwise plan: device relations");
+        const auto t0 = std::chrono::steady_clock::now();
+        int rc = amhj_pairwise_execute(ctx, hp, ws, dro, flags & ~AMJ_F_HOST_RESULT, out);
+        if (rc != AMJ_OK) {
+            amj_result_release(out);
+            return rc;
+        }
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        out->total_ms = out->probe_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        out->build_ms = 0;
+        if (materialize) {
+            rc = finish_result_columns(ctx, out, flags);
+            if (rc != AMJ_OK) {
+                amj_result_release(out);
+                return rc;
+            }
+        }
+        return AMJ_OK;
+    }
     bool host_builds = false;
     for (int i = 1; i < nrels; i++) host_builds |= rels[i]->where == AMJ_MEM_HOST_STREAMED;
     if (rels[0]->where == AMJ_MEM_HOST_STREAMED && !ooc)
@@ -938,6 +1029,35 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
         }
     } else if (ooc || hp.probe->where == AMJ_MEM_HOST_STREAMED) {
         rc = amhj_ooc_execute(ctx, PL, &X, hp.probe, use_ws, dro != 0, materialize, flags, out);
+    } else if (flags & AMJ_F_THREAD_PER_ROW) {
+        // the thread-per-row baseline (count only)
+        if (materialize || !thread_row_eligible(P)) {
+            rc = fail(AMJ_EUNSUPPORTED, "amhj_execute: the thread-per-row baseline counts over bucket indexes only");
+        } else {
+            DBuf<unsigned long long> c2;
+            rc = c2.alloc(ctx, 2);
+            if (rc == AMJ_OK && cudaMemsetAsync(c2.p, 0, 16, ctx->stream) != cudaSuccess)
+                rc = fail(AMJ_ECUDA, "thread-per-row: memset");
+            if (rc == AMJ_OK) {
+                P.row_lo = 0;
+                P.row_hi = hp.probe->n;
+                const uint64_t n = hp.probe->n;
+                note_launch(ctx);
+                (void)cudaEventRecord(ctx->kev[0], ctx->stream);
+                amhj_thread_row_kernel<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256,
+                                                                                             (uint64_t)ctx->num_sms * 8)),
+                                         256, 0, ctx->stream>>>(P, c2.p, c2.p + 1);
+                (void)cudaEventRecord(ctx->kev[1], ctx->stream);
+                unsigned long long h2[2] = {0, 0};
+                if (cudaGetLastError() != cudaSuccess ||
+                    cudaMemcpyAsync(h2, c2.p, 16, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+                    cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+                    rc = fail(AMJ_ECUDA, "thread-per-row kernel");
+                out->count = h2[0];
+                out->checksum = h2[1];
+                out->kernel_ms[0] = event_ms(ctx->kev[0], ctx->kev[1]);
+            }
+        }
     } else {
         PassResult pr;
         rc = run_passes(ctx, PL, X, use_ws, dro != 0, materialize, 0, hp.probe->n, &pr, out);

@@ -62,5 +62,10 @@ void plan_common(const HostPlan &hp, const amj_opts &o, ProbePlan *P);
 // hash partition of the intermediate result and one build relation into
 // parts that fit the memory budget, joined part by part (amhj_partitioned.cu).
 int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, int flags, amj_result *out);
+// AMJ_F_PAIRWISE: the plan as 2-relation joins with materialised intermediates.
+int amhj_pairwise_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, int flags, amj_result *out);
+// FOUR over one edge relation through the triangle matrices of its
+// degree-ranked copy (lftj_api.cu); *used is false where they do not apply.
+int amhj_four_by_matrices(amj_ctx *ctx, amj_rel *rel, int flags, amj_result *out, bool *used);
 
 }  // namespace amj

@@ -220,4 +220,65 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
     return AMJ_OK;
 }
 
+// ---- pairwise baseline (AMJ_F_PAIRWISE) ----
+// The plan as a chain of 2-relation joins on the device, each intermediate
+// result materialised before the next join: the binary-join plan a
+// multi-way join is compared with (the reference's exec_PW.cu runs such
+// plans with a pairwise radix join).  Attributes are renamed per join as in
+// the staged form above.
+int amhj_pairwise_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, int flags, amj_result *out) {
+    const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
+    amj_rel cur = *hp.probe;
+    cur.uid = 0;
+    cur.owned = false;
+    for (int c = 0; c < cur.ncols; c++) cur.attrs[c] = (uint32_t)hp.probe_attr[c];
+    amj_result prev;
+    bool have_prev = false;
+    int rc = AMJ_OK;
+    for (int j = 0; j < hp.L && rc == AMJ_OK; j++) {
+        const amj_rel *B = hp.lv[j].rel;
+        const bool last = j + 1 == hp.L;
+        std::vector<int> S;
+        for (int c = 0; c < cur.ncols; c++) S.push_back((int)cur.attrs[c]);
+        for (int c = 0; c < B->ncols; c++) S.push_back((int)B->attrs[c]);
+        std::sort(S.begin(), S.end());
+        S.erase(std::unique(S.begin(), S.end()), S.end());
+        auto rename = [&](int a) { return (uint32_t)(std::lower_bound(S.begin(), S.end(), a) - S.begin()); };
+        amj_rel pv = cur, bv = *B;
+        bv.uid = 0;
+        bv.owned = false;
+        for (int c = 0; c < pv.ncols; c++) pv.attrs[c] = rename((int)cur.attrs[c]);
+        for (int c = 0; c < bv.ncols; c++) bv.attrs[c] = rename((int)B->attrs[c]);
+        amj_rel *pair[2] = {&pv, &bv};
+        amj_result res;
+        std::memset(&res, 0, sizeof(res));
+        const int f = last ? (materialize ? AMJ_F_MATERIALIZE : 0) : AMJ_F_MATERIALIZE;
+        rc = amj_amhj_execute(ctx, AMJ_QUERY_NORMAL, pair, 2, 0, ws, dro, 0, f, &res);
+        if (rc != AMJ_OK) break;
+        if (have_prev) amj_result_release(&prev);
+        prev = res;
+        have_prev = true;
+        if (last) break;
+        // the next probe relation: this join's rows, on the device
+        cur = amj_rel();
+        cur.ctx = ctx;
+        cur.n = res.rows;
+        cur.ncols = (int)S.size();
+        cur.where = AMJ_MEM_DEVICE;
+        for (size_t a = 0; a < S.size(); a++) {
+            cur.attrs[a] = (uint32_t)S[a];
+            cur.d_cols[a] = res.cols[a];
+        }
+    }
+    if (rc != AMJ_OK) {
+        if (have_prev) amj_result_release(&prev);
+        return rc;
+    }
+    const int k = out->num_attrs;
+    *out = prev;   // the last join's result, columns (when kept) on the device
+    out->num_attrs = k;
+    out->stats[7] = (uint64_t)hp.L;
+    return AMJ_OK;
+}
+
 }  // namespace amj

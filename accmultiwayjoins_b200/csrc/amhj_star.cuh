@@ -1,0 +1,209 @@
+// AMHJ flat path for star-shaped count queries.
+//
+// When every build level is looked up by an attribute of the probe relation
+// (a star: a fact table and its dimensions) and compares nothing but that
+// key, the levels are independent: a probe row's result is the cross product
+// of its matches in each level.  The frontier DFS (amhj_kernel.cuh) visits
+// the levels one after another, so the latencies of a row's lookups add up.
+// Here one thread takes one probe row, issues the bucket-bound loads of every
+// level together, scans each (short) bucket for its key, and counts and
+// hashes the product's tuples in attribute order.  A row whose product
+// exceeds STAR_MAX_PRODUCT (a skewed dimension) is listed instead and joined
+// afterwards by the DFS kernel, which shares such work across warps.
+// Count mode only; bucket layout only.
+#pragma once
+#include "amhj_probe.cuh"
+
+namespace amj {
+
+constexpr uint32_t STAR_MAX_PRODUCT = 256;
+
+// whether plan P takes the flat path
+inline bool star_eligible(const ProbePlan &P) {
+    if (P.L < 1 || P.has_inl || P.sort_out || P.fib_level >= 0) return false;
+    for (int l = 0; l < P.L; l++) {
+        const LevelDesc &lv = P.lv[l];
+        if (lv.layout != AMJ_LAYOUT_BUCKET || lv.key_mode != KEY_SINGLE || lv.cmp_mask != 1u) return false;
+        bool from_probe = false;
+        for (int c = 0; c < P.probe_ncols; c++) from_probe |= P.probe_attr[c] == lv.key_attr[0];
+        if (!from_probe) return false;
+    }
+    return true;
+}
+
+__global__ __launch_bounds__(256) void amhj_star_kernel(const __grid_constant__ ProbePlan P,
+                                                        unsigned long long *count, unsigned long long *checksum,
+                                                        uint32_t *over, unsigned int *nover) {
+    unsigned long long cnt = 0, chk = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = P.row_lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < P.row_hi; r += stride) {
+        int32_t vals[AMJ_MAX_ATTRS];
+        for (int c = 0; c < P.probe_ncols; c++) vals[P.probe_attr[c]] = P.probe_col[c][r];
+        int32_t key[AMJ_MAX_BUILD_TABLES];
+        uint32_t s[AMJ_MAX_BUILD_TABLES], e[AMJ_MAX_BUILD_TABLES];
+        // every level's bucket bounds in flight together
+#pragma unroll
+        for (int l = 0; l < AMJ_MAX_BUILD_TABLES; l++) {
+            if (l >= P.L) break;
+            key[l] = vals[P.lv[l].key_attr[0]];
+            const uint32_t h = (uint32_t)key[l] & P.lv[l].mask;
+            s[l] = P.lv[l].buc_ptrs[h];
+            e[l] = P.lv[l].buc_ptrs[h + 1];
+        }
+        uint32_t first[AMJ_MAX_BUILD_TABLES];
+        uint64_t prod = 1;
+#pragma unroll
+        for (int l = 0; l < AMJ_MAX_BUILD_TABLES; l++) {
+            if (l >= P.L) break;
+            uint32_t nm = 0, f = e[l];
+            for (uint32_t i = s[l]; i < e[l]; i++)
+                if (P.lv[l].col[0][i] == key[l]) {
+                    if (nm == 0) f = i;
+                    nm++;
+                }
+            first[l] = f;
+            prod *= nm;
+        }
+        if (prod == 0) continue;
+        if (prod > STAR_MAX_PRODUCT) {
+            over[atomicAdd(nover, 1u)] = (uint32_t)(r - P.row_lo);
+            continue;
+        }
+        if (prod == 1) {   // unique keys in every level: one tuple
+#pragma unroll
+            for (int l = 0; l < AMJ_MAX_BUILD_TABLES; l++) {
+                if (l >= P.L) break;
+                for (int c = 1; c < P.lv[l].ncols; c++) vals[P.lv[l].attr[c]] = P.lv[l].col[c][first[l]];
+            }
+            uint64_t h = AMJ_CHECKSUM_SEED;
+            for (int a = 0; a < P.k; a++) h = amj_hash_step(h, vals[a]);
+            cnt++;
+            chk += h;
+            continue;
+        }
+        // the product's tuples: one matching row per level, the last level fastest
+        uint32_t pos[AMJ_MAX_BUILD_TABLES];
+#pragma unroll
+        for (int l = 0; l < AMJ_MAX_BUILD_TABLES; l++)
+            if (l < P.L) pos[l] = first[l];
+        while (true) {
+#pragma unroll
+            for (int l = 0; l < AMJ_MAX_BUILD_TABLES; l++) {
+                if (l >= P.L) break;
+                for (int c = 1; c < P.lv[l].ncols; c++) vals[P.lv[l].attr[c]] = P.lv[l].col[c][pos[l]];
+            }
+            uint64_t h = AMJ_CHECKSUM_SEED;
+            for (int a = 0; a < P.k; a++) h = amj_hash_step(h, vals[a]);
+            cnt++;
+            chk += h;
+            // next combination
+            int l = P.L - 1;
+            for (; l >= 0; l--) {
+                uint32_t i = pos[l] + 1;
+                while (i < e[l] && P.lv[l].col[0][i] != key[l]) i++;
+                if (i < e[l]) {
+                    pos[l] = i;
+                    break;
+                }
+                pos[l] = first[l];
+            }
+            if (l < 0) break;
+        }
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if ((threadIdx.x & 31) == 0 && cnt) {
+        atomicAdd(count, cnt);
+        atomicAdd(checksum, chk);
+    }
+}
+
+// the probe columns of the listed rows (row ids relative to row_lo)
+__global__ void star_gather_kernel(const __grid_constant__ ProbePlan P, const uint32_t *rows, uint32_t n,
+                                   int32_t *const *out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int c = 0; c < P.probe_ncols; c++) out[c][i] = P.probe_col[c][P.row_lo + rows[i]];
+}
+
+}  // namespace amj
+
+namespace amj {
+
+// ---- thread-per-row baseline ----
+// The reference's MHJ (MHJ-GPU/Joins/MHJ.cuh:18-122): one thread per probe
+// row walks the build levels depth first with backtracking, scanning each
+// bucket alone.  Kept as a comparator for the warp-cooperative frontier DFS
+// (AMJ_F_THREAD_PER_ROW); bucket layout, count mode.
+inline bool thread_row_eligible(const ProbePlan &P) {
+    if (P.L < 1 || P.fib_level >= 0) return false;
+    for (int l = 0; l < P.L; l++)
+        if (P.lv[l].layout != AMJ_LAYOUT_BUCKET) return false;
+    return true;
+}
+
+__device__ __forceinline__ void thread_row_range(const LevelDesc &lv, const int32_t *vals, uint32_t &s, uint32_t &e) {
+    const int32_t k0 = vals[lv.key_attr[0]];
+    const uint32_t h = (lv.key_mode == KEY_PAIR ? hash_pair(k0, vals[lv.key_attr[1]]) : (uint32_t)k0) & lv.mask;
+    s = lv.buc_ptrs[h];
+    e = lv.buc_ptrs[h + 1];
+}
+
+__global__ __launch_bounds__(256) void amhj_thread_row_kernel(const __grid_constant__ ProbePlan P,
+                                                              unsigned long long *count,
+                                                              unsigned long long *checksum) {
+    unsigned long long cnt = 0, chk = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = P.row_lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < P.row_hi; r += stride) {
+        int32_t vals[AMJ_MAX_ATTRS];
+        for (int c = 0; c < P.probe_ncols; c++) vals[P.probe_attr[c]] = P.probe_col[c][r];
+        uint32_t pos[AMJ_MAX_BUILD_TABLES], end[AMJ_MAX_BUILD_TABLES];
+        int d = 0;
+        thread_row_range(P.lv[0], vals, pos[0], end[0]);
+        while (true) {
+            if (pos[d] >= end[d]) {
+                if (d == 0) break;
+                d--;
+                pos[d]++;
+                continue;
+            }
+            const LevelDesc &lv = P.lv[d];
+            const uint32_t i = pos[d];
+            bool ok = true;
+            for (int c = 0; c < lv.ncols && ok; c++)
+                if ((lv.cmp_mask >> c) & 1u) ok = lv.col[c][i] == vals[lv.attr[c]];
+            if (!ok) {
+                pos[d]++;
+                continue;
+            }
+            for (int c = 0; c < lv.ncols; c++)
+                if ((lv.bind_mask >> c) & 1u) vals[lv.attr[c]] = lv.col[c][i];
+            if (d == P.L - 1) {
+                int32_t t[AMJ_MAX_ATTRS];
+                for (int a = 0; a < P.k; a++) t[a] = vals[a];
+                if (P.sort_out)   // a degree-ordered copy reports every tuple sorted
+                    for (int a = 1; a < P.k; a++)
+                        for (int b = a; b > 0 && t[b - 1] > t[b]; b--) {
+                            const int32_t x = t[b - 1];
+                            t[b - 1] = t[b];
+                            t[b] = x;
+                        }
+                uint64_t h = AMJ_CHECKSUM_SEED;
+                for (int a = 0; a < P.k; a++) h = amj_hash_step(h, t[a]);
+                cnt++;
+                chk += h;
+                pos[d]++;
+                continue;
+            }
+            d++;
+            thread_row_range(P.lv[d], vals, pos[d], end[d]);
+        }
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if ((threadIdx.x & 31) == 0 && cnt) {
+        atomicAdd(count, cnt);
+        atomicAdd(checksum, chk);
+    }
+}
+
+}  // namespace amj

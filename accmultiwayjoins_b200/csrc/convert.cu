@@ -10,6 +10,11 @@
 //    then the 2-level IndexedTrie of the pairs, serialised as a .tr file.
 //  * switch_el.py (MHJ-GPU/switch_el.py): the same edge list with the two
 //    columns swapped.
+//  * tbl_2_db (MHJ-GPU/exec_tbl_2_db.cu:26-118): selected fields of a
+//    delimited table (TPC-H .tbl files: fields separated by '|'; any run of
+//    tab, '|' or newline separates, spaces stay inside a field), each read
+//    with stoul and stored as int32, written to "<rows>_<attr>...db" with
+//    the attribute ids given for the columns.
 // Here one parser serves all three (swap = 1 reverses the columns).  The file
 // is mapped and cut into one chunk per thread at line boundaries; each thread
 // parses its lines into its own buffer, then the buffers are concatenated
@@ -22,6 +27,7 @@
 
 #include <omp.h>
 
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -151,7 +157,124 @@ int parse_edgelist(const char *path, int swap, std::vector<int32_t> *src, std::v
     return AMJ_OK;
 }
 
+inline bool is_tbl_sep(char c) { return c == '\t' || c == '|' || c == '\n'; }
+
+// One line [s, e) of a delimited table: the fields `want` (ascending field
+// indexes, nsel of them; pos[i] = the output column of want[i]) into v.
+// 0 = skipped (blank), 1 = a row, -1 = a selected field missing or not a number.
+int parse_tbl_line(const char *s, const char *e, const uint32_t *want, const int *pos, int nsel, int32_t *v) {
+    while (s < e && (*s == '\r' || is_tbl_sep(*s))) s++;
+    if (s == e) return 0;
+    uint32_t field = 0;
+    int got = 0;
+    while (s < e && got < nsel) {
+        while (s < e && is_tbl_sep(*s)) s++;
+        if (s == e) break;
+        const char *t = s;
+        while (t < e && !is_tbl_sep(*t)) t++;
+        if (field == want[got]) {
+            // stoul: leading spaces, a sign, at least one digit; the rest of the field ignored
+            const char *q = s;
+            while (q < t && (*q == ' ' || *q == '\r')) q++;
+            bool neg = false;
+            if (q < t && (*q == '-' || *q == '+')) neg = *q++ == '-';
+            if (q == t || *q < '0' || *q > '9') return -1;
+            uint64_t x = 0;
+            while (q < t && *q >= '0' && *q <= '9') x = x * 10 + (uint64_t)(*q++ - '0');
+            v[pos[got]] = (int32_t)(uint32_t)(neg ? (0 - x) : x);
+            got++;
+        }
+        field++;
+        s = t;
+    }
+    return got == nsel ? 1 : -1;
+}
+
+// Parse a delimited table's selected fields (fields[], in output order).
+int parse_table(const char *path, const uint32_t *fields, int ncols, std::vector<std::vector<int32_t>> *cols) {
+    Mapped m;
+    AMJ_TRY(map_file(path, &m));
+    // fields in ascending order, with their output columns
+    std::vector<std::pair<uint32_t, int>> order(ncols);
+    for (int c = 0; c < ncols; c++) order[c] = {fields[c], c};
+    std::sort(order.begin(), order.end());
+    for (int c = 1; c < ncols; c++)
+        if (order[c].first == order[c - 1].first) return amj::fail(AMJ_EINVAL, "tbl_to_db: a field selected twice");
+    std::vector<uint32_t> want(ncols);
+    std::vector<int> pos(ncols);
+    for (int c = 0; c < ncols; c++) {
+        want[c] = order[c].first;
+        pos[c] = order[c].second;
+    }
+    const int T = m.n < (1u << 20) ? 1 : omp_get_max_threads();
+    std::vector<size_t> cut(T + 1, m.n);
+    cut[0] = 0;
+    for (int t = 1; t < T; t++) {
+        size_t c = m.n / T * t;
+        while (c < m.n && m.p[c - 1] != '\n') c++;
+        cut[t] = c < cut[t - 1] ? cut[t - 1] : c;
+    }
+    std::vector<std::vector<std::vector<int32_t>>> part(T, std::vector<std::vector<int32_t>>(ncols));
+    std::vector<uint64_t> bad_line(T, 0), lines(T, 0);
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int t = 0; t < T; t++) {
+        const char *s = m.p + cut[t], *end = m.p + cut[t + 1];
+        uint64_t ln = 0;
+        int32_t v[AMJ_MAX_COLS];
+        while (s < end) {
+            const char *nl = (const char *)memchr(s, '\n', (size_t)(end - s));
+            const char *le = nl ? nl : end;
+            ln++;
+            const int r = parse_tbl_line(s, le, want.data(), pos.data(), ncols, v);
+            if (r < 0) {
+                bad_line[t] = ln;
+                break;
+            }
+            if (r > 0)
+                for (int c = 0; c < ncols; c++) part[t][c].push_back(v[c]);
+            s = nl ? nl + 1 : end;
+        }
+        lines[t] = ln;
+    }
+    uint64_t before = 0;
+    for (int t = 0; t < T; t++) {
+        if (bad_line[t])
+            return amj::fail(AMJ_EINVAL, std::string("tbl_to_db: ") + path + " line " +
+                                             std::to_string(before + bad_line[t]) +
+                                             ": a selected field is missing or not an integer");
+        before += lines[t];
+    }
+    cols->assign(ncols, {});
+    for (int c = 0; c < ncols; c++)
+        for (int t = 0; t < T; t++) (*cols)[c].insert((*cols)[c].end(), part[t][c].begin(), part[t][c].end());
+    return AMJ_OK;
+}
+
 }  // namespace
+
+extern "C" int amj_tbl_to_db(const char *tbl_path, const uint32_t *fields, const uint32_t *attrs, int ncols,
+                             const char *out_dir, char *out_path, uint64_t out_cap, uint64_t *rows) {
+    if (!tbl_path || !fields || !attrs || ncols <= 0 || ncols > AMJ_MAX_COLS)
+        return amj::fail(AMJ_EINVAL, "tbl_to_db: bad arguments");
+    for (int c = 0; c < ncols; c++)
+        if (attrs[c] >= AMJ_MAX_ATTRS) return amj::fail(AMJ_EINVAL, "tbl_to_db: attribute id >= AMJ_MAX_ATTRS");
+    std::vector<std::vector<int32_t>> cols;
+    AMJ_TRY(parse_table(tbl_path, fields, ncols, &cols));
+    const uint64_t n = cols[0].size();
+    std::string name = std::to_string(n);
+    for (int c = 0; c < ncols; c++) name += "_" + std::to_string(attrs[c]);
+    name += ".db";
+    const std::string path = (out_dir && *out_dir) ? std::string(out_dir) + "/" + name : name;
+    std::vector<const int32_t *> cp(ncols);
+    for (int c = 0; c < ncols; c++) cp[c] = cols[c].data();
+    AMJ_TRY(amj_db_write(path.c_str(), n, ncols, cp.data()));
+    if (out_path && out_cap) {
+        std::strncpy(out_path, path.c_str(), out_cap - 1);
+        out_path[out_cap - 1] = 0;
+    }
+    if (rows) *rows = n;
+    return AMJ_OK;
+}
 
 extern "C" int amj_edgelist_read(const char *path, int swap, int32_t *src, int32_t *dst, uint64_t cap,
                                  uint64_t *n) {

@@ -12,6 +12,7 @@
 // a repeated row counts once (the trie builds drop repeats; the reference's
 // inputs are deduplicated edge lists).
 #include "amj_ops.cuh"
+#include "amhj_host.h"
 
 #include <algorithm>
 #include <cstring>
@@ -83,11 +84,14 @@ static int build_rel_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t) {
 }
 
 // The 4-clique over one edge relation (AMJ_F_CLIQUE4): a count pass, then
-// with AMJ_F_MATERIALIZE a write pass into exactly allocated columns.
+// with AMJ_F_MATERIALIZE a write pass into exactly allocated columns.  With
+// matrices_only the query runs only where the triangle matrices apply;
+// otherwise *used is false and nothing is reported.
 static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int flags,
-                                amj_result *out) {
+                                amj_result *out, bool matrices_only = false, bool *used = nullptr) {
     if (nrels != 1) return fail(AMJ_EUNSUPPORTED, "LFTJ 4-clique: one edge relation");
     if (algo != AMJ_LFTJ_DFS) return fail(AMJ_EUNSUPPORTED, "LFTJ 4-clique: DFS only");
+    if (used) *used = false;
     result_init(out, 4);
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
     AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
@@ -102,11 +106,14 @@ static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         C4Matrix *m = nullptr;
         ~MatGuard() { lftj_clique4_matrix_release(m); }
     } mat;
-    if ((flags & AMJ_F_KEEP_ORDER) == 0) {
+    if ((flags & AMJ_F_KEEP_ORDER) == 0 && (flags & AMJ_F_CLIQUE4_LISTS)) {
+        AMJ_TRY(build_self_trie(ctx, rels[0], &t, &sorted_out, true));
+    } else if ((flags & AMJ_F_KEEP_ORDER) == 0) {
         DBuf<uint64_t> wedges;
         AMJ_TRY(build_ranked_trie(ctx, rels[0], &t, &inv, &nv, &wedges));
         if (nv) {
             AMJ_TRY(lftj_clique4_matrix_prepare(ctx, t, inv.p, wedges.p, nv, ctx->opts.lftj_rank_bits, &mat.m));
+            if (!mat.m && matrices_only) return AMJ_OK;
             if (!mat.m) {
                 t = Trie2();
                 inv.release();
@@ -116,6 +123,7 @@ static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     } else {
         AMJ_TRY(build_self_trie(ctx, rels[0], &t, &sorted_out, false));
     }
+    if (used) *used = true;
     AMJ_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
     uint64_t c = 0, h = 0;
     if (mat.m)
@@ -158,6 +166,19 @@ static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
         }
     }
     return AMJ_OK;
+}
+
+// AMHJ FOUR over one oriented edge relation (exec_AMHJ.cu:53-69): the last
+// three levels of the hash-join plan, R(0,3), R(1,3), R(2,3), look up the
+// fourth vertex by the pair keys of an edge and a triangle.  On the
+// degree-ranked copy those lookups are one AND of two rows of the triangle
+// matrix of the first vertex (lftj_clique4.cu); where the matrices apply
+// (out-degrees up to 1024 and memory for them) the query runs that way and
+// *used is true.
+int amj::amhj_four_by_matrices(amj_ctx *ctx, amj_rel *rel, int flags, amj_result *out, bool *used) {
+    amj_rel *rels[1] = {rel};
+    return lftj_clique4_execute(ctx, rels, 1, AMJ_LFTJ_DFS, 0, flags & ~(AMJ_F_CLIQUE4_LISTS | AMJ_F_KEEP_ORDER), out,
+                                true, used);
 }
 
 // The self-joined edge relation as the relations of the triangle (TRI

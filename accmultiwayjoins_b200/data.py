@@ -246,6 +246,19 @@ def edgelist_to_db(text_path: str, db_path: str = None, swap: bool = False) -> i
     return int(rows.value)
 
 
+def tbl_to_db(tbl_path: str, fields, attrs, out_dir: str = None) -> str:
+    """Selected fields of a delimited table (a TPC-H .tbl file) as a .db
+    relation named "<rows>_<attrs>...db" in out_dir; returns its path."""
+    if len(fields) != len(attrs):
+        raise ValueError("one attribute per field")
+    n = len(fields)
+    buf = C.create_string_buffer(4096)
+    rows = C.c_uint64()
+    L.check(L.load().amj_tbl_to_db(tbl_path.encode(), (C.c_uint32 * n)(*fields), (C.c_uint32 * n)(*attrs), n,
+                                   out_dir.encode() if out_dir else None, buf, 4096, C.byref(rows)), "tbl_to_db")
+    return buf.value.decode()
+
+
 def checksum(cols) -> int:
     """Checksum of column-major tuples (the definition in include/amj_checksum.h)."""
     cols = [np.ascontiguousarray(c, dtype=np.int32) for c in cols]

@@ -10,12 +10,15 @@ checksum.  The unit of work is one output tuple (one triangle).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--algo DFS|BFS|AMHJ] [--scale S]
-                  [--workload triangle|chain|four|batch|serve] [--no-configs]
+                  [--workload triangle|chain|four|star|batch|serve|ooc] [--no-configs]
 
 --scale S runs the same workload on a smaller R-MAT graph (2^S vertices,
 2^(S+4) edges), for profiling.  --workload chain runs the 3-way chain join
 R1(a,b) R2(b,c) R3(c,d) (3 x 1M rows, keys uniform in [0, 2^18), seeds 1-3)
-through AMHJ (count + checksum, hash builds included).  --workload batch
+through AMHJ (count + checksum, hash builds included).  --workload star
+runs the 4-way star (fact 60M rows x 4 Zipf(1.1) keys, dims 1M/200K/100K/10K)
+through AMHJ the same way; --workload four the skewed 4-clique (R-MAT
+scale 22).  --workload batch
 runs 512 heterogeneous queries as one batch (autotuned, CUDA-graph replay)
 and reports, beside its tuples/s, the one-query-per-call tuples/s on the
 same queries and p50/p99 latencies of both forms.
@@ -250,9 +253,10 @@ class Clique4:
     """The skewed 4-clique over an R-MAT graph of scale S (2^S vertices,
     2^(S+4) edges, quadrant probabilities 0.6/0.15/0.15/0.1), cleaned as the
     triangle graph; the full size is scale 22 (64 Mi edges).  --algo AMHJ
-    runs the configured operator, AMHJ FOUR with ws=1 fib=1 (about 6 minutes
-    a query at full size); the default runs the ALFTJ 4-clique, which gives
-    the same count and checksum."""
+    runs the configured operator, AMHJ FOUR with ws=1 fib=1, whose last three
+    levels (the fourth vertex, looked up by pair keys) are answered by the
+    triangle matrices of the degree-ranked copy; the default runs the ALFTJ
+    4-clique, which gives the same count and checksum."""
 
     def __init__(self, args, rank):
         from accmultiwayjoins_b200 import data
@@ -267,7 +271,8 @@ class Clique4:
 
     @staticmethod
     def describe_static(scale, algo, rank_note=""):
-        op = "AMHJ FOUR (ws=1 fib=1), hash builds" if algo == "AMHJ" else "ALFTJ 4-clique (DFS), trie build"
+        op = ("AMHJ FOUR (ws=1 fib=1; pair-key levels by triangle matrices), index build" if algo == "AMHJ"
+              else "ALFTJ 4-clique (DFS), trie build")
         return (f"4-clique, R-MAT scale {scale}, {1 << (scale + 4)} edges "
                 f"(0.6,0.15,0.15,0.1), seed 22{rank_note}; {op} included, count+checksum")
 
@@ -290,7 +295,7 @@ class Clique4:
         return None
 
     def kernel_name(self):
-        return "amhj_probe_kernel (count pass)" if self.algo == "AMHJ" else "lftj_clique4_kernel"
+        return "lftj_clique4_matrix_kernel"
 
     def cpu_baseline(self):
         """The reference's MHJ-CPU multi-key probe on the FOUR pattern over a
@@ -404,6 +409,63 @@ class Chain:
         t0 = time.perf_counter()
         cnt, chk = O.mhj(self.rels, nthreads=cores)
         return cnt, chk, time.perf_counter() - t0, cores, "port", "the full workload once (oracle restatement)"
+
+
+class Star:
+    """The 4-way star: a fact table of 60M rows of four Zipf(1.1) foreign
+    keys into dimensions of 1M, 200K, 100K and 10K rows (unique key, uniform
+    payload), seed 3; AMHJ NORMAL count+checksum including the four hash
+    builds.  The probe is the flat star path: one thread per fact row, every
+    dimension's lookup in flight together."""
+    DIMS = (1_000_000, 200_000, 100_000, 10_000)
+
+    def __init__(self, args, rank, gen=None):
+        from accmultiwayjoins_b200 import data
+        self.rows = args.star_rows
+        fact, dims = data.star_relations(self.rows, list(self.DIMS), theta=1.1, seed=3 + rank, gen=gen)
+        self.rels = [fact] + dims
+        self.h2d = sum(4 * len(c[0]) * len(c) for c, _ in self.rels)
+
+    def describe(self, rank_note):
+        return (f"4-way star, fact {self.rows} rows x 4 Zipf(1.1) foreign keys, dims 1M/200K/100K/10K "
+                f"(key, payload), seed 3{rank_note}; AMHJ NORMAL count+checksum incl. hash builds")
+
+    device_relations = Chain.device_relations
+    host_relations = Chain.host_relations
+    host_columns = Chain.host_columns
+    run = Chain.run
+
+    def algorithmic_bytes(self):
+        """Per fact row: its four keys (16 B); per dimension lookup: the
+        bucket bounds (8 B) and each candidate's key and payload (8 B), the
+        buckets being floorPow2(rows) wide as built."""
+        fact_cols = self.rels[0][0]
+        tot = len(fact_cols[0]) * 16
+        for j, (cols, _) in enumerate(self.rels[1:]):
+            B = 1 << (len(cols[0]).bit_length() - 1)
+            per = np.bincount(cols[0] & (B - 1), minlength=B).astype(np.int64)
+            tot += len(fact_cols[j]) * 8 + int(per[fact_cols[j] & (B - 1)].sum()) * 8
+        return tot
+
+    def kernel_name(self):
+        return "amhj_star_kernel"
+
+    def cpu_baseline(self, sample_rows=12_000_000):
+        """The reference MHJ-CPU over a bounded sample of the fact table (its
+        first rows, all dimensions), scaled to tuples/s."""
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        n = min(self.rows, sample_rows)
+        (fc, fa) = self.rels[0]
+        rels = [([c[:n] for c in fc], fa)] + self.rels[1:]
+        if O.ref_available():
+            cnt, _, sec = O.mhj_reference(rels, nthreads=cores)
+            kind = "reference"
+        else:
+            t0 = time.perf_counter()
+            cnt, _ = O.mhj(rels, nthreads=cores)
+            sec, kind = time.perf_counter() - t0, "port"
+        return cnt, None, sec, cores, kind, f"the first {n} fact rows with all four dimensions"
 
 
 class BatchMix:
@@ -836,6 +898,8 @@ def Batch_default_opts(L):
 def make_workload(args, rank):
     if args.workload == "four":
         return Clique4(args, rank)
+    if args.workload == "star":
+        return Star(args, rank)
     return Chain(args, rank) if args.workload == "chain" else Triangle(args, rank)
 
 
@@ -947,9 +1011,12 @@ def run_reference(args, rank, world):
         print(json.dumps(reference_line(args, tuples / sum(times), sum(times) / len(times) * 1e3, desc, cpu)),
               flush=True)
         return
-    if args.workload == "chain":
-        wl = Chain(args, 0, gen=gen)
-        step = lambda: wl.cpu_baseline()[::2][:2]  # noqa: E731  (count, seconds)
+    if args.workload in ("chain", "star"):
+        wl = Chain(args, 0, gen=gen) if args.workload == "chain" else Star(args, 0, gen=gen)
+        if args.workload == "chain":
+            step = lambda: wl.cpu_baseline()[::2][:2]  # noqa: E731  (count, seconds)
+        else:
+            step = lambda: wl.cpu_baseline(sample_rows=wl.rows)[::2][:2]  # noqa: E731
         desc, sample = wl.describe(""), "the full workload per step (reference MHJ-CPU as shipped, TBJ call timed)"
         kind = "reference" if O.ref_available() else "port"
     else:
@@ -1046,7 +1113,7 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     wl = make_workload(args, rank)
     stream = torch.cuda.current_stream(dev)
-    ctx = Context(local_rank, spin_limit_ms=args.spin_limit_ms)
+    ctx = Context(local_rank, layout=args.layout, spin_limit_ms=args.spin_limit_ms)
     lib = L.load()
     # run the library on torch's stream so torch's CUDA events see its kernels
     L.check(lib.amj_ctx_set_stream(ctx.handle, C.c_void_p(stream.cuda_stream)), "set_stream")
@@ -1122,7 +1189,9 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": tot_count / (max_ms * 1e-3), "unit": "tuples/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
-        "config": {"workload": wl.describe(rank_note), "tuples_per_rank": count,
+        "config": {"workload": wl.describe(rank_note) + ("" if args.layout == "bucket" else
+                                                          f"; {args.layout} hash tables"),
+                   "tuples_per_rank": count,
                    "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"independent instance per GPU x{world}"},
         "e2e": {"value": tot_count / (max_e2e * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": wl.h2d,
@@ -1160,7 +1229,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--algo", default="DFS", choices=["DFS", "BFS", "AMHJ"])
-    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain", "four", "batch", "serve", "ooc"])
+    ap.add_argument("--workload", default="triangle", choices=["triangle", "chain", "four", "star", "batch", "serve", "ooc"])
     ap.add_argument("--spin-limit-ms", type=int, default=5000, help="bound on every device-side wait")
     ap.add_argument("--rate", type=float, default=200.0, help="serve workload: requests per second")
     ap.add_argument("--lanes", type=int, default=3, help="serve workload: batches in flight")
@@ -1176,6 +1245,9 @@ def main():
     ap.add_argument("--max-rows", type=int, default=4_000_000, help="batch workload: largest relation")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="batch workload: skip the autotuner")
     ap.add_argument("--scale", type=int, default=SCALE)
+    ap.add_argument("--star-rows", type=int, default=60_000_000, help="star workload: fact table rows")
+    ap.add_argument("--layout", default="bucket", choices=["bucket", "oa", "cuckoo"],
+                    help="chain / star workloads: hash-table layout of the AMHJ builds")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="triangle workload: skip the chain and batched records carried on the line")

@@ -79,6 +79,19 @@ extern "C" {
                                    degree-ordered copy (the default for BFS, for DFS
                                    with ws=1 and for the 4-clique; the triangle paths
                                    join it with vertices renamed to their ranks) */
+#define AMJ_F_THREAD_PER_ROW 0x80 /* amj_amhj_execute, count only, bucket layout: the
+                                   reference's MHJ baseline, one thread per probe row
+                                   walking the levels alone (MHJ-GPU/Joins/MHJ.cuh:18) */
+#define AMJ_F_PAIRWISE     0x100 /* amj_amhj_execute, NORMAL: a plan of 2-relation joins,
+                                   every intermediate result materialised on the device
+                                   (the reference's pairwise baseline, MHJ-GPU/exec_PW.cu) */
+#define AMJ_F_CLIQUE4_LISTS 0x40 /* amj_lftj_execute with AMJ_F_CLIQUE4: join the
+                                   degree-ordered copy by list intersections even where
+                                   the triangle matrices fit (same result)          */
+#define AMJ_F_HASH_PLAN    0x200 /* amj_amhj_execute, FOUR over one edge relation: keep
+                                   the level-by-level hash-join plan where the triangle
+                                   matrices of the degree-ranked copy would answer the
+                                   last three levels (same result)                  */
 
 /* ---- relation residency ---- */
 #define AMJ_MEM_DEVICE 0   /* columns are device pointers, borrowed            */
@@ -425,6 +438,16 @@ int  amj_db_parse_name(const char *path, uint64_t *n, int *ncols, uint32_t *attr
 int  amj_edgelist_read(const char *path, int swap, int32_t *src, int32_t *dst, uint64_t cap, uint64_t *n);
 int  amj_edgelist_to_db(const char *text_path, const char *db_path, int swap, uint64_t *rows);
 int  amj_edgelist_to_tr(amj_ctx *ctx, const char *text_path, const char *tr_path, int swap, uint64_t *rows);
+/* amj_tbl_to_db: fields fields[0..ncols-1] (0-based, any order) of a
+ * delimited table (runs of tab, '|' or newline separate fields; a selected
+ * field is read as stoul does: its leading integer) as a .db file named
+ * "<rows>_<attrs[0]>_<attrs[1]>...db" in out_dir (null: the current
+ * directory); its path goes to out_path (out_cap bytes).  Blank lines are
+ * skipped; a line missing a selected field, or one that is not an integer,
+ * is an error naming the line.  Replaces tbl_2_db
+ * (MHJ-GPU/exec_tbl_2_db.cu:26-133), the ingestion of TPC-H .tbl files. */
+int  amj_tbl_to_db(const char *tbl_path, const uint32_t *fields, const uint32_t *attrs, int ncols,
+                   const char *out_dir, char *out_path, uint64_t out_cap, uint64_t *rows);
 
 /* ---- host checksum of column-major tuples (same definition as the GPU) ---- */
 int  amj_checksum_host(const int32_t *const *cols, int k, uint64_t n, uint64_t *out);

@@ -96,3 +96,104 @@ def test_cli_converter(tmp_path, built):
     assert np.frombuffer(open(tmp_path / "s.db", "rb").read(), np.int32).tolist() == [5, 7, 4, 6]
     r = subprocess.run([os.path.join(BIN, "edgelist-to-csr")], capture_output=True, text=True)
     assert r.returncode == 2 and "usage" in r.stderr
+
+
+# ---- delimited tables (amj_tbl_to_db; the reference's tbl_2_db, MHJ-GPU/exec_tbl_2_db.cu) ----
+
+REF_TBL2DB = os.path.join(ROOT, "oracle", "_ref", "exec_tbl_2_db")
+WORDS = ["quick", "pending", "final", "deposits", "sleep", "ironic", "ideas", "haggle", "blithely"]
+
+
+def synthetic_table(path, n, seed, nkeys=(1000, 300, 50)):
+    """A seeded '|'-delimited table shaped like a TPC-H fact table: three
+    integer keys, a decimal, a date, a flag, a free-text comment with spaces,
+    and a trailing '|'.  Returns the integer key columns."""
+    rng = np.random.default_rng(seed)
+    k = [rng.integers(0, m, n) for m in nkeys]
+    price = rng.integers(100, 10**7, n)
+    with open(path, "w") as f:
+        for i in range(n):
+            words = " ".join(WORDS[j] for j in rng.integers(0, len(WORDS), 1 + i % 4))
+            f.write(f"{k[0][i]}|{k[1][i]}|{k[2][i]}|{price[i] // 100}.{price[i] % 100:02d}|"
+                    f"199{i % 8}-0{1 + i % 9}-1{i % 10}|{'NOF'[i % 3]}|{words} |\n")
+    return k
+
+
+@pytest.mark.skipif(not os.path.exists(REF_TBL2DB), reason="reference converter not built (reference sources absent)")
+@pytest.mark.parametrize("fields,attrs", [([0, 1], [0, 1]), ([2, 0], [3, 1]), ([1, 2, 0], [2, 0, 1]), ([3], [5])])
+def test_tbl_bytes_and_name_equal_reference_converter(tmp_path, built, fields, attrs):
+    tbl = tmp_path / "fact.tbl"
+    synthetic_table(tbl, 3000, 11)
+    refdir = tmp_path / "ref"
+    refdir.mkdir()
+    subprocess.run([REF_TBL2DB, str(tbl)] + [str(x) for x in fields + attrs], check=True, capture_output=True,
+                   cwd=refdir)
+    (ref_name,) = os.listdir(refdir)
+    ours = data.tbl_to_db(str(tbl), fields, attrs, out_dir=str(tmp_path))
+    assert os.path.basename(ours) == ref_name
+    assert open(ours, "rb").read() == open(refdir / ref_name, "rb").read()
+
+
+def test_tbl_columns_in_given_order_and_renamed(tmp_path, built):
+    tbl = tmp_path / "t.tbl"
+    k = synthetic_table(tbl, 500, 4)
+    path = data.tbl_to_db(str(tbl), [2, 0, 3], [7, 1, 4], out_dir=str(tmp_path))
+    assert os.path.basename(path) == "500_7_1_4.db"
+    cols, attrs = data.read_db(path)
+    assert attrs == [7, 1, 4]
+    assert np.array_equal(cols[0], k[2]) and np.array_equal(cols[1], k[0])
+    # field 3 is a decimal: stoul keeps its integer part
+    want = []
+    for line in open(tbl):
+        want.append(int(line.split("|")[3].split(".")[0]))
+    assert cols[2].tolist() == want
+
+
+def test_tbl_parse_rules(tmp_path, built):
+    tbl = tmp_path / "r.tbl"
+    # runs of separators collapse (strtok), tabs separate too, spaces stay in
+    # a field and lead stoul, negative values and 2^32-1 wrap to int32, blank
+    # lines are skipped
+    tbl.write_text("1|2|x y|\n\n3\t|4|z|\n -5||4294967295|w\n7|8\n")
+    path = data.tbl_to_db(str(tbl), [0, 1], [0, 1], out_dir=str(tmp_path))
+    cols, _ = data.read_db(path)
+    assert cols[0].tolist() == [1, 3, -5, 7] and cols[1].tolist() == [2, 4, -1, 8]
+
+
+@pytest.mark.parametrize("text,fields", [("1|2|\n3|\n", [0, 1]), ("1|abc|\n", [1]), ("1|2\n", [0, 5])])
+def test_tbl_missing_or_non_integer_fields_are_errors(tmp_path, built, text, fields):
+    tbl = tmp_path / "bad.tbl"
+    tbl.write_text(text)
+    with pytest.raises(AmjError, match="line"):
+        data.tbl_to_db(str(tbl), fields, list(range(len(fields))), out_dir=str(tmp_path))
+
+
+def test_tbl_bad_arguments(tmp_path, built):
+    tbl = tmp_path / "t.tbl"
+    tbl.write_text("1|2|\n")
+    with pytest.raises(AmjError):
+        data.tbl_to_db(str(tbl), [0, 0], [0, 1], out_dir=str(tmp_path))
+    with pytest.raises(AmjError):
+        data.tbl_to_db(str(tmp_path / "missing.tbl"), [0], [0], out_dir=str(tmp_path))
+    with pytest.raises(ValueError):
+        data.tbl_to_db(str(tbl), [0, 1], [0], out_dir=str(tmp_path))
+
+
+def test_tbl_large_file_parsed_in_parallel_in_order(tmp_path, built):
+    tbl = tmp_path / "big.tbl"
+    k = synthetic_table(tbl, 60000, 8)   # a few MB: parsed in per-thread chunks
+    path = data.tbl_to_db(str(tbl), [0, 1, 2], [0, 1, 2], out_dir=str(tmp_path))
+    cols, _ = data.read_db(path)
+    for c in range(3):
+        assert np.array_equal(cols[c], k[c])
+
+
+def test_tbl_cli(tmp_path, built):
+    tbl = tmp_path / "c.tbl"
+    k = synthetic_table(tbl, 100, 2)
+    r = subprocess.run([os.path.join(BIN, "exec-tbl-2-db"), str(tbl), "1", "0", "4", "2"], cwd=tmp_path,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    cols, attrs = data.read_db(str(tmp_path / "100_4_2.db"))
+    assert attrs == [4, 2] and np.array_equal(cols[0], k[1]) and np.array_equal(cols[1], k[0])
+    assert subprocess.run([os.path.join(BIN, "exec-tbl-2-db"), str(tbl), "1"], capture_output=True).returncode == 2

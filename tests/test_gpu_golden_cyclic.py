@@ -6,7 +6,8 @@ driven through oracle/mhj_ref/mhj_ref_harness.cpp) over seeded R-MAT edge
 relations, up to the full triangle configuration (R-MAT scale 20, 2^24
 generated edges).  Every CUDA path that answers these queries is compared
 with them through the C ABI: AMHJ TRI / FOUR with each work-sharing switch,
-on the relation as given and on its degree-ordered copy; ALFTJ DFS (wedge
+on the relation as given and on its degree-ordered copy, FOUR also through
+the triangle matrices; ALFTJ DFS (wedge
 kernel, lane merge), BFS; the ALFTJ 4-clique through the triangle matrices
 and through the list-intersection kernel.
 """
@@ -56,6 +57,8 @@ def test_four_clique_paths_match_reference_golden(ctx, case):
     runs = [("ALFTJ 4-clique (triangle matrices)", lambda: ctx.lftj([e], clique4=True)),
             ("ALFTJ 4-clique as given (list kernel)", lambda: ctx.lftj([e], clique4=True, degree_order=False)),
             ("AMHJ FOUR ws=1 fib=1", lambda: ctx.amhj("FOUR", [e], ws=1, fib=1)),
+            ("AMHJ FOUR ws=1 fib=1, hash plan", lambda: ctx.amhj("FOUR", [e], ws=1, fib=1, plan="hash")),
+            ("AMHJ FOUR ws=0 dro=1, hash plan", lambda: ctx.amhj("FOUR", [e], dro=1, plan="hash")),
             ("AMHJ FOUR ws=0 as given", lambda: ctx.amhj("FOUR", [e], degree_order=False))]
     for name, run in runs:
         r = run()

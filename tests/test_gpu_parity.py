@@ -270,6 +270,62 @@ def test_amhj_star(layout):
             assert (got.count, got.checksum) == O.mhj(rels)
 
 
+@pytest.mark.parametrize("shape", ["chain4", "star", "tri", "four"])
+def test_amhj_baseline_plans_match_oracle(ctx, shape):
+    """The comparators of the reference's baselines: one thread per probe
+    row (MHJ-GPU/Joins/MHJ.cuh) and a pairwise plan with materialised
+    intermediates (MHJ-GPU/exec_PW.cu) give the operator's result."""
+    if shape == "chain4":
+        rels = data.chain_relations(30000, 1 << 12, 4, seed=12)
+    elif shape == "star":
+        fact, dims = data.star_relations(50000, [5000, 1000, 500, 50], theta=1.1, seed=13)
+        rels = [fact] + dims
+    else:
+        s, d = data.rmat(10, 8000, 0.57, 0.19, 0.19, seed=14)
+        rels = [([s, d], [0, 1])]
+    hs = [ctx.relation(c, a) for c, a in rels]
+    qt = {"tri": "TRI", "four": "FOUR"}.get(shape, "NORMAL")
+    want = O.mhj(rels) if qt == "NORMAL" else (O.triangle(*rels[0][0]) if qt == "TRI" else O.four_clique(*rels[0][0]))
+    for dego in (True, False):
+        t = ctx.amhj(qt, hs, plan="thread_per_row", degree_order=dego)
+        assert (t.count, t.checksum) == want
+    if qt == "NORMAL":
+        p = ctx.amhj(qt, hs, plan="pairwise")
+        assert (p.count, p.checksum) == want and p.stats["slices"] == len(rels) - 1
+        m = ctx.amhj(qt, hs, plan="pairwise", materialize=True)
+        assert data.checksum(m.columns) == want[1]
+        assert np.array_equal(sorted_rows(m.columns), sorted_rows(O.mhj(rels, tuples=True)[2]))
+    with pytest.raises(AmjError):
+        ctx.amhj(qt, hs, plan="thread_per_row", materialize=True)
+
+
+def test_amhj_star_flat_path_with_repeated_dimension_keys(ctx):
+    """Star count queries take the flat kernel (one thread per fact row, all
+    dimension lookups together).  Dimensions with repeated keys give rows a
+    product of matches; rows whose product exceeds the flat kernel's bound
+    (a key repeated in every dimension) are joined by the DFS kernel after it.
+    Equal to the oracle, count mode and materialised."""
+    rng = np.random.Generator(np.random.PCG64(17))
+    n = 100_000
+    fact = [rng.integers(0, 500, n).astype(np.int32) for _ in range(3)]
+    fact[0][:2000] = 7
+    fact[1][:2000] = 7
+    fact[2][:2000] = 7
+    dims = []
+    for j in range(3):
+        keys = rng.integers(0, 500, 3000).astype(np.int32)
+        keys[:40] = 7                          # 40^3 = 64000 tuples per hub row
+        dims.append(([keys, rng.integers(-1000, 1000, 3000).astype(np.int32)], [j, 3 + j]))
+    rels = [(fact, [0, 1, 2])] + dims
+    want = O.mhj(rels)
+    hs = [ctx.relation(c, a) for c, a in rels]
+    for ws in (0, 1):
+        got = ctx.amhj("NORMAL", hs, ws=ws)
+        assert (got.count, got.checksum) == want, ws
+    m = ctx.amhj("NORMAL", hs, materialize=True)
+    assert (m.count, m.checksum) == want
+
+
 @pytest.mark.parametrize("qt", ["TRI", "FOUR"])
 @pytest.mark.parametrize("reorder", [True, False])
 @pytest.mark.parametrize("degree_order", [True, False])
@@ -890,6 +946,39 @@ def test_c2_triangle_full_size(ctx):
     assert (got.count, got.checksum) == want
 
 
+def test_c3a_four_clique_full_size(ctx):
+    """The skewed 4-clique configuration (R-MAT scale 22, 2^26 generated
+    edges, 0.6/0.15/0.15/0.1, seed 22) through the two fast paths: the
+    triangle matrices and the list-intersection kernel over the
+    degree-ordered copy give the same count and checksum (the reference's
+    multi-key probe pins both paths on smaller graphs of the same
+    generator, tests/test_gpu_golden_cyclic.py)."""
+    s, d = data.rmat(22, 1 << 26, 0.6, 0.15, 0.15, 22)
+    e = ctx.relation([s, d], [0, 1])
+    m = ctx.lftj([e], clique4=True)
+    lists = ctx.lftj([e], clique4=True, clique4_lists=True)
+    assert (m.count, m.checksum) == (lists.count, lists.checksum)
+    assert (m.count, m.checksum) == (94478795231, 0x56807E4A9FC45902)
+    # the configured operator, AMHJ FOUR ws=1 fib=1 (its last three levels
+    # through the triangle matrices)
+    a = ctx.amhj("FOUR", [e], ws=1, fib=1)
+    assert (a.count, a.checksum) == (m.count, m.checksum)
+    e.release()
+
+
+def test_amhj_four_matrix_plan_materialises_the_hash_plan_tuples(ctx):
+    """AMHJ FOUR through the triangle matrices writes the same tuples (each
+    sorted, from the degree-ordered copy) as the level-by-level hash plan,
+    to host and device result columns."""
+    s, d = data.rmat(11, 1 << 15, 0.57, 0.19, 0.19, seed=5)
+    e = ctx.relation([s, d], [0, 1])
+    a = ctx.amhj("FOUR", [e], ws=1, fib=1, materialize=True)
+    b = ctx.amhj("FOUR", [e], ws=1, plan="hash", materialize=True)
+    assert a.count > 1000 and (a.count, a.checksum) == (b.count, b.checksum)
+    assert np.array_equal(sorted_rows(a.columns), sorted_rows(b.columns))
+    assert data.checksum(a.columns) == a.checksum
+
+
 # ----------------------------------------------------- failure detection
 
 def test_bounded_wait_times_out_and_context_survives(ctx):
@@ -954,3 +1043,40 @@ def test_cli_exec_amhj_and_exec_lftj(tmp_path):
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     assert json.loads(r.stdout.strip().splitlines()[-1])["count"] == want[0]
+
+
+def test_tbl_tables_join_end_to_end(ctx, tmp_path):
+    """Delimited tables (TPC-H .tbl shape: '|'-separated, text fields with
+    spaces, a trailing '|') go through amj_tbl_to_db to .db relations and
+    then through the multi-way joins: a star (a fact table and three
+    dimensions) and a 3-table chain, both equal to the oracle."""
+    rng = np.random.default_rng(31)
+
+    def table(name, cols, text=True):
+        n = len(cols[0])
+        with open(tmp_path / name, "w") as f:
+            for i in range(n):
+                f.write("|".join(str(c[i]) for c in cols) + ("|note %d x|" % i if text else "|") + "\n")
+        return str(tmp_path / name)
+
+    n = 80_000
+    fact = table("lineitem.tbl", [rng.integers(0, 20000, n), rng.integers(0, 2000, n), rng.integers(0, 100, n),
+                                  rng.integers(1, 50, n)])
+    part = table("part.tbl", [np.arange(2000), rng.integers(0, 25, 2000)])
+    supp = table("supplier.tbl", [rng.integers(0, 100, 300), rng.integers(0, 25, 300)])   # repeated keys
+    orders = table("orders.tbl", [np.arange(20000), rng.integers(0, 1500, 20000)], text=False)
+    cust = table("customer.tbl", [np.arange(1500), rng.integers(0, 25, 1500)])
+    out = str(tmp_path)
+    star = [data.tbl_to_db(fact, [0, 1, 2], [0, 1, 2], out), data.tbl_to_db(part, [0, 1], [1, 3], out),
+            data.tbl_to_db(supp, [0, 1], [2, 4], out), data.tbl_to_db(orders, [0, 1], [0, 5], out)]
+    chain = [data.tbl_to_db(fact, [0, 3], [0, 1], out), data.tbl_to_db(orders, [0, 1], [0, 2], out),
+             data.tbl_to_db(cust, [0, 1], [2, 3], out)]
+    assert os.path.basename(star[0]) == f"{n}_0_1_2.db"
+    for files in (star, chain):
+        rels = [data.read_db(p) for p in files]
+        want = O.mhj(rels)
+        assert want[0] > 0
+        got = ctx.amhj("NORMAL", rels_on(ctx, rels))
+        assert (got.count, got.checksum) == want
+        got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=1, dro=1, materialize=True)
+        assert (got.count, got.checksum) == want and data.checksum(got.columns) == want[1]
