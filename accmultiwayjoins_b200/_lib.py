@@ -188,6 +188,7 @@ SIGNATURES = {
     "amj_ctx_sync": (C.c_int, [_P]),
     "amj_stat_name": (C.c_char_p, [C.c_int]),
     "amj_ctx_launch_count": (C.c_int, [_P, _U64P]),
+    "amj_ctx_trim": (C.c_int, [_P]),
     "amj_rel_create": (C.c_int, [_P, C.c_uint64, C.c_int, _U32P, C.POINTER(_I32P), C.c_int, C.POINTER(_P)]),
     "amj_rel_release": (None, [_P]),
     "amj_rel_info": (C.c_int, [_P, _U64P, C.POINTER(C.c_int), _U32P]),

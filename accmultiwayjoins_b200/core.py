@@ -425,6 +425,10 @@ class Context:
         self._batches.add(srv)
         return srv
 
+    def trim(self):
+        """Give back the pinned host blocks and matrix area kept for reuse."""
+        L.check(L.load().amj_ctx_trim(self.handle), "ctx_trim")
+
     def sync(self):
         L.check(L.load().amj_ctx_sync(self.handle), "ctx_sync")
 

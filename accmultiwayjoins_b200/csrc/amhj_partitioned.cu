@@ -9,86 +9,243 @@
 //   stage j joins the intermediate result I (the probe relation at stage 0)
 //   with build relation B_j on B_j's key attribute, which I binds.  Both are
 //   hash-partitioned on the key into P parts (P a power of two chosen so one
-//   part of each fits the memory budget: opts.mem_budget, else half the free
-//   device memory); part p of I can only match part p of B_j.  Each pair is
-//   copied to the device and joined by the 2-relation AMHJ operator (every
-//   bound attribute compared, as in the full plan).  The rows of every stage
-//   but the last go back to host memory and form the next intermediate; the
-//   last stage sums counts and checksums (and collects the rows when asked).
+//   part of each, twice for the double buffer, and B_j's index fit the
+//   memory budget: opts.mem_budget, else half the free device memory); part
+//   p of I can only match part p of B_j.  Each pair is copied to the device
+//   and joined by the 2-relation AMHJ operator (every bound attribute
+//   compared, as in the full plan).  The rows of every stage but the last go
+//   back to host memory and form the next intermediate; the last stage sums
+//   counts and checksums (and collects the rows when asked).
 // Every result tuple of the full plan is produced exactly once: its key at
 // stage j puts it in exactly one part.  The relations of a stage are
 // renamed to attributes 0..m-1 in id order, which leaves the last stage's
 // tuples (all attributes) in attribute-id order, so its checksum is the
 // query's.
+//
+// Host memory: the partitions and intermediates live in pinned blocks that
+// the context keeps after the call (pinning tens of GB takes seconds, and a
+// served system runs the same stages again); they are freed with the context.
+// Partitioning runs on all host cores into those blocks; part p+1 is copied
+// to the device on a side stream while part p is joined, and each part's
+// rows come back straight into a pinned block of the next intermediate.
 #include "amhj_host.h"
 
 #include <omp.h>
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <vector>
 
 namespace amj {
 
+// ---- pinned host blocks kept by the context ----
+struct PinnedCache {
+    std::multimap<size_t, void *> free_blocks;   // by size
+};
+
 namespace {
 
-// A host relation: columns in attribute order `attrs`.
-struct HostTable {
-    std::vector<int> attrs;
-    std::vector<std::vector<int32_t>> cols;
+size_t pinned_round(size_t b) {
+    const size_t g = b <= (64ull << 20) ? (1ull << 20) : (64ull << 20);
+    return (b + g - 1) / g * g;
+}
+
+PinnedCache *pinned_cache(amj_ctx *ctx) {
+    if (!ctx->pinned_cache) ctx->pinned_cache = new PinnedCache();
+    return static_cast<PinnedCache *>(ctx->pinned_cache);
+}
+
+void pinned_trim(amj_ctx *ctx) {
+    PinnedCache *pc = pinned_cache(ctx);
+    for (auto &kv : pc->free_blocks) (void)cudaFreeHost(kv.second);
+    pc->free_blocks.clear();
+}
+
+// A pinned block of at least `bytes`: a kept block of up to 4/3 the rounded
+// request, else a new one (after dropping the kept ones if pinning fails).
+int pinned_get(amj_ctx *ctx, size_t bytes, void **p, size_t *size) {
+    PinnedCache *pc = pinned_cache(ctx);
+    const size_t r = pinned_round(bytes ? bytes : 1);
+    auto it = pc->free_blocks.lower_bound(r);
+    if (it != pc->free_blocks.end() && it->first <= r + r / 3) {
+        *p = it->second;
+        *size = it->first;
+        pc->free_blocks.erase(it);
+        return AMJ_OK;
+    }
+    cudaError_t e = cudaHostAlloc(p, r, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        pinned_trim(ctx);
+        e = cudaHostAlloc(p, r, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            *p = nullptr;
+            return fail(AMJ_ENOMEM, "AMHJ ooc: pinned host allocation of " + std::to_string(r) + " bytes failed");
+        }
+    }
+    *size = r;
+    return AMJ_OK;
+}
+
+// A pinned block, back to the context's cache when dropped.
+struct Pinned {
+    amj_ctx *ctx = nullptr;
+    void *p = nullptr;
+    size_t size = 0;
+    Pinned() = default;
+    Pinned(const Pinned &) = delete;
+    Pinned &operator=(const Pinned &) = delete;
+    Pinned(Pinned &&o) noexcept : ctx(o.ctx), p(o.p), size(o.size) { o.p = nullptr; }
+    int get(amj_ctx *c, size_t bytes) {
+        drop();
+        ctx = c;
+        return pinned_get(c, bytes, &p, &size);
+    }
+    void drop() {
+        if (p) pinned_cache(ctx)->free_blocks.emplace(size, p);
+        p = nullptr;
+    }
+    int32_t *i32() const { return static_cast<int32_t *>(p); }
+    ~Pinned() { drop(); }
+};
+
+// Rows of a host table: pieces, each with one pointer per column.
+struct Piece {
+    const int32_t *col[AMJ_MAX_COLS] = {};
     uint64_t n = 0;
 };
 
-// Hash partition of n rows (columns cols) on column kc into P parts: the
-// rows of part p are out[c][off[p] .. off[p+1]).
-void partition_rows(const std::vector<const int32_t *> &cols, uint64_t n, int kc, uint32_t P,
-                    std::vector<std::vector<int32_t>> *out, std::vector<uint64_t> *off) {
-    const int nc = (int)cols.size();
-    out->assign(nc, std::vector<int32_t>(n));
-    off->assign(P + 1, 0);
+struct HostTable {
+    std::vector<int> attrs;
+    std::vector<Piece> pieces;
+    std::vector<Pinned> own;   // pinned blocks holding the pieces (intermediates)
+    uint64_t n = 0;
+};
+
+// A table hash-partitioned on one column: part p is a list of pieces.
+struct Parts {
+    std::vector<std::vector<Piece>> part;
+    std::vector<uint64_t> rows;
+    Pinned block;
+    uint64_t max_rows = 0;
+};
+
+// Hash partition of X on column kc into P parts, on all host cores: one
+// counting pass, then every column scattered into one pinned block (column
+// c of part p at c * n + off[p]).  P = 1 keeps X's pieces.
+int partition_table(amj_ctx *ctx, const HostTable &X, int kc, uint32_t P, Parts *out) {
+    out->part.assign(P, {});
+    out->rows.assign(P, 0);
+    out->max_rows = 0;
+    const uint64_t n = X.n;
     if (P == 1) {
-        for (int c = 0; c < nc; c++)
-            if (n) std::memcpy((*out)[c].data(), cols[c], n * 4);
-        (*off)[1] = n;
-        return;
+        for (const Piece &pc : X.pieces)
+            if (pc.n) out->part[0].push_back(pc);
+        out->rows[0] = out->max_rows = n;
+        return AMJ_OK;
     }
+    if (n == 0) return AMJ_OK;
+    const int nc = (int)X.attrs.size();
+    AMJ_TRY(out->block.get(ctx, (size_t)nc * n * sizeof(int32_t)));
+    int32_t *base = out->block.i32();
+    std::vector<uint64_t> start(X.pieces.size() + 1, 0);   // first row of every piece
+    for (size_t i = 0; i < X.pieces.size(); i++) start[i + 1] = start[i] + X.pieces[i].n;
     const int T = n < (1u << 16) ? 1 : omp_get_max_threads();
     std::vector<uint64_t> cnt((size_t)T * P, 0);
-    const int32_t *key = cols[kc];
+    std::vector<uint64_t> off(P + 1, 0);
+    // rows [lo, hi) of the concatenated pieces, piece by piece
+    auto for_range = [&](uint64_t lo, uint64_t hi, auto &&f) {
+        size_t i = std::upper_bound(start.begin(), start.end(), lo) - start.begin() - 1;
+        for (; lo < hi && i < X.pieces.size(); i++) {
+            const uint64_t e = std::min(hi, start[i + 1]);
+            if (e > lo) f(X.pieces[i], lo - start[i], e - start[i]);
+            lo = e;
+        }
+    };
 #pragma omp parallel num_threads(T)
     {
         const int t = omp_get_thread_num();
         const uint64_t lo = n * t / T, hi = n * (t + 1) / T;
         uint64_t *mine = cnt.data() + (size_t)t * P;
-        for (uint64_t i = lo; i < hi; i++) mine[hash_key(key[i]) & (P - 1)]++;
+        for_range(lo, hi, [&](const Piece &pc, uint64_t a, uint64_t b) {
+            const int32_t *key = pc.col[kc];
+            for (uint64_t i = a; i < b; i++) mine[hash_key(key[i]) & (P - 1)]++;
+        });
 #pragma omp barrier
 #pragma omp single
         {
             uint64_t acc = 0;
             for (uint32_t p = 0; p < P; p++) {
-                (*off)[p] = acc;
+                off[p] = acc;
                 for (int u = 0; u < T; u++) {
                     const uint64_t c = cnt[(size_t)u * P + p];
                     cnt[(size_t)u * P + p] = acc;
                     acc += c;
                 }
             }
-            (*off)[P] = acc;
+            off[P] = acc;
         }
-        for (uint64_t i = lo; i < hi; i++) {
-            const uint64_t pos = mine[hash_key(key[i]) & (P - 1)]++;
-            for (int c = 0; c < nc; c++) (*out)[c][pos] = cols[c][i];
-        }
+        for_range(lo, hi, [&](const Piece &pc, uint64_t a, uint64_t b) {
+            const int32_t *key = pc.col[kc];
+            for (uint64_t i = a; i < b; i++) {
+                const uint64_t pos = mine[hash_key(key[i]) & (P - 1)]++;
+                for (int c = 0; c < nc; c++) base[(uint64_t)c * n + pos] = pc.col[c][i];
+            }
+        });
     }
+    for (uint32_t p = 0; p < P; p++) {
+        const uint64_t np = off[p + 1] - off[p];
+        out->rows[p] = np;
+        out->max_rows = std::max(out->max_rows, np);
+        if (!np) continue;
+        Piece pc;
+        for (int c = 0; c < nc; c++) pc.col[c] = base + (uint64_t)c * n + off[p];
+        pc.n = np;
+        out->part[p].push_back(pc);
+    }
+    return AMJ_OK;
 }
 
-uint32_t parts_for(uint64_t bytes, uint64_t budget) {
+// Smallest power-of-two P with one stage's per-part device memory within
+// the budget: probe and build parts twice (double buffer), the build part's
+// index (about three times its columns) and the part's result (about twice
+// the probe part).
+uint32_t parts_for(uint64_t ibytes, uint64_t bbytes, uint64_t budget) {
+    const uint64_t need = 4 * ibytes + 5 * bbytes;
     uint64_t p = 1;
-    while (p < (1u << 20) && bytes > budget * p) p <<= 1;
+    while (p < (1u << 20) && need > budget * p) p <<= 1;
     return (uint32_t)p;
 }
 
+// A device relation's columns copied into a pinned block: one piece.
+int device_to_host(amj_ctx *ctx, const amj_rel *r, HostTable *t) {
+    t->n = r->n;
+    if (!r->n) return AMJ_OK;
+    Pinned b;
+    AMJ_TRY(b.get(ctx, (size_t)r->ncols * r->n * sizeof(int32_t)));
+    Piece pc;
+    pc.n = r->n;
+    for (int c = 0; c < r->ncols; c++) {
+        int32_t *dst = b.i32() + (uint64_t)c * r->n;
+        AMJ_CUDA_TRY(cudaMemcpyAsync(dst, r->d_cols[c], r->n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        pc.col[c] = dst;
+    }
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    t->pieces.push_back(pc);
+    t->own.push_back(std::move(b));
+    return AMJ_OK;
+}
+
 }  // namespace
+
+void pinned_cache_release(amj_ctx *ctx) {
+    if (!ctx || !ctx->pinned_cache) return;
+    pinned_trim(ctx);
+    delete static_cast<PinnedCache *>(ctx->pinned_cache);
+    ctx->pinned_cache = nullptr;
+}
 
 int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, int flags, amj_result *out) {
     uint64_t budget = ctx->opts.mem_budget;
@@ -98,27 +255,29 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
         budget = fr / 2;
     }
     const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
+    cudaStream_t up = ctx->side_stream[0];
+    struct Events {
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        ~Events() {
+            for (auto x : e)
+                if (x) (void)cudaEventDestroy(x);
+        }
+    } ev;
+    for (auto &x : ev.e) AMJ_CUDA_TRY(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
     // stage 0's intermediate: the probe relation (host or device columns)
     HostTable I;
     const amj_rel *pr = hp.probe;
-    I.n = pr->n;
-    std::vector<const int32_t *> icols;
-    for (int c = 0; c < pr->ncols; c++) {
-        I.attrs.push_back(hp.probe_attr[c]);
-        if (pr->where == AMJ_MEM_HOST_STREAMED) {
-            icols.push_back(pr->h_cols[c]);
-        } else {
-            I.cols.emplace_back(pr->n);
-            if (pr->n)
-                AMJ_CUDA_TRY(cudaMemcpyAsync(I.cols.back().data(), pr->d_cols[c], pr->n * 4, cudaMemcpyDeviceToHost,
-                                             ctx->stream));
-        }
+    for (int c = 0; c < pr->ncols; c++) I.attrs.push_back(hp.probe_attr[c]);
+    if (pr->where == AMJ_MEM_HOST_STREAMED) {
+        Piece pc;
+        for (int c = 0; c < pr->ncols; c++) pc.col[c] = pr->h_cols[c];
+        pc.n = I.n = pr->n;
+        if (pc.n) I.pieces.push_back(pc);
+    } else {
+        AMJ_TRY(device_to_host(ctx, pr, &I));
     }
-    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    if (pr->where != AMJ_MEM_HOST_STREAMED)
-        for (auto &c : I.cols) icols.push_back(c.data());
     uint64_t count = 0, checksum = 0, joins = 0;
-    std::vector<std::vector<int32_t>> final_cols(materialize ? hp.k : 0);
+    HostTable fin;   // the last stage's rows, when materialised
     for (int j = 0; j < hp.L; j++) {
         const LevelSpec &ls = hp.lv[j];
         const amj_rel *B = ls.rel;
@@ -132,45 +291,80 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
         const int ka = ls.attr[0];
         const int ik = (int)(std::find(I.attrs.begin(), I.attrs.end(), ka) - I.attrs.begin());
         if (ik == (int)I.attrs.size()) return fail(AMJ_EUNSUPPORTED, "AMHJ ooc: a build key the plan does not bind");
-        std::vector<const int32_t *> bcols;
-        for (int c = 0; c < B->ncols; c++) bcols.push_back(B->where == AMJ_MEM_HOST_STREAMED ? B->h_cols[c] : nullptr);
-        std::vector<std::vector<int32_t>> bhost;
-        if (B->where != AMJ_MEM_HOST_STREAMED) {
-            bhost.assign(B->ncols, std::vector<int32_t>(B->n));
-            for (int c = 0; c < B->ncols; c++) {
-                if (B->n)
-                    AMJ_CUDA_TRY(cudaMemcpyAsync(bhost[c].data(), B->d_cols[c], B->n * 4, cudaMemcpyDeviceToHost,
-                                                 ctx->stream));
-                bcols[c] = bhost[c].data();
-            }
-            AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        HostTable Bt;
+        for (int c = 0; c < B->ncols; c++) Bt.attrs.push_back((int)B->attrs[c]);
+        if (B->where == AMJ_MEM_HOST_STREAMED) {
+            Piece pc;
+            for (int c = 0; c < B->ncols; c++) pc.col[c] = B->h_cols[c];
+            pc.n = Bt.n = B->n;
+            if (pc.n) Bt.pieces.push_back(pc);
+        } else {
+            AMJ_TRY(device_to_host(ctx, B, &Bt));
         }
-        // a part of each side within the budget: the probe part's columns, the
-        // build part's columns and its index (about three times its columns)
-        const uint64_t bytes = I.n * 4 * I.attrs.size() + B->n * 4 * (uint64_t)B->ncols * 4;
-        const uint32_t P = parts_for(bytes, budget);
-        std::vector<std::vector<int32_t>> ip, bp;
-        std::vector<uint64_t> ioff, boff;
-        partition_rows(icols, I.n, ik, P, &ip, &ioff);
-        partition_rows(bcols, B->n, ls.src_col[0], P, &bp, &boff);
+        const int nci = (int)I.attrs.size(), ncb = B->ncols, ncs = (int)S.size();
+        const uint32_t P = parts_for(I.n * 4 * (uint64_t)nci, B->n * 4 * (uint64_t)ncb, budget);
+        Parts ip, bp;
+        AMJ_TRY(partition_table(ctx, I, ik, P, &ip));
+        AMJ_TRY(partition_table(ctx, Bt, ls.src_col[0], P, &bp));
+        // device slots for two part pairs
+        DBuf<int32_t> dI[2], dB[2];
+        for (int s = 0; s < 2; s++) {
+            AMJ_TRY(dI[s].alloc(ctx, std::max<uint64_t>(ip.max_rows, 1) * nci));
+            AMJ_TRY(dB[s].alloc(ctx, std::max<uint64_t>(bp.max_rows, 1) * ncb));
+        }
+        AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));   // the slots exist before the side stream writes them
+        std::vector<uint32_t> todo;
+        for (uint32_t p = 0; p < P; p++)
+            if (ip.rows[p] && bp.rows[p]) todo.push_back(p);
+        // copy part pair p into slot s on the side stream (columns back to back)
+        auto upload = [&](uint32_t p, int s) -> int {
+            const uint64_t ni = ip.rows[p], nb = bp.rows[p];
+            uint64_t o = 0;
+            for (const Piece &pc : ip.part[p]) {
+                for (int c = 0; c < nci; c++)
+                    AMJ_CUDA_TRY(cudaMemcpyAsync(dI[s].p + (uint64_t)c * ni + o, pc.col[c], pc.n * 4,
+                                                 cudaMemcpyHostToDevice, up));
+                o += pc.n;
+            }
+            o = 0;
+            for (const Piece &pc : bp.part[p]) {
+                for (int c = 0; c < ncb; c++)
+                    AMJ_CUDA_TRY(cudaMemcpyAsync(dB[s].p + (uint64_t)c * nb + o, pc.col[c], pc.n * 4,
+                                                 cudaMemcpyHostToDevice, up));
+                o += pc.n;
+            }
+            AMJ_CUDA_TRY(cudaEventRecord(ev.e[s], up));
+            return AMJ_OK;
+        };
+        uint32_t pattrs[AMJ_MAX_COLS], battrs[AMJ_MAX_COLS];
+        for (int c = 0; c < nci; c++) pattrs[c] = rename(I.attrs[c]);
+        for (int c = 0; c < ncb; c++) battrs[c] = rename((int)B->attrs[c]);
         HostTable next;
         next.attrs = S;
-        next.cols.assign(S.size(), {});
-        uint32_t pattrs[AMJ_MAX_COLS], battrs[AMJ_MAX_COLS];
-        for (size_t c = 0; c < I.attrs.size(); c++) pattrs[c] = rename(I.attrs[c]);
-        for (int c = 0; c < B->ncols; c++) battrs[c] = rename((int)B->attrs[c]);
-        for (uint32_t p = 0; p < P; p++) {
-            const uint64_t np = ioff[p + 1] - ioff[p], nb = boff[p + 1] - boff[p];
-            if (np == 0 || nb == 0) continue;
+        HostTable &dst = last ? fin : next;
+        dst.attrs = S;
+        const int f = (last && !materialize) ? 0 : AMJ_F_MATERIALIZE;   // result columns stay on the device
+        int rc = todo.empty() ? AMJ_OK : upload(todo[0], 0);
+        for (size_t t = 0; t < todo.size() && rc == AMJ_OK; t++) {
+            const uint32_t p = todo[t];
+            const int s = (int)(t & 1);
+            // the other slot's join has returned: fill it with the next pair
+            if (t + 1 < todo.size()) rc = upload(todo[t + 1], s ^ 1);
+            if (rc != AMJ_OK) break;
+            const cudaError_t we = cudaStreamWaitEvent(ctx->stream, ev.e[s], 0);
+            if (we != cudaSuccess) {
+                rc = cuda_fail(we, "AMHJ ooc: wait for a part copy");
+                break;
+            }
+            const uint64_t ni = ip.rows[p], nb = bp.rows[p];
             const int32_t *pc[AMJ_MAX_COLS], *bc[AMJ_MAX_COLS];
-            for (size_t c = 0; c < I.attrs.size(); c++) pc[c] = ip[c].data() + ioff[p];
-            for (int c = 0; c < B->ncols; c++) bc[c] = bp[c].data() + boff[p];
+            for (int c = 0; c < nci; c++) pc[c] = dI[s].p + (uint64_t)c * ni;
+            for (int c = 0; c < ncb; c++) bc[c] = dB[s].p + (uint64_t)c * nb;
             amj_rel *rp = nullptr, *rb = nullptr;
-            AMJ_TRY(amj_rel_create(ctx, np, (int)I.attrs.size(), pattrs, pc, AMJ_MEM_HOST, &rp));
-            int rc = amj_rel_create(ctx, nb, B->ncols, battrs, bc, AMJ_MEM_HOST, &rb);
+            rc = amj_rel_create(ctx, ni, nci, pattrs, pc, AMJ_MEM_DEVICE, &rp);
+            if (rc == AMJ_OK) rc = amj_rel_create(ctx, nb, ncb, battrs, bc, AMJ_MEM_DEVICE, &rb);
             amj_result res;
             std::memset(&res, 0, sizeof(res));
-            const int f = (last && !materialize) ? 0 : (AMJ_F_MATERIALIZE | AMJ_F_HOST_RESULT);
             amj_rel *pair[2] = {rp, rb};
             if (rc == AMJ_OK) rc = amj_amhj_execute(ctx, AMJ_QUERY_NORMAL, pair, 2, 0, ws, dro, 0, f, &res);
             if (rc == AMJ_OK) {
@@ -179,26 +373,38 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
                     count += res.count;
                     checksum += res.checksum;
                 }
-                if (f) {
-                    std::vector<std::vector<int32_t>> &dst = last ? final_cols : next.cols;
-                    for (size_t a = 0; a < S.size(); a++) {
-                        const size_t old = dst[a].size();
-                        dst[a].resize(old + res.rows);
-                        if (res.rows) std::memcpy(dst[a].data() + old, res.cols[a], res.rows * 4);
+                if (f && res.rows) {
+                    // the part's rows into a pinned block of the next table
+                    Pinned b;
+                    rc = b.get(ctx, (size_t)ncs * res.rows * sizeof(int32_t));
+                    Piece out_pc;
+                    out_pc.n = res.rows;
+                    for (int a = 0; a < ncs && rc == AMJ_OK; a++) {
+                        int32_t *d = b.i32() + (uint64_t)a * res.rows;
+                        const cudaError_t e = cudaMemcpyAsync(d, res.cols[a], res.rows * 4, cudaMemcpyDeviceToHost,
+                                                              ctx->stream);
+                        if (e != cudaSuccess) rc = cuda_fail(e, "AMHJ ooc: part result copy");
+                        out_pc.col[a] = d;
                     }
-                    if (!last) next.n += res.rows;
+                    if (rc == AMJ_OK) {
+                        dst.pieces.push_back(out_pc);
+                        dst.own.push_back(std::move(b));
+                        dst.n += res.rows;
+                    }
                 }
-                amj_result_release(&res);
+                amj_result_release(&res);   // device columns: freed in stream order after the copies
             }
-            amj_rel_release(rp);
+            if (rp) amj_rel_release(rp);
             if (rb) amj_rel_release(rb);
-            if (rc != AMJ_OK) return rc;
         }
-        if (!last) {
-            I = std::move(next);
-            icols.clear();
-            for (auto &c : I.cols) icols.push_back(c.data());
-        }
+        // the side stream's copies and the result copies end before the
+        // partitions and slots go
+        const cudaError_t e1 = cudaStreamSynchronize(up);
+        const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+        if (rc != AMJ_OK) return rc;
+        if (e1 != cudaSuccess) return cuda_fail(e1, "AMHJ ooc: part copies");
+        if (e2 != cudaSuccess) return cuda_fail(e2, "AMHJ ooc: part joins");
+        if (!last) I = std::move(next);
     }
     out->count = count;
     out->checksum = checksum;
@@ -214,8 +420,14 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
                 (void)cudaGetLastError();
                 return fail(AMJ_ENOMEM, "AMHJ ooc: pinned result allocation failed");
             }
-            if (count) std::memcpy(out->cols[a], final_cols[a].data(), count * 4);
         }
+        // the pieces in order, copied on all host cores
+        std::vector<uint64_t> at(fin.pieces.size() + 1, 0);
+        for (size_t i = 0; i < fin.pieces.size(); i++) at[i + 1] = at[i] + fin.pieces[i].n;
+#pragma omp parallel for schedule(dynamic, 1)
+        for (long long i = 0; i < (long long)fin.pieces.size(); i++)
+            for (int a = 0; a < hp.k; a++)
+                std::memcpy(out->cols[a] + at[i], fin.pieces[i].col[a], fin.pieces[i].n * 4);
     }
     return AMJ_OK;
 }

@@ -135,6 +135,7 @@ struct amj_ctx {
     amj::IndexProvider *iprov = nullptr;   // indexes kept across calls (set by the request server)
     void *c4_mtx = nullptr;                // 4-clique triangle matrices, kept across calls (grow-only)
     uint64_t c4_mtx_words = 0;
+    void *pinned_cache = nullptr;          // pinned host blocks of out-of-core stages, kept across calls
 };
 
 struct amj_rel {
@@ -156,6 +157,8 @@ inline void note_launch(amj_ctx *ctx) { ctx->launches++; }
 // Stream-ordered device allocation on the context stream.
 int dev_alloc(amj_ctx *ctx, void **p, size_t bytes);
 void dev_free(amj_ctx *ctx, void *p);
+// Free the pinned host blocks the context keeps for out-of-core stages.
+void pinned_cache_release(amj_ctx *ctx);
 
 template <typename T>
 struct DBuf {

@@ -98,6 +98,16 @@ __global__ void degree_sample_kernel(const int32_t *__restrict__ s, const int32_
     }
 }
 
+// the largest of nv degrees
+__global__ void degree_max_kernel(const unsigned int *__restrict__ deg, uint64_t nv, unsigned int *out) {
+    unsigned int m = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nv; i += (uint64_t)gridDim.x * blockDim.x)
+        m = max(m, deg[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(AMJ_FULL_MASK, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 // key (degree << idbits | id) of every vertex id in [0, nv)
 __global__ void rank_keys_kernel(const unsigned int *__restrict__ deg, uint64_t nv, int idbits,
                                  uint64_t *__restrict__ keys) {
@@ -160,16 +170,25 @@ int degree_ranks(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n,
     AMJ_TRY(ka.alloc(ctx, V));
     AMJ_TRY(kb.alloc(ctx, V));
     const unsigned gv = (unsigned)std::min<uint64_t>((V + 255) / 256, (uint64_t)ctx->num_sms * 16);
-    // a vertex has degree at most 2n: keys of idbits + degbits bits
+    // the largest degree sets the key width: keys of idbits + degbits bits
+    AMJ_CUDA_TRY(cudaMemsetAsync(&pr.p->bad, 0, sizeof(unsigned int), ctx->stream));
+    note_launch(ctx);
+    degree_max_kernel<<<gv, 256, 0, ctx->stream>>>(deg.p, V, &pr.p->bad);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    unsigned int maxdeg = 0;
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&maxdeg, &pr.p->bad, sizeof(maxdeg), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     int idbits = 1, degbits = 1;
     while (idbits < 31 && (V - 1) >> idbits) idbits++;
-    while ((2 * n) >> degbits) degbits++;
+    while (degbits < 32 && (uint64_t)maxdeg >> degbits) degbits++;
     if (idbits + degbits > 64) return fail(AMJ_EUNSUPPORTED, "degree ranks: relation too large");
     note_launch(ctx);
     rank_keys_kernel<<<gv, 256, 0, ctx->stream>>>(deg.p, V, idbits, ka.p);
     AMJ_CUDA_TRY(cudaGetLastError());
+    // the keys start in id order and the sort is stable: sorting the degree
+    // bits alone leaves them in (degree, id) order
     uint64_t *sorted = nullptr;
-    AMJ_TRY(radix_sort_u64(ctx, ka.p, kb.p, V, SK_IDENT, 0, idbits + degbits, &sorted));
+    AMJ_TRY(radix_sort_u64(ctx, ka.p, kb.p, V, SK_IDENT, idbits, idbits + degbits, &sorted));
     AMJ_TRY(rank->alloc(ctx, V));
     AMJ_TRY(inv->alloc(ctx, V));
     note_launch(ctx);

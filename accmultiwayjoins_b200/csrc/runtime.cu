@@ -183,6 +183,7 @@ extern "C" void amj_ctx_destroy(amj_ctx *c) {
     if (c->d_status) (void)cudaFree(c->d_status);
     if (c->h_status) (void)cudaFreeHost(c->h_status);
     if (c->c4_mtx) (void)cudaFree(c->c4_mtx);
+    amj::pinned_cache_release(c);
     if (c->own_stream && c->stream) (void)cudaStreamDestroy(c->stream);
     (void)cudaGetLastError();
     delete c;
@@ -206,6 +207,19 @@ extern "C" int amj_ctx_sync(amj_ctx *c) {
 extern "C" int amj_ctx_launch_count(const amj_ctx *c, uint64_t *out) {
     if (!c || !out) return fail(AMJ_EINVAL, "ctx_launch_count: null argument");
     *out = c->launches;
+    return AMJ_OK;
+}
+
+extern "C" int amj_ctx_trim(amj_ctx *c) {
+    if (!c) return fail(AMJ_EINVAL, "ctx_trim: null ctx");
+    AMJ_CUDA_TRY(cudaSetDevice(c->device));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    amj::pinned_cache_release(c);
+    if (c->c4_mtx) {
+        AMJ_CUDA_TRY(cudaFree(c->c4_mtx));
+        c->c4_mtx = nullptr;
+        c->c4_mtx_words = 0;
+    }
     return AMJ_OK;
 }
 

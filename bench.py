@@ -848,6 +848,7 @@ def run_ooc(args, rank, world, local_rank):
     clocks = sampler.stop()
     want = (r.count, r.checksum)
     check = {}
+    ctx.trim()   # the staged join's pinned blocks: host memory for the checks
     try:
         dev = [ctx.relation(c, a) for c, a in rels[1:]]
         x = ctx.amhj("NORMAL", [host[0]] + dev, ooc=1)

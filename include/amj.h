@@ -154,6 +154,10 @@ int  amj_ctx_sync(amj_ctx *ctx);
 const char *amj_stat_name(int i);
 /* number of kernels this context has launched (all entry points) */
 int  amj_ctx_launch_count(const amj_ctx *ctx, uint64_t *out);
+/* give back what the context keeps between calls for reuse: the pinned host
+ * blocks of out-of-core stages and the 4-clique matrix area (both are
+ * allocated again when needed) */
+int  amj_ctx_trim(amj_ctx *ctx);
 
 /* ---- relations (MHJ-GPU/Relation.cuh:9-38) ---- */
 int  amj_rel_create(amj_ctx *ctx, uint64_t n, int ncols, const uint32_t *attrs,

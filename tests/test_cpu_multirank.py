@@ -8,7 +8,7 @@ import pytest
 import torch.multiprocessing as mp
 
 from accmultiwayjoins_b200 import data
-from accmultiwayjoins_b200.dist import M64, allreduce_result, shard_range
+from accmultiwayjoins_b200.dist import M64, allreduce_result, shard_range, shard_relation
 
 
 def free_port():
@@ -30,9 +30,7 @@ def _rank_main(rank, world, port, q):
     try:
         # strong form: one chain query, probe rows sharded
         rels = data.chain_relations(4000, 1 << 9, 3, seed=3)
-        (c0, c1), attrs = rels[0]
-        lo, hi = shard_range(len(c0), rank, world)
-        mine = [([c0[lo:hi], c1[lo:hi]], attrs)] + rels[1:]
+        mine = [shard_relation(rels[0], rank, world)] + rels[1:]
         cnt, chk = O.mhj(mine)
         tot = allreduce_result(cnt, chk)
         # weak form: an independent triangle instance per rank

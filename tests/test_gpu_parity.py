@@ -500,7 +500,9 @@ def test_amhj_out_of_core_build_relations_in_host_memory(shape):
             got = ctx.amhj("NORMAL", host, ooc=1, **sw)
             assert (got.count, got.checksum) == want, sw
             assert got.stats["slices"] >= 4
-        # a device probe with host builds, and the materialised tuples
+        # the pinned blocks the stages keep, given back; then a device probe
+        # with host builds, and the materialised tuples
+        ctx.trim()
         got = ctx.amhj("NORMAL", [dev[0]] + host[1:], ooc=1, materialize=True)
         assert (got.count, got.checksum) == want
         assert data.checksum(got.columns) == want[1]
@@ -1080,3 +1082,20 @@ def test_tbl_tables_join_end_to_end(ctx, tmp_path):
         assert (got.count, got.checksum) == want
         got = ctx.amhj("NORMAL", rels_on(ctx, rels), ws=1, dro=1, materialize=True)
         assert (got.count, got.checksum) == want and data.checksum(got.columns) == want[1]
+
+
+def test_sharded_join_shares_sum_to_the_query(ctx):
+    """The multi-GPU form (accmultiwayjoins_b200.dist.sharded_join): the
+    probe relation's rows split over 4 ranks, the other relations whole;
+    the ranks' (count, checksum) pairs, summed mod 2^64, equal the query's.
+    Run here as 4 shares in turn on one GPU (no collective)."""
+    from accmultiwayjoins_b200.dist import M64, sharded_join
+    chain = data.chain_relations(200_000, 1 << 14, 3, seed=21)
+    s, d = data.rmat(14, 1 << 18, 0.57, 0.19, 0.19, seed=20)
+    tri = [([s, d], [0, 1]), ([s, d], [1, 2]), ([s, d], [0, 2])]
+    for rels, op, want in ((chain, "amhj", O.mhj(chain)), (tri, "amhj", O.triangle(s, d)),
+                           (tri, "lftj", O.triangle(s, d))):
+        parts = [sharded_join(ctx, rels, r, 4, op=op, reduce=False) for r in range(4)]
+        got = (sum(c for c, _ in parts) & M64, sum(h for _, h in parts) & M64)
+        assert got == want, op
+        assert all(c > 0 for c, _ in parts)
