@@ -357,9 +357,10 @@ class Context:
              plan: str = "multiway") -> Result:
         """degree_order=False joins a TRI / FOUR edge relation as given, never its
         degree-ordered copy (the results are the same).  plan: "multiway" (the
-        operator; FOUR over one edge relation answers its last three levels from
-        the triangle matrices where they apply), "hash" (the operator with every
-        level a hash lookup), or a baseline to compare it with: "thread_per_row"
+        operator; TRI / FOUR over one oriented edge relation without repeated rows
+        answer their pair-key levels from a bitmap of b's children / the triangle
+        matrices of the degree-ranked copy), "hash" (the operator with every level
+        a hash lookup), or a baseline to compare it with: "thread_per_row"
         (one thread per probe row, count only) or "pairwise" (2-relation joins
         with materialised intermediates)."""
         lib = L.load()

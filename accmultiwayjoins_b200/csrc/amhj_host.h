@@ -64,8 +64,12 @@ void plan_common(const HostPlan &hp, const amj_opts &o, ProbePlan *P);
 int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, int flags, amj_result *out);
 // AMJ_F_PAIRWISE: the plan as 2-relation joins with materialised intermediates.
 int amhj_pairwise_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, int flags, amj_result *out);
-// FOUR over one edge relation through the triangle matrices of its
-// degree-ranked copy (lftj_api.cu); *used is false where they do not apply.
+// FOUR over one oriented edge relation without repeated rows through the
+// triangle matrices of its degree-ranked copy (lftj_api.cu); *used is false
+// where they do not apply.
 int amhj_four_by_matrices(amj_ctx *ctx, amj_rel *rel, int flags, amj_result *out, bool *used);
+// TRI over one edge relation through the wedge kernel on its degree-ranked
+// copy (lftj_api.cu); *used is false where that does not apply.
+int amhj_tri_by_wedges(amj_ctx *ctx, amj_rel *rel, int flags, amj_result *out, bool *used);
 
 }  // namespace amj

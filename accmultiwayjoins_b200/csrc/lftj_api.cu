@@ -111,6 +111,9 @@ static int lftj_clique4_execute(amj_ctx *ctx, amj_rel *const *rels, int nrels, i
     } else if ((flags & AMJ_F_KEEP_ORDER) == 0) {
         DBuf<uint64_t> wedges;
         AMJ_TRY(build_ranked_trie(ctx, rels[0], &t, &inv, &nv, &wedges));
+        // the hash join's bag semantics: only a relation that is oriented
+        // and has no repeated rows (the trie dropped none) joins as a set
+        if (matrices_only && (!nv || t.len1 != rels[0]->n)) return AMJ_OK;
         if (nv) {
             AMJ_TRY(lftj_clique4_matrix_prepare(ctx, t, inv.p, wedges.p, nv, ctx->opts.lftj_rank_bits, &mat.m));
             if (!mat.m && matrices_only) return AMJ_OK;
@@ -181,6 +184,30 @@ int amj::amhj_four_by_matrices(amj_ctx *ctx, amj_rel *rel, int flags, amj_result
                                 true, used);
 }
 
+static int triangle_run(amj_ctx *ctx, const Trie2 &R_, const Trie2 &S_, const Trie2 &T_, int algo, int ws,
+                        int flags, int sorted_out, const int32_t *rank_inv, const uint64_t *wedge, uint64_t nv,
+                        amj_result *out);
+
+// AMHJ TRI over one oriented edge relation (exec_AMHJ.cu:32-49): the levels
+// R(0,2) keyed on a and the pair-key filter R(1,2) become, on the
+// degree-ranked copy, the suffix of a's child list after b tested against a
+// bitmap of b's children (the wedge kernel, lftj.cu).  Taken where the
+// relation is oriented and has no repeated rows (the hash join counts
+// repeats, the trie joins sets); otherwise *used is false.
+int amj::amhj_tri_by_wedges(amj_ctx *ctx, amj_rel *rel, int flags, amj_result *out, bool *used) {
+    *used = false;
+    result_init(out, 3);
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->ev[0], ctx->stream));
+    Trie2 t;
+    DBuf<int32_t> inv;
+    DBuf<uint64_t> wedges;
+    uint64_t nv = 0;
+    AMJ_TRY(build_ranked_trie(ctx, rel, &t, &inv, &nv, &wedges));
+    if (!nv || t.len1 != rel->n) return AMJ_OK;
+    *used = true;
+    return triangle_run(ctx, t, t, t, AMJ_LFTJ_DFS, 1, flags, 1, inv.p, wedges.p, nv, out);
+}
+
 // The self-joined edge relation as the relations of the triangle (TRI
 // pattern) or 4-clique (FOUR pattern), for the generic join in a given
 // attribute order: views of the same device columns, none owning them.
@@ -229,6 +256,66 @@ extern "C" int amj_lftj_execute_ordered(amj_ctx *ctx, amj_rel *const *rels, int 
     return lftj_execute_impl(ctx, rels, nrels, algo, ooc, ws, flags, attr_order, attr_order ? k : 0, out);
 }
 
+// The triangle over tries R(0,1), S(1,2), T(0,2) built since ctx->ev[0]
+// was recorded: a count pass, with AMJ_F_MATERIALIZE a write pass into
+// exactly allocated columns, and the result's timings.
+static int triangle_run(amj_ctx *ctx, const Trie2 &R_, const Trie2 &S_, const Trie2 &T_, int algo, int ws,
+                        int flags, int sorted_out, const int32_t *rank_inv, const uint64_t *wedge, uint64_t nv,
+                        amj_result *out) {
+    const Trie2 *R = &R_, *S = &S_, *T = &T_;
+    cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
+    AMJ_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
+
+    // ws=0: every (a,b) pair intersected by its own lane; ws=1: long pairs
+    // shared by the whole warp
+    const int small_sum = ws ? 48 : 0x7fffffff;
+    // ws=1 also hands vertices with many children to the block-wide bitmap kernel
+    const uint32_t heavy_deg = ws ? (ctx->opts.lftj_heavy_degree ? ctx->opts.lftj_heavy_degree : 32u) : 0u;
+    const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
+    const uint64_t nr = R->len1;
+    uint64_t c = 0, h = 0, w = 0;
+    int rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, 0, nr, heavy_deg,
+                           out->kernel_ms, sorted_out, rank_inv, wedge, nv, ctx->opts.lftj_rank_bits);
+    if (rc != AMJ_OK) return rc;
+    int32_t *dcols[3] = {nullptr, nullptr, nullptr};
+    if (materialize) {
+        for (int a = 0; a < 3 && rc == AMJ_OK; a++) rc = dev_alloc(ctx, (void **)&dcols[a], (c ? c : 1) * 4);
+        uint64_t c2 = 0, h2 = 0;
+        if (rc == AMJ_OK)
+            rc = lftj_triangle(ctx, *R, *S, *T, algo, dcols, c, &c2, &h2, &w, small_sum, 0, nr, heavy_deg,
+                               out->kernel_ms + 2, sorted_out, rank_inv, wedge, nv, ctx->opts.lftj_rank_bits);
+        if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
+            rc = fail(AMJ_ECUDA, "LFTJ: write pass disagrees with count pass");
+        if (rc != AMJ_OK) {
+            for (int a = 0; a < 3; a++) dev_free(ctx, dcols[a]);
+            return rc;
+        }
+    }
+    out->count = c;
+    out->checksum = h;
+    out->stats[7] = 1;
+    if (materialize) {
+        auto *o = new ResultOwner();
+        o->ctx = ctx;
+        out->priv = o;
+        out->rows = c;
+        for (int a = 0; a < 3; a++) out->cols[a] = dcols[a];
+    }
+    AMJ_CUDA_TRY(cudaEventRecord(e2, ctx->stream));
+    AMJ_CUDA_TRY(cudaEventSynchronize(e2));
+    out->build_ms = event_ms(e0, e1);
+    out->probe_ms = event_ms(e1, e2);
+    out->total_ms = event_ms(e0, e2);
+    if (materialize) {
+        rc = finish_result_columns(ctx, out, flags);
+        if (rc != AMJ_OK) {
+            amj_result_release(out);
+            return rc;
+        }
+    }
+    return AMJ_OK;
+}
+
 static int lftj_execute_impl(amj_ctx *ctx, amj_rel *const *rels, int nrels, int algo, int ooc, int ws, int flags,
                              const uint32_t *order, int norder, amj_result *out) {
     if (!ctx || !out || !rels || nrels <= 0) return fail(AMJ_EINVAL, "lftj_execute: bad arguments");
@@ -272,8 +359,7 @@ static int lftj_execute_impl(amj_ctx *ctx, amj_rel *const *rels, int nrels, int 
         if (!tri) return lftj_generic_execute(ctx, rels, nrels, ooc, flags, nullptr, out);
     }
     result_init(out, 3);
-    cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1], e2 = ctx->ev[2];
-    AMJ_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->ev[0], ctx->stream));
 
     Trie2 tries[3];
     const Trie2 *R = nullptr, *S = nullptr, *T = nullptr;
@@ -308,55 +394,5 @@ static int lftj_execute_impl(amj_ctx *ctx, amj_rel *const *rels, int nrels, int 
             *slot = &tries[i];
         }
     }
-    AMJ_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
-
-    // ws=0: every (a,b) pair intersected by its own lane; ws=1: long pairs
-    // shared by the whole warp
-    const int small_sum = ws ? 48 : 0x7fffffff;
-    // ws=1 also hands vertices with many children to the block-wide bitmap kernel
-    const uint32_t heavy_deg = ws ? (ctx->opts.lftj_heavy_degree ? ctx->opts.lftj_heavy_degree : 32u) : 0u;
-    const int32_t *rank_inv = nv ? inv.p : nullptr;
-    const bool materialize = (flags & AMJ_F_MATERIALIZE) != 0;
-    const uint64_t nr = R->len1;
-    uint64_t c = 0, h = 0, w = 0;
-    int rc = lftj_triangle(ctx, *R, *S, *T, algo, nullptr, 0, &c, &h, nullptr, small_sum, 0, nr, heavy_deg,
-                           out->kernel_ms, sorted_out, rank_inv, wedges.p, nv, ctx->opts.lftj_rank_bits);
-    if (rc != AMJ_OK) return rc;
-    int32_t *dcols[3] = {nullptr, nullptr, nullptr};
-    if (materialize) {
-        for (int a = 0; a < 3 && rc == AMJ_OK; a++) rc = dev_alloc(ctx, (void **)&dcols[a], (c ? c : 1) * 4);
-        uint64_t c2 = 0, h2 = 0;
-        if (rc == AMJ_OK)
-            rc = lftj_triangle(ctx, *R, *S, *T, algo, dcols, c, &c2, &h2, &w, small_sum, 0, nr, heavy_deg,
-                               out->kernel_ms + 2, sorted_out, rank_inv, wedges.p, nv, ctx->opts.lftj_rank_bits);
-        if (rc == AMJ_OK && (c2 != c || h2 != h || w != c))
-            rc = fail(AMJ_ECUDA, "LFTJ: write pass disagrees with count pass");
-        if (rc != AMJ_OK) {
-            for (int a = 0; a < 3; a++) dev_free(ctx, dcols[a]);
-            return rc;
-        }
-    }
-    out->count = c;
-    out->checksum = h;
-    out->stats[7] = 1;
-    if (materialize) {
-        auto *o = new ResultOwner();
-        o->ctx = ctx;
-        out->priv = o;
-        out->rows = c;
-        for (int a = 0; a < 3; a++) out->cols[a] = dcols[a];
-    }
-    AMJ_CUDA_TRY(cudaEventRecord(e2, ctx->stream));
-    AMJ_CUDA_TRY(cudaEventSynchronize(e2));
-    out->build_ms = event_ms(e0, e1);
-    out->probe_ms = event_ms(e1, e2);
-    out->total_ms = event_ms(e0, e2);
-    if (materialize) {
-        rc = finish_result_columns(ctx, out, flags);
-        if (rc != AMJ_OK) {
-            amj_result_release(out);
-            return rc;
-        }
-    }
-    return AMJ_OK;
+    return triangle_run(ctx, *R, *S, *T, algo, ws, flags, sorted_out, nv ? inv.p : nullptr, wedges.p, nv, out);
 }

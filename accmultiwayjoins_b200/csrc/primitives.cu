@@ -56,43 +56,24 @@ static int radix_sort_impl(amj_ctx *ctx, uint64_t *d_a, uint64_t *d_b, uint64_t 
     if (n <= 1 || nbits <= 0) return AMJ_OK;
     if (n > 0xffffffffull - RS_TILE) return fail(AMJ_EINVAL, "radix sort: more than 2^32 items");
     if (lo_bit < 0 || hi_bit > 64) return fail(AMJ_EINVAL, "radix sort: bad bit range");
-    // digits of up to 10 bits where that saves a pass over a large input
-    // (a wider digit costs a 4x larger count scan per pass)
-    const bool wide = n >= (1u << 20) && (nbits + RS_WIDE_BITS - 1) / RS_WIDE_BITS < (nbits + 7) / 8;
-    const int passes = wide ? (nbits + RS_WIDE_BITS - 1) / RS_WIDE_BITS : (nbits + 7) / 8;
+    const int passes = (nbits + 7) / 8;
     const int width = (nbits + passes - 1) / passes;
     const uint32_t nblocks = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
     DBuf<uint32_t> counts;
-    AMJ_TRY(counts.alloc(ctx, (size_t)(1u << width) * nblocks));
-    if (wide) {
-        static bool attr_set = false;   // per template instance
-        if (!attr_set) {
-            AMJ_CUDA_TRY(cudaFuncSetAttribute(rs_downsweep_wide_kernel<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)rs_wide_smem()));
-            attr_set = true;
-        }
-    }
+    AMJ_TRY(counts.alloc(ctx, (size_t)256 * nblocks));
     uint64_t *src = d_a, *dst = d_b;
     for (int p = 0; p < passes; p++) {
         const int shift = lo_bit + p * width;
         const int bits = (hi_bit - shift) < width ? (hi_bit - shift) : width;
         if (bits <= 0) break;
         note_launch(ctx);
-        if (wide)
-            rs_upsweep_kernel<KK, RS_WIDE_BITS><<<nblocks, RS_THREADS, 0, ctx->stream>>>(src, (uint32_t)n, shift, bits,
-                                                                                         counts.p, nblocks);
-        else
-            rs_upsweep_kernel<KK><<<nblocks, RS_THREADS, 0, ctx->stream>>>(src, (uint32_t)n, shift, bits, counts.p,
-                                                                           nblocks);
+        rs_upsweep_kernel<KK><<<nblocks, RS_THREADS, 0, ctx->stream>>>(src, (uint32_t)n, shift, bits, counts.p,
+                                                                       nblocks);
         AMJ_CUDA_TRY(cudaGetLastError());
         AMJ_TRY(scan_exclusive_u32(ctx, counts.p, counts.p, (uint64_t)(1u << bits) * nblocks, nullptr));
         note_launch(ctx);
-        if (wide)
-            rs_downsweep_wide_kernel<KK><<<nblocks, RS_THREADS, rs_wide_smem(), ctx->stream>>>(
-                src, dst, (uint32_t)n, shift, bits, counts.p, nblocks);
-        else
-            rs_downsweep_kernel<KK><<<nblocks, RS_THREADS, 0, ctx->stream>>>(src, dst, (uint32_t)n, shift, bits,
-                                                                             counts.p, nblocks);
+        rs_downsweep_kernel<KK><<<nblocks, RS_THREADS, 0, ctx->stream>>>(src, dst, (uint32_t)n, shift, bits,
+                                                                         counts.p, nblocks);
         AMJ_CUDA_TRY(cudaGetLastError());
         uint64_t *t = src;
         src = dst;

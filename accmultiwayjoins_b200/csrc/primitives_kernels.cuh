@@ -97,17 +97,15 @@ __device__ __forceinline__ uint64_t sort_key(uint64_t it) {
     return hash_pair((int32_t)(uint32_t)it, (int32_t)(uint32_t)(it >> 32));
 }
 
-// RB: the widest digit the kernels take (8, or 10 for the wide passes)
-template <int KK, int RB = 8>
+template <int KK>
 __global__ __launch_bounds__(RS_THREADS) void rs_upsweep_kernel(const uint64_t *__restrict__ in, uint32_t n,
                                                                  int shift, int bits,
                                                                  uint32_t *__restrict__ counts,
                                                                  uint32_t nblocks) {
-    constexpr int DM = 1 << RB;
-    __shared__ uint32_t h[RS_WARPS][DM];
+    __shared__ uint32_t h[RS_WARPS][256];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t D = 1u << bits, dmask = D - 1;
-    for (int i = threadIdx.x; i < RS_WARPS * DM; i += RS_THREADS) (&h[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_THREADS) (&h[0][0])[i] = 0;
     __syncthreads();
     const uint64_t base = (uint64_t)blockIdx.x * RS_TILE + (uint64_t)warp * RS_WARP_ITEMS;
 #pragma unroll 4
@@ -119,11 +117,11 @@ __global__ __launch_bounds__(RS_THREADS) void rs_upsweep_kernel(const uint64_t *
         }
     }
     __syncthreads();
-    for (uint32_t d = threadIdx.x; d < D; d += RS_THREADS) {
+    if ((uint32_t)threadIdx.x < D) {
         uint32_t s = 0;
 #pragma unroll
-        for (int w = 0; w < RS_WARPS; w++) s += h[w][d];
-        counts[(uint64_t)d * nblocks + blockIdx.x] = s;
+        for (int w = 0; w < RS_WARPS; w++) s += h[w][threadIdx.x];
+        counts[(uint64_t)threadIdx.x * nblocks + blockIdx.x] = s;
     }
 }
 
@@ -195,112 +193,6 @@ __global__ __launch_bounds__(RS_THREADS, 3) void rs_downsweep_kernel(const uint6
         if (idx < n) {
             const uint32_t d = (uint32_t)(sort_key<KK>(it[r]) >> shift) & dmask;
             tile[bstart[d] + wcnt[warp][d] + rk[r]] = it[r];
-        }
-    }
-    __syncthreads();
-    const uint64_t rem = n - tile_base;
-    const uint32_t cnt = rem < (uint64_t)RS_TILE ? (uint32_t)rem : (uint32_t)RS_TILE;
-    for (uint32_t i = threadIdx.x; i < cnt; i += RS_THREADS) {
-        const uint64_t v = tile[i];
-        const uint32_t d = (uint32_t)(sort_key<KK>(v) >> shift) & dmask;
-        out[goff[d] + (i - bstart[d])] = v;
-    }
-}
-
-// The down-sweep for digits of up to 10 bits (1024 digit runs per tile):
-// the same ranking, with the tile, the per-warp digit counts and the digit
-// offsets in dynamic shared memory (rs_wide_smem bytes), each thread owning
-// RS_WIDE_D / RS_THREADS consecutive digits for the tile's digit scan.
-constexpr int RS_WIDE_BITS = 10;
-constexpr int RS_WIDE_D = 1 << RS_WIDE_BITS;
-constexpr size_t rs_wide_smem() {
-    return RS_TILE * sizeof(uint64_t) + (size_t)(RS_WARPS + 2) * RS_WIDE_D * sizeof(uint32_t) +
-           RS_WARPS * sizeof(uint32_t);
-}
-
-template <int KK>
-__global__ __launch_bounds__(RS_THREADS, 3) void rs_downsweep_wide_kernel(const uint64_t *__restrict__ in,
-                                                                        uint64_t *__restrict__ out, uint32_t n,
-                                                                        int shift, int bits,
-                                                                        const uint32_t *__restrict__ offs,
-                                                                        uint32_t nblocks) {
-    constexpr int DM = RS_WIDE_D, DPT = DM / RS_THREADS;
-    extern __shared__ __align__(16) unsigned char rs_smem[];
-    uint64_t *tile = reinterpret_cast<uint64_t *>(rs_smem);
-    uint32_t *wcnt = reinterpret_cast<uint32_t *>(tile + RS_TILE);   // [RS_WARPS][DM]
-    uint32_t *bstart = wcnt + RS_WARPS * DM;
-    uint32_t *goff = bstart + DM;
-    uint32_t *wsum = goff + DM;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t D = 1u << bits, dmask = D - 1;
-    for (int i = threadIdx.x; i < RS_WARPS * DM; i += RS_THREADS) wcnt[i] = 0;
-    __syncthreads();
-
-    const uint64_t tile_base = (uint64_t)blockIdx.x * RS_TILE;
-    const uint64_t base = tile_base + (uint64_t)warp * RS_WARP_ITEMS;
-    const unsigned lt = lanemask_lt();
-    uint32_t *mycnt = wcnt + warp * DM;
-    uint64_t it[RS_IPT];
-    uint32_t rk[RS_IPT / 2] = {};   // ranks inside the tile (< 2^12), two per register
-#pragma unroll
-    for (int r = 0; r < RS_IPT; r++) {
-        const uint64_t idx = base + (uint64_t)r * 32 + lane;
-        it[r] = idx < n ? in[idx] : 0ull;
-    }
-#pragma unroll
-    for (int r = 0; r < RS_IPT; r++) {
-        const uint64_t idx = base + (uint64_t)r * 32 + lane;
-        const bool valid = idx < n;
-        const uint32_t d = valid ? ((uint32_t)(sort_key<KK>(it[r]) >> shift) & dmask) : 0u;
-        const unsigned peers = __match_any_sync(AMJ_FULL_MASK, valid ? d : 0xffffffffu) &
-                               __ballot_sync(AMJ_FULL_MASK, valid);
-        const uint32_t rank = __popc(peers & lt);
-        const uint32_t before = valid ? mycnt[d] : 0u;
-        __syncwarp();
-        if (valid && rank == 0) mycnt[d] = before + __popc(peers);
-        __syncwarp();
-        rk[r >> 1] |= (before + rank) << (16 * (r & 1));
-    }
-    __syncthreads();
-    // digits threadIdx.x * DPT .. + DPT - 1: exclusive counts over the warps,
-    // then the tile's exclusive digit starts
-    // (the digit totals wait in bstart, each thread reading back its own)
-    uint32_t tsum = 0;
-#pragma unroll
-    for (int k = 0; k < DPT; k++) {
-        const uint32_t d = threadIdx.x * DPT + k;
-        uint32_t run = 0;
-        if (d < D) {
-#pragma unroll
-            for (int w = 0; w < RS_WARPS; w++) {
-                const uint32_t c = wcnt[w * DM + d];
-                wcnt[w * DM + d] = run;
-                run += c;
-            }
-        }
-        bstart[d] = run;
-        tsum += run;
-    }
-    const uint32_t incl = warp_inclusive_scan(tsum, lane);
-    if (lane == 31) wsum[warp] = incl;
-    __syncthreads();
-    uint32_t ex = incl - tsum;
-    for (int w = 0; w < warp; w++) ex += wsum[w];
-#pragma unroll
-    for (int k = 0; k < DPT; k++) {
-        const uint32_t d = threadIdx.x * DPT + k;
-        const uint32_t t = bstart[d];
-        bstart[d] = ex;
-        ex += t;
-    }
-    for (uint32_t d = threadIdx.x; d < D; d += RS_THREADS) goff[d] = offs[(uint64_t)d * nblocks + blockIdx.x];
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < RS_IPT; r++) {
-        const uint64_t idx = base + (uint64_t)r * 32 + lane;
-        if (idx < n) {
-            const uint32_t d = (uint32_t)(sort_key<KK>(it[r]) >> shift) & dmask;
-            tile[bstart[d] + mycnt[d] + ((rk[r >> 1] >> (16 * (r & 1))) & 0xFFFFu)] = it[r];
         }
     }
     __syncthreads();

@@ -167,15 +167,15 @@ class Triangle:
         return ctx.lftj(rels, algo=self.algo, ws=1)
 
     def algorithmic_bytes(self):
-        """DFS (the wedge kernel over the degree-ranked copy): per edge its
-        (b, entry) item (8 B), the level-0 value a (4 B) and the end of a's
-        child range (8 B); per tested value 4 B, sum over a of C(d+(a), 2)
-        values with d+ the out-degree in (degree, id) order.  BFS / AMHJ:
+        """DFS and AMHJ TRI (the wedge kernel over the degree-ranked copy):
+        per edge its (b, entry) item (8 B), the level-0 value a (4 B) and the
+        end of a's child range (8 B); per tested value 4 B, sum over a of
+        C(d+(a), 2) values with d+ the out-degree in (degree, id) order.  BFS:
         every edge once (8 B), two row-pointer pairs (32 B) and the shorter
         child list of the edge once (4 B each), in the relation's order."""
         V = 1 << self.scale
         src, dst = self.src.astype(np.int64), self.dst.astype(np.int64)
-        if self.algo == "DFS":
+        if self.algo in ("DFS", "AMHJ"):
             deg = np.bincount(src, minlength=V) + np.bincount(dst, minlength=V)
             key_s, key_d = deg[src] * V + src, deg[dst] * V + dst
             lo = np.where(key_s < key_d, src, dst)
@@ -186,7 +186,8 @@ class Triangle:
         return self.E * (8 + 32) + 4 * int(shorter.sum())
 
     def kernel_name(self):
-        return "lftj_tri_wedge_kernel (intersection)" if self.algo == "DFS" else "lftj_tri_bfs kernels (intersection)"
+        return ("lftj_tri_wedge_kernel (intersection)" if self.algo in ("DFS", "AMHJ")
+                else "lftj_tri_bfs kernels (intersection)")
 
     def cpu_baseline(self):
         """The reference's MHJ-CPU multi-key probe on a bounded sample of

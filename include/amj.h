@@ -88,10 +88,12 @@ extern "C" {
 #define AMJ_F_CLIQUE4_LISTS 0x40 /* amj_lftj_execute with AMJ_F_CLIQUE4: join the
                                    degree-ordered copy by list intersections even where
                                    the triangle matrices fit (same result)          */
-#define AMJ_F_HASH_PLAN    0x200 /* amj_amhj_execute, FOUR over one edge relation: keep
-                                   the level-by-level hash-join plan where the triangle
-                                   matrices of the degree-ranked copy would answer the
-                                   last three levels (same result)                  */
+#define AMJ_F_HASH_PLAN    0x200 /* amj_amhj_execute, TRI / FOUR over one edge relation:
+                                   keep the level-by-level hash-join plan where a bitmap
+                                   of b's children (TRI) or the triangle matrices (FOUR)
+                                   of the degree-ranked copy would answer the pair-key
+                                   levels (same result; those apply to oriented
+                                   relations without repeated rows)                 */
 
 /* ---- relation residency ---- */
 #define AMJ_MEM_DEVICE 0   /* columns are device pointers, borrowed            */

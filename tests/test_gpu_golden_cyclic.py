@@ -6,8 +6,9 @@ driven through oracle/mhj_ref/mhj_ref_harness.cpp) over seeded R-MAT edge
 relations, up to the full triangle configuration (R-MAT scale 20, 2^24
 generated edges).  Every CUDA path that answers these queries is compared
 with them through the C ABI: AMHJ TRI / FOUR with each work-sharing switch,
-on the relation as given and on its degree-ordered copy, FOUR also through
-the triangle matrices; ALFTJ DFS (wedge
+on the relation as given and on its degree-ordered copy, through the
+bitmap / triangle-matrix levels and with every level a hash lookup; ALFTJ
+DFS (wedge
 kernel, lane merge), BFS; the ALFTJ 4-clique through the triangle matrices
 and through the list-intersection kernel.
 """
@@ -39,13 +40,15 @@ def test_triangle_paths_match_reference_golden(ctx, case):
     full = case["edges"] > 4_000_000
     runs = [("ALFTJ DFS ws=1", lambda: ctx.lftj([e], algo="DFS", ws=1)),
             ("ALFTJ BFS", lambda: ctx.lftj([e], algo="BFS")),
-            ("AMHJ TRI ws=1", lambda: ctx.amhj("TRI", [e], ws=1))]
+            ("AMHJ TRI ws=1", lambda: ctx.amhj("TRI", [e], ws=1)),
+            ("AMHJ TRI ws=1, hash plan", lambda: ctx.amhj("TRI", [e], ws=1, plan="hash"))]
     if not full:
         runs += [("ALFTJ DFS ws=0", lambda: ctx.lftj([e], algo="DFS", ws=0)),
                  ("ALFTJ DFS as given", lambda: ctx.lftj([e], algo="DFS", ws=1, degree_order=False)),
                  ("ALFTJ BFS as given", lambda: ctx.lftj([e], algo="BFS", degree_order=False)),
                  ("AMHJ TRI ws=0 as given", lambda: ctx.amhj("TRI", [e], degree_order=False)),
-                 ("AMHJ TRI ws=1 dro=1", lambda: ctx.amhj("TRI", [e], ws=1, dro=1))]
+                 ("AMHJ TRI ws=1 dro=1", lambda: ctx.amhj("TRI", [e], ws=1, dro=1)),
+                 ("AMHJ TRI ws=0 dro=1, hash plan", lambda: ctx.amhj("TRI", [e], dro=1, plan="hash"))]
     for name, run in runs:
         r = run()
         assert (r.count, r.checksum) == want(case), name

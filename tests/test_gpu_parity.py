@@ -329,20 +329,41 @@ def test_amhj_star_flat_path_with_repeated_dimension_keys(ctx):
 @pytest.mark.parametrize("qt", ["TRI", "FOUR"])
 @pytest.mark.parametrize("reorder", [True, False])
 @pytest.mark.parametrize("degree_order", [True, False])
-def test_amhj_tri_four(ctx, qt, reorder, degree_order):
+@pytest.mark.parametrize("plan", ["multiway", "hash"])
+def test_amhj_tri_four(ctx, qt, reorder, degree_order, plan):
     """Every switch, on the relation as given and on its degree-ordered copy
-    (the default for an oriented relation); tuples come out in increasing
-    order either way."""
+    (the default for an oriented relation), through the bitmap / triangle
+    matrix levels (plan "multiway" on the degree-ranked copy) and with every
+    level a hash lookup; tuples come out in increasing order either way."""
     s, d = data.rmat(10, 6000, 0.57, 0.19, 0.19, seed=21)
     e = ctx.relation([s, d], [0, 1])
     want = O.triangle(s, d) if qt == "TRI" else O.four_clique(s, d)
     for sw in SWITCHES:
-        got = ctx.amhj(qt, [e], reorder=reorder, degree_order=degree_order, **sw)
+        got = ctx.amhj(qt, [e], reorder=reorder, degree_order=degree_order, plan=plan, **sw)
         assert (got.count, got.checksum) == want, sw
-    got = ctx.amhj(qt, [e], materialize=True, reorder=reorder, degree_order=degree_order)
+    got = ctx.amhj(qt, [e], materialize=True, reorder=reorder, degree_order=degree_order, plan=plan)
     assert data.checksum(got.columns) == want[1]
     t = got.tuples()
     assert np.all(t[:, :-1] < t[:, 1:])
+
+
+@pytest.mark.parametrize("qt", ["TRI", "FOUR"])
+def test_amhj_tri_four_repeated_rows_keep_bag_semantics(ctx, qt):
+    """The hash join counts a repeated edge once per copy (a bag), the trie
+    paths join sets: an oriented relation with repeated rows takes the
+    level-by-level hash plan, equal to the oracle's multi-way join of the
+    attribute pattern, while ALFTJ gives the set result."""
+    s, d = data.rmat(9, 3000, 0.6, 0.15, 0.15, seed=3)
+    s2, d2 = np.concatenate([s, s[:300]]), np.concatenate([d, d[:300]])
+    e = ctx.relation([s2, d2], [0, 1])
+    pattern = O.tri_relations(s2, d2) if qt == "TRI" else O.four_relations(s2, d2)
+    want = O.mhj(pattern)
+    for sw in ({}, {"ws": 1}, {"ws": 1, "fib": 1}):
+        got = ctx.amhj(qt, [e], **sw)
+        assert (got.count, got.checksum) == want, sw
+    sets = ctx.lftj([e], clique4=qt == "FOUR")
+    assert sets.count < want[0]
+    assert (sets.count, sets.checksum) == (O.triangle(s, d) if qt == "TRI" else O.four_clique(s, d))
 
 
 def test_amhj_dro_residual_resume():
