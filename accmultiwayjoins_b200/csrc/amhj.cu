@@ -266,42 +266,15 @@ static int run_star_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws
     AMJ_TRY(ctr.alloc(ctx, 1));
     AMJ_TRY(over.alloc(ctx, rows ? rows : 1));
     AMJ_CUDA_TRY(cudaMemsetAsync(ctr.p, 0, sizeof(Ctr), ctx->stream));
-    // two-column levels (key, payload) interleaved: one sector per match
-    ProbePlan Pk = P;
-    std::vector<DBuf<int2>> kv(P.L);
-    for (int l = 0; l < P.L; l++) {
-        LevelDesc &lv = Pk.lv[l];
-        const uint32_t nrows = lv.nrows;
-        if (lv.ncols != 2 || lv.slots || !nrows) continue;
-        AMJ_TRY(kv[l].alloc(ctx, nrows));
-        note_launch(ctx);
-        star_interleave_kernel<<<(unsigned)std::min<uint64_t>((nrows + 255) / 256, (uint64_t)ctx->num_sms * 8), 256,
-                                 0, ctx->stream>>>(lv.col[0], lv.col[1], nrows, kv[l].p);
-        AMJ_CUDA_TRY(cudaGetLastError());
-        lv.slots = kv[l].p;
-    }
-    // the fact rows by bulk copies where every column's first row is
-    // 16-byte aligned and there is a full batch
-    bool bulk = rows >= (uint64_t)STAR_BATCH;
-    for (int c = 0; c < P.probe_ncols; c++) bulk &= ((uintptr_t)(P.probe_col[c] + row_lo) & 15u) == 0;
+    const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 8);
     note_launch(ctx);
     AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
-    if (bulk) {
-        int per_sm = 0;
-        AMJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, amhj_star_bulk_kernel, 256, 0));
-        const unsigned g = (unsigned)std::min<uint64_t>(rows / STAR_BATCH, (uint64_t)ctx->num_sms * std::max(per_sm, 1));
-        amhj_star_bulk_kernel<<<g, 256, 0, ctx->stream>>>(Pk, &ctr.p->count, &ctr.p->checksum, over.p,
-                                                          &ctr.p->nover, ctx->d_status);
-    } else {
-        const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 8);
-        amhj_star_kernel<<<g ? g : 1, 256, 0, ctx->stream>>>(Pk, &ctr.p->count, &ctr.p->checksum, over.p,
-                                                            &ctr.p->nover);
-    }
+    amhj_star_kernel<<<g ? g : 1, 256, 0, ctx->stream>>>(P, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover);
     AMJ_CUDA_TRY(cudaGetLastError());
     AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
     Ctr h{};
     AMJ_CUDA_TRY(cudaMemcpyAsync(&h, ctr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_TRY(status_check(ctx, "AMHJ star probe"));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     res->kernel_ms[0] += event_ms(ctx->kev[0], ctx->kev[1]);
     pr->count = h.count;
     pr->checksum = h.checksum;
@@ -725,7 +698,6 @@ void fill_level_desc(const LevelSpec &ls, int layout, int key_mode, uint32_t mas
 void fill_level_from_index(const LevelSpec &ls, const HashIndex &ix, LevelDesc *d) {
     const int32_t *cols[4] = {ix.cols[0].p, ix.cols[1].p, ix.cols[2].p, ix.cols[3].p};
     fill_level_desc(ls, ix.layout, ix.key_mode, ix.mask, ix.buc_ptrs.p, cols, ix.slots.p, d);
-    d->nrows = ix.n <= 0xffffffffull ? (uint32_t)ix.n : 0u;
 }
 
 static void fill_level(const LevelSpec &ls, const HashIndex &ix, LevelDesc *d) { fill_level_from_index(ls, ix, d); }

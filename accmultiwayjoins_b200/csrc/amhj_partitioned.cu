@@ -33,6 +33,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <vector>
@@ -277,6 +278,7 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
         AMJ_TRY(device_to_host(ctx, pr, &I));
     }
     uint64_t count = 0, checksum = 0, joins = 0;
+    double part_ms = 0, join_ms = 0;   // host clock: partitioning; part copies and joins
     HostTable fin;   // the last stage's rows, when materialised
     for (int j = 0; j < hp.L; j++) {
         const LevelSpec &ls = hp.lv[j];
@@ -304,8 +306,11 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
         const int nci = (int)I.attrs.size(), ncb = B->ncols, ncs = (int)S.size();
         const uint32_t P = parts_for(I.n * 4 * (uint64_t)nci, B->n * 4 * (uint64_t)ncb, budget);
         Parts ip, bp;
+        const auto tp0 = std::chrono::steady_clock::now();
         AMJ_TRY(partition_table(ctx, I, ik, P, &ip));
         AMJ_TRY(partition_table(ctx, Bt, ls.src_col[0], P, &bp));
+        const auto tp1 = std::chrono::steady_clock::now();
+        part_ms += std::chrono::duration<double, std::milli>(tp1 - tp0).count();
         // device slots for two part pairs
         DBuf<int32_t> dI[2], dB[2];
         for (int s = 0; s < 2; s++) {
@@ -401,6 +406,7 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
         // partitions and slots go
         const cudaError_t e1 = cudaStreamSynchronize(up);
         const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+        join_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp1).count();
         if (rc != AMJ_OK) return rc;
         if (e1 != cudaSuccess) return cuda_fail(e1, "AMHJ ooc: part copies");
         if (e2 != cudaSuccess) return cuda_fail(e2, "AMHJ ooc: part joins");
@@ -409,6 +415,8 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
     out->count = count;
     out->checksum = checksum;
     out->stats[7] = joins;   // partition pairs joined
+    out->kernel_ms[0] = part_ms;
+    out->kernel_ms[1] = join_ms;
     if (materialize) {
         auto *o = new ResultOwner();
         o->ctx = ctx;

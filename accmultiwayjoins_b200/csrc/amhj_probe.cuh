@@ -37,7 +37,6 @@ struct LevelDesc {
     int8_t key_attr[2];
     uint8_t cmp_mask, bind_mask;
     int8_t attr[4];
-    uint32_t nrows;   // rows of the index (bucket layout), 0 when not known
 };
 
 struct alignas(16) ProbePlan {

@@ -47,7 +47,6 @@ enum ErrSite : unsigned int {
     SITE_FIB = 7,          // frequent-item buffer state wait
     SITE_LFTJ_STACK = 8,   // LFTJ depth beyond the compiled bound
     SITE_TEST_WAIT = 9,    // bounded wait exercised by the self test
-    SITE_BULK_COPY = 10,   // completion of a bulk asynchronous copy
 };
 
 __device__ __forceinline__ void report_error(DevStatus *st, unsigned int code, unsigned int where,

@@ -63,7 +63,6 @@ static const char *site_name(unsigned w) {
         case SITE_FIB: return "frequent-item buffer";
         case SITE_LFTJ_STACK: return "LFTJ stack";
         case SITE_TEST_WAIT: return "test wait";
-        case SITE_BULK_COPY: return "bulk copy completion";
         default: return "kernel";
     }
 }

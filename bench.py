@@ -841,11 +841,13 @@ def run_ooc(args, rank, world, local_rank):
         r = ctx.amhj("NORMAL", host, ooc=1)
     sampler = ClockSampler(local_rank)
     sampler.start()
-    ms = []
+    ms, part_ms, join_ms = [], [], []
     for _ in range(args.steps):
         t1 = time.perf_counter()
         r = ctx.amhj("NORMAL", host, ooc=1)
         ms.append((time.perf_counter() - t1) * 1e3)
+        part_ms.append(r.kernel_ms[0])
+        join_ms.append(r.kernel_ms[1])
     clocks = sampler.stop()
     want = (r.count, r.checksum)
     check = {}
@@ -884,6 +886,8 @@ def run_ooc(args, rank, world, local_rank):
             "e2e": {"value": r.count / (m * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": 32 * n,
                     "d2h_bytes_per_step": 16, "note": "inputs start in host memory every step"},
             "check": check, "clocks": clocks,
+            "phase_ms": {"host_partitioning": sum(part_ms) / len(part_ms),
+                         "part_copies_and_joins": sum(join_ms) / len(join_ms)},
         }
         print(json.dumps(line), flush=True)
     for h in host:

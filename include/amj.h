@@ -142,7 +142,9 @@ typedef struct amj_result {
                                          [0] rank or bitmap [1] warp intersection, BFS
                                          [0] candidate count [1] expand ([2], [3]
                                          the same in a write pass); AMHJ [0] count
-                                         passes [1] write passes                  */
+                                         passes [1] write passes; AMHJ with build
+                                         relations in host memory (host clock) [0]
+                                         partitioning [1] part copies and joins   */
     void    *priv;                    /* library-owned                          */
 } amj_result;
 
