@@ -123,7 +123,73 @@ struct HostTable {
     std::vector<Piece> pieces;
     std::vector<Pinned> own;   // pinned blocks holding the pieces (intermediates)
     uint64_t n = 0;
+    // rows already grouped on the device by hash_key(column sub_col) &
+    // (SUB_PARTS - 1): sub[s] lists the pieces of group s (also in `pieces`)
+    int sub_col = -1;
+    std::vector<std::vector<Piece>> sub;
 };
+
+// ---- grouping a part's result rows on the device ----
+// The rows a stage returns form the next stage's intermediate, which is
+// partitioned on the next key.  They are grouped on the device into
+// SUB_PARTS groups by that key's hash before they are copied back, so that
+// a part of the next stage (P <= SUB_PARTS parts, P a power of two) is the
+// union of the groups s with s & (P - 1) == p, and the host scatters
+// nothing.  One count pass, a scan of the counts, then tiles of rows
+// scattered with one atomic reservation per group and tile.
+constexpr uint32_t SUB_PARTS = 256;
+constexpr uint32_t SUB_TILE = 4096;
+
+struct SubCols {
+    const int32_t *src[AMJ_MAX_ATTRS];
+    int nc;
+    int kc;
+};
+
+__global__ void sub_count_kernel(const int32_t *__restrict__ key, uint64_t n, unsigned int *__restrict__ cnt) {
+    __shared__ unsigned int h[SUB_PARTS];
+    for (uint32_t i = threadIdx.x; i < SUB_PARTS; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&h[hash_key(key[i]) & (SUB_PARTS - 1)], 1u);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < SUB_PARTS; i += blockDim.x)
+        if (h[i]) atomicAdd(&cnt[i], h[i]);
+}
+
+// cursor[s]: the next free row of group s in dst (column c at dst + c * n)
+__global__ void sub_scatter_kernel(const SubCols C, uint64_t n, unsigned int *__restrict__ cursor,
+                                   int32_t *__restrict__ dst) {
+    __shared__ unsigned int h[SUB_PARTS], base[SUB_PARTS];
+    for (uint64_t t0 = (uint64_t)blockIdx.x * SUB_TILE; t0 < n; t0 += (uint64_t)gridDim.x * SUB_TILE) {
+        for (uint32_t i = threadIdx.x; i < SUB_PARTS; i += blockDim.x) h[i] = 0;
+        __syncthreads();
+        const uint64_t t1 = t0 + SUB_TILE < n ? t0 + SUB_TILE : n;
+        constexpr int IPT = SUB_TILE / 256;
+        uint32_t grp[IPT], rk[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const uint64_t i = t0 + (uint64_t)k * blockDim.x + threadIdx.x;
+            if (i < t1) {
+                grp[k] = hash_key(C.src[C.kc][i]) & (SUB_PARTS - 1);
+                rk[k] = atomicAdd(&h[grp[k]], 1u);
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < SUB_PARTS; i += blockDim.x)
+            base[i] = h[i] ? atomicAdd(&cursor[i], h[i]) : 0u;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const uint64_t i = t0 + (uint64_t)k * blockDim.x + threadIdx.x;
+            if (i < t1) {
+                const uint64_t pos = (uint64_t)base[grp[k]] + rk[k];
+                for (int c = 0; c < C.nc; c++) dst[(uint64_t)c * n + pos] = C.src[c][i];
+            }
+        }
+        __syncthreads();
+    }
+}
 
 // A table hash-partitioned on one column: part p is a list of pieces.
 struct Parts {
@@ -145,6 +211,16 @@ int partition_table(amj_ctx *ctx, const HostTable &X, int kc, uint32_t P, Parts 
         for (const Piece &pc : X.pieces)
             if (pc.n) out->part[0].push_back(pc);
         out->rows[0] = out->max_rows = n;
+        return AMJ_OK;
+    }
+    if (X.sub_col == kc && P <= SUB_PARTS && X.sub.size() == SUB_PARTS) {
+        // grouped on the device already: part p is the union of its groups
+        for (uint32_t g = 0; g < SUB_PARTS; g++)
+            for (const Piece &pc : X.sub[g]) {
+                out->part[g & (P - 1)].push_back(pc);
+                out->rows[g & (P - 1)] += pc.n;
+            }
+        for (uint32_t p = 0; p < P; p++) out->max_rows = std::max(out->max_rows, out->rows[p]);
         return AMJ_OK;
     }
     if (n == 0) return AMJ_OK;
@@ -239,6 +315,200 @@ int device_to_host(amj_ctx *ctx, const amj_rel *r, HostTable *t) {
     return AMJ_OK;
 }
 
+// A part result's rows (device columns res.cols[0..nc-1]) grouped on column
+// kc into SUB_PARTS groups and copied into one pinned block of T: column c
+// at c * rows, group g's rows contiguous in every column.
+int group_rows(amj_ctx *ctx, const amj_result &res, int nc, int kc, HostTable *T) {
+    const uint64_t rows = res.rows;
+    Pinned b;
+    // the columns, then the group counts
+    AMJ_TRY(b.get(ctx, (size_t)nc * rows * sizeof(int32_t) + SUB_PARTS * sizeof(unsigned int)));
+    DBuf<unsigned int> cnt;
+    DBuf<int32_t> grouped;
+    AMJ_TRY(cnt.alloc(ctx, 2 * SUB_PARTS));   // counts, then cursors
+    AMJ_TRY(grouped.alloc(ctx, (size_t)nc * rows));
+    AMJ_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, SUB_PARTS * sizeof(unsigned int), ctx->stream));
+    const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 8);
+    note_launch(ctx);
+    sub_count_kernel<<<g, 256, 0, ctx->stream>>>(res.cols[kc], rows, cnt.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_TRY(scan_exclusive_u32(ctx, cnt.p, cnt.p + SUB_PARTS, SUB_PARTS, nullptr));
+    SubCols C{};
+    for (int c = 0; c < nc; c++) C.src[c] = res.cols[c];
+    C.nc = nc;
+    C.kc = kc;
+    const unsigned gt = (unsigned)std::min<uint64_t>((rows + SUB_TILE - 1) / SUB_TILE, (uint64_t)ctx->num_sms * 8);
+    note_launch(ctx);
+    sub_scatter_kernel<<<gt, 256, 0, ctx->stream>>>(C, rows, cnt.p + SUB_PARTS, grouped.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    int32_t *h = b.i32();
+    unsigned int *hcnt = reinterpret_cast<unsigned int *>(h + (uint64_t)nc * rows);
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h, grouped.p, (size_t)nc * rows * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(hcnt, cnt.p, SUB_PARTS * sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    uint64_t off = 0;
+    for (uint32_t s = 0; s < SUB_PARTS; s++) {
+        if (hcnt[s]) {
+            Piece pc;
+            pc.n = hcnt[s];
+            for (int c = 0; c < nc; c++) pc.col[c] = h + (uint64_t)c * rows + off;
+            T->sub[s].push_back(pc);
+            T->pieces.push_back(pc);
+        }
+        off += hcnt[s];
+    }
+    if (off != rows) return fail(AMJ_ECUDA, "AMHJ ooc: grouped rows do not add up");
+    T->n += rows;
+    T->own.push_back(std::move(b));
+    return AMJ_OK;
+}
+
+// X's rows grouped on column kc into SUB_PARTS groups on the device: the
+// rows stream through the device in chunks (copied in on the side stream
+// while the previous chunk is grouped), and each chunk comes back grouped
+// into a pinned block.  Replaces host scattering for tables in host memory.
+int group_on_device(amj_ctx *ctx, const HostTable &X, int kc, uint64_t budget, HostTable *out) {
+    HostTable T;
+    T.attrs = X.attrs;
+    T.sub_col = kc;
+    T.sub.assign(SUB_PARTS, {});
+    const int nc = (int)X.attrs.size();
+    if (X.n == 0) {
+        *out = std::move(T);
+        return AMJ_OK;
+    }
+    // chunk rows: three chunk buffers within a quarter of the budget
+    uint64_t CH = budget / 4 / (3 * (uint64_t)nc * sizeof(int32_t));
+    CH = std::max<uint64_t>(1u << 16, std::min<uint64_t>(CH, 1u << 24));
+    CH = std::min<uint64_t>(CH, X.n);
+    // the chunks as segments of pieces
+    struct Seg {
+        size_t piece;
+        uint64_t lo, hi;
+    };
+    std::vector<std::vector<Seg>> chunks;
+    std::vector<uint64_t> chunk_rows;
+    {
+        std::vector<Seg> cur;
+        uint64_t have = 0;
+        for (size_t i = 0; i < X.pieces.size(); i++) {
+            uint64_t lo = 0;
+            const uint64_t n = X.pieces[i].n;
+            while (lo < n) {
+                const uint64_t take = std::min(n - lo, CH - have);
+                cur.push_back({i, lo, lo + take});
+                lo += take;
+                have += take;
+                if (have == CH) {
+                    chunks.push_back(std::move(cur));
+                    chunk_rows.push_back(have);
+                    cur.clear();
+                    have = 0;
+                }
+            }
+        }
+        if (have) {
+            chunks.push_back(std::move(cur));
+            chunk_rows.push_back(have);
+        }
+    }
+    DBuf<int32_t> in[2], grouped;
+    DBuf<unsigned int> cnt;
+    for (auto &b : in) AMJ_TRY(b.alloc(ctx, (size_t)nc * CH));
+    AMJ_TRY(grouped.alloc(ctx, (size_t)nc * CH));
+    AMJ_TRY(cnt.alloc(ctx, 2 * SUB_PARTS));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));   // the buffers exist before the side stream writes them
+    cudaStream_t up = ctx->side_stream[0];
+    struct Events {
+        cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};   // [s]: chunk in slot s copied; [2+s]: slot s read
+        ~Events() {
+            for (auto x : e)
+                if (x) (void)cudaEventDestroy(x);
+        }
+    } ev;
+    for (auto &x : ev.e) AMJ_CUDA_TRY(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    auto upload = [&](size_t k, int s) -> int {
+        AMJ_CUDA_TRY(cudaStreamWaitEvent(up, ev.e[2 + s], 0));
+        uint64_t o = 0;
+        for (const Seg &g : chunks[k]) {
+            const Piece &pc = X.pieces[g.piece];
+            for (int c = 0; c < nc; c++)
+                AMJ_CUDA_TRY(cudaMemcpyAsync(in[s].p + (uint64_t)c * CH + o, pc.col[c] + g.lo, (g.hi - g.lo) * 4,
+                                             cudaMemcpyHostToDevice, up));
+            o += g.hi - g.lo;
+        }
+        AMJ_CUDA_TRY(cudaEventRecord(ev.e[s], up));
+        return AMJ_OK;
+    };
+    // slot events start out completed
+    AMJ_CUDA_TRY(cudaEventRecord(ev.e[2], ctx->stream));
+    AMJ_CUDA_TRY(cudaEventRecord(ev.e[3], ctx->stream));
+    std::vector<Pinned> blocks(chunks.size());
+    int rc = upload(0, 0);
+    for (size_t k = 0; k < chunks.size() && rc == AMJ_OK; k++) {
+        const int s = (int)(k & 1);
+        if (k + 1 < chunks.size()) rc = upload(k + 1, s ^ 1);
+        if (rc != AMJ_OK) break;
+        const uint64_t rows = chunk_rows[k];
+        rc = blocks[k].get(ctx, (size_t)nc * rows * sizeof(int32_t) + SUB_PARTS * sizeof(unsigned int));
+        if (rc != AMJ_OK) break;
+        cudaError_t e = cudaStreamWaitEvent(ctx->stream, ev.e[s], 0);
+        if (e == cudaSuccess) e = cudaMemsetAsync(cnt.p, 0, SUB_PARTS * sizeof(unsigned int), ctx->stream);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "AMHJ ooc: grouping");
+            break;
+        }
+        const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 8);
+        note_launch(ctx);
+        sub_count_kernel<<<g, 256, 0, ctx->stream>>>(in[s].p + (uint64_t)kc * CH, rows, cnt.p);
+        rc = scan_exclusive_u32(ctx, cnt.p, cnt.p + SUB_PARTS, SUB_PARTS, nullptr);
+        if (rc != AMJ_OK) break;
+        SubCols C{};
+        for (int c = 0; c < nc; c++) C.src[c] = in[s].p + (uint64_t)c * CH;
+        C.nc = nc;
+        C.kc = kc;
+        const unsigned gt = (unsigned)std::min<uint64_t>((rows + SUB_TILE - 1) / SUB_TILE, (uint64_t)ctx->num_sms * 8);
+        note_launch(ctx);
+        sub_scatter_kernel<<<gt, 256, 0, ctx->stream>>>(C, rows, cnt.p + SUB_PARTS, grouped.p);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventRecord(ev.e[2 + s], ctx->stream);   // slot s may be refilled
+        int32_t *h = blocks[k].i32();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h, grouped.p, (size_t)nc * rows * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h + (uint64_t)nc * rows, cnt.p, SUB_PARTS * sizeof(unsigned int),
+                                cudaMemcpyDeviceToHost, ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "AMHJ ooc: grouping");
+    }
+    const cudaError_t e1 = cudaStreamSynchronize(up);
+    const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+    if (rc != AMJ_OK) return rc;
+    if (e1 != cudaSuccess) return cuda_fail(e1, "AMHJ ooc: grouping copies");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "AMHJ ooc: grouping");
+    for (size_t k = 0; k < chunks.size(); k++) {
+        const uint64_t rows = chunk_rows[k];
+        int32_t *h = blocks[k].i32();
+        const unsigned int *hc = reinterpret_cast<const unsigned int *>(h + (uint64_t)nc * rows);
+        uint64_t off = 0;
+        for (uint32_t g = 0; g < SUB_PARTS; g++) {
+            if (hc[g]) {
+                Piece pc;
+                pc.n = hc[g];
+                for (int c = 0; c < nc; c++) pc.col[c] = h + (uint64_t)c * rows + off;
+                T.sub[g].push_back(pc);
+                T.pieces.push_back(pc);
+            }
+            off += hc[g];
+        }
+        if (off != rows) return fail(AMJ_ECUDA, "AMHJ ooc: grouped rows do not add up");
+        T.n += rows;
+        T.own.push_back(std::move(blocks[k]));
+    }
+    *out = std::move(T);
+    return AMJ_OK;
+}
+
 }  // namespace
 
 void pinned_cache_release(amj_ctx *ctx) {
@@ -307,6 +577,11 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
         const uint32_t P = parts_for(I.n * 4 * (uint64_t)nci, B->n * 4 * (uint64_t)ncb, budget);
         Parts ip, bp;
         const auto tp0 = std::chrono::steady_clock::now();
+        if (P > 1 && P <= SUB_PARTS) {
+            // rows not grouped on this key yet go through the device
+            if (I.sub_col != ik) AMJ_TRY(group_on_device(ctx, I, ik, budget, &I));
+            AMJ_TRY(group_on_device(ctx, Bt, ls.src_col[0], budget, &Bt));
+        }
         AMJ_TRY(partition_table(ctx, I, ik, P, &ip));
         AMJ_TRY(partition_table(ctx, Bt, ls.src_col[0], P, &bp));
         const auto tp1 = std::chrono::steady_clock::now();
@@ -348,6 +623,13 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
         next.attrs = S;
         HostTable &dst = last ? fin : next;
         dst.attrs = S;
+        // the next stage's key column among this stage's attributes
+        const int next_kc =
+            last ? -1 : (int)(std::lower_bound(S.begin(), S.end(), hp.lv[j + 1].attr[0]) - S.begin());
+        if (!last) {
+            next.sub_col = next_kc;
+            next.sub.assign(SUB_PARTS, {});
+        }
         const int f = (last && !materialize) ? 0 : AMJ_F_MATERIALIZE;   // result columns stay on the device
         int rc = todo.empty() ? AMJ_OK : upload(todo[0], 0);
         for (size_t t = 0; t < todo.size() && rc == AMJ_OK; t++) {
@@ -378,8 +660,12 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
                     count += res.count;
                     checksum += res.checksum;
                 }
-                if (f && res.rows) {
-                    // the part's rows into a pinned block of the next table
+                if (f && res.rows && !last) {
+                    // the part's rows grouped by the next key on the device,
+                    // then into a pinned block of the next table
+                    rc = group_rows(ctx, res, ncs, next_kc, &dst);
+                } else if (f && res.rows) {
+                    // the last stage's rows into a pinned block of the result
                     Pinned b;
                     rc = b.get(ctx, (size_t)ncs * res.rows * sizeof(int32_t));
                     Piece out_pc;
