@@ -31,10 +31,11 @@ same queries and p50/p99 latencies of both forms.
 * roofline: the intersection kernels (triangle) or the probe kernel (chain),
   timed with CUDA events inside the library; algorithmic bytes per launch
   as documented below; traffic from the committed ncu capture.
-* configs (default triangle run, one GPU): the chain and the batched
-  configurations measured in the same run, each with its own value, e2e and
-  CPU figure; the batched record carries batched vs one-query-per-call
-  tuples/s and p50/p99 latencies.
+* configs (default triangle run, one GPU): the chain, skewed 4-clique (AMHJ
+  FOUR ws=1 fib=1, R-MAT scale 22), star and batched configurations measured
+  in the same run, each with its own value, e2e and CPU figure; the batched
+  record carries batched vs one-query-per-call tuples/s and p50/p99
+  latencies.
 * cpu_baseline and --impl reference: the reference's MHJ-CPU
   (MHJ-CPU/MHJ.cpp) compiled from its sources into oracle/_ref, on all host
   cores: as shipped for chains and stars; its multi-key probe branch for the
@@ -1046,8 +1047,14 @@ def chain_record(args, ctx, dev, stream, steps=10, warmup=3):
     AMHJ NORMAL: device time per query with the relations resident, the same
     through the C ABI from pinned host buffers, and the reference's MHJ-CPU
     on the full workload."""
+    return config_record(args, ctx, dev, stream, Chain(args, 0), steps, warmup)
+
+
+def config_record(args, ctx, dev, stream, wl, steps=10, warmup=3):
+    """One configuration measured beside the headline: device time per query
+    with the relations resident, the same through the C ABI from pinned host
+    buffers, the main kernel's roofline fraction, and the CPU figure."""
     import torch
-    wl = Chain(args, 0)
     rels = wl.device_relations(ctx, dev)
     for _ in range(warmup):
         r = wl.run(ctx, rels)
@@ -1083,22 +1090,34 @@ def chain_record(args, ctx, dev, stream, steps=10, warmup=3):
     kms = sum(probe) / len(probe)
     alg = wl.algorithmic_bytes()
     rec = {"workload": wl.describe(""), "value": want[0] / (m * 1e-3), "unit": "tuples/s", "ms_per_step": m,
-           "steps": steps, "output_tuples": want[0],
+           "steps": steps, "output_tuples": want[0], "checksum": f"{want[1]:016x}",
            "e2e": {"value": want[0] / (e * 1e-3), "unit": "tuples/s", "h2d_bytes_per_step": wl.h2d,
                    "d2h_bytes_per_step": 16, "ms_per_step": e},
-           "probe_kernel": {"ms": kms, "alg_bytes": alg, "frac_of_hbm": alg / (kms * 1e-3) / 1e9 / hbm}}
+           "probe_kernel": {"kernel": wl.kernel_name(), "ms": kms}}
+    if alg:
+        rec["probe_kernel"].update({"alg_bytes": alg, "frac_of_hbm": alg / (kms * 1e-3) / 1e9 / hbm})
     if not args.no_cpu_baseline:
         c_cnt, c_chk, sec, cores, kind, sample = wl.cpu_baseline()
         rec["cpu_baseline"] = {"value": c_cnt / sec, "unit": "tuples/s", "cores": cores, "kind": kind,
-                               "sample": sample, "matches_gpu": bool((c_cnt, c_chk) == want)}
+                               "sample": sample}
+        if c_chk is not None:
+            rec["cpu_baseline"]["matches_gpu"] = bool((c_cnt, c_chk) == want)
     return rec
 
 
 def other_configs(args, ctx, dev, stream, local_rank):
-    """Records of the chain (C1) and batched (C4) configurations, carried on
-    the default line beside the triangle headline."""
+    """Records of the chain (C1), skewed 4-clique (C3a, the configured AMHJ
+    FOUR ws=1 fib=1 on R-MAT scale 22), star (C3b) and batched (C4)
+    configurations, carried on the default line beside the triangle
+    headline."""
     import copy
     out = {"chain": chain_record(args, ctx, dev, stream)}
+    fargs = copy.copy(args)
+    fargs.scale, fargs.algo = 22, "AMHJ"
+    out["four"] = config_record(fargs, ctx, dev, stream, Clique4(fargs, 0), steps=3, warmup=2)
+    sargs = copy.copy(args)
+    sargs.star_rows = 60_000_000
+    out["star"] = config_record(sargs, ctx, dev, stream, Star(sargs, 0), steps=10, warmup=3)
     bargs = copy.copy(args)
     bargs.queries, bargs.steps, bargs.warmup = 512, 5, 3
     bl = batch_line(bargs, 0, 1, local_rank, fixed_point=TUNED_BATCH_POINT, cpu_budget=10.0)
