@@ -945,6 +945,7 @@ __global__ void lftj_tri_bfs_count_kernel(const __grid_constant__ TriArgs A, uns
 constexpr int BFS_TILE = 2048;
 constexpr int BFS_THREADS = 256;
 constexpr int BFS_SMEM_ENTRIES = 2048;
+constexpr int BFS_RUN = BFS_TILE / BFS_THREADS;   // consecutive candidates per thread
 
 __device__ __forceinline__ uint64_t upper_bound_u64(const unsigned long long *a, uint64_t lo, uint64_t hi,
                                                     unsigned long long v) {
@@ -979,27 +980,47 @@ __global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const 
         if (in_smem)
             for (uint64_t k = threadIdx.x; k < ne; k += BFS_THREADS) s_off[k] = offs[e0 + k];
         __syncthreads();
-        for (unsigned long long t = tile + threadIdx.x; t < tend; t += BFS_THREADS) {
-            uint64_t e;
-            if (in_smem) {
-                uint64_t lo = 0, hi = ne;
-                while (lo < hi) {
-                    uint64_t mid = (lo + hi) >> 1;
-                    if (s_off[mid] <= t) lo = mid + 1;
-                    else hi = mid;
+        // each thread takes a run of BFS_RUN consecutive candidates: its
+        // edge is searched once, then followed forward, and the edge's child
+        // ranges and ids are read when the edge changes
+        const unsigned long long t0 = tile + (unsigned long long)threadIdx.x * BFS_RUN;
+        const unsigned long long t1 = t0 + BFS_RUN < tend ? t0 + BFS_RUN : tend;
+        uint64_t e = ~0ull, sb = 0, eb = 0, ta = 0, ea = 0, nxt = 0, cur = 0;
+        int32_t a = 0, b = 0, xa = 0, xb = 0;
+        uint64_t hab = 0;
+        bool s_short = false;
+        for (unsigned long long t = t0; t < t1; t++) {
+            if (e == ~0ull || t >= nxt) {
+                if (e == ~0ull) {
+                    if (in_smem) {
+                        uint64_t lo = 0, hi = ne;
+                        while (lo < hi) {
+                            uint64_t mid = (lo + hi) >> 1;
+                            if (s_off[mid] <= t) lo = mid + 1;
+                            else hi = mid;
+                        }
+                        e = e0 + lo - 1;
+                    } else {
+                        e = upper_bound_u64(offs, e0, e1 + 1, t) - 1;
+                    }
+                } else {
+                    do e++;
+                    while (offs[e + 1] <= t);   // edges without candidates are passed over
                 }
-                e = e0 + lo - 1;
-            } else {
-                e = upper_bound_u64(offs, e0, e1 + 1, t) - 1;
+                cur = offs[e];
+                nxt = offs[e + 1];
+                a = A.r_src[e];
+                b = A.r_dst[e];
+                child_range(A.S, b, sb, eb);
+                child_range(A.T, a, ta, ea);
+                // expand the shorter list, search the longer (wedge form:
+                // expand T(a) after b, search S(b))
+                s_short = !A.bfs_wedge && (eb - sb) <= (ea - ta);
+                xa = A.inv ? A.inv[a] : a;
+                xb = A.inv ? A.inv[b] : b;
+                hab = amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, xa), xb);
             }
-            const unsigned long long k = t - offs[e];
-            const int32_t a = A.r_src[e], b = A.r_dst[e];
-            uint64_t sb, eb, ta, ea;
-            child_range(A.S, b, sb, eb);
-            child_range(A.T, a, ta, ea);
-            // expand the shorter list, search the longer (wedge form: expand
-            // T(a) after b, search S(b))
-            const bool s_short = !A.bfs_wedge && (eb - sb) <= (ea - ta);
+            const unsigned long long k = t - cur;
             const int32_t c = s_short ? A.S.data1[sb + k]
                                       : A.T.data1[(A.bfs_wedge ? A.r_lo + e + 1 : ta) + k];
             const int32_t *hay = s_short ? A.T.data1 : A.S.data1;
@@ -1011,9 +1032,9 @@ __global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const 
             }
             const bool found = lo < (s_short ? ea : eb) && hay[lo] == c;
             if (found) {
-                const int32_t xa = A.inv ? A.inv[a] : a, xb = A.inv ? A.inv[b] : b, xc = A.inv ? A.inv[c] : c;
+                const int32_t xc = A.inv ? A.inv[c] : c;
                 cnt++;
-                chk += tri_chk(A, amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, xa), xb), xa, xb, xc);
+                chk += tri_chk(A, hab, xa, xb, xc);
                 if (WRITE) {
                     const unsigned long long p = atomicAdd(A.out_cursor, 1ull);
                     if (p < A.out_cap) tri_store(A, p, xa, xb, xc);
