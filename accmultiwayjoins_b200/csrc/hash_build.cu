@@ -125,6 +125,85 @@ static unsigned grid_for(amj_ctx *ctx, uint64_t n, int threads = 256) {
     return (unsigned)g;
 }
 
+// ---- counting build (the operator's indexes up to BUCKET_COUNT_MAX rows) ----
+// One count pass over the rows' buckets, a scan, and one scatter pass that
+// claims each row's slot with an atomic on its bucket's cursor: three
+// kernels instead of the radix sort's passes, which are launch-bound at
+// these sizes.  The lanes of a warp that fall in one bucket share one atomic
+// (a hot key costs one atomic per warp, not per row).  Rows keep no order
+// inside a bucket, as in the reference's build (shared-memory atomics); every
+// probe path reads a bucket as a set.
+constexpr uint64_t BUCKET_COUNT_MAX = 1ull << 23;
+
+struct BucketCols {
+    const int32_t *in[4];
+    int32_t *out[4];
+    int ncols;
+    int key_mode;
+    uint32_t mask;
+};
+
+__device__ __forceinline__ uint32_t row_bucket(const BucketCols &C, uint64_t i) {
+    const uint32_t k = C.key_mode == KEY_PAIR ? hash_pair(C.in[0][i], C.in[1][i]) : (uint32_t)C.in[0][i];
+    return k & C.mask;
+}
+
+__global__ void bucket_count_kernel(const BucketCols C, uint64_t n, uint32_t *__restrict__ counts) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint64_t i = base + lane;
+        const bool valid = i < n;
+        const uint32_t b = valid ? row_bucket(C, i) : 0xffffffffu;
+        const unsigned peers = __match_any_sync(AMJ_FULL_MASK, b);
+        if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&counts[b], (uint32_t)__popc(peers));
+    }
+}
+
+__global__ void bucket_scatter_kernel(const BucketCols C, uint64_t n, uint32_t *__restrict__ cursor) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint64_t i = base + lane;
+        const bool valid = i < n;
+        const uint32_t b = valid ? row_bucket(C, i) : 0xffffffffu;
+        const unsigned peers = __match_any_sync(AMJ_FULL_MASK, b);
+        const int leader = __ffs(peers) - 1;
+        uint32_t at = 0;
+        if (valid && lane == leader) at = atomicAdd(&cursor[b], (uint32_t)__popc(peers));
+        at = __shfl_sync(AMJ_FULL_MASK, at, leader);
+        if (valid) {
+            const uint32_t pos = at + __popc(peers & lanemask_lt());
+            for (int c = 0; c < C.ncols; c++) C.out[c][pos] = C.in[c][i];
+        }
+    }
+}
+
+static int build_bucket_counting(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, uint64_t n, int key_mode,
+                                 uint64_t B, HashIndex *out) {
+    BucketCols C{};
+    for (int c = 0; c < ncols; c++) {
+        C.in[c] = d_cols[c];
+        C.out[c] = out->cols[c].p;
+    }
+    C.ncols = ncols;
+    C.key_mode = key_mode;
+    C.mask = out->mask;
+    AMJ_CUDA_TRY(cudaMemsetAsync(out->buc_ptrs.p, 0, (B + 1) * sizeof(uint32_t), ctx->stream));
+    note_launch(ctx);
+    bucket_count_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(C, n, out->buc_ptrs.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_TRY(scan_exclusive_u32(ctx, out->buc_ptrs.p, out->buc_ptrs.p, B + 1, nullptr));
+    DBuf<uint32_t> cursor;
+    AMJ_TRY(cursor.alloc(ctx, B));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(cursor.p, out->buc_ptrs.p, B * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                 ctx->stream));
+    note_launch(ctx);
+    bucket_scatter_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(C, n, cursor.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    return AMJ_OK;
+}
+
 static int build_bucket(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, uint64_t n, int key_mode,
                         HashIndex *out) {
     const uint64_t B = n ? floor_pow2(n) : 1;
@@ -137,6 +216,7 @@ static int build_bucket(amj_ctx *ctx, const int32_t *const *d_cols, int ncols, u
         AMJ_CUDA_TRY(cudaMemsetAsync(out->buc_ptrs.p, 0, (B + 1) * sizeof(uint32_t), ctx->stream));
         return AMJ_OK;
     }
+    if (n <= BUCKET_COUNT_MAX) return build_bucket_counting(ctx, d_cols, ncols, n, key_mode, B, out);
     DBuf<uint64_t> a, b;
     AMJ_TRY(a.alloc(ctx, n));
     AMJ_TRY(b.alloc(ctx, n));
