@@ -316,37 +316,64 @@ int device_to_host(amj_ctx *ctx, const amj_rel *r, HostTable *t) {
 }
 
 // A part result's rows (device columns res.cols[0..nc-1]) grouped on column
-// kc into SUB_PARTS groups and copied into one pinned block of T: column c
-// at c * rows, group g's rows contiguous in every column.
-int group_rows(amj_ctx *ctx, const amj_result &res, int nc, int kc, HostTable *T) {
-    const uint64_t rows = res.rows;
-    Pinned b;
-    // the columns, then the group counts
-    AMJ_TRY(b.get(ctx, (size_t)nc * rows * sizeof(int32_t) + SUB_PARTS * sizeof(unsigned int)));
+// kc into SUB_PARTS groups on the context stream, then copied into one
+// pinned block (column c at c * rows, group g's rows contiguous in every
+// column, the group counts after the columns) on the second side stream, so
+// that the copy overlaps the next part's join.  group_rows_finish waits for
+// the copy and hands the groups to the next table.
+struct PendingGroup {
+    bool active = false;
+    Pinned block;
     DBuf<unsigned int> cnt;
     DBuf<int32_t> grouped;
-    AMJ_TRY(cnt.alloc(ctx, 2 * SUB_PARTS));   // counts, then cursors
-    AMJ_TRY(grouped.alloc(ctx, (size_t)nc * rows));
-    AMJ_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, SUB_PARTS * sizeof(unsigned int), ctx->stream));
+    uint64_t rows = 0;
+    int nc = 0;
+    cudaEvent_t done = nullptr;
+};
+
+int group_rows_start(amj_ctx *ctx, const amj_result &res, int nc, int kc, cudaEvent_t grouped_ev, cudaEvent_t done_ev,
+                     PendingGroup *pg) {
+    const uint64_t rows = res.rows;
+    pg->rows = rows;
+    pg->nc = nc;
+    pg->done = done_ev;
+    AMJ_TRY(pg->block.get(ctx, (size_t)nc * rows * sizeof(int32_t) + SUB_PARTS * sizeof(unsigned int)));
+    AMJ_TRY(pg->cnt.alloc(ctx, 2 * SUB_PARTS));   // counts, then cursors
+    AMJ_TRY(pg->grouped.alloc(ctx, (size_t)nc * rows));
+    AMJ_CUDA_TRY(cudaMemsetAsync(pg->cnt.p, 0, SUB_PARTS * sizeof(unsigned int), ctx->stream));
     const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 8);
     note_launch(ctx);
-    sub_count_kernel<<<g, 256, 0, ctx->stream>>>(res.cols[kc], rows, cnt.p);
+    sub_count_kernel<<<g, 256, 0, ctx->stream>>>(res.cols[kc], rows, pg->cnt.p);
     AMJ_CUDA_TRY(cudaGetLastError());
-    AMJ_TRY(scan_exclusive_u32(ctx, cnt.p, cnt.p + SUB_PARTS, SUB_PARTS, nullptr));
+    AMJ_TRY(scan_exclusive_u32(ctx, pg->cnt.p, pg->cnt.p + SUB_PARTS, SUB_PARTS, nullptr));
     SubCols C{};
     for (int c = 0; c < nc; c++) C.src[c] = res.cols[c];
     C.nc = nc;
     C.kc = kc;
     const unsigned gt = (unsigned)std::min<uint64_t>((rows + SUB_TILE - 1) / SUB_TILE, (uint64_t)ctx->num_sms * 8);
     note_launch(ctx);
-    sub_scatter_kernel<<<gt, 256, 0, ctx->stream>>>(C, rows, cnt.p + SUB_PARTS, grouped.p);
+    sub_scatter_kernel<<<gt, 256, 0, ctx->stream>>>(C, rows, pg->cnt.p + SUB_PARTS, pg->grouped.p);
     AMJ_CUDA_TRY(cudaGetLastError());
-    int32_t *h = b.i32();
-    unsigned int *hcnt = reinterpret_cast<unsigned int *>(h + (uint64_t)nc * rows);
-    AMJ_CUDA_TRY(cudaMemcpyAsync(h, grouped.p, (size_t)nc * rows * sizeof(int32_t), cudaMemcpyDeviceToHost,
-                                 ctx->stream));
-    AMJ_CUDA_TRY(cudaMemcpyAsync(hcnt, cnt.p, SUB_PARTS * sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
-    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    AMJ_CUDA_TRY(cudaEventRecord(grouped_ev, ctx->stream));
+    cudaStream_t back = ctx->side_stream[1];
+    AMJ_CUDA_TRY(cudaStreamWaitEvent(back, grouped_ev, 0));
+    int32_t *h = pg->block.i32();
+    pg->active = true;   // from here the copies may be in flight
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h, pg->grouped.p, (size_t)nc * rows * sizeof(int32_t), cudaMemcpyDeviceToHost, back));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h + (uint64_t)nc * rows, pg->cnt.p, SUB_PARTS * sizeof(unsigned int),
+                                 cudaMemcpyDeviceToHost, back));
+    AMJ_CUDA_TRY(cudaEventRecord(done_ev, back));
+    return AMJ_OK;
+}
+
+int group_rows_finish(amj_ctx *ctx, PendingGroup *pg, HostTable *T) {
+    (void)ctx;
+    AMJ_CUDA_TRY(cudaEventSynchronize(pg->done));
+    pg->active = false;
+    const uint64_t rows = pg->rows;
+    const int nc = pg->nc;
+    int32_t *h = pg->block.i32();
+    const unsigned int *hcnt = reinterpret_cast<const unsigned int *>(h + (uint64_t)nc * rows);
     uint64_t off = 0;
     for (uint32_t s = 0; s < SUB_PARTS; s++) {
         if (hcnt[s]) {
@@ -360,7 +387,9 @@ int group_rows(amj_ctx *ctx, const amj_result &res, int nc, int kc, HostTable *T
     }
     if (off != rows) return fail(AMJ_ECUDA, "AMHJ ooc: grouped rows do not add up");
     T->n += rows;
-    T->own.push_back(std::move(b));
+    T->own.push_back(std::move(pg->block));
+    pg->grouped.release();   // the copies are done: stream-ordered frees are safe
+    pg->cnt.release();
     return AMJ_OK;
 }
 
@@ -631,6 +660,16 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
             next.sub.assign(SUB_PARTS, {});
         }
         const int f = (last && !materialize) ? 0 : AMJ_F_MATERIALIZE;   // result columns stay on the device
+        PendingGroup pend[2];
+        uint32_t npend = 0;
+        struct GroupEvents {
+            cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};   // [s]: grouped; [2+s]: copied back
+            ~GroupEvents() {
+                for (auto x : e)
+                    if (x) (void)cudaEventDestroy(x);
+            }
+        } gev;
+        for (auto &x : gev.e) AMJ_CUDA_TRY(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
         int rc = todo.empty() ? AMJ_OK : upload(todo[0], 0);
         for (size_t t = 0; t < todo.size() && rc == AMJ_OK; t++) {
             const uint32_t p = todo[t];
@@ -662,8 +701,14 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
                 }
                 if (f && res.rows && !last) {
                     // the part's rows grouped by the next key on the device,
-                    // then into a pinned block of the next table
-                    rc = group_rows(ctx, res, ncs, next_kc, &dst);
+                    // then copied into a pinned block of the next table while
+                    // the next part is joined (the copy two parts back is
+                    // finished first)
+                    PendingGroup &pg = pend[npend & 1];
+                    if (pg.active) rc = group_rows_finish(ctx, &pg, &dst);
+                    if (rc == AMJ_OK)
+                        rc = group_rows_start(ctx, res, ncs, next_kc, gev.e[npend & 1], gev.e[2 + (npend & 1)], &pg);
+                    npend++;
                 } else if (f && res.rows) {
                     // the last stage's rows into a pinned block of the result
                     Pinned b;
@@ -688,10 +733,15 @@ int amhj_partitioned_execute(amj_ctx *ctx, const HostPlan &hp, int ws, int dro, 
             if (rp) amj_rel_release(rp);
             if (rb) amj_rel_release(rb);
         }
-        // the side stream's copies and the result copies end before the
+        // the side streams' copies and the result copies end before the
         // partitions and slots go
         const cudaError_t e1 = cudaStreamSynchronize(up);
+        const cudaError_t e3 = cudaStreamSynchronize(ctx->side_stream[1]);
         const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+        for (PendingGroup &pg : pend)
+            if (pg.active && rc == AMJ_OK && e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess)
+                rc = group_rows_finish(ctx, &pg, &dst);
+        if (e3 != cudaSuccess && rc == AMJ_OK) rc = cuda_fail(e3, "AMHJ ooc: result copies");
         join_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp1).count();
         if (rc != AMJ_OK) return rc;
         if (e1 != cudaSuccess) return cuda_fail(e1, "AMHJ ooc: part copies");
