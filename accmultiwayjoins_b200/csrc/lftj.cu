@@ -985,7 +985,7 @@ __global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const 
         // ranges and ids are read when the edge changes
         const unsigned long long t0 = tile + (unsigned long long)threadIdx.x * BFS_RUN;
         const unsigned long long t1 = t0 + BFS_RUN < tend ? t0 + BFS_RUN : tend;
-        uint64_t e = ~0ull, sb = 0, eb = 0, ta = 0, ea = 0, nxt = 0, cur = 0, last = 0;
+        uint64_t e = ~0ull, sb = 0, eb = 0, ta = 0, ea = 0, nxt = 0, cur = 0;
         int32_t a = 0, b = 0, xa = 0, xb = 0;
         uint64_t hab = 0;
         bool s_short = false;
@@ -1019,32 +1019,18 @@ __global__ __launch_bounds__(BFS_THREADS) void lftj_tri_bfs_expand_kernel(const 
                 xa = A.inv ? A.inv[a] : a;
                 xb = A.inv ? A.inv[b] : b;
                 hab = amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, xa), xb);
-                last = s_short ? ta : sb;
             }
             const unsigned long long k = t - cur;
             const int32_t c = s_short ? A.S.data1[sb + k]
                                       : A.T.data1[(A.bfs_wedge ? A.r_lo + e + 1 : ta) + k];
             const int32_t *hay = s_short ? A.T.data1 : A.S.data1;
-            // the run's candidates of one edge increase: search from the last
-            // position found, galloping, then bisecting
-            const uint64_t end = s_short ? ea : eb;
-            uint64_t lo = last;
-            if (lo < end && hay[lo] < c) {
-                uint64_t step = 1;
-                while (lo + step < end && hay[lo + step] < c) {
-                    lo += step;
-                    step <<= 1;
-                }
-                uint64_t hi = lo + step < end ? lo + step : end;
-                lo++;
-                while (lo < hi) {
-                    const uint64_t mid = (lo + hi) >> 1;
-                    if (hay[mid] < c) lo = mid + 1;
-                    else hi = mid;
-                }
+            uint64_t lo = s_short ? ta : sb, hi = s_short ? ea : eb;
+            while (lo < hi) {
+                uint64_t mid = (lo + hi) >> 1;
+                if (hay[mid] < c) lo = mid + 1;
+                else hi = mid;
             }
-            last = lo;
-            const bool found = lo < end && hay[lo] == c;
+            const bool found = lo < (s_short ? ea : eb) && hay[lo] == c;
             if (found) {
                 const int32_t xc = A.inv ? A.inv[c] : c;
                 cnt++;
