@@ -302,10 +302,55 @@ static int run_star_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws
     return AMJ_OK;
 }
 
+// Materialised star plan (dro=0): per-row tuple counts, a scan, exact
+// allocation, and one flat write pass (amhj_star.cuh).
+static int run_star_write(amj_ctx *ctx, ProbeLaunch &PL, uint64_t row_lo, uint64_t row_hi, PassResult *pr,
+                          amj_result *res) {
+    PL.P.row_lo = row_lo;
+    PL.P.row_hi = row_hi;
+    ProbePlan P = PL.P;
+    const uint64_t rows = row_hi - row_lo;
+    DBuf<unsigned long long> off, ctr;
+    AMJ_TRY(off.alloc(ctx, rows + 1));
+    AMJ_TRY(ctr.alloc(ctx, 2));
+    const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 8);
+    note_launch(ctx);
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
+    star_rowcount_kernel<<<g ? g : 1, 256, 0, ctx->stream>>>(P, off.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
+    AMJ_TRY(scan_exclusive_u64(ctx, (const uint64_t *)off.p, (uint64_t *)off.p, rows, (uint64_t *)off.p + rows));
+    unsigned long long total = 0;
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&total, off.p + rows, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    res->kernel_ms[0] += event_ms(ctx->kev[0], ctx->kev[1]);
+    AMJ_TRY(alloc_cols(ctx, P.k, total, pr->cols));
+    for (int a = 0; a < P.k; a++) P.out[a] = pr->cols[a];
+    P.out_cap = total;
+    AMJ_CUDA_TRY(cudaMemsetAsync(ctr.p, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    note_launch(ctx);
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[2], ctx->stream));
+    star_write_kernel<<<g ? g : 1, 256, 0, ctx->stream>>>(P, off.p, ctr.p, ctr.p + 1);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[3], ctx->stream));
+    unsigned long long h[2] = {0, 0};
+    AMJ_CUDA_TRY(cudaMemcpyAsync(h, ctr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    res->kernel_ms[1] += event_ms(ctx->kev[2], ctx->kev[3]);
+    if (h[0] != total) return fail(AMJ_ECUDA, "AMHJ: star write pass disagrees with its row counts");
+    pr->count = total;
+    pr->checksum = h[1];
+    pr->rows = total;
+    res->stats[3] += total;
+    return AMJ_OK;
+}
+
 static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bool dro, bool materialize,
                       uint64_t row_lo, uint64_t row_hi, PassResult *pr, amj_result *res, bool allow_flat) {
     if (!materialize && allow_flat && star_eligible(PL.P))
         return run_star_count(ctx, PL, X, ws, row_lo, row_hi, pr, res);
+    if (materialize && !dro && allow_flat && star_eligible(PL.P))
+        return run_star_write(ctx, PL, row_lo, row_hi, pr, res);
     ProbePlan &P = PL.P;
     P.row_lo = row_lo;
     P.row_hi = row_hi;

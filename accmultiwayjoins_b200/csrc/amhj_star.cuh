@@ -118,6 +118,85 @@ __global__ __launch_bounds__(256) void amhj_star_kernel(const __grid_constant__ 
     }
 }
 
+// ---- materialised star joins (two flat passes) ----
+// Pass 1: every probe row's number of result tuples (the product of its
+// matches per level).  A scan turns them into output offsets.  Pass 2: every
+// row writes its product's tuples from its offset, the last level fastest,
+// and adds them to the count and checksum.  A row's tuples are written by
+// its own thread, so the pass suits plans whose rows have few matches (the
+// 2-relation parts of a staged join, stars over dimensions with unique
+// keys); rows are independent, so the result is exact for any product.
+__global__ __launch_bounds__(256) void star_rowcount_kernel(const __grid_constant__ ProbePlan P,
+                                                            unsigned long long *__restrict__ rc) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = P.row_lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < P.row_hi; r += stride) {
+        int32_t vals[AMJ_MAX_ATTRS];
+        for (int c = 0; c < P.probe_ncols; c++) vals[P.probe_attr[c]] = P.probe_col[c][r];
+        unsigned long long prod = 1;
+        for (int l = 0; l < P.L && prod; l++) {
+            const int32_t key = vals[P.lv[l].key_attr[0]];
+            const uint32_t h = (uint32_t)key & P.lv[l].mask;
+            const uint32_t s = P.lv[l].buc_ptrs[h], e = P.lv[l].buc_ptrs[h + 1];
+            uint32_t nm = 0;
+            for (uint32_t i = s; i < e; i++) nm += P.lv[l].col[0][i] == key;
+            prod *= nm;
+        }
+        rc[r - P.row_lo] = prod;
+    }
+}
+
+__global__ __launch_bounds__(256) void star_write_kernel(const __grid_constant__ ProbePlan P,
+                                                         const unsigned long long *__restrict__ off,
+                                                         unsigned long long *count, unsigned long long *checksum) {
+    unsigned long long cnt = 0, chk = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = P.row_lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < P.row_hi; r += stride) {
+        unsigned long long at = off[r - P.row_lo];
+        if (off[r - P.row_lo + 1] == at) continue;   // no tuples
+        int32_t vals[AMJ_MAX_ATTRS];
+        for (int c = 0; c < P.probe_ncols; c++) vals[P.probe_attr[c]] = P.probe_col[c][r];
+        int32_t key[AMJ_MAX_BUILD_TABLES];
+        uint32_t first[AMJ_MAX_BUILD_TABLES], pos[AMJ_MAX_BUILD_TABLES], e[AMJ_MAX_BUILD_TABLES];
+        for (int l = 0; l < P.L; l++) {
+            key[l] = vals[P.lv[l].key_attr[0]];
+            const uint32_t h = (uint32_t)key[l] & P.lv[l].mask;
+            uint32_t i = P.lv[l].buc_ptrs[h];
+            e[l] = P.lv[l].buc_ptrs[h + 1];
+            while (P.lv[l].col[0][i] != key[l]) i++;   // a match exists: the row has tuples
+            first[l] = pos[l] = i;
+        }
+        while (true) {
+            for (int l = 0; l < P.L; l++)
+                for (int c = 1; c < P.lv[l].ncols; c++) vals[P.lv[l].attr[c]] = P.lv[l].col[c][pos[l]];
+            uint64_t hsh = AMJ_CHECKSUM_SEED;
+            for (int a = 0; a < P.k; a++) {
+                hsh = amj_hash_step(hsh, vals[a]);
+                P.out[a][at] = vals[a];
+            }
+            at++;
+            cnt++;
+            chk += hsh;
+            int l = P.L - 1;
+            for (; l >= 0; l--) {
+                uint32_t i = pos[l] + 1;
+                while (i < e[l] && P.lv[l].col[0][i] != key[l]) i++;
+                if (i < e[l]) {
+                    pos[l] = i;
+                    break;
+                }
+                pos[l] = first[l];
+            }
+            if (l < 0) break;
+        }
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if ((threadIdx.x & 31) == 0 && cnt) {
+        atomicAdd(count, cnt);
+        atomicAdd(checksum, chk);
+    }
+}
+
 // the probe columns of the listed rows (row ids relative to row_lo)
 __global__ void star_gather_kernel(const __grid_constant__ ProbePlan P, const uint32_t *rows, uint32_t n,
                                    int32_t *const *out) {
