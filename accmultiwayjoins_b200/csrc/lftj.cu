@@ -806,8 +806,7 @@ int build_wedges(amj_ctx *ctx, const Trie2 &R, uint64_t nv, DBuf<uint64_t> *out)
     while (bits < 32 && (nv - 1) >> bits) bits++;
     uint64_t *sorted = nullptr;
     AMJ_TRY(radix_sort_u64(ctx, out->p, other.p, n, SK_IDENT, 32, 32 + bits, &sorted));
-    if (sorted != out->p)
-        AMJ_CUDA_TRY(cudaMemcpyAsync(out->p, sorted, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (sorted != out->p) std::swap(*out, other);   // the sorted buffer becomes the result
     return AMJ_OK;
 }
 
