@@ -24,10 +24,13 @@
 //
 // Host memory: the partitions and intermediates live in pinned blocks that
 // the context keeps after the call (pinning tens of GB takes seconds, and a
-// served system runs the same stages again); they are freed with the context.
-// Partitioning runs on all host cores into those blocks; part p+1 is copied
-// to the device on a side stream while part p is joined, and each part's
-// rows come back straight into a pinned block of the next intermediate.
+// served system runs the same stages again); amj_ctx_trim and the context's
+// destruction free them.  Rows are grouped by key hash on the device (input
+// tables stream through it in chunks; each part result is grouped before it
+// is copied back), so a part is a union of groups and the host scatters
+// nothing up to 256 parts.  Part p+1 is copied to the device on one side
+// stream while part p is joined, and part p's grouped result goes back on
+// the other side stream while part p+1 is joined.
 #include "amhj_host.h"
 
 #include <omp.h>
@@ -64,7 +67,8 @@ void pinned_trim(amj_ctx *ctx) {
 }
 
 // A pinned block of at least `bytes`: a kept block of up to 4/3 the rounded
-// request, else a new one (after dropping the kept ones if pinning fails).
+// request, else a new one (the kept ones dropped first when they hold at
+// least as much, or when pinning fails).
 int pinned_get(amj_ctx *ctx, size_t bytes, void **p, size_t *size) {
     PinnedCache *pc = pinned_cache(ctx);
     const size_t r = pinned_round(bytes ? bytes : 1);
@@ -75,6 +79,12 @@ int pinned_get(amj_ctx *ctx, size_t bytes, void **p, size_t *size) {
         pc->free_blocks.erase(it);
         return AMJ_OK;
     }
+    // kept blocks that cannot serve this request go first when they hold at
+    // least as much as it asks: what the context keeps stays bounded by what
+    // its largest stages use
+    size_t kept = 0;
+    for (auto &kv : pc->free_blocks) kept += kv.first;
+    if (kept >= r) pinned_trim(ctx);
     cudaError_t e = cudaHostAlloc(p, r, cudaHostAllocDefault);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
