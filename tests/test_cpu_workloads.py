@@ -52,3 +52,22 @@ def test_bench_percentiles():
     import bench
     xs = [5.0, 1.0, 3.0, 2.0, 4.0]
     assert bench.pct(xs, 50) == 3.0 and bench.pct(xs, 99) == 5.0 and bench.pct(xs, 0) == 1.0
+
+
+def test_bench_star_algorithmic_bytes_match_a_direct_count():
+    """The star workload's algorithmic bytes (16 B per fact row, and per
+    dimension lookup the bucket bounds plus 8 B per row of the bucket, with
+    floorPow2(rows) buckets) against a direct per-row count."""
+    import argparse
+    import bench
+    wl = bench.Star(argparse.Namespace(star_rows=1500), 0, gen=O.GENERATORS)
+    fact_cols = wl.rels[0][0]
+    want = 0
+    for r in range(len(fact_cols[0])):
+        want += 16
+        for j, (cols, _) in enumerate(wl.rels[1:]):
+            B = 1 << (len(cols[0]).bit_length() - 1)
+            b = fact_cols[j][r] & (B - 1)
+            want += 8 + 8 * int(np.count_nonzero((cols[0] & (B - 1)) == b))
+    assert wl.algorithmic_bytes() == want
+    assert wl.h2d == sum(4 * len(c[0]) * len(c) for c, _ in wl.rels)
