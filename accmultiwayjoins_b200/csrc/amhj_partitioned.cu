@@ -67,8 +67,10 @@ void pinned_trim(amj_ctx *ctx) {
 }
 
 // A pinned block of at least `bytes`: a kept block of up to 4/3 the rounded
-// request, else a new one (the kept ones dropped first when they hold at
-// least as much, or when pinning fails).
+// request, else a new one (after dropping the kept ones if pinning fails).
+// Kept blocks are not dropped on a miss: pinning is slow (dropping them
+// whenever they could not serve a request made a 3.4 s staged join take
+// 27 s), so they stay until amj_ctx_trim or the context's end.
 int pinned_get(amj_ctx *ctx, size_t bytes, void **p, size_t *size) {
     PinnedCache *pc = pinned_cache(ctx);
     const size_t r = pinned_round(bytes ? bytes : 1);
@@ -79,12 +81,6 @@ int pinned_get(amj_ctx *ctx, size_t bytes, void **p, size_t *size) {
         pc->free_blocks.erase(it);
         return AMJ_OK;
     }
-    // kept blocks that cannot serve this request go first when they hold at
-    // least as much as it asks: what the context keeps stays bounded by what
-    // its largest stages use
-    size_t kept = 0;
-    for (auto &kv : pc->free_blocks) kept += kv.first;
-    if (kept >= r) pinned_trim(ctx);
     cudaError_t e = cudaHostAlloc(p, r, cudaHostAllocDefault);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
