@@ -352,6 +352,13 @@ class RefClique4:
         return tuples, None, secs, self.cores, self.kind, f"{n} slices: " + self.describe()
 
 
+def plan_note(plan):
+    """The workload text of a baseline plan run in place of the operator."""
+    return {"multiway": "", "thread_per_row": " (baseline plan: one thread per probe row, MHJ.cuh)",
+            "pairwise": " (baseline plan: 2-relation joins with materialised intermediates, exec_PW.cu)",
+            "hash": ""}[plan]
+
+
 class Chain:
     B = 1 << 19   # buckets = floorPow2(1e6)
 
@@ -359,10 +366,11 @@ class Chain:
         from accmultiwayjoins_b200 import data
         self.rels = data.chain_relations(1_000_000, 1 << 18, 3, seed=1 + 3 * rank, gen=gen)
         self.h2d = sum(4 * len(c[0]) * len(c) for c, _ in self.rels)
+        self.plan = getattr(args, "plan", "multiway")
 
     def describe(self, rank_note):
         return ("3-way chain R1(a,b)R2(b,c)R3(c,d), 3 x 1M rows, keys U[0,2^18), seeds 1,2,3" + rank_note +
-                "; AMHJ NORMAL count+checksum incl. hash builds")
+                "; AMHJ NORMAL count+checksum incl. hash builds" + plan_note(self.plan))
 
     def device_relations(self, ctx, dev):
         import torch
@@ -379,13 +387,15 @@ class Chain:
         return [c for cols, _ in self.rels for c in cols]
 
     def run(self, ctx, rels):
-        return ctx.amhj("NORMAL", rels)
+        return ctx.amhj("NORMAL", rels, plan=self.plan)
 
     def algorithmic_bytes(self):
         """Per probe row: its two columns (8 B) and its level-0 bucket bounds
         (8 B); per level-0 candidate its two co-located columns (8 B) and, for
         a match, its level-1 bucket bounds (8 B); per level-1 candidate its
         two columns (8 B)."""
+        if self.plan != "multiway":
+            return None   # a baseline plan: its kernels are not the operator's
         (p0, p1), _ = self.rels[0]
         (b0, b1), _ = self.rels[1]
         (c0, _), _ = self.rels[2]
@@ -427,10 +437,12 @@ class Star:
         fact, dims = data.star_relations(self.rows, list(self.DIMS), theta=1.1, seed=3 + rank, gen=gen)
         self.rels = [fact] + dims
         self.h2d = sum(4 * len(c[0]) * len(c) for c, _ in self.rels)
+        self.plan = getattr(args, "plan", "multiway")
 
     def describe(self, rank_note):
         return (f"4-way star, fact {self.rows} rows x 4 Zipf(1.1) foreign keys, dims 1M/200K/100K/10K "
-                f"(key, payload), seed 3{rank_note}; AMHJ NORMAL count+checksum incl. hash builds")
+                f"(key, payload), seed 3{rank_note}; AMHJ NORMAL count+checksum incl. hash builds"
+                + plan_note(self.plan))
 
     device_relations = Chain.device_relations
     host_relations = Chain.host_relations
@@ -441,6 +453,8 @@ class Star:
         """Per fact row: its four keys (16 B); per dimension lookup: the
         bucket bounds (8 B) and each candidate's key and payload (8 B), the
         buckets being floorPow2(rows) wide as built."""
+        if self.plan != "multiway":
+            return None   # a baseline plan: its kernels are not the operator's
         fact_cols = self.rels[0][0]
         tot = len(fact_cols[0]) * 16
         for j, (cols, _) in enumerate(self.rels[1:]):
@@ -1273,6 +1287,8 @@ def main():
     ap.add_argument("--star-rows", type=int, default=60_000_000, help="star workload: fact table rows")
     ap.add_argument("--layout", default="bucket", choices=["bucket", "oa", "cuckoo"],
                     help="chain / star workloads: hash-table layout of the AMHJ builds")
+    ap.add_argument("--plan", default="multiway", choices=["multiway", "thread_per_row", "pairwise"],
+                    help="chain / star workloads: the operator, or one of the reference's baseline plans")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="triangle workload: skip the chain and batched records carried on the line")
