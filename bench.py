@@ -18,7 +18,8 @@ R1(a,b) R2(b,c) R3(c,d) (3 x 1M rows, keys uniform in [0, 2^18), seeds 1-3)
 through AMHJ (count + checksum, hash builds included).  --workload star
 runs the 4-way star (fact 60M rows x 4 Zipf(1.1) keys, dims 1M/200K/100K/10K)
 through AMHJ the same way; --workload four the skewed 4-clique (R-MAT
-scale 22).  --workload batch
+scale 22).  --plan thread_per_row|pairwise runs the chain or star through
+the reference's baseline plans instead of the operator.  --workload batch
 runs 512 heterogeneous queries as one batch (autotuned, CUDA-graph replay)
 and reports, beside its tuples/s, the one-query-per-call tuples/s on the
 same queries and p50/p99 latencies of both forms.
