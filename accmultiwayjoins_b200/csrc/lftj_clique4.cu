@@ -246,6 +246,7 @@ struct C4MArgs {
     const int32_t *src1;     // rank a of every level-1 entry
     const int32_t *id1;      // vertex id of every level-1 value
     const int32_t *inv;      // rank -> vertex id
+    const uint64_t *h1;      // first tuple-hash step of every vertex id
     TrieRef T;
     const uint64_t *moff;    // first matrix word of every rank
     const uint32_t *mtx;
@@ -296,8 +297,8 @@ __global__ __launch_bounds__(C4M_THREADS) void lftj_clique4_matrix_kernel(const 
         }
         if (mine) {
             cnt++;
-            chk += amj_hash_step(amj_hash_step(amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, v[0]), v[1]), v[2]),
-                                 v[3]);
+            // the first step from the per-id table: one load instead of a mix
+            chk += amj_hash_step(amj_hash_step(amj_hash_step(A.h1[v[0]], v[1]), v[2]), v[3]);
         }
         qh = (qh + n) & (C4M_QCAP - 1);
         qn -= n;
@@ -416,7 +417,14 @@ struct C4Matrix {
     DBuf<uint64_t> moff;
     uint32_t *mtx = nullptr;   // the context's matrix buffer
     DBuf<int32_t> id1;
+    DBuf<uint64_t> h1;         // amj_hash_step(AMJ_CHECKSUM_SEED, id) of every vertex id
 };
+
+// the first step of the tuple hash of every vertex id in [0, nv)
+__global__ void id_hash_kernel(uint64_t nv, uint64_t *__restrict__ h1) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nv; i += (uint64_t)gridDim.x * blockDim.x)
+        h1[i] = amj_hash_step(AMJ_CHECKSUM_SEED, (int32_t)i);
+}
 
 // Whether the matrix path takes the degree-ranked trie T (every out-degree at
 // most 1024, the matrices within half the free device memory), and if so the
@@ -445,6 +453,14 @@ int lftj_clique4_matrix_prepare(amj_ctx *ctx, const Trie2 &T, const int32_t *inv
                             ctx->stream>>>(T.data1.p, T.len1, inv, m->id1.p);
         if (cudaGetLastError() != cudaSuccess) rc = fail(AMJ_ECUDA, "LFTJ 4-clique: level-1 ids");
     }
+    // vertex ids are the ranks' images, all below nv
+    if (rc == AMJ_OK) rc = m->h1.alloc(ctx, nv ? nv : 1);
+    if (rc == AMJ_OK && nv) {
+        note_launch(ctx);
+        id_hash_kernel<<<(unsigned)std::min<uint64_t>((nv + 255) / 256, (uint64_t)ctx->num_sms * 16), 256, 0,
+                         ctx->stream>>>(nv, m->h1.p);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(AMJ_ECUDA, "LFTJ 4-clique: id hashes");
+    }
     if (rc != AMJ_OK) {
         delete m;
         return rc;
@@ -470,6 +486,7 @@ int lftj_clique4_matrix(amj_ctx *ctx, const Trie2 &T, const int32_t *inv, const 
     A.src1 = T.src1.p;
     A.id1 = m->id1.p;
     A.inv = inv;
+    A.h1 = m->h1.p;
     A.T = trie_ref(T);
     A.moff = m->moff.p;
     A.mtx = m->mtx;
