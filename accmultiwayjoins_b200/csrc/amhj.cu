@@ -73,22 +73,26 @@ int compile_plan(int query_type, amj_rel *const *rels, int nrels, int flags, Hos
     for (int c = 0; c < tabs[0].ncols; c++) hp->probe_attr[c] = tabs[0].attr[c];
     uint32_t bound = 0;
     for (int c = 0; c < tabs[0].ncols; c++) bound |= 1u << tabs[0].attr[c];
-    std::vector<RelAttrs> rem(tabs.begin() + 1, tabs.end());
+    // the build relations not placed yet, in query order
+    std::vector<size_t> rem;
+    for (size_t i = 1; i < tabs.size(); i++) rem.push_back(i);
     int L = 0;
     while (!rem.empty()) {
         size_t pick = 0;
         if (!(flags & AMJ_F_NO_REORDER)) {
             for (size_t i = 0; i < rem.size(); i++) {
+                const RelAttrs &r = tabs[rem[i]];
                 bool all = true;
-                for (int c = 0; c < rem[i].ncols; c++) all &= ((bound >> rem[i].attr[c]) & 1) != 0;
+                for (int c = 0; c < r.ncols; c++) all &= ((bound >> r.attr[c]) & 1) != 0;
                 if (all) {
                     pick = i;
                     break;
                 }
             }
         }
-        RelAttrs t = rem[pick];
-        rem.erase(rem.begin() + pick);
+        const RelAttrs t = tabs[rem[pick]];
+        for (size_t i = pick + 1; i < rem.size(); i++) rem[i - 1] = rem[i];
+        rem.pop_back();
         if (t.ncols > 4) return fail(AMJ_EUNSUPPORTED, "AMHJ: build relations have at most 4 columns");
         int kc = -1;   // key column: the first column whose attribute is bound
         for (int c = 0; c < t.ncols && kc < 0; c++)
