@@ -89,13 +89,29 @@ int degree_ordered_copy(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint
 // degrees counted on every stride-th edge: an estimate that keeps the order
 // of the hubs (the counts that matter for the orientation) at a fraction of
 // the atomics; any total order gives the same join result
+// The counts of ids below DEG_SMEM_IDS (where generators and real graphs put
+// their hubs first: R-MAT's low ids) gather in shared memory per block and
+// reach the global array once per block, so a hub's increments do not
+// serialise on one global counter.
+constexpr uint32_t DEG_SMEM_IDS = 8192;
+
 __global__ void degree_sample_kernel(const int32_t *__restrict__ s, const int32_t *__restrict__ d, uint64_t n,
-                                     uint32_t stride, unsigned int *deg) {
+                                     uint32_t stride, uint64_t nv, unsigned int *deg) {
+    __shared__ unsigned int h[DEG_SMEM_IDS];
+    for (uint32_t i = threadIdx.x; i < DEG_SMEM_IDS; i += blockDim.x) h[i] = 0;
+    __syncthreads();
     const uint64_t m = (n + stride - 1) / stride;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
-        atomicAdd(&deg[s[i * stride]], 1u);
-        atomicAdd(&deg[d[i * stride]], 1u);
+        const uint32_t a = (uint32_t)s[i * stride], b = (uint32_t)d[i * stride];
+        if (a < DEG_SMEM_IDS) atomicAdd(&h[a], 1u);
+        else atomicAdd(&deg[a], 1u);
+        if (b < DEG_SMEM_IDS) atomicAdd(&h[b], 1u);
+        else atomicAdd(&deg[b], 1u);
     }
+    __syncthreads();
+    const uint32_t top = nv < DEG_SMEM_IDS ? (uint32_t)nv : DEG_SMEM_IDS;
+    for (uint32_t i = threadIdx.x; i < top; i += blockDim.x)
+        if (h[i]) atomicAdd(&deg[i], h[i]);
 }
 
 // the largest of nv degrees
@@ -164,7 +180,8 @@ int degree_ranks(amj_ctx *ctx, const int32_t *c0, const int32_t *c1, uint64_t n,
     // relations of 2^20 edges or more rank by degrees counted on every 4th edge
     const uint32_t stride = n >= (1ull << 20) ? 4u : 1u;
     note_launch(ctx);
-    degree_sample_kernel<<<g, 256, 0, ctx->stream>>>(c0, c1, n, stride, deg.p);
+    degree_sample_kernel<<<(unsigned)std::min<uint64_t>(g, (uint64_t)ctx->num_sms * 4), 256, 0, ctx->stream>>>(
+        c0, c1, n, stride, V, deg.p);
     AMJ_CUDA_TRY(cudaGetLastError());
     DBuf<uint64_t> ka, kb;
     AMJ_TRY(ka.alloc(ctx, V));
