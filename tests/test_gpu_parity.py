@@ -299,6 +299,26 @@ def test_amhj_baseline_plans_match_oracle(ctx, shape):
         ctx.amhj(qt, hs, plan="thread_per_row", materialize=True)
 
 
+def test_amhj_out_of_core_many_parts_host_partitioning():
+    """A device budget so small that a stage needs more than 256 parts: the
+    rows are then partitioned by the scatter on the host cores instead of the
+    device grouping (which serves up to 256 parts).  Equal to the oracle and
+    to the same query under a budget that groups on the device."""
+    rels = [([data.uniform(50_000, 0, 50_000, 71 + i, 0), data.uniform(50_000, 0, 50_000, 71 + i, 1)], [i, i + 1])
+            for i in range(3)]
+    want = O.mhj(rels)
+    with Context(0, mem_budget=4 << 10) as ctx:
+        host = [ctx.relation(c, a, streamed=True) for c, a in rels]
+        got = ctx.amhj("NORMAL", host, ooc=1)
+        assert (got.count, got.checksum) == want
+        assert got.stats["slices"] > 2 * 256   # part joins
+    with Context(0, mem_budget=256 << 10) as ctx:
+        host = [ctx.relation(c, a, streamed=True) for c, a in rels]
+        got = ctx.amhj("NORMAL", host, ooc=1, materialize=True)
+        assert (got.count, got.checksum) == want
+        assert data.checksum(got.columns) == want[1]
+
+
 def test_amhj_star_flat_path_with_repeated_dimension_keys(ctx):
     """Star count queries take the flat kernel (one thread per fact row, all
     dimension lookups together).  Dimensions with repeated keys give rows a
