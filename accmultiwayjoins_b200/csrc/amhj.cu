@@ -271,9 +271,42 @@ static int run_star_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws
     AMJ_TRY(over.alloc(ctx, rows ? rows : 1));
     AMJ_CUDA_TRY(cudaMemsetAsync(ctr.p, 0, sizeof(Ctr), ctx->stream));
     const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 8);
-    note_launch(ctx);
+    StarCanon S{};
+    int canon = star_canon(P, S);
+    DBuf<BucketHead> heads;
+    uint32_t maxnb = 0;
+    if (canon) {
+        size_t tot = 0;
+        for (int c = 0; c < canon; c++) {
+            tot += S.nb[c];
+            maxnb = std::max(maxnb, S.nb[c]);
+        }
+        AMJ_TRY(heads.alloc(ctx, tot));
+        // the heads are read by 256-bit loads, which need 32-byte alignment
+        if (reinterpret_cast<uintptr_t>(heads.p) % alignof(BucketHead) != 0) canon = 0;
+    }
     AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
-    amhj_star_kernel<<<g ? g : 1, 256, 0, ctx->stream>>>(P, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover);
+    if (canon) {
+        HeadOut H{};
+        size_t at = 0;
+        for (int c = 0; c < canon; c++) {
+            H.p[c] = heads.p + at;
+            S.head[c] = heads.p + at;
+            at += S.nb[c];
+        }
+        const unsigned gx = (unsigned)std::min<uint64_t>((maxnb + 255) / 256, (uint64_t)ctx->num_sms * 4);
+        note_launch(ctx);
+        bucket_heads_kernel<<<dim3(gx ? gx : 1, canon), 256, 0, ctx->stream>>>(S, H);
+        AMJ_CUDA_TRY(cudaGetLastError());
+    }
+    note_launch(ctx);
+    switch (canon) {
+    case 1: amhj_star_canon_kernel<1><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
+    case 2: amhj_star_canon_kernel<2><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
+    case 3: amhj_star_canon_kernel<3><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
+    case 4: amhj_star_canon_kernel<4><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
+    default: amhj_star_kernel<<<g ? g : 1, 256, 0, ctx->stream>>>(P, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover);
+    }
     AMJ_CUDA_TRY(cudaGetLastError());
     AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[1], ctx->stream));
     Ctr h{};

@@ -118,6 +118,192 @@ __global__ __launch_bounds__(256) void amhj_star_kernel(const __grid_constant__ 
     }
 }
 
+// ---- the canonical star, count mode: one 32-byte bucket head a lookup ----
+// The shape of the reference's star benchmarks: probe F(0..L-1) and, for
+// each key attribute c, one level D_c(c, L + c) of (key, payload) looked up
+// by c.  The tuple is then (F's row, the payloads in key order), so every
+// index below is a compile-time constant and the row's values stay in
+// registers (the general kernel above indexes an attribute array at run time,
+// a local-memory array, and loops over the levels).
+//
+// A probe of random lookups is bound by the L1's tag lookups, one for every
+// distinct line a warp's load touches: the general kernel makes four per
+// level (two bucket bounds, a key, a payload).  Before the probe every bucket
+// of a level gets a 32-byte head, one sector: its bounds and its first
+// STAR_HEAD_ROWS rows (key, payload), read by one 256-bit load.  Dimension
+// buckets hold one or two rows (keys unique, floorPow2(rows) buckets), so a
+// lookup is that one load.  A row whose buckets all hold at most
+// STAR_HEAD_ROWS rows, one of them with the key, is one tuple, hashed from
+// the keys' shared prefix.  Other rows count their matches per level from
+// the bounds and enumerate the product (an odometer over the levels, the
+// last fastest); products above STAR_MAX_PRODUCT are listed for the DFS
+// kernel as above.
+constexpr int STAR_HEAD_ROWS = 3;
+
+struct __align__(32) BucketHead {
+    uint32_t s, e;                      // the bucket's rows [s, e)
+    int32_t kp[2 * STAR_HEAD_ROWS];     // its first rows' (key, payload), 0 past e
+};
+static_assert(sizeof(BucketHead) == 32, "a bucket head is one sector");
+
+struct StarCanon {
+    const int32_t *fact[AMJ_MAX_BUILD_TABLES];     // probe column c (attribute c)
+    const BucketHead *head[AMJ_MAX_BUILD_TABLES];  // bucket heads of the level keyed by c
+    const int32_t *key[AMJ_MAX_BUILD_TABLES];      // its key column
+    const int32_t *pay[AMJ_MAX_BUILD_TABLES];      // its payload column (attribute L + c)
+    const uint32_t *bp[AMJ_MAX_BUILD_TABLES];      // its bucket starts
+    uint32_t nb[AMJ_MAX_BUILD_TABLES];             // its buckets (mask + 1)
+    uint32_t mask[AMJ_MAX_BUILD_TABLES];
+    uint64_t row_lo, row_hi;
+};
+
+// L when star plan P has the canonical shape (filling S but the heads), else 0
+inline int star_canon(const ProbePlan &P, StarCanon &S) {
+    const int L = P.L;
+    if (L < 1 || 2 * L > AMJ_MAX_ATTRS || P.probe_ncols != L || P.k != 2 * L) return 0;
+    for (int c = 0; c < L; c++)
+        if (P.probe_attr[c] != c) return 0;
+    bool seen[AMJ_MAX_BUILD_TABLES] = {};
+    for (int l = 0; l < L; l++) {
+        const LevelDesc &lv = P.lv[l];
+        const int c = lv.key_attr[0];
+        if (c < 0 || c >= L || seen[c] || lv.ncols != 2 || lv.attr[0] != c || lv.attr[1] != L + c) return 0;
+        seen[c] = true;
+        S.fact[c] = P.probe_col[c];
+        S.key[c] = lv.col[0];
+        S.pay[c] = lv.col[1];
+        S.bp[c] = lv.buc_ptrs;
+        S.nb[c] = lv.mask + 1u;
+        S.mask[c] = lv.mask;
+    }
+    S.row_lo = P.row_lo;
+    S.row_hi = P.row_hi;
+    return L;
+}
+
+struct HeadOut {
+    BucketHead *p[AMJ_MAX_BUILD_TABLES];
+};
+
+// the heads of level blockIdx.y
+__global__ void bucket_heads_kernel(const __grid_constant__ StarCanon S, const __grid_constant__ HeadOut H) {
+    const int c = blockIdx.y;
+    const uint32_t nb = S.nb[c];
+    const uint32_t *bp = S.bp[c];
+    for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < nb; h += gridDim.x * blockDim.x) {
+        BucketHead o;
+        o.s = bp[h];
+        o.e = bp[h + 1];
+#pragma unroll
+        for (int i = 0; i < STAR_HEAD_ROWS; i++) {
+            const bool in = o.s + i < o.e;
+            o.kp[2 * i] = in ? S.key[c][o.s + i] : 0;
+            o.kp[2 * i + 1] = in ? S.pay[c][o.s + i] : 0;
+        }
+        H.p[c][h] = o;
+    }
+}
+
+// one 256-bit load of a head (32-byte aligned), through the read-only path
+__device__ __forceinline__ void load_head(const BucketHead *p, uint32_t (&w)[8]) {
+    asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+        : "l"(p));
+}
+
+template <int L>
+__global__ __launch_bounds__(256, 4) void amhj_star_canon_kernel(const __grid_constant__ StarCanon S,
+                                                              unsigned long long *count, unsigned long long *checksum,
+                                                              uint32_t *over, unsigned int *nover) {
+    unsigned long long cnt = 0, chk = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = S.row_lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < S.row_hi; r += stride) {
+        int32_t k[L];
+#pragma unroll
+        for (int c = 0; c < L; c++) k[c] = __ldcs(S.fact[c] + r);
+        uint32_t w[L][8];
+#pragma unroll
+        for (int c = 0; c < L; c++) load_head(S.head[c] + ((uint32_t)k[c] & S.mask[c]), w[c]);
+        bool one = true;
+        int32_t pay[L];
+#pragma unroll
+        for (int c = 0; c < L; c++) {
+            const uint32_t n = w[c][1] - w[c][0];
+            uint32_t nm = 0;
+            int32_t p = 0;
+#pragma unroll
+            for (int i = 0; i < STAR_HEAD_ROWS; i++) {
+                const bool m = (uint32_t)i < n && (int32_t)w[c][2 + 2 * i] == k[c];
+                nm += m ? 1u : 0u;
+                p = m ? (int32_t)w[c][3 + 2 * i] : p;
+            }
+            one &= (n <= (uint32_t)STAR_HEAD_ROWS) & (nm == 1u);
+            pay[c] = p;
+        }
+        uint64_t hk = AMJ_CHECKSUM_SEED;
+#pragma unroll
+        for (int c = 0; c < L; c++) hk = amj_hash_step(hk, k[c]);
+        if (one) {
+            uint64_t h = hk;
+#pragma unroll
+            for (int c = 0; c < L; c++) h = amj_hash_step(h, pay[c]);
+            cnt++;
+            chk += h;
+            continue;
+        }
+        uint32_t first[L], e[L];
+        uint64_t prod = 1;
+#pragma unroll
+        for (int c = 0; c < L; c++) {
+            e[c] = w[c][1];
+            uint32_t nm = 0, f = e[c];
+            for (uint32_t i = w[c][0]; i < e[c]; i++)
+                if (S.key[c][i] == k[c]) {
+                    if (nm == 0) f = i;
+                    nm++;
+                }
+            first[c] = f;
+            prod *= nm;
+        }
+        if (prod == 0) continue;
+        if (prod > STAR_MAX_PRODUCT) {
+            over[atomicAdd(nover, 1u)] = (uint32_t)(r - S.row_lo);
+            continue;
+        }
+        uint32_t pos[L];
+#pragma unroll
+        for (int c = 0; c < L; c++) pos[c] = first[c];
+        while (true) {
+            uint64_t h = hk;
+#pragma unroll
+            for (int c = 0; c < L; c++) h = amj_hash_step(h, S.pay[c][pos[c]]);
+            cnt++;
+            chk += h;
+            bool carry = true;
+#pragma unroll
+            for (int c = L - 1; c >= 0; c--) {
+                if (carry) {
+                    uint32_t i = pos[c] + 1;
+                    while (i < e[c] && S.key[c][i] != k[c]) i++;
+                    if (i < e[c]) {
+                        pos[c] = i;
+                        carry = false;
+                    } else {
+                        pos[c] = first[c];
+                    }
+                }
+            }
+            if (carry) break;
+        }
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if ((threadIdx.x & 31) == 0 && cnt) {
+        atomicAdd(count, cnt);
+        atomicAdd(checksum, chk);
+    }
+}
+
 // ---- materialised star joins (two flat passes) ----
 // Pass 1: every probe row's number of result tuples (the product of its
 // matches per level).  A scan turns them into output offsets.  Pass 2: every

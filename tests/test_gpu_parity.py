@@ -346,6 +346,35 @@ def test_amhj_star_flat_path_with_repeated_dimension_keys(ctx):
     assert (m.count, m.checksum) == want
 
 
+@pytest.mark.parametrize("ndims", [1, 2, 3, 4])
+def test_amhj_star_canonical_and_general_attribute_numbering(ctx, ndims):
+    """The flat star count path has two kernels: one for the canonical
+    numbering F(0..d-1), D_j(j, d + j), whose values stay in registers, and
+    the general one for any other numbering.  The same star under both
+    numberings (and dimensions given in reverse order) equals the oracle,
+    with unique dimension keys, repeated keys (products of 2-256) and absent
+    keys (empty products)."""
+    rng = np.random.Generator(np.random.PCG64(40 + ndims))
+    n = 60_000
+    fact = [rng.integers(0, 3000, n).astype(np.int32) for _ in range(ndims)]
+    dims = []
+    for j in range(ndims):
+        if j % 2 == 0:
+            keys = rng.permutation(3000).astype(np.int32)[:2500]         # unique, some absent
+        else:
+            keys = rng.integers(0, 3000, 7000).astype(np.int32)          # repeated, some absent
+        dims.append([keys, rng.integers(-(1 << 31), 1 << 31, len(keys), dtype=np.int64).astype(np.int32)])
+    canon = [(fact, list(range(ndims)))] + [(dims[j], [j, ndims + j]) for j in range(ndims)][::-1]
+    other = [(fact, [2 * j + 1 for j in range(ndims)])] + [(dims[j], [2 * j + 1, 2 * j]) for j in range(ndims)]
+    for rels in (canon, other):
+        want = O.mhj(rels)
+        assert want[0] > 0
+        hs = [ctx.relation(c, a) for c, a in rels]
+        for ws in (0, 1):
+            got = ctx.amhj("NORMAL", hs, ws=ws)
+            assert (got.count, got.checksum) == want, (rels[0][1], ws)
+
+
 @pytest.mark.parametrize("qt", ["TRI", "FOUR"])
 @pytest.mark.parametrize("reorder", [True, False])
 @pytest.mark.parametrize("degree_order", [True, False])
