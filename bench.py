@@ -451,21 +451,29 @@ class Star:
     run = Chain.run
 
     def algorithmic_bytes(self):
-        """Per fact row: its four keys (16 B); per dimension lookup: the
-        bucket bounds (8 B) and each candidate's key and payload (8 B), the
-        buckets being floorPow2(rows) wide as built."""
+        """The HBM bytes the probe must move: per fact row its four keys
+        (16 B, streamed once); per dimension the build of its bucket heads
+        (the bucket bounds, 4 B a bucket, and the rows, 8 B each, read; one
+        32-byte head a bucket written) and the heads read back once.  The
+        lookups themselves (one head a dimension and fact row) are served by
+        L1 and L2, which hold every head (23 MB): they are counted by
+        lookups_per_launch, not here."""
         if self.plan != "multiway":
             return None   # a baseline plan: its kernels are not the operator's
-        fact_cols = self.rels[0][0]
-        tot = len(fact_cols[0]) * 16
-        for j, (cols, _) in enumerate(self.rels[1:]):
-            B = 1 << (len(cols[0]).bit_length() - 1)
-            per = np.bincount(cols[0] & (B - 1), minlength=B).astype(np.int64)
-            tot += len(fact_cols[j]) * 8 + int(per[fact_cols[j] & (B - 1)].sum()) * 8
+        tot = len(self.rels[0][0][0]) * 16
+        for cols, _ in self.rels[1:]:
+            n = len(cols[0])
+            B = 1 << (n.bit_length() - 1)
+            tot += 4 * (B + 1) + 8 * n + 2 * 32 * B
         return tot
 
+    def lookups_per_launch(self):
+        """Random line lookups of the probe: one bucket head per dimension
+        and fact row."""
+        return len(self.rels[0][0][0]) * (len(self.rels) - 1)
+
     def kernel_name(self):
-        return "amhj_star_kernel"
+        return "amhj_star_canon_kernel"
 
     def cpu_baseline(self, sample_rows=12_000_000):
         """The reference MHJ-CPU over a bounded sample of the fact table (its
@@ -1111,6 +1119,8 @@ def config_record(args, ctx, dev, stream, wl, steps=10, warmup=3):
            "probe_kernel": {"kernel": wl.kernel_name(), "ms": kms}}
     if alg:
         rec["probe_kernel"].update({"alg_bytes": alg, "frac_of_hbm": alg / (kms * 1e-3) / 1e9 / hbm})
+    if hasattr(wl, "lookups_per_launch") and kms > 0:
+        rec["probe_kernel"]["lookups_per_s"] = wl.lookups_per_launch() / (kms * 1e-3)
     if not args.no_cpu_baseline:
         c_cnt, c_chk, sec, cores, kind, sample = wl.cpu_baseline()
         rec["cpu_baseline"] = {"value": c_cnt / sec, "unit": "tuples/s", "cores": cores, "kind": kind,
@@ -1250,6 +1260,8 @@ def run_ours(args, rank, world, local_rank):
         line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                             "frac": achieved / hbm, "traffic": profiled_traffic(args), "peak_kind": peak_kind,
                             "kernel": wl.kernel_name(), "alg_bytes_per_launch": alg}
+        if hasattr(wl, "lookups_per_launch"):
+            line["roofline"]["lookups_per_s"] = wl.lookups_per_launch() / (kms * 1e-3)
     if isinstance(wl, Triangle) and world == 1 and not args.no_configs:
         line["configs"] = other_configs(args, ctx, dev, stream, local_rank)
     if not args.no_cpu_baseline:

@@ -55,19 +55,20 @@ def test_bench_percentiles():
 
 
 def test_bench_star_algorithmic_bytes_match_a_direct_count():
-    """The star workload's algorithmic bytes (16 B per fact row, and per
-    dimension lookup the bucket bounds plus 8 B per row of the bucket, with
-    floorPow2(rows) buckets) against a direct per-row count."""
+    """The star workload's HBM bytes: 16 B per fact row, and per dimension
+    the build of its bucket heads (floorPow2(rows) buckets: bounds read,
+    rows read, one 32-byte head written) and the heads read back once; the
+    lookups, one head per dimension and fact row, are counted apart."""
     import argparse
     import bench
     wl = bench.Star(argparse.Namespace(star_rows=1500), 0, gen=O.GENERATORS)
     fact_cols = wl.rels[0][0]
-    want = 0
-    for r in range(len(fact_cols[0])):
-        want += 16
-        for j, (cols, _) in enumerate(wl.rels[1:]):
-            B = 1 << (len(cols[0]).bit_length() - 1)
-            b = fact_cols[j][r] & (B - 1)
-            want += 8 + 8 * int(np.count_nonzero((cols[0] & (B - 1)) == b))
+    want = 16 * len(fact_cols[0])
+    for cols, _ in wl.rels[1:]:
+        B = 1
+        while 2 * B <= len(cols[0]):
+            B *= 2
+        want += 4 * (B + 1) + 8 * len(cols[0]) + 32 * B + 32 * B
     assert wl.algorithmic_bytes() == want
+    assert wl.lookups_per_launch() == 4 * len(fact_cols[0])
     assert wl.h2d == sum(4 * len(c[0]) * len(c) for c, _ in wl.rels)
