@@ -253,9 +253,10 @@ struct PassResult {
 static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bool dro, bool materialize,
                       uint64_t row_lo, uint64_t row_hi, PassResult *pr, amj_result *res, bool allow_flat = true);
 
-// Count mode of a star plan (amhj_star.cuh): the flat kernel, then the DFS
-// kernel over the rows whose match product was too large for one thread.
-static int run_star_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, uint64_t row_lo, uint64_t row_hi,
+// Count mode of a star or canonical chain plan (amhj_star.cuh): the flat
+// kernel, then the DFS kernel over the rows that were too much work for one
+// thread (a star's match product, a chain walk's bucket rows).
+static int run_flat_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, uint64_t row_lo, uint64_t row_hi,
                           PassResult *pr, amj_result *res) {
     ProbePlan &P = PL.P;
     P.row_lo = row_lo;
@@ -271,8 +272,13 @@ static int run_star_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws
     AMJ_TRY(over.alloc(ctx, rows ? rows : 1));
     AMJ_CUDA_TRY(cudaMemsetAsync(ctr.p, 0, sizeof(Ctr), ctx->stream));
     const unsigned g = (unsigned)std::min<uint64_t>((rows + 255) / 256, (uint64_t)ctx->num_sms * 8);
-    StarCanon S{};
+    CanonPlan S{};
     int canon = star_canon(P, S);
+    bool chain = false;
+    if (!canon) {
+        canon = chain_canon(P, S);
+        chain = canon > 0;
+    }
     DBuf<BucketHead> heads;
     uint32_t maxnb = 0;
     if (canon) {
@@ -300,7 +306,16 @@ static int run_star_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws
         AMJ_CUDA_TRY(cudaGetLastError());
     }
     note_launch(ctx);
-    switch (canon) {
+    if (chain) {
+        switch (canon) {
+        case 1: amhj_chain_canon_kernel<1><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
+        case 2: amhj_chain_canon_kernel<2><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
+        case 3: amhj_chain_canon_kernel<3><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
+        case 4: amhj_chain_canon_kernel<4><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
+        case 5: amhj_chain_canon_kernel<5><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
+        default: amhj_chain_canon_kernel<6><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover);
+        }
+    } else switch (canon) {
     case 1: amhj_star_canon_kernel<1><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
     case 2: amhj_star_canon_kernel<2><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
     case 3: amhj_star_canon_kernel<3><<<g ? g : 1, 256, 0, ctx->stream>>>(S, &ctr.p->count, &ctr.p->checksum, over.p, &ctr.p->nover); break;
@@ -384,8 +399,9 @@ static int run_star_write(amj_ctx *ctx, ProbeLaunch &PL, uint64_t row_lo, uint64
 
 static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bool dro, bool materialize,
                       uint64_t row_lo, uint64_t row_hi, PassResult *pr, amj_result *res, bool allow_flat) {
-    if (!materialize && allow_flat && star_eligible(PL.P))
-        return run_star_count(ctx, PL, X, ws, row_lo, row_hi, pr, res);
+    CanonPlan cp_;
+    if (!materialize && allow_flat && (star_eligible(PL.P) || chain_canon(PL.P, cp_)))
+        return run_flat_count(ctx, PL, X, ws, row_lo, row_hi, pr, res);
     if (materialize && !dro && allow_flat && star_eligible(PL.P))
         return run_star_write(ctx, PL, row_lo, row_hi, pr, res);
     ProbePlan &P = PL.P;

@@ -146,11 +146,13 @@ struct __align__(32) BucketHead {
 };
 static_assert(sizeof(BucketHead) == 32, "a bucket head is one sector");
 
-struct StarCanon {
-    const int32_t *fact[AMJ_MAX_BUILD_TABLES];     // probe column c (attribute c)
-    const BucketHead *head[AMJ_MAX_BUILD_TABLES];  // bucket heads of the level keyed by c
+// A star (star_canon) or chain (chain_canon) plan with its levels in key
+// order: star level c is keyed by attribute c, chain level d by d + 1.
+struct CanonPlan {
+    const int32_t *fact[AMJ_MAX_BUILD_TABLES];     // probe columns (star: attribute c; chain: 0 and 1)
+    const BucketHead *head[AMJ_MAX_BUILD_TABLES];  // bucket heads of level c
     const int32_t *key[AMJ_MAX_BUILD_TABLES];      // its key column
-    const int32_t *pay[AMJ_MAX_BUILD_TABLES];      // its payload column (attribute L + c)
+    const int32_t *pay[AMJ_MAX_BUILD_TABLES];      // its payload column (star: attribute L + c; chain: c + 2)
     const uint32_t *bp[AMJ_MAX_BUILD_TABLES];      // its bucket starts
     uint32_t nb[AMJ_MAX_BUILD_TABLES];             // its buckets (mask + 1)
     uint32_t mask[AMJ_MAX_BUILD_TABLES];
@@ -158,7 +160,7 @@ struct StarCanon {
 };
 
 // L when star plan P has the canonical shape (filling S but the heads), else 0
-inline int star_canon(const ProbePlan &P, StarCanon &S) {
+inline int star_canon(const ProbePlan &P, CanonPlan &S) {
     const int L = P.L;
     if (L < 1 || 2 * L > AMJ_MAX_ATTRS || P.probe_ncols != L || P.k != 2 * L) return 0;
     for (int c = 0; c < L; c++)
@@ -186,7 +188,7 @@ struct HeadOut {
 };
 
 // the heads of level blockIdx.y
-__global__ void bucket_heads_kernel(const __grid_constant__ StarCanon S, const __grid_constant__ HeadOut H) {
+__global__ void bucket_heads_kernel(const __grid_constant__ CanonPlan S, const __grid_constant__ HeadOut H) {
     const int c = blockIdx.y;
     const uint32_t nb = S.nb[c];
     const uint32_t *bp = S.bp[c];
@@ -212,7 +214,7 @@ __device__ __forceinline__ void load_head(const BucketHead *p, uint32_t (&w)[8])
 }
 
 template <int L>
-__global__ __launch_bounds__(256, 4) void amhj_star_canon_kernel(const __grid_constant__ StarCanon S,
+__global__ __launch_bounds__(256, 4) void amhj_star_canon_kernel(const __grid_constant__ CanonPlan S,
                                                               unsigned long long *count, unsigned long long *checksum,
                                                               uint32_t *over, unsigned int *nover) {
     unsigned long long cnt = 0, chk = 0;
@@ -294,6 +296,100 @@ __global__ __launch_bounds__(256, 4) void amhj_star_canon_kernel(const __grid_co
                 }
             }
             if (carry) break;
+        }
+    }
+    cnt = warp_sum(cnt);
+    chk = warp_sum(chk);
+    if ((threadIdx.x & 31) == 0 && cnt) {
+        atomicAdd(count, cnt);
+        atomicAdd(checksum, chk);
+    }
+}
+
+// ---- the canonical chain, count mode: a depth-first walk in registers ----
+// The shape of the reference's chain benchmarks: probe R0(0, 1) and levels
+// R_d(d + 1, d + 2), level d looked up by the payload of level d - 1 (by
+// attribute 1 at d = 0).  One thread walks one probe row's matches depth
+// first, each level's lookup one bucket head (its bounds and first rows) and
+// the tuple hash extended by one step a level, so a tuple costs one step at
+// the last level.  A row whose walk would scan more than CHAIN_ROW_BUDGET
+// bucket rows (skewed keys) drops what it counted and is listed for the DFS
+// kernel, which shares such work across warps.
+constexpr uint32_t CHAIN_ROW_BUDGET = 512;
+
+// L when plan P has the canonical chain shape (filling S but the heads), else 0
+inline int chain_canon(const ProbePlan &P, CanonPlan &S) {
+    const int L = P.L;
+    if (L < 1 || L + 2 > AMJ_MAX_ATTRS || P.probe_ncols != 2 || P.k != L + 2) return 0;
+    if (P.has_inl || P.sort_out || P.fib_level >= 0 || P.probe_attr[0] != 0 || P.probe_attr[1] != 1) return 0;
+    bool seen[AMJ_MAX_BUILD_TABLES] = {};
+    for (int l = 0; l < L; l++) {
+        const LevelDesc &lv = P.lv[l];
+        const int d = lv.key_attr[0] - 1;
+        if (d < 0 || d >= L || seen[d] || lv.layout != AMJ_LAYOUT_BUCKET || lv.key_mode != KEY_SINGLE ||
+            lv.cmp_mask != 1u || lv.ncols != 2 || lv.attr[0] != d + 1 || lv.attr[1] != d + 2)
+            return 0;
+        seen[d] = true;
+        S.key[d] = lv.col[0];
+        S.pay[d] = lv.col[1];
+        S.bp[d] = lv.buc_ptrs;
+        S.nb[d] = lv.mask + 1u;
+        S.mask[d] = lv.mask;
+    }
+    S.fact[0] = P.probe_col[0];
+    S.fact[1] = P.probe_col[1];
+    S.row_lo = P.row_lo;
+    S.row_hi = P.row_hi;
+    return L;
+}
+
+// the matches of key at level D and, through them, the levels below; false
+// when the walk ran out of budget
+template <int D, int L>
+__device__ __forceinline__ bool chain_walk(const CanonPlan &S, int32_t key, uint64_t h, unsigned long long &rc,
+                                           unsigned long long &rchk, uint32_t &budget) {
+    uint32_t w[8];
+    load_head(S.head[D] + ((uint32_t)key & S.mask[D]), w);
+    const uint32_t n = w[1] - w[0];
+    if (n > budget) return false;
+    budget -= n;
+    for (uint32_t i = 0; i < n; i++) {
+        int32_t k, v;
+        if (i < (uint32_t)STAR_HEAD_ROWS) {
+            k = (int32_t)(i == 0 ? w[2] : (i == 1 ? w[4] : w[6]));
+            v = (int32_t)(i == 0 ? w[3] : (i == 1 ? w[5] : w[7]));
+        } else {
+            k = S.key[D][w[0] + i];
+            v = S.pay[D][w[0] + i];
+        }
+        if (k != key) continue;
+        const uint64_t hv = amj_hash_step(h, v);
+        if constexpr (D == L - 1) {
+            rc++;
+            rchk += hv;
+        } else {
+            if (!chain_walk<D + 1, L>(S, v, hv, rc, rchk, budget)) return false;
+        }
+    }
+    return true;
+}
+
+template <int L>
+__global__ __launch_bounds__(256, 4) void amhj_chain_canon_kernel(const __grid_constant__ CanonPlan S,
+                                                               unsigned long long *count, unsigned long long *checksum,
+                                                               uint32_t *over, unsigned int *nover) {
+    unsigned long long cnt = 0, chk = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = S.row_lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < S.row_hi; r += stride) {
+        const int32_t a0 = __ldcs(S.fact[0] + r), a1 = __ldcs(S.fact[1] + r);
+        const uint64_t h = amj_hash_step(amj_hash_step(AMJ_CHECKSUM_SEED, a0), a1);
+        unsigned long long rc = 0, rchk = 0;
+        uint32_t budget = CHAIN_ROW_BUDGET;
+        if (chain_walk<0, L>(S, a1, h, rc, rchk, budget)) {
+            cnt += rc;
+            chk += rchk;
+        } else {
+            over[atomicAdd(nover, 1u)] = (uint32_t)(r - S.row_lo);
         }
     }
     cnt = warp_sum(cnt);

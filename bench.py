@@ -391,10 +391,11 @@ class Chain:
         return ctx.amhj("NORMAL", rels, plan=self.plan)
 
     def algorithmic_bytes(self):
-        """Per probe row: its two columns (8 B) and its level-0 bucket bounds
-        (8 B); per level-0 candidate its two co-located columns (8 B) and, for
-        a match, its level-1 bucket bounds (8 B); per level-1 candidate its
-        two columns (8 B)."""
+        """B_probe of the AMHJ count probe: the probe columns (4 B each a
+        row) and, for every lookup, its bucket bounds (8 B), the keys of its
+        bucket scanned (4 B each) and per match a row id and the gathered
+        payload (8 B); a lookup at level 0 per probe row, at level 1 per
+        level-0 match.  Buckets are floorPow2(rows) wide, as built."""
         if self.plan != "multiway":
             return None   # a baseline plan: its kernels are not the operator's
         (p0, p1), _ = self.rels[0]
@@ -403,15 +404,22 @@ class Chain:
         m = self.B - 1
         n1 = np.bincount(b0 & m, minlength=self.B).astype(np.int64)
         n2 = np.bincount(c0 & m, minlength=self.B).astype(np.int64)
-        cand0 = int(n1[p1 & m].sum())
-        per_key = np.zeros(1 << 18, np.int64)        # level-1 candidates behind each level-1 key
-        np.add.at(per_key, b0, n2[b1 & m])
-        match0 = int(np.bincount(b0, minlength=1 << 18)[p1].sum())
-        cand1 = int(per_key[p1].sum())
-        return len(p0) * 16 + cand0 * 8 + match0 * 8 + cand1 * 8
+        k1 = np.bincount(b0, minlength=1 << 18).astype(np.int64)   # level-0 matches of a key
+        k2 = np.bincount(c0, minlength=1 << 18).astype(np.int64)   # level-1 matches of a key
+        per1 = 8 + 4 * n2[b1 & m] + 8 * k2[b1]                     # the level-1 lookup of each level-0 row
+        behind = np.zeros(1 << 18, np.int64)
+        np.add.at(behind, b0, per1)                                # level-1 bytes behind a level-0 key
+        tot = 8 * len(p0) + int((8 + 4 * n1[p1 & m] + 8 * k1[p1]).sum()) + int(behind[p1].sum())
+        return tot
+
+    def lookups_per_launch(self):
+        """Bucket lookups: one per probe row and one per level-0 match."""
+        (p0, p1), _ = self.rels[0]
+        (b0, _), _ = self.rels[1]
+        return len(p0) + int(np.bincount(b0, minlength=1 << 18)[p1].sum())
 
     def kernel_name(self):
-        return "amhj_probe_kernel (count pass)"
+        return "amhj_chain_canon_kernel"
 
     def cpu_baseline(self):
         from oracle import oracle as O
@@ -451,20 +459,23 @@ class Star:
     run = Chain.run
 
     def algorithmic_bytes(self):
-        """The HBM bytes the probe must move: per fact row its four keys
-        (16 B, streamed once); per dimension the build of its bucket heads
-        (the bucket bounds, 4 B a bucket, and the rows, 8 B each, read; one
-        32-byte head a bucket written) and the heads read back once.  The
-        lookups themselves (one head a dimension and fact row) are served by
-        L1 and L2, which hold every head (23 MB): they are counted by
-        lookups_per_launch, not here."""
+        """B_probe of the AMHJ count probe: the fact row's four keys (16 B)
+        and, for each dimension lookup, its bucket bounds (8 B), the keys of
+        its bucket scanned (4 B each) and per match a row id and the gathered
+        payload (8 B), with floorPow2(rows) buckets as built.  The lookups are
+        served by L1 and L2 (the dimensions and their bucket heads are
+        L2-resident), so the fraction of HBM can exceed 1."""
         if self.plan != "multiway":
             return None   # a baseline plan: its kernels are not the operator's
-        tot = len(self.rels[0][0][0]) * 16
-        for cols, _ in self.rels[1:]:
+        fact_cols = self.rels[0][0]
+        tot = len(fact_cols[0]) * 16
+        for j, (cols, _) in enumerate(self.rels[1:]):
             n = len(cols[0])
             B = 1 << (n.bit_length() - 1)
-            tot += 4 * (B + 1) + 8 * n + 2 * 32 * B
+            per = np.bincount(cols[0] & (B - 1), minlength=B).astype(np.int64)
+            f = fact_cols[j]
+            hits = np.bincount(cols[0], minlength=int(max(n, f.max() + 1))).astype(np.int64)
+            tot += 8 * len(f) + 4 * int(per[f & (B - 1)].sum()) + 8 * int(hits[f].sum())
         return tot
 
     def lookups_per_launch(self):

@@ -54,21 +54,51 @@ def test_bench_percentiles():
     assert bench.pct(xs, 50) == 3.0 and bench.pct(xs, 99) == 5.0 and bench.pct(xs, 0) == 1.0
 
 
+def _lookup_bytes(build_keys, B, key):
+    """B_probe's bytes of one lookup: bounds, the bucket's keys, 8 B a match."""
+    bucket = build_keys[(build_keys & (B - 1)) == (key & (B - 1))]
+    return 8 + 4 * len(bucket) + 8 * int(np.count_nonzero(bucket == key))
+
+
 def test_bench_star_algorithmic_bytes_match_a_direct_count():
-    """The star workload's HBM bytes: 16 B per fact row, and per dimension
-    the build of its bucket heads (floorPow2(rows) buckets: bounds read,
-    rows read, one 32-byte head written) and the heads read back once; the
-    lookups, one head per dimension and fact row, are counted apart."""
+    """The star workload's B_probe (16 B a fact row; per dimension lookup the
+    bucket bounds, 4 B a key scanned, 8 B a match; floorPow2(rows) buckets)
+    against a row-by-row count."""
     import argparse
     import bench
     wl = bench.Star(argparse.Namespace(star_rows=1500), 0, gen=O.GENERATORS)
     fact_cols = wl.rels[0][0]
-    want = 16 * len(fact_cols[0])
-    for cols, _ in wl.rels[1:]:
-        B = 1
-        while 2 * B <= len(cols[0]):
-            B *= 2
-        want += 4 * (B + 1) + 8 * len(cols[0]) + 32 * B + 32 * B
+    want = 0
+    for r in range(len(fact_cols[0])):
+        want += 16
+        for j, (cols, _) in enumerate(wl.rels[1:]):
+            B = 1 << (len(cols[0]).bit_length() - 1)
+            want += _lookup_bytes(cols[0], B, fact_cols[j][r])
     assert wl.algorithmic_bytes() == want
     assert wl.lookups_per_launch() == 4 * len(fact_cols[0])
     assert wl.h2d == sum(4 * len(c[0]) * len(c) for c, _ in wl.rels)
+
+
+def test_bench_chain_algorithmic_bytes_match_a_direct_count():
+    """The chain workload's B_probe (8 B a probe row; a level-0 lookup per
+    probe row and a level-1 lookup per level-0 match, each the bucket
+    bounds, 4 B a key scanned and 8 B a match) against a row-by-row count,
+    on a small chain of the same shape."""
+    import bench
+    rng = np.random.Generator(np.random.PCG64(5))
+    n = 3000
+    wl = bench.Chain.__new__(bench.Chain)
+    wl.rels = [([rng.integers(0, 1 << 18, n).astype(np.int32), rng.integers(0, 1500, n).astype(np.int32)], [0, 1]),
+               ([rng.integers(0, 1500, n).astype(np.int32), rng.integers(0, 1500, n).astype(np.int32)], [1, 2]),
+               ([rng.integers(0, 1500, n).astype(np.int32), rng.integers(0, 1 << 18, n).astype(np.int32)], [2, 3])]
+    wl.B, wl.plan = 2048, "multiway"
+    (p0, p1), (b0, b1), (c0, _) = wl.rels[0][0], wl.rels[1][0], wl.rels[2][0]
+    want, lookups = 0, 0
+    for r in range(n):
+        want += 8 + _lookup_bytes(b0, wl.B, p1[r])
+        lookups += 1
+        for j in np.nonzero(b0 == p1[r])[0]:
+            want += _lookup_bytes(c0, wl.B, b1[j])
+            lookups += 1
+    assert wl.algorithmic_bytes() == want
+    assert wl.lookups_per_launch() == lookups

@@ -375,6 +375,35 @@ def test_amhj_star_canonical_and_general_attribute_numbering(ctx, ndims):
             assert (got.count, got.checksum) == want, (rels[0][1], ws)
 
 
+@pytest.mark.parametrize("nlev", [1, 2, 3, 4])
+def test_amhj_chain_flat_walk_and_listed_rows(ctx, nlev):
+    """Count queries over a canonical chain R0(0, 1) R_d(d + 1, d + 2) take
+    the flat walk (one thread per probe row, one bucket head a lookup).
+    Buckets of one to three rows are read from the head, longer ones from
+    the columns, and rows whose walk exceeds its budget (a hot key) are
+    joined by the DFS kernel.  Equal to the oracle for ws 0 and 1, and equal
+    under another attribute numbering, which the DFS kernel joins."""
+    rng = np.random.Generator(np.random.PCG64(60 + nlev))
+    n = 40_000
+    rels = [([rng.integers(0, 5000, n).astype(np.int32), rng.integers(0, 4000, n).astype(np.int32)], [0, 1])]
+    for d in range(nlev):
+        keys = rng.integers(0, 4000, 6000 + 3000 * d).astype(np.int32)
+        keys[:700] = 11                      # a hot key: its rows exceed the walk's budget
+        pay = rng.integers(0, 4000, len(keys)).astype(np.int32)
+        rels.append(([keys, pay], [d + 1, d + 2]))
+    rels[0][0][1][:50] = 11
+    want = O.mhj(rels)
+    assert want[0] > 0
+    hs = [ctx.relation(c, a) for c, a in rels]
+    for ws in (0, 1):
+        got = ctx.amhj("NORMAL", hs, ws=ws)
+        assert (got.count, got.checksum) == want, ws
+    k = nlev + 2
+    other = [(c, [k - 1 - x for x in a]) for c, a in rels]   # the same chain, attributes numbered from the end
+    got = ctx.amhj("NORMAL", [ctx.relation(c, a) for c, a in other])
+    assert (got.count, got.checksum) == O.mhj(other)
+
+
 @pytest.mark.parametrize("qt", ["TRI", "FOUR"])
 @pytest.mark.parametrize("reorder", [True, False])
 @pytest.mark.parametrize("degree_order", [True, False])
