@@ -38,7 +38,7 @@ AMJ_LFTJ_BFS, AMJ_LFTJ_DFS = 0, 1
 AMJ_LAYOUT_BUCKET, AMJ_LAYOUT_OPEN_ADDR, AMJ_LAYOUT_CUCKOO = 0, 1, 2
 AMJ_F_MATERIALIZE, AMJ_F_HOST_RESULT, AMJ_F_NO_REORDER, AMJ_F_CLIQUE4 = 0x1, 0x2, 0x4, 0x8
 AMJ_F_KEEP_ORDER, AMJ_F_DEGREE_ORDER, AMJ_F_CLIQUE4_LISTS = 0x10, 0x20, 0x40
-AMJ_F_THREAD_PER_ROW, AMJ_F_PAIRWISE, AMJ_F_HASH_PLAN = 0x80, 0x100, 0x200
+AMJ_F_THREAD_PER_ROW, AMJ_F_PAIRWISE, AMJ_F_HASH_PLAN, AMJ_F_FRONTIER = 0x80, 0x100, 0x200, 0x400
 AMJ_MEM_DEVICE, AMJ_MEM_HOST, AMJ_MEM_HOST_STREAMED = 0, 1, 2
 
 

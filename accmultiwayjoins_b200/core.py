@@ -360,9 +360,11 @@ class Context:
         operator; TRI / FOUR over one oriented edge relation without repeated rows
         answer their pair-key levels from a bitmap of b's children / the triangle
         matrices of the degree-ranked copy), "hash" (the operator with every level
-        a hash lookup), or a baseline to compare it with: "thread_per_row"
-        (one thread per probe row, count only) or "pairwise" (2-relation joins
-        with materialised intermediates)."""
+        a hash lookup), "frontier" (the operator with every plan joined by the
+        frontier-DFS kernel, no flat star / chain kernel), or a baseline to
+        compare it with: "thread_per_row" (one thread per probe row, count
+        only) or "pairwise" (2-relation joins with materialised
+        intermediates)."""
         lib = L.load()
         qt = _QUERY[query_type] if isinstance(query_type, str) else int(query_type)
         arr = (C.c_void_p * len(relations))(*[r.handle for r in relations])
@@ -372,7 +374,7 @@ class Context:
         if not degree_order:
             flags |= L.AMJ_F_KEEP_ORDER
         flags |= {"multiway": 0, "thread_per_row": L.AMJ_F_THREAD_PER_ROW, "pairwise": L.AMJ_F_PAIRWISE,
-                  "hash": L.AMJ_F_HASH_PLAN}[plan]
+                  "hash": L.AMJ_F_HASH_PLAN, "frontier": L.AMJ_F_FRONTIER}[plan]
         res = L.amj_result()
         L.check(lib.amj_amhj_execute(self.handle, qt, arr, len(relations), int(ooc), int(ws), int(dro), int(fib),
                                      flags, C.byref(res)), "amhj_execute")

@@ -825,7 +825,6 @@ void plan_common(const HostPlan &hp, const amj_opts &o, ProbePlan *P) {
 // resident, as in the reference.
 int amhj_ooc_execute(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch *X, const amj_rel *probe, bool ws, bool dro,
                      bool materialize, int flags, amj_result *out) {
-    (void)flags;
     const int nc = probe->ncols;
     const uint64_t n = probe->n;
     const bool host = probe->where == AMJ_MEM_HOST_STREAMED;
@@ -901,7 +900,7 @@ int amhj_ooc_execute(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch *X, const amj_re
             if (rc != AMJ_OK) break;
         }
         PassResult pr;
-        rc = run_passes(ctx, PL, *X, ws, dro, materialize, rlo, rhi, &pr, out);
+        rc = run_passes(ctx, PL, *X, ws, dro, materialize, rlo, rhi, &pr, out, !(flags & AMJ_F_FRONTIER));
         if (rc != AMJ_OK) break;
         count += pr.count;
         checksum += pr.checksum;
@@ -1162,7 +1161,7 @@ extern "C" int amj_amhj_execute(amj_ctx *ctx, int query_type, amj_rel *const *re
         }
     } else {
         PassResult pr;
-        rc = run_passes(ctx, PL, X, use_ws, dro != 0, materialize, 0, hp.probe->n, &pr, out);
+        rc = run_passes(ctx, PL, X, use_ws, dro != 0, materialize, 0, hp.probe->n, &pr, out, !(flags & AMJ_F_FRONTIER));
         if (rc == AMJ_OK) {
             out->count = pr.count;
             out->checksum = pr.checksum;

@@ -19,7 +19,8 @@ through AMHJ (count + checksum, hash builds included).  --workload star
 runs the 4-way star (fact 60M rows x 4 Zipf(1.1) keys, dims 1M/200K/100K/10K)
 through AMHJ the same way; --workload four the skewed 4-clique (R-MAT
 scale 22).  --plan thread_per_row|pairwise runs the chain or star through
-the reference's baseline plans instead of the operator.  --workload batch
+the reference's baseline plans instead of the operator; --plan frontier
+through the operator's frontier-DFS kernel instead of its flat kernels.  --workload batch
 runs 512 heterogeneous queries as one batch (autotuned, CUDA-graph replay)
 and reports, beside its tuples/s, the one-query-per-call tuples/s on the
 same queries and p50/p99 latencies of both forms.
@@ -357,7 +358,7 @@ def plan_note(plan):
     """The workload text of a baseline plan run in place of the operator."""
     return {"multiway": "", "thread_per_row": " (baseline plan: one thread per probe row, MHJ.cuh)",
             "pairwise": " (baseline plan: 2-relation joins with materialised intermediates, exec_PW.cu)",
-            "hash": ""}[plan]
+            "hash": "", "frontier": " (the operator's frontier-DFS kernel, no flat kernel)"}[plan]
 
 
 class Chain:
@@ -396,7 +397,7 @@ class Chain:
         bucket scanned (4 B each) and per match a row id and the gathered
         payload (8 B); a lookup at level 0 per probe row, at level 1 per
         level-0 match.  Buckets are floorPow2(rows) wide, as built."""
-        if self.plan != "multiway":
+        if self.plan not in ("multiway", "frontier"):
             return None   # a baseline plan: its kernels are not the operator's
         (p0, p1), _ = self.rels[0]
         (b0, b1), _ = self.rels[1]
@@ -419,7 +420,7 @@ class Chain:
         return len(p0) + int(np.bincount(b0, minlength=1 << 18)[p1].sum())
 
     def kernel_name(self):
-        return "amhj_chain_canon_kernel"
+        return "amhj_probe_kernel (count pass)" if self.plan == "frontier" else "amhj_chain_canon_kernel"
 
     def cpu_baseline(self):
         from oracle import oracle as O
@@ -465,7 +466,7 @@ class Star:
         payload (8 B), with floorPow2(rows) buckets as built.  The lookups are
         served by L1 and L2 (the dimensions and their bucket heads are
         L2-resident), so the fraction of HBM can exceed 1."""
-        if self.plan != "multiway":
+        if self.plan not in ("multiway", "frontier"):
             return None   # a baseline plan: its kernels are not the operator's
         fact_cols = self.rels[0][0]
         tot = len(fact_cols[0]) * 16
@@ -484,7 +485,7 @@ class Star:
         return len(self.rels[0][0][0]) * (len(self.rels) - 1)
 
     def kernel_name(self):
-        return "amhj_star_canon_kernel"
+        return "amhj_probe_kernel (count pass)" if self.plan == "frontier" else "amhj_star_canon_kernel"
 
     def cpu_baseline(self, sample_rows=12_000_000):
         """The reference MHJ-CPU over a bounded sample of the fact table (its
@@ -1311,8 +1312,9 @@ def main():
     ap.add_argument("--star-rows", type=int, default=60_000_000, help="star workload: fact table rows")
     ap.add_argument("--layout", default="bucket", choices=["bucket", "oa", "cuckoo"],
                     help="chain / star workloads: hash-table layout of the AMHJ builds")
-    ap.add_argument("--plan", default="multiway", choices=["multiway", "thread_per_row", "pairwise"],
-                    help="chain / star workloads: the operator, or one of the reference's baseline plans")
+    ap.add_argument("--plan", default="multiway", choices=["multiway", "thread_per_row", "pairwise", "frontier"],
+                    help="chain / star workloads: the operator, one of the reference's baseline plans, or the "
+                         "operator's frontier-DFS kernel for every plan")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="triangle workload: skip the chain and batched records carried on the line")

@@ -88,6 +88,9 @@ extern "C" {
 #define AMJ_F_CLIQUE4_LISTS 0x40 /* amj_lftj_execute with AMJ_F_CLIQUE4: join the
                                    degree-ordered copy by list intersections even where
                                    the triangle matrices fit (same result)          */
+#define AMJ_F_FRONTIER     0x400 /* amj_amhj_execute: join every plan with the frontier-DFS
+                                   kernel, never the flat kernels of star and canonical
+                                   chain count plans (same result; a comparator)   */
 #define AMJ_F_HASH_PLAN    0x200 /* amj_amhj_execute, TRI / FOUR over one edge relation:
                                    keep the level-by-level hash-join plan where a bitmap
                                    of b's children (TRI) or the triangle matrices (FOUR)

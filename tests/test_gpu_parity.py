@@ -373,6 +373,8 @@ def test_amhj_star_canonical_and_general_attribute_numbering(ctx, ndims):
         for ws in (0, 1):
             got = ctx.amhj("NORMAL", hs, ws=ws)
             assert (got.count, got.checksum) == want, (rels[0][1], ws)
+        got = ctx.amhj("NORMAL", hs, plan="frontier")
+        assert (got.count, got.checksum) == want
 
 
 @pytest.mark.parametrize("nlev", [1, 2, 3, 4])
@@ -398,6 +400,8 @@ def test_amhj_chain_flat_walk_and_listed_rows(ctx, nlev):
     for ws in (0, 1):
         got = ctx.amhj("NORMAL", hs, ws=ws)
         assert (got.count, got.checksum) == want, ws
+    got = ctx.amhj("NORMAL", hs, plan="frontier")        # the frontier-DFS kernel for every row
+    assert (got.count, got.checksum) == want
     k = nlev + 2
     other = [(c, [k - 1 - x for x in a]) for c, a in rels]   # the same chain, attributes numbered from the end
     got = ctx.amhj("NORMAL", [ctx.relation(c, a) for c, a in other])
