@@ -347,8 +347,19 @@ static int run_flat_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws
     AMJ_CUDA_TRY(cudaGetLastError());
     ProbeLaunch sub = PL;
     for (int c = 0; c < P.probe_ncols; c++) sub.P.probe_col[c] = cp[c];
+    // The listed rows are the heavy ones, and gathered they sit in few warps'
+    // row chunks: join them with work sharing whatever the query's ws, so
+    // their frontiers spread over all warps (the same result).
+    if (!ws) {
+        if (!X.tasks.p) {
+            AMJ_TRY(X.tasks.alloc(ctx, P.task_cap));
+            AMJ_TRY(X.ready.alloc(ctx, P.task_cap));
+        }
+        sub.tasks = X.tasks.p;
+        sub.task_ready = X.ready.p;
+    }
     PassResult rest;
-    AMJ_TRY(run_passes(ctx, sub, X, ws, false, false, 0, h.nover, &rest, res, false));
+    AMJ_TRY(run_passes(ctx, sub, X, true, false, false, 0, h.nover, &rest, res, false));
     pr->count += rest.count;
     pr->checksum += rest.checksum;
     return AMJ_OK;

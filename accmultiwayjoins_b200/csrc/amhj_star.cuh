@@ -315,7 +315,7 @@ __global__ __launch_bounds__(256, 4) void amhj_star_canon_kernel(const __grid_co
 // the last level.  A row whose walk would scan more than CHAIN_ROW_BUDGET
 // bucket rows (skewed keys) drops what it counted and is listed for the DFS
 // kernel, which shares such work across warps.
-constexpr uint32_t CHAIN_ROW_BUDGET = 512;
+constexpr uint32_t CHAIN_ROW_BUDGET = 128;
 
 // L when plan P has the canonical chain shape (filling S but the heads), else 0
 inline int chain_canon(const ProbePlan &P, CanonPlan &S) {
