@@ -287,9 +287,23 @@ static int run_flat_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws
             tot += S.nb[c];
             maxnb = std::max(maxnb, S.nb[c]);
         }
-        AMJ_TRY(heads.alloc(ctx, tot));
-        // the heads are read by 256-bit loads, which need 32-byte alignment
-        if (reinterpret_cast<uintptr_t>(heads.p) % alignof(BucketHead) != 0) canon = 0;
+        // the heads (32 B a bucket, up to four times the levels' columns)
+        // are built only while they take at most a quarter of the free
+        // device memory; otherwise a star takes the general kernel and a
+        // chain the DFS kernel
+        size_t fr = 0, dtot = 0;
+        AMJ_CUDA_TRY(cudaMemGetInfo(&fr, &dtot));
+        if (tot * sizeof(BucketHead) > fr / 4) {
+            if (chain) return run_passes(ctx, PL, X, ws, false, false, row_lo, row_hi, pr, res, false);
+            canon = 0;
+        } else {
+            AMJ_TRY(heads.alloc(ctx, tot));
+            // the heads are read by 256-bit loads, which need 32-byte alignment
+            if (reinterpret_cast<uintptr_t>(heads.p) % alignof(BucketHead) != 0) {
+                if (chain) return run_passes(ctx, PL, X, ws, false, false, row_lo, row_hi, pr, res, false);
+                canon = 0;
+            }
+        }
     }
     AMJ_CUDA_TRY(cudaEventRecord(ctx->kev[0], ctx->stream));
     if (canon) {
