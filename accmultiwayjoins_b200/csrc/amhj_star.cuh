@@ -374,8 +374,10 @@ __device__ __forceinline__ bool chain_walk(const CanonPlan &S, int32_t key, uint
     return true;
 }
 
+// four blocks per SM (64 registers) up to three levels; deeper walks keep
+// their per-level state in two blocks' worth of registers
 template <int L>
-__global__ __launch_bounds__(256, 4) void amhj_chain_canon_kernel(const __grid_constant__ CanonPlan S,
+__global__ __launch_bounds__(256, L <= 3 ? 4 : 2) void amhj_chain_canon_kernel(const __grid_constant__ CanonPlan S,
                                                                unsigned long long *count, unsigned long long *checksum,
                                                                uint32_t *over, unsigned int *nover) {
     unsigned long long cnt = 0, chk = 0;
