@@ -60,6 +60,10 @@ constexpr uint64_t TRIE_LEVEL1_PAD = 4;
 // vmax >= 0: every value of both columns lies in [0, vmax] (no min/max pass)
 int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, Trie2 *out,
                 bool distinct = false, int32_t vmax = -1);
+// The distinct 2-level trie of a degree-ranked copy: every value in [0, nv)
+// and each row's first value below its second (rows bucketed by counting,
+// each row sorted on its own; the radix-sort build where a row is too long).
+int build_trie2_ranked(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, uint64_t nv, Trie2 *out);
 
 // time between two events recorded on the context stream (ms)
 double event_ms(cudaEvent_t a, cudaEvent_t b);

@@ -68,7 +68,7 @@ static int build_ranked_trie(amj_ctx *ctx, const amj_rel *r, Trie2 *t, DBuf<int3
     bool oriented = false;
     AMJ_TRY(degree_ranked_copy(ctx, c0, c1, r->n, &ns, &nd, inv, nv, &oriented));
     if (!oriented) return build_trie2(ctx, c0, c1, r->n, t, true);
-    AMJ_TRY(build_trie2(ctx, ns.p, nd.p, r->n, t, true, (int32_t)(*nv - 1)));
+    AMJ_TRY(build_trie2_ranked(ctx, ns.p, nd.p, r->n, *nv, t));
     if (wedges) AMJ_TRY(build_wedges(ctx, *t, *nv, wedges));
     return AMJ_OK;
 }

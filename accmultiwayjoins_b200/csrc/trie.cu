@@ -222,6 +222,329 @@ int build_trie2(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t
     return AMJ_OK;
 }
 
+// ---- 2-level tries of a degree-ranked copy: rows by counting ----
+// Every value lies in [0, nv) and every row's first value is below its
+// second, so the rows can be bucketed by their first value directly: a count
+// per value, a scan into row starts, and one scatter of the second values
+// into their rows, then each row sorted on its own.  After the degree
+// ranking a row holds the higher-ranked neighbours of one vertex, at most
+// sqrt(2 n) of them, and most rows hold a few: a warp sorts a row of up to
+// 32 values in registers (a bitonic network over shuffles) and up to
+// RK_WARP_MAX in its shared-memory slice; a block sorts the longer rows, up to
+// RK_BLOCK_MAX.  A graph with a longer row takes the radix-sort build.
+// Repeated rows (adjacent after the sort) are dropped by a compaction pass
+// when there are any.
+constexpr uint32_t RK_WARP_MAX = 1024;
+constexpr uint32_t RK_BLOCK_MAX = 8192;
+constexpr int RK_SORT_WARPS = 8;
+
+__global__ void rk_count_kernel(const int32_t *__restrict__ c0, uint64_t n, uint32_t *__restrict__ cnt) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[c0[i]], 1u);
+}
+
+__global__ void rk_max_kernel(const uint32_t *__restrict__ cnt, uint64_t nv, unsigned int *__restrict__ mx) {
+    uint32_t m = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nv; v += (uint64_t)gridDim.x * blockDim.x)
+        m = max(m, cnt[v]);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) m = max(m, __shfl_xor_sync(AMJ_FULL_MASK, m, d));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(mx, m);
+}
+
+// fill[] starts at zero: the row of value c0[i] gets c1[i] at its next free slot
+__global__ void rk_scatter_kernel(const int32_t *__restrict__ c0, const int32_t *__restrict__ c1, uint64_t n,
+                                  const uint32_t *__restrict__ start, uint32_t *__restrict__ fill,
+                                  int32_t *__restrict__ data1) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const int32_t v = c0[i];
+        data1[start[v] + atomicAdd(&fill[v], 1u)] = c1[i];
+    }
+}
+
+// ascending bitonic sort of the pow2-sized x[0, m) by the threads t of a
+// group of nt, with sync() between stages
+template <class Sync>
+__device__ __forceinline__ void rk_bitonic(int32_t *x, uint32_t m, uint32_t t, uint32_t nt, Sync &&sync) {
+    for (uint32_t k = 2; k <= m; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = t; i < m; i += nt) {
+                const uint32_t p = i ^ j;
+                if (p > i) {
+                    const int32_t a = x[i], b = x[p];
+                    if ((a > b) == ((i & k) == 0)) {
+                        x[i] = b;
+                        x[p] = a;
+                    }
+                }
+            }
+            sync();
+        }
+}
+
+// distinct values of the sorted row x[0, len) (shared memory), counted by a group
+__device__ __forceinline__ uint32_t rk_distinct(const int32_t *x, uint32_t len, uint32_t t, uint32_t nt) {
+    uint32_t u = 0;
+    for (uint32_t i = t; i < len; i += nt) u += (i == 0 || x[i] != x[i - 1]) ? 1u : 0u;
+    return u;
+}
+
+// A row of up to 32 E values sorted by one warp in registers: value i of the
+// sorted row ends in register i % E of lane i / E.  The values may start in
+// any lanes and registers.  A bitonic network: a stage whose partner distance
+// j is E or more exchanges registers between lanes (shuffles), a shorter one
+// within a lane.
+template <int E>
+__device__ __forceinline__ void rk_warp_bitonic(int32_t (&x)[E], uint32_t lane) {
+#pragma unroll
+    for (uint32_t k = 2; k <= 32u * E; k <<= 1)
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j >= (uint32_t)E) {
+                const uint32_t lj = j / E;
+                const bool lower = (lane & lj) == 0;
+#pragma unroll
+                for (int e = 0; e < E; e++) {
+                    const bool up = ((lane * E + e) & k) == 0;
+                    const int32_t y = __shfl_xor_sync(AMJ_FULL_MASK, x[e], lj);
+                    x[e] = (lower == up) ? min(x[e], y) : max(x[e], y);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; e++) {
+                    const int p = e ^ (int)j;
+                    if (p > e) {
+                        const bool up = ((lane * E + e) & k) == 0;
+                        const int32_t a = x[e], b = x[p];
+                        x[e] = up ? min(a, b) : max(a, b);
+                        x[p] = up ? max(a, b) : min(a, b);
+                    }
+                }
+            }
+        }
+}
+
+// row v = data1[s, s + len), 32 (E / 2) < len <= 32 E: sorted in place, its
+// level-0 value into src1, its number of distinct values into uniq[v]
+template <int E>
+__device__ __forceinline__ void rk_warp_row(int32_t *__restrict__ data1, int32_t *__restrict__ src1,
+                                            uint32_t *__restrict__ uniq, uint32_t s, uint32_t len, uint64_t v,
+                                            uint32_t lane) {
+    int32_t x[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+        const uint32_t i = e * 32u + lane;   // coalesced loads; the network fixes the order
+        x[e] = i < len ? data1[s + i] : INT32_MAX;
+    }
+    rk_warp_bitonic<E>(x, lane);
+    const int32_t prev = __shfl_up_sync(AMJ_FULL_MASK, x[E - 1], 1);
+    uint32_t u = 0;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+        const uint32_t i = lane * E + e;
+        if (i < len) {
+            const int32_t before = e ? x[e - 1] : prev;
+            u += (i == 0 || x[e] != before) ? 1u : 0u;
+            data1[s + i] = x[e];
+            src1[s + i] = (int32_t)v;
+        }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) u += __shfl_xor_sync(AMJ_FULL_MASK, u, d);
+    if (lane == 0) uniq[v] = u;
+}
+
+// One warp a row, the row's values in registers (rows of up to RK_WARP_MAX);
+// longer rows are listed for the block kernel.
+__global__ __launch_bounds__(RK_SORT_WARPS * 32, 4) void rk_sort_rows_kernel(const uint32_t *__restrict__ start,
+                                                                           uint64_t nv, int32_t *__restrict__ data1,
+                                                                           int32_t *__restrict__ src1,
+                                                                           uint32_t *__restrict__ uniq,
+                                                                           uint32_t *__restrict__ longs,
+                                                                           unsigned int *__restrict__ nlong) {
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint64_t warps = (uint64_t)gridDim.x * RK_SORT_WARPS;
+    for (uint64_t v = blockIdx.x * (uint64_t)RK_SORT_WARPS + w; v < nv; v += warps) {
+        const uint32_t s = start[v], len = start[v + 1] - s;
+        if (len <= 1) {
+            if (len == 1 && lane == 0) src1[s] = (int32_t)v;
+            if (lane == 0) uniq[v] = len;
+        } else if (len <= 32) {
+            rk_warp_row<1>(data1, src1, uniq, s, len, v, lane);
+        } else if (len <= 64) {
+            rk_warp_row<2>(data1, src1, uniq, s, len, v, lane);
+        } else if (len <= 128) {
+            rk_warp_row<4>(data1, src1, uniq, s, len, v, lane);
+        } else if (len <= 256) {
+            rk_warp_row<8>(data1, src1, uniq, s, len, v, lane);
+        } else if (len <= 512) {
+            rk_warp_row<16>(data1, src1, uniq, s, len, v, lane);
+        } else if (len <= RK_WARP_MAX) {
+            rk_warp_row<32>(data1, src1, uniq, s, len, v, lane);
+        } else if (lane == 0) {
+            longs[atomicAdd(nlong, 1u)] = (uint32_t)v;
+            uniq[v] = 0;
+        }
+    }
+}
+
+// One block a listed row (RK_WARP_MAX < length <= RK_BLOCK_MAX); the blocks
+// take the list's rows in turn
+__global__ __launch_bounds__(512) void rk_sort_long_kernel(const uint32_t *__restrict__ start,
+                                                           int32_t *__restrict__ data1, int32_t *__restrict__ src1,
+                                                           uint32_t *__restrict__ uniq,
+                                                           const uint32_t *__restrict__ longs,
+                                                           const unsigned int *__restrict__ nlong) {
+    __shared__ int32_t x[RK_BLOCK_MAX];
+    __shared__ uint32_t usum;
+    const uint32_t t = threadIdx.x, nt = blockDim.x;
+    for (uint32_t r = blockIdx.x; r < *nlong; r += gridDim.x) {
+        const uint32_t v = longs[r], s = start[v], len = start[v + 1] - s;
+        uint32_t m = 64;
+        while (m < len) m <<= 1;
+        if (t == 0) usum = 0;
+        for (uint32_t i = t; i < m; i += nt) x[i] = i < len ? data1[s + i] : INT32_MAX;
+        __syncthreads();
+        rk_bitonic(x, m, t, nt, [] { __syncthreads(); });
+        const uint32_t u = rk_distinct(x, len, t, nt);
+        if (u) atomicAdd(&usum, u);
+        for (uint32_t i = t; i < len; i += nt) {
+            data1[s + i] = x[i];
+            src1[s + i] = (int32_t)v;
+        }
+        __syncthreads();
+        if (t == 0) uniq[v] = usum;
+        __syncthreads();
+    }
+}
+
+// repeated rows present: row v's distinct values move to ustart[v] (a warp a row)
+__global__ void rk_compact_kernel(const uint32_t *__restrict__ start, const uint32_t *__restrict__ ustart,
+                                  uint64_t nv, const int32_t *__restrict__ data1, int32_t *__restrict__ out1,
+                                  int32_t *__restrict__ outsrc) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nv; v += warps) {
+        const uint32_t s = start[v], len = start[v + 1] - s;
+        uint32_t at = ustart[v];
+        for (uint32_t i0 = 0; i0 < len; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            const bool keep = i < len && (i == 0 || data1[s + i] != data1[s + i - 1]);
+            const unsigned b = __ballot_sync(AMJ_FULL_MASK, keep);
+            if (keep) {
+                const uint32_t o = at + __popc(b & ((1u << lane) - 1u));
+                out1[o] = data1[s + i];
+                outsrc[o] = (int32_t)v;
+            }
+            at += __popc(b);
+        }
+    }
+}
+
+// level 0 (the values with children) and the dense row pointers
+__global__ void rk_level0_kernel(const uint32_t *__restrict__ ustart, const uint32_t *__restrict__ pos, uint64_t nv,
+                                 int32_t *__restrict__ data0, uint64_t *__restrict__ off0,
+                                 uint64_t *__restrict__ rowptr, uint64_t len0) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v <= nv; v += (uint64_t)gridDim.x * blockDim.x) {
+        rowptr[v] = ustart[v];
+        if (v == nv) {
+            off0[len0] = ustart[nv];
+        } else if (ustart[v + 1] > ustart[v]) {
+            data0[pos[v]] = (int32_t)v;
+            off0[pos[v]] = ustart[v];
+        }
+    }
+}
+
+// 1 for the values with a row (every row keeps a value after deduplication)
+__global__ void rk_nonempty_kernel(const uint32_t *__restrict__ start, uint64_t nv, uint32_t *__restrict__ flag) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nv; v += (uint64_t)gridDim.x * blockDim.x)
+        flag[v] = start[v + 1] > start[v] ? 1u : 0u;
+}
+
+int build_trie2_ranked(amj_ctx *ctx, const int32_t *d_c0, const int32_t *d_c1, uint64_t n, uint64_t nv, Trie2 *out) {
+    if (n == 0 || nv == 0 || nv >= (1ull << 31) || n >= (1ull << 32) - 4096)
+        return build_trie2(ctx, d_c0, d_c1, n, out, true, nv ? (int32_t)(nv - 1) : -1);
+    // per-value row lengths, the longest, the row starts, and the values with
+    // children (level 0) numbered by a scan of their flags
+    DBuf<uint32_t> start, fill, flag;
+    DBuf<unsigned int> ctr;   // [0] longest row, [1] rows listed for the block kernel
+    AMJ_TRY(start.alloc(ctx, nv + 1));
+    AMJ_TRY(fill.alloc(ctx, nv));
+    AMJ_TRY(flag.alloc(ctx, nv + 1));
+    AMJ_TRY(ctr.alloc(ctx, 2));
+    AMJ_CUDA_TRY(cudaMemsetAsync(start.p, 0, (nv + 1) * sizeof(uint32_t), ctx->stream));
+    AMJ_CUDA_TRY(cudaMemsetAsync(ctr.p, 0, 2 * sizeof(unsigned int), ctx->stream));
+    note_launch(ctx);
+    rk_count_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_c0, n, start.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    note_launch(ctx);
+    rk_max_kernel<<<grid_for(ctx, nv), 256, 0, ctx->stream>>>(start.p, nv, ctr.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_TRY(scan_exclusive_u32(ctx, start.p, start.p, nv + 1, nullptr));
+    note_launch(ctx);
+    rk_nonempty_kernel<<<grid_for(ctx, nv), 256, 0, ctx->stream>>>(start.p, nv, flag.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    AMJ_TRY(scan_exclusive_u32(ctx, flag.p, flag.p, nv, flag.p + nv));
+    uint32_t h[2] = {0, 0};   // longest row, values with children
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&h[0], ctr.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&h[1], flag.p + nv, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    const uint32_t longest = h[0], len0 = h[1];
+    if (longest > RK_BLOCK_MAX) return build_trie2(ctx, d_c0, d_c1, n, out, true, (int32_t)(nv - 1));
+    // the rows, each sorted, with their distinct counts
+    AMJ_TRY(out->data1.alloc(ctx, n + TRIE_LEVEL1_PAD));
+    AMJ_TRY(out->src1.alloc(ctx, n));
+    DBuf<uint32_t> uniq, longs;
+    AMJ_TRY(uniq.alloc(ctx, nv + 1));
+    AMJ_TRY(longs.alloc(ctx, std::max<uint64_t>(1, n / (RK_WARP_MAX + 1) + 1)));
+    AMJ_CUDA_TRY(cudaMemsetAsync(fill.p, 0, nv * sizeof(uint32_t), ctx->stream));
+    note_launch(ctx);
+    rk_scatter_kernel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(d_c0, d_c1, n, start.p, fill.p, out->data1.p);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    const unsigned gs = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((nv + RK_SORT_WARPS - 1) / RK_SORT_WARPS,
+                                                                           (uint64_t)ctx->num_sms * 8));
+    note_launch(ctx);
+    rk_sort_rows_kernel<<<gs, RK_SORT_WARPS * 32, 0, ctx->stream>>>(start.p, nv, out->data1.p, out->src1.p, uniq.p,
+                                                                    longs.p, ctr.p + 1);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    if (longest > RK_WARP_MAX) {
+        note_launch(ctx);
+        rk_sort_long_kernel<<<ctx->num_sms, 512, 0, ctx->stream>>>(start.p, out->data1.p, out->src1.p, uniq.p,
+                                                                   longs.p, ctr.p + 1);
+        AMJ_CUDA_TRY(cudaGetLastError());
+    }
+    // distinct rows: scan the distinct counts; a compaction when some differ
+    uint32_t h_total = 0;
+    AMJ_TRY(scan_exclusive_u32(ctx, uniq.p, uniq.p, nv + 1, nullptr));
+    AMJ_CUDA_TRY(cudaMemcpyAsync(&h_total, uniq.p + nv, sizeof(h_total), cudaMemcpyDeviceToHost, ctx->stream));
+    AMJ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (h_total != n) {
+        DBuf<int32_t> d1, s1;
+        AMJ_TRY(d1.alloc(ctx, (uint64_t)h_total + TRIE_LEVEL1_PAD));
+        AMJ_TRY(s1.alloc(ctx, h_total ? h_total : 1));
+        note_launch(ctx);
+        rk_compact_kernel<<<grid_for(ctx, nv * 32), 256, 0, ctx->stream>>>(start.p, uniq.p, nv, out->data1.p, d1.p,
+                                                                            s1.p);
+        AMJ_CUDA_TRY(cudaGetLastError());
+        out->data1 = std::move(d1);
+        out->src1 = std::move(s1);
+    }
+    out->len1 = h_total;
+    // level 0 and the dense row pointers (a row with values keeps at least one)
+    out->len0 = len0;
+    AMJ_TRY(out->data0.alloc(ctx, len0 ? len0 : 1));
+    AMJ_TRY(out->off0.alloc(ctx, (uint64_t)len0 + 1));
+    AMJ_TRY(out->rowptr.alloc(ctx, nv + 1));
+    out->rp_min = 0;
+    out->rp_count = nv;
+    note_launch(ctx);
+    rk_level0_kernel<<<grid_for(ctx, nv + 1), 256, 0, ctx->stream>>>(uniq.p, flag.p, nv, out->data0.p, out->off0.p,
+                                                                     out->rowptr.p, len0);
+    AMJ_CUDA_TRY(cudaGetLastError());
+    return AMJ_OK;
+}
+
 // ---- N-level tries ----
 // Rows are ordered by a stable LSD radix sort of the row permutation, one
 // column at a time from the last: items (column value - min) << 32 | row,

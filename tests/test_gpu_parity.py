@@ -971,6 +971,29 @@ def test_lftj_joins_relations_as_sets(ctx):
     assert (dup.count, dup.checksum) == (plain.count, plain.checksum) and plain.count > 0
 
 
+def test_ranked_trie_rows_past_the_warp_sort():
+    """The degree-ranked copy's trie sorts each row on its own: a warp sorts
+    rows of up to 1024 values, a block the longer ones.  A 1100-vertex clique
+    gives its lowest-ranked vertex 1099 higher-ranked neighbours; joined with
+    a sparse graph, the triangles and 4-cliques equal the oracle through the
+    ALFTJ and AMHJ paths that use the copy."""
+    s, d = data.rmat(12, 30000, 0.57, 0.19, 0.19, seed=31)
+    k = np.arange(5000, 6100, dtype=np.int32)
+    ci, cj = np.triu_indices(len(k), 1)
+    s2 = np.concatenate([s, k[ci]]).astype(np.int32)
+    d2 = np.concatenate([d, k[cj]]).astype(np.int32)
+    want = O.triangle(s2, d2)
+    with Context(0) as c:
+        e = c.relation([s2, d2], [0, 1])
+        for ws in (0, 1):
+            got = c.lftj([e], algo="DFS", ws=ws, degree_order=True)
+            assert (got.count, got.checksum) == want, ws
+        got = c.lftj([e], algo="BFS", degree_order=True)
+        assert (got.count, got.checksum) == want
+        got = c.amhj("TRI", [e])
+        assert (got.count, got.checksum) == want
+
+
 def test_lftj_out_of_core_slices():
     """ooc=1 (the reference's OOCWrapper, LFTJ-GPU/ooc_wrapper.cuh): tries in
     pinned host memory, a memory budget split over the heading attributes,
