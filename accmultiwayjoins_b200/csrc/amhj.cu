@@ -288,12 +288,10 @@ static int run_flat_count(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws
             maxnb = std::max(maxnb, S.nb[c]);
         }
         // the heads (32 B a bucket, up to four times the levels' columns)
-        // are built only while they take at most a quarter of the free
-        // device memory; otherwise a star takes the general kernel and a
-        // chain the DFS kernel
-        size_t fr = 0, dtot = 0;
-        AMJ_CUDA_TRY(cudaMemGetInfo(&fr, &dtot));
-        if (tot * sizeof(BucketHead) > fr / 4) {
+        // are built only while they take at most an eighth of the device's
+        // memory; otherwise a star takes the general kernel and a chain the
+        // DFS kernel
+        if (tot * sizeof(BucketHead) > ctx->device_mem / 8) {
             if (chain) return run_passes(ctx, PL, X, ws, false, false, row_lo, row_hi, pr, res, false);
             canon = 0;
         } else {

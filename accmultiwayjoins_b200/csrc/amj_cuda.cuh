@@ -125,6 +125,7 @@ struct amj_ctx {
     amj_opts opts{};
     int num_sms = 148;
     int max_smem_optin = 227 * 1024;
+    size_t device_mem = 0;               // total device memory (bytes)
     size_t l2_bytes = 0;
     amj::DevStatus *d_status = nullptr;    // device status block
     amj::DevStatus *h_status = nullptr;    // pinned host mirror

@@ -142,6 +142,7 @@ extern "C" int amj_ctx_create(int device, const amj_opts *opts, amj_ctx **out) {
     AMJ_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
     c->num_sms = prop.multiProcessorCount;
     c->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
+    c->device_mem = prop.totalGlobalMem;
     c->l2_bytes = prop.l2CacheSize;
     int rc = AMJ_OK;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) rc = AMJ_ECUDA;
