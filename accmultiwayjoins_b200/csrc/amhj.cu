@@ -422,8 +422,8 @@ static int run_star_write(amj_ctx *ctx, ProbeLaunch &PL, uint64_t row_lo, uint64
 
 static int run_passes(amj_ctx *ctx, ProbeLaunch &PL, ExecScratch &X, bool ws, bool dro, bool materialize,
                       uint64_t row_lo, uint64_t row_hi, PassResult *pr, amj_result *res, bool allow_flat) {
-    CanonPlan cp_;
-    if (!materialize && allow_flat && (star_eligible(PL.P) || chain_canon(PL.P, cp_)))
+    CanonPlan chain_shape;   // filled only to test the shape
+    if (!materialize && allow_flat && (star_eligible(PL.P) || chain_canon(PL.P, chain_shape)))
         return run_flat_count(ctx, PL, X, ws, row_lo, row_hi, pr, res);
     if (materialize && !dro && allow_flat && star_eligible(PL.P))
         return run_star_write(ctx, PL, row_lo, row_hi, pr, res);
