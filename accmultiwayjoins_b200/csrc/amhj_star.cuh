@@ -1,4 +1,4 @@
-// AMHJ flat path for star-shaped count queries.
+// AMHJ flat paths for star- and chain-shaped queries.
 //
 // When every build level is looked up by an attribute of the probe relation
 // (a star: a fact table and its dimensions) and compares nothing but that
@@ -10,7 +10,11 @@
 // hashes the product's tuples in attribute order.  A row whose product
 // exceeds STAR_MAX_PRODUCT (a skewed dimension) is listed instead and joined
 // afterwards by the DFS kernel, which shares such work across warps.
-// Count mode only; bucket layout only.
+// Count mode only; bucket layout only.  Stars and chains in the numbering of
+// the reference's benchmarks also have register kernels over 32-byte bucket
+// heads (amhj_star_canon_kernel, amhj_chain_canon_kernel, below), and
+// materialised stars two flat passes (star_rowcount_kernel,
+// star_write_kernel).
 #pragma once
 #include "amhj_probe.cuh"
 
